@@ -1,0 +1,402 @@
+#!/usr/bin/env python
+"""Benchmark of the explicit species / electron-energy update (cell-updates/s).
+
+Workload (default ``precision3d``): one 3-D box of 128^3 cells, a 24-species /
+150-reaction mechanism (seeded Arrhenius rates), densities log-uniform 1e8-1e22,
+Te 0.3-10 eV, WENO-Z drift fluxes, Joule heating, one explicit step
+n += dt*(-div F + S) per "step".  The state (134^3 x 34 comps, 654 MB) and the six
+face fields are larger than the 126 MB L2, so every step streams them from HBM.
+
+One JSON line on rank 0:
+  value        cell-updates/s of the mixed-precision fused update (inputs resident)
+  e2e          the same through the C ABI with the step's inputs copied from pinned
+               host memory and its updated densities copied back, inside the timing
+  fp64         the plain-FP64 fused update on the same inputs, and the per-species
+               error of the mixed result against it
+  roofline     dominant kernel: algorithmic bytes / average launch time vs the
+               measured HBM copy bandwidth
+  cpu_baseline the reference's own hot-path code (oracle/_ref, all host cores) on a
+               bounded slab of the same workload
+Multi-GPU: one process per GPU, each updating its own box (independent boxes, as
+AMReX distributes boxes over ranks; no data-path collective); value sums the
+cells of all ranks over the slowest rank's time.
+
+``--impl reference`` times the reference's own CPU code instead (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    "precision3d": "3-D 128^3 box, 24 species / 150 reactions, WENO-Z, one explicit step",
+    "argon2d": "2-D 256^2 box, E/Ar+/Ar*/Ar, 10 reactions, WENO-Z, one explicit step",
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="precision3d", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
+    return ap.parse_args()
+
+
+def make_case(workload: str, rank: int = 0):
+    from vidyut_b200 import inputs as vin
+    seed = vin.BASE_SEED + 1000 * rank
+    if workload == "precision3d":
+        return vin.config_precision3d(seed=seed) if rank else vin.config_precision3d()
+    return vin.config_argon2d(seed=seed) if rank else vin.config_argon2d()
+
+
+def ref_case_name(case) -> str:
+    return case.mech.name
+
+
+def algorithmic_bytes_per_cell(case) -> dict:
+    """Algorithmic bytes of one cell-update (FP64 storage).  Reads: NS densities,
+    the electron energy, Te and D field components of the state plus 2*D face
+    values (E on faces, grad ne on faces); writes: NS+1 updated densities/energy
+    minus the background species that only carry over.  The transport kernel moves
+    all of them; the prep kernel reads the NS densities and Te."""
+    ns, d = case.mech.ns, case.dim
+    reads = ns + 2 + d + 2 * d
+    writes = ns + 1
+    return {"step": 8 * (reads + writes), "k_transport": 8 * (reads + writes), "k_prep": 8 * (ns + 1)}
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, power, throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev: int):
+        self.dev = dev
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", delete=False, suffix=".csv")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.dev)], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for i, nm in enumerate(names):
+                    if r[5 + i].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(case, target_s: float, threads: int | None = None, warm: bool = True):
+    """Cell-updates/s of the reference's own code (oracle/_ref) or, if that was not
+    built, the C restatement, on a slab of the case sized for about target_s."""
+    import oracle
+    kind = "reference"
+    try:
+        lib = oracle.RefLib(ref_case_name(case), case.dim)
+    except FileNotFoundError:
+        lib = oracle.Port(case.mech)
+        kind = "port"
+    prm = case.vd_params()
+    ax = case.dim - 1  # slab along the slowest swept direction
+    n_ax = case.n[ax]
+
+    def run(nplanes):
+        hi = list(case.hi)
+        hi[ax] = nplanes - 1
+        t0 = time.perf_counter()
+        lib.update_all(case, prm, lo=case.lo, hi=tuple(hi))
+        return time.perf_counter() - t0
+
+    probe = 1 if case.dim == 3 else max(1, n_ax // 64)
+    if warm:
+        run(probe)
+    t = run(probe)
+    per_plane = t / probe
+    nplanes = int(max(1, min(n_ax, math.ceil(target_s / max(per_plane, 1e-6)))))
+    cells_per_plane = case.ncell // n_ax
+    return lib, kind, run, nplanes, cells_per_plane
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    case = make_case(args.workload)
+    lib, kind, run, nplanes, cpp = cpu_reference_rate(case, max(1.0, args.cpu_seconds / max(1, args.steps)))
+    for _ in range(args.warmup):
+        run(nplanes)
+    ts = [run(nplanes) for _ in range(args.steps)]
+    cells = nplanes * cpp
+    t = sum(ts)
+    value = cells * args.steps / t
+    sample = f"{nplanes} of {case.n[case.dim - 1]} planes ({cells} cells) per step"
+    line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": WORKLOADS[args.workload], "cells": case.ncell, "species": case.mech.ns,
+                       "reactions": len(case.mech.reactions)},
+            "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def read_profile_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch from the committed ncu summary (profiles/), if any."""
+    p = ROOT / "profiles" / f"{kernel}_{workload}.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.strip().startswith("dram_bytes_per_launch_full:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from vidyut_b200 import _abi as abi
+    from vidyut_b200 import api
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    L = abi.lib()
+    case = make_case(args.workload, rank)
+    ns = case.mech.ns
+    api.mech_init(case.mech)
+    dc = api.upload(case)
+    phi_new, _, _ = dc.new_outputs()
+    stream = torch.cuda.current_stream()
+    prm_mixed = case.vd_params(precision=abi.PREC_MIXED)
+    prm_fp64 = case.vd_params(precision=abi.PREC_FP64)
+
+    def timed(prm, steps, warmup):
+        for _ in range(warmup):
+            api.explicit_update_all(dc, prm, phi_new)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n0 = L.vd_launch_count()
+        e0.record(stream)
+        for _ in range(steps):
+            api.explicit_update_all(dc, prm, phi_new)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        return max_over_ranks(ms) / steps, L.vd_launch_count() - n0
+
+    clock = ClockSampler(local)
+    clock.start()
+    ms_mixed, launches = timed(prm_mixed, args.steps, args.warmup)
+    clocks = clock.stop()
+    cells = case.ncell
+    value = world * cells / (ms_mixed * 1e-3)
+
+    # per-kernel device time of the same steps (CUDA events on the launch stream)
+    L.vd_profile_enable(1)
+    for _ in range(args.steps):
+        api.explicit_update_all(dc, prm_mixed, phi_new)
+    torch.cuda.synchronize()
+    prof = abi.profile_read()
+    L.vd_profile_enable(0)
+
+    # plain FP64 path on the same inputs
+    fp64_steps = max(2, args.steps // 2)
+    ms_fp64, _ = timed(prm_fp64, fp64_steps, 1)
+    L.vd_profile_enable(1)
+    api.explicit_update_all(dc, prm_fp64, phi_new)
+    torch.cuda.synchronize()
+    prof64 = abi.profile_read()
+    L.vd_profile_enable(0)
+
+    # per-species error of the mixed result against the FP64 result (which matches
+    # the CPU oracle to 1e-12, tests/test_gpu_parity.py)
+    api.explicit_update_all(dc, prm_fp64, phi_new)
+    ref64 = phi_new[:ns + 1].clone()
+    api.explicit_update_all(dc, prm_mixed, phi_new)
+    mix = phi_new[:ns + 1]
+    rel = ((mix - ref64).abs() / ref64.abs().clamp_min(1e-300)).reshape(ns + 1, -1)
+    err_max = rel.max(dim=1).values.cpu().numpy()
+    err_l2 = (((mix - ref64) ** 2).reshape(ns + 1, -1).sum(1).sqrt() /
+              (ref64 ** 2).reshape(ns + 1, -1).sum(1).sqrt()).cpu().numpy()
+
+    # end to end through the C ABI: pinned host inputs -> device -> update -> host
+    e2e = None
+    if not args.no_e2e:
+        h_state = torch.from_numpy(case.state).pin_memory()
+        h_ef = [torch.from_numpy(a).pin_memory() for a in case.efield]
+        h_gn = [torch.from_numpy(a).pin_memory() for a in case.gradne]
+        h_out = torch.empty((ns + 1,) + tuple(phi_new.shape[1:]), dtype=torch.float64).pin_memory()
+        h2d = h_state.numel() * 8 + sum(a.numel() * 8 for a in h_ef[:case.dim] + h_gn[:case.dim])
+        d2h = h_out.numel() * 8
+
+        def e2e_step():
+            dc.state.copy_(h_state, non_blocking=True)
+            for d in range(case.dim):
+                dc.efield[d].copy_(h_ef[d], non_blocking=True)
+                dc.gradne[d].copy_(h_gn[d], non_blocking=True)
+            api.explicit_update_all(dc, prm_mixed, phi_new)
+            h_out.copy_(phi_new[:ns + 1], non_blocking=True)
+
+        e2e_steps = max(3, args.steps // 2)
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms_e2e = max_over_ranks(e0.elapsed_time(e1)) / e2e_steps
+        e2e = {"value": world * cells / (ms_e2e * 1e-3), "unit": "cell-updates/s", "ms_per_step": ms_e2e,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "path": "vd_explicit_update_all with pinned-host copies in the timed region"}
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    # roofline of the dominant kernel
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    hbm = peaks.get("hbm_gbs")
+    peak_src = "measured" if hbm else "fallback"
+    hbm = hbm or 6650.0
+    dom = max(prof.items(), key=lambda kv: kv[1][1])
+    kname, (kcount, kms) = dom
+    alg = algorithmic_bytes_per_cell(case)
+    per_launch_ms = kms / kcount
+    bytes_per_launch = alg.get(kname, alg["step"]) * cells
+    achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
+    traffic = read_profile_traffic(kname, args.workload)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": traffic, "kernel": kname, "peak_source": peak_src,
+                "kernel_ms": per_launch_ms,
+                "kernel_share": kms / sum(v[1] for v in prof.values()),
+                "step_achieved_gbs": alg["step"] * cells / (ms_mixed * 1e-3) / 1e9}
+
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        threads = os.cpu_count() or 1
+        lib, kind, run, nplanes, cpp = cpu_reference_rate(case, args.cpu_seconds)
+        t = run(nplanes)
+        cpu = {"value": nplanes * cpp / t, "unit": "cell-updates/s", "cores": threads, "kind": kind,
+               "sample": f"{nplanes} of {case.n[case.dim - 1]} planes ({nplanes * cpp} cells), one step, "
+                         f"{t:.1f} s"}
+
+    line = {
+        "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 (mixed: FP32 WENO, rates, fluxes; FP64 accumulate)",
+        "data": "synthetic",
+        "config": {"workload": WORKLOADS[args.workload], "cells_per_gpu": cells, "species": ns,
+                   "reactions": len(case.mech.reactions), "dim": case.dim, "hyp_order": 5, "weno_scheme": 3,
+                   "precision": "mixed", "l2": "inputs larger than L2 (state + faces stream from HBM every step)",
+                   "parallelism": f"{world} independent boxes (one per GPU)"},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "fp64": {"value": world * cells / (ms_fp64 * 1e-3), "ms_per_step": ms_fp64,
+                 "mixed_speedup": ms_fp64 / ms_mixed,
+                 "kernels_ms": {k: v[1] / v[0] for k, v in prof64.items()}},
+        "kernels_ms": {k: v[1] / v[0] for k, v in prof.items()},
+        "mixed_vs_fp64_error": {"max_rel_per_species": [float(x) for x in err_max],
+                                "l2_rel_per_species": [float(x) for x in err_l2],
+                                "max_rel": float(np.max(err_max))},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

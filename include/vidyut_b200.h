@@ -1,0 +1,268 @@
+/*
+ * vidyut_b200.h -- C ABI of the B200 (sm_100a) explicit species / electron-energy
+ * update of the Vidyut plasma fluid solver.
+ *
+ * The entry points take the same box / Array4 / scalar arguments as the per-box
+ * loops of the reference solver, so an AMReX host can call them where those loops
+ * sit today.  All device pointers are owned by the caller; every call is
+ * asynchronous on the caller's stream and returns VD_OK (0) or a negative status
+ * (the reference calls amrex::Abort in the same situations).
+ *
+ * Reference interfaces replaced (paths relative to the hsitaram/vidyut3d tree):
+ *   vd_mech_init               plasmachem::init (Source/PlasmaChem.cpp:19-26) plus the
+ *                              compile-time case header Chemistry.H (CKWC, productionRate,
+ *                              comp_ener_exch, specMob, specDiff, CKCHRG, mw; e.g.
+ *                              test/models/Ar_DC_1d/Chemistry.H:177-506)
+ *   vd_compute_explicit_flux   the ParallelFor over one face box that calls compute_flux
+ *                              (Source/ScalarSolve.cpp:226-250, Source/compute_explicit_flux.H:200-326)
+ *   vd_compute_dsdt            Vidyut::compute_dsdt (Source/ScalarSolve.cpp:17-55)
+ *   vd_reaction_source         the rxnsrc lambda of Vidyut::update_rxnsrc_at_all_levels
+ *                              (Source/ScalarSolve.cpp:113-168)
+ *   vd_elecenergy_source       Vidyut::compute_elecenergy_source (Source/ElecEnergySource.cpp:16-173)
+ *   vd_explicit_update_all     one explicit step of the whole path: rxnsrc, every transported
+ *                              species' flux + dsdt (Source/ScalarSolve.cpp:57-111), the Joule
+ *                              term, the background-species update (Source/Evolve.cpp:267-287)
+ *                              and the accumulation n += dt*dsdt, fused into two launches.
+ *   vd_batch_*                 no single reference counterpart: the per-box MFIter loops of the
+ *                              functions above run over many independent boxes in one
+ *                              persistent launch (the reference iterates boxes with MFIter).
+ *   vd_server_*                no reference counterpart (continuous-batching request loop).
+ */
+#ifndef VIDYUT_B200_H
+#define VIDYUT_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VD_ABI_VERSION 1
+
+/* ---- limits of the runtime mechanism table ---------------------------------- */
+#define VD_MAX_SPECIES   64
+#define VD_MAX_REACTIONS 512
+#define VD_MAX_REACTANTS 3
+#define VD_MAX_TERMS     6
+
+/* ---- status codes ---------------------------------------------------------- */
+#define VD_OK             0
+#define VD_ERR_ARG       -1   /* null pointer, empty/inverted box, bad component count      */
+#define VD_ERR_SCHEME    -2   /* hyp_order not 1/2/5 or weno_scheme not 1/2/3               */
+#define VD_ERR_GHOST     -3   /* input Array4 does not cover the stencil (too few ghosts)   */
+#define VD_ERR_DIM       -4   /* dim not 1, 2 or 3                                          */
+#define VD_ERR_MECH      -5   /* no mechanism loaded, or the mechanism table is invalid     */
+#define VD_ERR_CUDA      -6   /* a CUDA runtime call failed (vd_last_error has the text)    */
+#define VD_ERR_TIMEOUT   -7   /* a persistent kernel gave up waiting (bounded spin)         */
+#define VD_ERR_NOMEM     -8   /* device scratch could not be obtained                       */
+#define VD_ERR_NONFINITE -9   /* input scan found NaN/Inf                                   */
+#define VD_ERR_BUDGET   -10   /* serving: case does not fit the HBM budget                  */
+#define VD_ERR_STATE    -11   /* call out of order (e.g. batch not built)                   */
+
+/* ---- species / BC codes (Source/VarDefines.H:5-22) -------------------------- */
+/* State component n of an Array4 with NVAR = nspecies + 10 components:
+ *   [0, NS)      species number densities [1/m^3]
+ *   NS+0 EEN     electron energy density [J/m^3]
+ *   NS+1 ETEMP   electron temperature [K]
+ *   NS+2 POT     potential [V]
+ *   NS+3..5      cell-centred E field x, y, z [V/m]
+ *   NS+6 EJH     Joule heating diagnostic, NS+7 EIH inelastic, NS+8 EEH elastic
+ *   NS+9 REF     reduced field E/N [Td]                                         */
+#define VD_EEN(ns)   ((ns) + 0)
+#define VD_ETEMP(ns) ((ns) + 1)
+#define VD_POT(ns)   ((ns) + 2)
+#define VD_EFX(ns)   ((ns) + 3)
+#define VD_EFY(ns)   ((ns) + 4)
+#define VD_EFZ(ns)   ((ns) + 5)
+#define VD_EJH(ns)   ((ns) + 6)
+#define VD_EIH(ns)   ((ns) + 7)
+#define VD_EEH(ns)   ((ns) + 8)
+#define VD_REF(ns)   ((ns) + 9)
+#define VD_NVAR(ns)  ((ns) + 10)
+
+#define VD_BC_PER   0
+#define VD_BC_DIRC  1
+#define VD_BC_HNEU  2
+#define VD_BC_IHNEU 3   /* compute_flux forces a zero face flux on such domain faces */
+#define VD_BC_ROBIN 4
+
+/* species classes used to pick the boundary codes (Source/Evolve.cpp:208-288) */
+#define VD_CLASS_ELECTRON 0
+#define VD_CLASS_ENERGY   1
+#define VD_CLASS_ION      2
+#define VD_CLASS_NEUTRAL  3
+
+/* ---- data descriptors ------------------------------------------------------ */
+/* Same fields and byte layout as amrex::Array4<amrex::Real>: element (i,j,k,n) is
+ * p[(i-begin[0]) + (j-begin[1])*jstride + (k-begin[2])*kstride + n*nstride];
+ * end[] is exclusive.  A 2-D caller has begin[2] = 0, end[2] = 1.              */
+typedef struct vd_array4 {
+    double*  p;
+    int64_t  jstride, kstride, nstride;
+    int32_t  begin[3], end[3];
+    int32_t  ncomp;
+} vd_array4;
+
+/* amrex::Box: smallEnd lo[], bigEnd hi[] (inclusive), index type itype[] (0 cell,
+ * 1 node) and the spatial dimension of the caller's build (AMREX_SPACEDIM).      */
+typedef struct vd_box {
+    int32_t lo[3], hi[3], itype[3];
+    int32_t dim;
+} vd_box;
+
+/* ---- runtime mechanism (replaces the compile-time Chemistry.H) --------------- */
+/* rate kinds: k_f as a function of Te [K] (productionRate in the case header)     */
+#define VD_RATE_ARRHENIUS_TE 0   /* k = A * Te^b * exp(-C/Te)                      */
+#define VD_RATE_CONST        1   /* k = A                                           */
+#define VD_RATE_ARRHENIUS_TG 2   /* k = A * Tg^b * exp(-C/Tg)                       */
+
+/* electron-energy exchange types (comp_ener_exch, rxntype) */
+#define VD_RXN_NONE       0
+#define VD_RXN_EXCITATION 1
+#define VD_RXN_IONIZATION 2
+#define VD_RXN_RECOMB     3
+#define VD_RXN_ELASTIC    5
+
+/* mobility models (specMob): mob_kind[s] for s in [0, NS]; s = NS is the energy  */
+#define VD_MOB_ZERO      0   /* mu = 0                                                     */
+#define VD_MOB_ELECTRON  1   /* nu = sqrt(8 kB Te/(pi me)) N sigma;  mu = -e/me/nu         */
+#define VD_MOB_ION_TG    2   /* nu = sqrt(8 kB Tg/(pi M)) N sigma;   mu =  e/M/nu          */
+#define VD_MOB_SCALED    3   /* mu = p0 * mu[ref]                                          */
+#define VD_MOB_CONST_N   4   /* mu = p0 / N                                                */
+#define VD_MOB_CONST     5   /* mu = p0                                                    */
+/* diffusion models (specDiff) */
+#define VD_DIFF_ZERO       0
+#define VD_DIFF_TE_ABSMOB  1   /* D = (factor * Te/eV) * |mu[ref]|  */
+#define VD_DIFF_TG_MOB     2   /* D = (factor * Tg/eV) *  mu[ref]   */
+
+typedef struct vd_reaction {
+    int32_t kind;                       /* VD_RATE_*                                   */
+    int32_t nreac;                      /* q_f = k_f * sc[reac[0]] * ... (in order)    */
+    int32_t reac[VD_MAX_REACTANTS];
+    int32_t rxntype;                    /* VD_RXN_*                                    */
+    int32_t elidx;                      /* collision partner for VD_RXN_ELASTIC        */
+    int32_t nterms;                     /* wdot[term_sp[t]] += term_coef[t] * qdot     */
+    int32_t term_sp[VD_MAX_TERMS];
+    double  term_coef[VD_MAX_TERMS];
+    double  A, b, C;                    /* C in kelvin, A in (m^3/mol)^(nreac-1)/s     */
+    double  eexci;                      /* threshold energy [eV]                       */
+} vd_reaction;
+
+typedef struct vd_mech {
+    int32_t nspecies, nreactions;
+    int32_t e_id;                                   /* electron species index         */
+    int32_t charge[VD_MAX_SPECIES];                 /* CKCHRG                         */
+    double  mw[VD_MAX_SPECIES];                     /* g/mol (get_mw)                 */
+    int32_t mob_kind[VD_MAX_SPECIES + 1];
+    int32_t mob_ref[VD_MAX_SPECIES + 1];
+    double  mob_p0[VD_MAX_SPECIES + 1];             /* cross section [m^2] / factor   */
+    double  mob_p1[VD_MAX_SPECIES + 1];             /* particle mass [kg]             */
+    int32_t diff_kind[VD_MAX_SPECIES + 1];
+    int32_t diff_ref[VD_MAX_SPECIES + 1];
+    double  diff_factor[VD_MAX_SPECIES + 1];
+    int32_t elastic_loss;                           /* trailing elastic-collision loss */
+    int32_t pad0;
+    double  elastic_mass;                           /* heavy-partner mass [kg]        */
+    vd_reaction rxn[VD_MAX_REACTIONS];
+} vd_mech;
+
+/* ---- run parameters (Vidyut::ReadParameters keys, Source/Vidyut.cpp:258-392) -- */
+#define VD_PREC_FP64  0
+#define VD_PREC_MIXED 1   /* FP32 WENO / rates / flux arithmetic, FP64 accumulation */
+
+typedef struct vd_params {
+    int32_t dim;                 /* AMREX_SPACEDIM of the caller                  */
+    int32_t hyp_order;           /* vidyut.hyp_order: 1, 2 or 5                    */
+    int32_t weno_scheme;         /* vidyut.weno_scheme: 1 JS, 2 M, 3 Z              */
+    int32_t user_defined_vel;    /* 1: constant velocity user_vel for vel_species  */
+    int32_t vel_species;
+    int32_t precision;           /* VD_PREC_*                                       */
+    double  user_vel[3];
+    double  Tg, Pg, time, dt;
+    double  dx[3];
+    int32_t domlo[3], domhi[3];
+    int32_t bc_lo[4][3], bc_hi[4][3];   /* per VD_CLASS_*, per direction             */
+    int32_t elecenergy_solve, do_reactions, do_transport, do_bg_reactions;
+    int32_t floor_jh, const_ele_trans, cs_technique, bound_specden;
+    double  ele_mob, ele_diff;
+    double  min_species_density, min_electron_density, min_electron_temp;
+    uint64_t bg_mask;            /* bit s: species s is a background species       */
+    int32_t update_te;           /* 1: Te = (2/3) eps/(kB ne_old), floored         */
+    int32_t gradne_from_state;   /* 1: gradne_fc = face difference of ne (state)   */
+} vd_params;
+
+/* ---- library ------------------------------------------------------------- */
+int         vd_abi_version(void);
+/* sizeof of the ABI structs, for binding checks: which = 0 vd_array4, 1 vd_box,
+ * 2 vd_reaction, 3 vd_mech, 4 vd_params (no reference counterpart).           */
+size_t      vd_sizeof(int which);
+const char* vd_last_error(void);           /* text of the last failure on this thread */
+const char* vd_status_string(int status);
+
+/* Validates and loads the mechanism on the current device (the reference compiles
+ * it into the binary).  Must be called before any compute entry point.           */
+int vd_mech_init(const vd_mech* m);
+
+/* Face fluxes of one species in one sweep direction over the face box
+ * convert(bx, dir) (Source/ScalarSolve.cpp:208-250).  phi holds NVAR components
+ * with at least 1/2/3 ghost cells for hyp_order 1/2/5; fx is the face array.     */
+int vd_compute_explicit_flux(const vd_box* bx, int dir, int specid, vd_array4 phi,
+                             const int32_t bclo[3], const int32_t bchi[3],
+                             const int32_t domlo[3], const int32_t domhi[3],
+                             vd_array4 fx, double Tg, double Pg, double time,
+                             const double dx[3], double dt, int hyp_order,
+                             int user_defined_vel, int weno_scheme,
+                             const double user_vel[3], int vel_species, void* stream);
+
+/* dsdt(i,j,k) = sum_d (F_d(lo) - F_d(hi)) / dx_d + rxn(i,j,k,specid). */
+int vd_compute_dsdt(const vd_box* bx, int specid, const vd_array4 flux[3],
+                    vd_array4 rxn, vd_array4 dsdt, const double dx[3], void* stream);
+
+/* rxn(i,j,k,0..NS-1) = species production rates [1/m^3/s], rxn(i,j,k,NS) = electron
+ * energy exchange [W/m^3] from CKWC of the loaded mechanism.                      */
+int vd_reaction_source(const vd_box* bx, vd_array4 sborder, vd_array4 rxn,
+                       double Tg, double Pg, double time, void* stream);
+
+/* Joule heating: dsdt += Q_J, phi_new(EJH) = Q_J, phi_new(EIH) = rxn(NS).        */
+int vd_elecenergy_source(const vd_box* bx, vd_array4 sborder, vd_array4 rxn,
+                         const vd_array4 efield_ec[3], const vd_array4 gradne_fc[3],
+                         vd_array4 dsdt, vd_array4 phi_new, const vd_params* prm,
+                         void* stream);
+
+/* One explicit step over one box: phi_new = sborder + dt * dsdt for every
+ * transported species and the electron energy (when elecenergy_solve), background
+ * species += dt * rxn (when do_bg_reactions), EJH/EIH diagnostics.  dsdt (NT = NS+1
+ * components, species index order) and rxn (NS+1 components) are optional outputs
+ * (p == NULL to skip).  efield_ec/gradne_fc are the face arrays of the reference
+ * (gradne_fc ignored when prm->gradne_from_state).                               */
+int vd_explicit_update_all(const vd_box* bx, vd_array4 sborder,
+                           const vd_array4 efield_ec[3], const vd_array4 gradne_fc[3],
+                           vd_array4 phi_new, vd_array4 dsdt, vd_array4 rxn,
+                           const vd_params* prm, void* stream);
+
+/* Per-box FP64 checksums of an update (conservation checks, north_star):
+ * out[0] = sum over cells of sum_s charge_s * rxn_s   (charge production; 0 up to rounding)
+ * out[1] = sum over cells of sum_s |charge_s * rxn_s| (scale for out[0])
+ * out[2] = sum over cells of rxn(NS)                  (energy exchange)
+ * out[3] = sum over cells and species of phi_new_s    (total particle count)
+ * out is a device pointer to 4 doubles.                                           */
+int vd_box_checksums(const vd_box* bx, vd_array4 rxn, vd_array4 phi_new,
+                     double* out_dev, void* stream);
+
+/* ---- measurement (no reference counterpart; the reference only prints the
+ * whole-run wall time, Source/main.cpp:45-46) --------------------------------
+ * vd_launch_count: kernels launched by this library since load (all entry points).
+ * vd_profile_enable(1): from now on every launch is bracketed by CUDA events on
+ * its own stream; vd_profile_read synchronises those events and returns, per
+ * kernel name, the number of launches and their summed device time [ms] (at most
+ * max entries, names NUL-separated in names, up to names_len bytes).
+ * vd_profile_enable(0) stops recording and clears the records.                  */
+int64_t vd_launch_count(void);
+int     vd_profile_enable(int on);
+int     vd_profile_read(char* names, int names_len, int64_t* counts, double* ms, int max);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VIDYUT_B200_H */

@@ -1,0 +1,72 @@
+"""C-ABI checks that need no GPU: the library loads, exports every function that
+include/vidyut_b200.h declares, and its struct layouts match the ctypes mirror."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+from vidyut_b200 import _abi as abi
+from vidyut_b200 import build as vbuild
+from vidyut_b200 import mechanism as mm
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "vidyut_b200.h"
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not abi.LIB_PATH.exists():
+        vbuild.build()
+    return abi.lib()
+
+
+def declared_functions():
+    txt = HEADER.read_text()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(vd_\w+)\s*\(", txt)))
+
+
+def test_exports_every_declared_symbol(lib):
+    names = declared_functions()
+    assert len(names) >= 10
+    for n in names:
+        assert hasattr(lib, n), f"{n} declared in the header but not exported"
+    assert set(abi.PROTOTYPES) <= set(names)
+
+
+def test_struct_layouts(lib):
+    abi.check_layout(lib)
+    assert lib.vd_abi_version() == 1
+    # vd_array4 has amrex::Array4<Real>'s layout: pointer, 3 strides, begin/end Dim3, ncomp
+    assert C.sizeof(abi.VdArray4) == 64
+
+
+def test_status_strings(lib):
+    assert lib.vd_status_string(abi.ERR_GHOST) == b"too few ghost cells"
+    assert lib.vd_status_string(0) == b"ok"
+
+
+def test_mechanism_validation_rejects_bad_tables(lib):
+    """vd_mech_init checks the table before touching the device."""
+    m = mm.argon(10, 1).to_c()
+    m.nspecies = 0
+    assert lib.vd_mech_init(C.byref(m)) == abi.ERR_MECH
+    m = mm.argon(10, 1).to_c()
+    m.rxn[3].reac[0] = 17
+    assert lib.vd_mech_init(C.byref(m)) == abi.ERR_MECH
+    assert b"reactant" in lib.vd_last_error()
+    m = mm.argon(10, 1).to_c()
+    m.mob_kind[4] = abi.MOB_SCALED
+    m.mob_ref[4] = 4
+    assert lib.vd_mech_init(C.byref(m)) == abi.ERR_MECH
+    m = mm.argon(10, 1).to_c()
+    m.rxn[0].A = -1.0
+    assert lib.vd_mech_init(C.byref(m)) == abi.ERR_MECH
+
+
+def test_calls_before_mech_init_fail_cleanly(lib):
+    """Without a loaded mechanism (or without a GPU) nothing is launched."""
+    b = abi.make_box((0, 0, 0), (3, 3, 0), 2)
+    z = abi.null_array4()
+    rc = lib.vd_reaction_source(C.byref(b), z, z, 300.0, 0.0, 0.0, None)
+    assert rc in (abi.ERR_MECH, abi.ERR_CUDA, abi.ERR_ARG)

@@ -1,0 +1,236 @@
+"""GPU parity: every C-ABI entry point against the CPU oracle (and the golden
+fixtures written by the reference's own code).
+
+Tolerances (stated per north_star):
+  FP64 path   normwise relative error max|gpu - ref| / max|ref| <= 1e-12 for every
+              output component (fluxes, rxn, dsdt, Joule), and elementwise
+              relative <= 1e-12 for the updated densities n + dt*dsdt;
+  mixed path  elementwise relative error of every updated species density and the
+              electron energy <= 1e-5 against the FP64 oracle.
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from tests._util import FIXTURES, load_fixture, normwise_rel, per_component_rel, max_elem_rel
+from vidyut_b200 import _abi as abi
+from vidyut_b200 import api
+from vidyut_b200 import inputs as vin
+from vidyut_b200 import mechanism as mm
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL_MIXED = 1e-5
+SCHEMES = [(1, 3), (2, 3), (5, 1), (5, 2), (5, 3)]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _gpu():
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    abi.lib()
+    abi.check_layout()
+
+
+def seeded_cases():
+    S = vin.BASE_SEED
+    return {
+        "argon2d": vin.build_case(mm.argon(10, S + 1), 2, (70, 45), (1e-5, 1e-5), S + 201, density="blob"),
+        "synth24_3d": vin.build_case(mm.synthetic(24, 150, S + 11), 3, (19, 13, 11), (1e-5,) * 3, S + 202,
+                                     density="loguniform", dens_range=(1e8, 1e22), te_range_ev=(0.3, 10.0)),
+        "synth8_1d": vin.build_case(mm.synthetic(8, 40, S + 21), 1, (300,), (1e-5,), S + 203,
+                                    density="loguniform", dens_range=(1e10, 1e18)),
+        "synth8_2d": vin.build_case(mm.synthetic(8, 40, S + 21), 2, (45, 33), (1e-5, 2e-5), S + 204,
+                                    density="loguniform", dens_range=(1e10, 1e18)),
+    }
+
+
+CASES = seeded_cases()
+
+
+def _gpu_flux(dc, d, s, h, w, **kw):
+    fx = api.face_tensor(dc.case, d)
+    api.compute_explicit_flux(dc, d, s, fx, hyp_order=h, weno=w, **kw)
+    torch.cuda.synchronize()
+    return fx.cpu().numpy()
+
+
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("name", FIXTURES)
+def test_golden_fixtures_on_gpu(name):
+    """GPU entry points reproduce the reference's own outputs (golden fixtures)."""
+    case, meta, outs = load_fixture(name)
+    api.mech_init(case.mech)
+    dc = api.upload(case)
+    udv = 1 if "uvel" in meta else 0
+    kw = dict(udv=udv, uvel=tuple(meta.get("uvel", (0, 0, 0))), vel_species=meta.get("vel_species", 0))
+    if udv:
+        kw.update(bclo=(0, 0, 0), bchi=(0, 0, 0))
+    for key, want in outs.items():
+        if key.startswith("flux_"):
+            _, s, d, h, w = key.split("_")
+            got = _gpu_flux(dc, int(d[1:]), int(s[1:]), int(h[1:]), int(w[1:]), **kw)
+            assert normwise_rel(got, want) <= TOL64, key
+    if "rxn" in outs:
+        _, _, rxn = dc.new_outputs()
+        api.reaction_source(dc, rxn)
+        assert per_component_rel(rxn.cpu().numpy(), outs["rxn"]).max() <= TOL64
+    if "upd_phi_new" in outs:
+        phi_new, dsdt, rxn = dc.new_outputs()
+        api.explicit_update_all(dc, case.vd_params(), phi_new, dsdt, rxn)
+        torch.cuda.synchronize()
+        ns = case.mech.ns
+        assert per_component_rel(dsdt.cpu().numpy(), outs["upd_dsdt"]).max() <= TOL64
+        assert per_component_rel(rxn.cpu().numpy(), outs["upd_rxn"]).max() <= TOL64
+        pn, want = phi_new.cpu().numpy(), outs["upd_phi_new"]
+        assert max_elem_rel(pn[:ns + 1], want[:ns + 1]) <= TOL64
+        assert per_component_rel(pn, want).max() <= TOL64
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_reaction_source_fp64(name):
+    case = CASES[name]
+    api.mech_init(case.mech)
+    dc = api.upload(case)
+    _, _, rxn = dc.new_outputs()
+    api.reaction_source(dc, rxn)
+    want = oracle.Port(case.mech).reaction_source(case)
+    err = per_component_rel(rxn.cpu().numpy(), want)
+    assert err.max() <= TOL64, err
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_explicit_flux_all_schemes(name):
+    case = CASES[name]
+    api.mech_init(case.mech)
+    dc = api.upload(case)
+    port = oracle.Port(case.mech)
+    m = case.mech
+    ion = next(s for s in range(m.ns) if m.charge[s] > 0)
+    for s in (m.e_id, ion, m.ns):
+        for d in range(case.dim):
+            for h, w in SCHEMES:
+                got = _gpu_flux(dc, d, s, h, w)
+                want = port.flux(case, d, s, hyp_order=h, weno=w)
+                assert normwise_rel(got, want) <= TOL64, (s, d, h, w)
+
+
+def test_ihneubc_zero_flux_and_periodic_faces():
+    """IHNEUBC forces zero flux on the domain faces (compute_explicit_flux.H:318-325);
+    other codes leave them computed."""
+    case = CASES["argon2d"]
+    api.mech_init(case.mech)
+    dc = api.upload(case)
+    for d in range(2):
+        z = _gpu_flux(dc, d, 0, 5, 3, bclo=(3, 3, 3), bchi=(3, 3, 3))
+        nz = _gpu_flux(dc, d, 0, 5, 3, bclo=(2, 2, 2), bchi=(1, 1, 1))
+        sl_lo = [slice(None)] * 4
+        sl_hi = [slice(None)] * 4
+        sl_lo[3 - d] = 0
+        sl_hi[3 - d] = -1
+        assert np.all(z[tuple(sl_lo)] == 0.0) and np.all(z[tuple(sl_hi)] == 0.0)
+        assert np.any(nz[tuple(sl_lo)] != 0.0)
+
+
+def test_dsdt_and_joule():
+    case = CASES["synth8_2d"]
+    m = case.mech
+    api.mech_init(m)
+    dc = api.upload(case)
+    port = oracle.Port(m)
+    rxn_np = port.reaction_source(case)
+    rxn = torch.from_numpy(rxn_np).cuda()
+    for s in (m.e_id, m.ns):
+        fl_np = [port.flux(case, d, s) for d in range(2)]
+        fl = [torch.from_numpy(f).cuda() for f in fl_np]
+        out = torch.zeros((1, 1, case.n[1], case.n[0]), dtype=torch.float64, device="cuda")
+        api.compute_dsdt(dc, s, fl, rxn, out)
+        want = port.dsdt(case, s, fl_np, rxn_np)
+        assert normwise_rel(out.cpu().numpy(), want) <= 1e-14
+    prm = case.vd_params()
+    de_want, pn_want = port.elecenergy(case, rxn_np, prm)
+    de = torch.zeros((1, 1, case.n[1], case.n[0]), dtype=torch.float64, device="cuda")
+    phi_new, _, _ = dc.new_outputs()
+    api.compute_elecenergy_source(dc, rxn, de, phi_new, prm)
+    torch.cuda.synchronize()
+    assert normwise_rel(de.cpu().numpy(), de_want) <= TOL64
+    ns = m.ns
+    assert normwise_rel(phi_new.cpu().numpy()[abi.EJH(ns)], pn_want[abi.EJH(ns)]) <= TOL64
+    assert np.array_equal(phi_new.cpu().numpy()[abi.EIH(ns)], pn_want[abi.EIH(ns)])
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("hw", [(5, 3), (5, 1), (2, 3), (1, 3)])
+def test_update_all_fp64(name, hw):
+    case = CASES[name]
+    api.mech_init(case.mech)
+    dc = api.upload(case)
+    prm = case.vd_params(hyp_order=hw[0], weno_scheme=hw[1])
+    phi_new, dsdt, rxn = dc.new_outputs()
+    api.explicit_update_all(dc, prm, phi_new, dsdt, rxn)
+    torch.cuda.synchronize()
+    want = oracle.Port(case.mech).update_all(case, prm)
+    ns = case.mech.ns
+    assert per_component_rel(rxn.cpu().numpy(), want["rxn"]).max() <= TOL64
+    assert per_component_rel(dsdt.cpu().numpy(), want["dsdt"]).max() <= TOL64
+    pn = phi_new.cpu().numpy()
+    assert max_elem_rel(pn[:ns + 1], want["phi_new"][:ns + 1]) <= TOL64
+    assert per_component_rel(pn, want["phi_new"]).max() <= TOL64
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_update_all_mixed_precision(name):
+    """FP32 WENO / rates / fluxes with FP64 accumulation: every updated density and
+    the electron energy within 1e-5 of the FP64 oracle (elementwise)."""
+    case = CASES[name]
+    api.mech_init(case.mech)
+    dc = api.upload(case)
+    prm = case.vd_params(precision=abi.PREC_MIXED)
+    phi_new, dsdt, rxn = dc.new_outputs()
+    api.explicit_update_all(dc, prm, phi_new, dsdt, rxn)
+    torch.cuda.synchronize()
+    want = oracle.Port(case.mech).update_all(case, case.vd_params())
+    ns = case.mech.ns
+    pn = phi_new.cpu().numpy()
+    per_species = [max_elem_rel(pn[s], want["phi_new"][s]) for s in range(ns + 1)]
+    assert max(per_species) <= TOL_MIXED, per_species
+
+
+def test_checksums_charge_conservation():
+    case = CASES["synth24_3d"]
+    api.mech_init(case.mech)
+    dc = api.upload(case)
+    phi_new, dsdt, rxn = dc.new_outputs()
+    api.explicit_update_all(dc, case.vd_params(), phi_new, dsdt, rxn)
+    cs = api.box_checksums(dc, rxn, phi_new)
+    assert abs(cs[0]) <= 1e-12 * cs[1]
+    want = oracle.Port(case.mech).update_all(case, case.vd_params())
+    assert abs(cs[3] - want["phi_new"][:case.mech.ns].sum()) <= 1e-12 * abs(cs[3])
+
+
+def test_status_codes_without_launch():
+    """Invalid calls return the reference's abort conditions as status codes and
+    launch nothing."""
+    case = CASES["argon2d"]
+    api.mech_init(case.mech)
+    dc = api.upload(case)
+    fx = api.face_tensor(case, 0)
+    with pytest.raises(abi.VidyutError) as e:
+        api.compute_explicit_flux(dc, 0, 0, fx, hyp_order=3)
+    assert e.value.status == abi.ERR_SCHEME
+    with pytest.raises(abi.VidyutError) as e:
+        api.compute_explicit_flux(dc, 0, 0, fx, hyp_order=5, weno=7)
+    assert e.value.status == abi.ERR_SCHEME
+    # a state with only one ghost layer cannot feed WENO-5
+    small = vin.build_case(case.mech, 2, (16, 12), (1e-5, 1e-5), 7, density="blob", ghost=1)
+    ds = api.upload(small)
+    fx = api.face_tensor(small, 0)
+    with pytest.raises(abi.VidyutError) as e:
+        api.compute_explicit_flux(ds, 0, 0, fx, hyp_order=5)
+    assert e.value.status == abi.ERR_GHOST
+    api.compute_explicit_flux(ds, 0, 0, fx, hyp_order=1)  # one ghost suffices for upwind
+    phi_new, dsdt, rxn = dc.new_outputs()
+    with pytest.raises(abi.VidyutError) as e:
+        api.explicit_update_all(dc, case.vd_params(dim=3), phi_new, dsdt, rxn)
+    assert e.value.status == abi.ERR_DIM

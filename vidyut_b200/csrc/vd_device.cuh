@@ -1,0 +1,316 @@
+// vd_device.cuh -- device-side data layout and physics of the explicit species /
+// electron-energy update (sm_100a).
+//
+// The mechanism lives in __constant__ memory (every thread of a warp reads the
+// same reaction at the same time, so the constant cache broadcasts it).  Two
+// arithmetic flavours share the code:
+//   PREC_FP64   all arithmetic in FP64; results agree with the reference CPU build
+//               to ~1e-14 (FMA contraction and exp(log) rate evaluation are the
+//               only differences);
+//   PREC_MIXED  WENO weights, reconstructions, flux arithmetic and mobilities in
+//               FP32 (values rescaled by an exact power of two per stencil), rate
+//               constants through the FP32 special-function unit, and FP64 for the
+//               production/loss sums, the energy-exchange sum and n += dt*dsdt.
+#pragma once
+#include "vd_types.cuh"
+
+namespace vd {
+
+// The loaded mechanism (one translation unit: vd_kernels.cu includes this header).
+__constant__ VdMechDev c_mech;
+
+// ---------------------------------------------------------------------------
+// Mobility (specMob, test/models/Ar_DC_1d/Chemistry.H:177-202) by model kind.
+// FP64: mob_c = -e/me / sqrt(8 kB/(pi me)) (electron) or e/M / sqrt(8 kB/(pi M))
+// (ion), so mu = mob_c / (sqrt(T) N sigma): one sqrt and one division.
+__device__ __forceinline__ double mob_base_fp64(int s, double Te, double N, double Tg)
+{
+    switch (c_mech.mob_kind[s]) {
+    case VD_MOB_ELECTRON: return c_mech.mob_c[s] / (sqrt(Te) * N * c_mech.mob_p0[s]);
+    case VD_MOB_ION_TG: return c_mech.mob_c[s] / (sqrt(Tg) * N * c_mech.mob_p0[s]);
+    case VD_MOB_CONST_N: return c_mech.mob_p0[s] / N;
+    case VD_MOB_CONST: return c_mech.mob_p0[s];
+    default: return 0.0;
+    }
+}
+__device__ __forceinline__ double mob_fp64(int s, double Te, double N, double Tg)
+{
+    if (c_mech.mob_kind[s] == VD_MOB_SCALED)
+        return c_mech.mob_p0[s] * mob_base_fp64(c_mech.mob_ref[s], Te, N, Tg);
+    return mob_base_fp64(s, Te, N, Tg);
+}
+__device__ __forceinline__ float mob_base_f32(int s, float Te, float N, float Tg)
+{
+    switch (c_mech.mob_kind[s]) {
+    case VD_MOB_ELECTRON: return (float)c_mech.mob_c[s] * rsqrtf(Te) / (N * (float)c_mech.mob_p0[s]);
+    case VD_MOB_ION_TG: return (float)c_mech.mob_c[s] * rsqrtf(Tg) / (N * (float)c_mech.mob_p0[s]);
+    case VD_MOB_CONST_N: return (float)c_mech.mob_p0[s] / N;
+    case VD_MOB_CONST: return (float)c_mech.mob_p0[s];
+    default: return 0.0f;
+    }
+}
+__device__ __forceinline__ float mob_f32(int s, float Te, float N, float Tg)
+{
+    if (c_mech.mob_kind[s] == VD_MOB_SCALED)
+        return (float)c_mech.mob_p0[s] * mob_base_f32(c_mech.mob_ref[s], Te, N, Tg);
+    return mob_base_f32(s, Te, N, Tg);
+}
+// specDiff (test/models/Ar_DC_1d/Chemistry.H:204-239) by model kind.
+__device__ __forceinline__ double diff_fp64(int s, double Te, double N, double Tg)
+{
+    switch (c_mech.diff_kind[s]) {
+    case VD_DIFF_TE_ABSMOB:
+        return c_mech.diff_factor[s] * (Te / EV) * fabs(mob_fp64(c_mech.diff_ref[s], Te, N, Tg));
+    case VD_DIFF_TG_MOB:
+        return c_mech.diff_factor[s] * (Tg / EV) * mob_fp64(c_mech.diff_ref[s], Te, N, Tg);
+    default: return 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// WENO-5 reconstruction at i+1/2 from (im2, im1, i, ip1, ip2)
+// (Source/compute_explicit_flux.H:25-112).  SCHEME 1 JS, 2 M, 3 Z.
+template <class R>
+__device__ __forceinline__ R gk_map(R wk, R g)
+{
+    return wk * (g + g * g - R(3) * g * wk + wk * wk) / (g * g + wk * (R(1) - R(2) * g));
+}
+
+__device__ __forceinline__ double weno_fp64(double a, double b, double c, double d, double e, int scheme)
+{
+    const double eps = 1e-20;
+    double p1 = (1.0 / 3.0) * a - (7.0 / 6.0) * b + (11.0 / 6.0) * c;
+    double p2 = -(1.0 / 6.0) * b + (5.0 / 6.0) * c + (1.0 / 3.0) * d;
+    double p3 = (1.0 / 3.0) * c + (5.0 / 6.0) * d - (1.0 / 6.0) * e;
+    double t1 = a - 2.0 * b + c, t2 = a - 4.0 * b + 3.0 * c;
+    double b1 = (13.0 / 12.0) * (t1 * t1) + 0.25 * (t2 * t2);
+    double t3 = b - 2.0 * c + d, t4 = b - d;
+    double b2 = (13.0 / 12.0) * (t3 * t3) + 0.25 * (t4 * t4);
+    double t5 = c - 2.0 * d + e, t6 = 3.0 * c - 4.0 * d + e;
+    double b3 = (13.0 / 12.0) * (t5 * t5) + 0.25 * (t6 * t6);
+    double a1, a2, a3;
+    if (scheme == 3) {
+        double tau = fabs(b1 - b3);
+        double r1 = tau / (b1 + eps), r2 = tau / (b2 + eps), r3 = tau / (b3 + eps);
+        a1 = 0.1 * (1.0 + r1 * r1);
+        a2 = 0.6 * (1.0 + r2 * r2);
+        a3 = 0.3 * (1.0 + r3 * r3);
+    } else {
+        double q1 = b1 + eps, q2 = b2 + eps, q3 = b3 + eps;
+        a1 = 0.1 / (q1 * q1);
+        a2 = 0.6 / (q2 * q2);
+        a3 = 0.3 / (q3 * q3);
+        if (scheme == 2) {
+            double s = a1 + a2 + a3;
+            double w1 = a1 / s, w2 = a2 / s, w3 = a3 / s;
+            a1 = gk_map(w1, 0.1);
+            a2 = gk_map(w2, 0.6);
+            a3 = gk_map(w3, 0.3);
+        }
+    }
+    double s = a1 + a2 + a3;
+    return (a1 / s) * p1 + (a2 / s) * p2 + (a3 / s) * p3;
+}
+
+// FP32 reconstruction of values already scaled to O(1).  The nonlinear weights
+// use one reciprocal: with B_k = beta_k + eps normalised by max_k B_k,
+// w_k is proportional to gamma_k (B_k^2 + tau^2) prod_{j!=k} B_j^2 (WENO-Z) or
+// gamma_k prod_{j!=k} B_j^2 (WENO-JS); WENO-M keeps its explicit map.
+__device__ __forceinline__ float weno_f32(float a, float b, float c, float d, float e, int scheme,
+                                          float eps)
+{
+    float p1 = fmaf(1.0f / 3.0f, a, fmaf(-7.0f / 6.0f, b, (11.0f / 6.0f) * c));
+    float p2 = fmaf(-1.0f / 6.0f, b, fmaf(5.0f / 6.0f, c, (1.0f / 3.0f) * d));
+    float p3 = fmaf(1.0f / 3.0f, c, fmaf(5.0f / 6.0f, d, (-1.0f / 6.0f) * e));
+    float t1 = fmaf(-2.0f, b, a) + c, t2 = fmaf(-4.0f, b, a) + 3.0f * c;
+    float b1 = fmaf(13.0f / 12.0f, t1 * t1, 0.25f * (t2 * t2));
+    float t3 = fmaf(-2.0f, c, b) + d, t4 = b - d;
+    float b2 = fmaf(13.0f / 12.0f, t3 * t3, 0.25f * (t4 * t4));
+    float t5 = fmaf(-2.0f, d, c) + e, t6 = fmaf(3.0f, c, fmaf(-4.0f, d, e));
+    float b3 = fmaf(13.0f / 12.0f, t5 * t5, 0.25f * (t6 * t6));
+    float q1 = b1 + eps, q2 = b2 + eps, q3 = b3 + eps;
+    float a1, a2, a3;
+    if (scheme == 2) {
+        float i1 = __frcp_rn(q1 * q1), i2 = __frcp_rn(q2 * q2), i3 = __frcp_rn(q3 * q3);
+        a1 = 0.1f * i1;
+        a2 = 0.6f * i2;
+        a3 = 0.3f * i3;
+        float is = __frcp_rn(a1 + a2 + a3);
+        a1 = gk_map(a1 * is, 0.1f);
+        a2 = gk_map(a2 * is, 0.6f);
+        a3 = gk_map(a3 * is, 0.3f);
+    } else {
+        float mx = fmaxf(q1, fmaxf(q2, q3));
+        float im = __frcp_rn(mx);
+        q1 *= im;
+        q2 *= im;
+        q3 *= im;
+        float s1 = q1 * q1, s2 = q2 * q2, s3 = q3 * q3;
+        if (scheme == 3) {
+            float tau = fabsf(b1 - b3) * im;
+            float tt = tau * tau;
+            a1 = 0.1f * (s1 + tt) * (s2 * s3);
+            a2 = 0.6f * (s2 + tt) * (s1 * s3);
+            a3 = 0.3f * (s3 + tt) * (s1 * s2);
+        } else {
+            a1 = 0.1f * (s2 * s3);
+            a2 = 0.6f * (s1 * s3);
+            a3 = 0.3f * (s1 * s2);
+        }
+    }
+    float is = __frcp_rn(a1 + a2 + a3);
+    return fmaf(a1, p1, fmaf(a2, p2, a3 * p3)) * is;
+}
+
+// ---------------------------------------------------------------------------
+// Face flux from the 6-cell stencil u[0..5] = cells (i-3 .. i+2), velocities v[0..5]
+// (compute_flux, Source/compute_explicit_flux.H:245-316).  hyp_order 1 and 2 use
+// u[1..4] / v[2..3] only.
+__device__ __forceinline__ double face_flux_fp64(const double* u, const double* v, int hyp_order,
+                                                 int scheme, double dxmin, double dt)
+{
+    const double vL = v[2], vR = v[3], pL = u[2], pR = u[3];
+    if (hyp_order == 1) {
+        double fL = pL * vL, fR = pR * vR;
+        double sgn = copysign(1.0, 0.5 * (vL + vR));
+        return fL * 0.5 * (1.0 + sgn) + fR * 0.5 * (1.0 - sgn);
+    }
+    if (hyp_order == 2) {
+        double dl = pL - u[1], dm = pR - pL, dr = u[4] - pR;
+        double vmid = 0.5 * (vL + vR);
+        double sgn = copysign(1.0, vmid);
+        double cfl = vmid * dt / dxmin;
+        double fL = pL * vL, fR = pR * vR;
+        double r = (cfl >= 0.0) ? dl / (dm + 1.0e-30) : dr / (dm + 1.0e-30);
+        double lim = (r <= 0.0) ? 1.0 : ((r <= 1.0) ? 1.0 - (1.0 - fabs(cfl)) * r : fabs(cfl));
+        return 0.5 * (fL + fR) - 0.5 * sgn * lim * (fR - fL);
+    }
+    double f[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) f[q] = u[q] * v[q];
+    double lam = fabs(0.5 * (vL + vR));
+    double fp = weno_fp64(f[0], f[1], f[2], f[3], f[4], scheme);
+    double fm = weno_fp64(f[5], f[4], f[3], f[2], f[1], scheme);
+    double up = weno_fp64(u[0], u[1], u[2], u[3], u[4], scheme);
+    double um = weno_fp64(u[5], u[4], u[3], u[2], u[1], scheme);
+    return 0.5 * (fp + lam * up) + 0.5 * (fm - lam * um);
+}
+
+// Exact power-of-two scale 2^-e with 2^(e-1) <= m < 2^e (m > 0 finite), else 1.
+__device__ __forceinline__ double pow2_inv_scale(double m)
+{
+    if (!(m > 0.0) || !isfinite(m)) return 1.0;
+    int e = ((int)((__double_as_longlong(m) >> 52) & 0x7ff)) - 1022;  // m in [2^(e-1), 2^e)
+    return __longlong_as_double((long long)(1023 - e) << 52);
+}
+
+__device__ __forceinline__ double face_flux_mixed(const double* u, const float* v, int hyp_order,
+                                                  int scheme, double dxmin, double dt)
+{
+    if (hyp_order != 5) {
+        double vd[6];
+#pragma unroll
+        for (int q = 0; q < 6; q++) vd[q] = (double)v[q];
+        return face_flux_fp64(u, vd, hyp_order, scheme, dxmin, dt);
+    }
+    double m = fmax(fmax(fmax(fabs(u[0]), fabs(u[1])), fmax(fabs(u[2]), fabs(u[3]))),
+                    fmax(fabs(u[4]), fabs(u[5])));
+    double s = pow2_inv_scale(m);
+    float us[6], fs[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        us[q] = (float)(u[q] * s);
+        fs[q] = us[q] * v[q];
+    }
+    // eps = 1e-20 in the unscaled units of u (and of f for |v| ~ 1)
+    float s2 = (float)(s * s);
+    float eps = fmaxf(1e-20f * s2, 1e-30f);
+    float lam = fabsf(0.5f * (v[2] + v[3]));
+    float fp = weno_f32(fs[0], fs[1], fs[2], fs[3], fs[4], scheme, eps);
+    float fm = weno_f32(fs[5], fs[4], fs[3], fs[2], fs[1], scheme, eps);
+    float up = weno_f32(us[0], us[1], us[2], us[3], us[4], scheme, eps);
+    float um = weno_f32(us[5], us[4], us[3], us[2], us[1], scheme, eps);
+    float F = 0.5f * (fmaf(lam, up, fp) + fmaf(-lam, um, fm));
+    return (double)F / s;
+}
+
+// ---------------------------------------------------------------------------
+// CKWC for one cell (Source/ScalarSolve.cpp:143-157 + the generated productionRate,
+// test/models/Ar_DC_1d/Chemistry.H:315-506).  n: number densities [1/m^3] of all
+// species; out[0..NS-1] = rxn [1/m^3/s]; out[NS] = energy exchange [W/m^3].
+// sc and wdot live in thread-local arrays indexed by the table.
+template <int PREC>
+__device__ __forceinline__ void chem_cell(const double* n, double Te, double Tg, double* out)
+{
+    const int ns = c_mech.ns;
+    const int eid = c_mech.e_id;
+    double sc[VD_MAX_SPECIES];
+    double wdot[VD_MAX_SPECIES];
+    for (int s = 0; s < ns; s++) {
+        sc[s] = n[s] * 1.0e-6 / N_A * 1.0e6;
+        wdot[s] = 0.0;
+    }
+    const double ne = sc[eid] * NA_CE;
+    const double Ue = 1.5 * Te * ne * KB_CE;
+    const double mee_na = Ue / ne * NA_CE;
+    const double sefact = (tanh((Te - Tg) / 0.5) + 1.0) / 2.0;
+    const double dT = Te - Tg;
+    double lnTe, invTe, lnTg, invTg;
+    if (PREC == PREC_FP64) {
+        lnTe = log(Te);
+        lnTg = log(Tg);
+    } else {
+        lnTe = log2(Te);
+        lnTg = log2(Tg);
+    }
+    invTe = 1.0 / Te;
+    invTg = 1.0 / Tg;
+    double ee = 0.0;
+    const int nr = c_mech.nr;
+    for (int r = 0; r < nr; r++) {
+        const VdRxnDev& R = c_mech.rxn[r];
+        double k;
+        if (R.kind == VD_RATE_CONST) {
+            k = R.A;
+        } else {
+            const bool te = (R.kind == VD_RATE_ARRHENIUS_TE);
+            const double lT = te ? lnTe : lnTg;
+            const double iT = te ? invTe : invTg;
+            if (PREC == PREC_FP64) {
+                k = exp(fma(R.b, lT, R.lnA) - R.C * iT);
+            } else {
+                // x = log2 k assembled in FP64; 2^x = 2^round(x) * 2^frac on the FP32 SFU
+                double x = fma(R.b, lT, R.l2A) - R.Cl2 * iT;
+                if (x < -1000.0) {
+                    k = 0.0;
+                } else {
+                    double xi = rint(x);
+                    float ef = exp2f((float)(x - xi));
+                    k = ldexp((double)ef, (int)xi);
+                }
+            }
+        }
+        double prod = sc[R.reac[0]];
+        for (int t = 1; t < R.nreac; t++) prod *= sc[R.reac[t]];
+        const double q = k * prod;
+        for (int t = 0; t < R.nterms; t++) wdot[R.sp[t]] = fma(R.coef[t], q, wdot[R.sp[t]]);
+        if (R.rxntype == VD_RXN_EXCITATION || R.rxntype == VD_RXN_IONIZATION) {
+            ee -= R.ex * q * sefact;
+        } else if (R.rxntype == VD_RXN_RECOMB) {
+            ee -= mee_na * q;
+        } else if (R.rxntype == VD_RXN_ELASTIC) {
+            ee -= R.ex * dT * (sc[eid] * sc[R.elidx] * k) * NA_CE;
+        }
+    }
+    if (c_mech.elastic_loss) {
+        double nd = 0.0;
+        for (int s = 0; s < ns; s++) nd += sc[s] * N_A;
+        double mu = mob_fp64(eid, Te, nd, Tg);
+        double nu = -ECHARGE / ME / mu;
+        ee -= 1.5 * K_B * sc[eid] * N_A * dT * nu * c_mech.elastic_coef;
+    }
+    for (int s = 0; s < ns; s++) out[s] = wdot[s] * 1.0e-6 * N_A * 1.0e6;
+    out[ns] = ee;
+}
+
+}  // namespace vd

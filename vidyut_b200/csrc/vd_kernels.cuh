@@ -1,0 +1,78 @@
+// vd_kernels.cuh -- host-visible launch interface of the device code in vd_kernels.cu.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "vd_types.cuh"
+
+namespace vd {
+
+// Box-loop geometry: cells lo..hi inclusive.
+struct BoxIdx {
+    int lo[3], hi[3];
+    int n[3];
+    int64_t ncell;
+};
+
+// Arguments of the fused transport kernel (per box).
+struct TransportArgs {
+    A4 sb, pn, dsdt, rxn, Nv;
+    A4 ef[3], gne[3];
+    int lo[3], hi[3];
+    int ntile[3];
+    double dx[3], dt, Tg, dxmin;
+    int domlo[3], domhi[3];
+    int8_t zlo[4][3], zhi[4][3];  // 1: IHNEUBC zero flux on that domain face, per class
+    int ntr, nbg;
+    int8_t tr_sp[VD_MAX_SPECIES + 1], tr_cls[VD_MAX_SPECIES + 1], tr_flux[VD_MAX_SPECIES + 1];
+    int8_t bg_sp[VD_MAX_SPECIES];
+    int ns, e_id, hyp_order, weno, udv, vel_sp;
+    double uvel[3];
+    int elecenergy, do_bg, bound_specden, floor_jh, const_ele_trans, cs_technique, gradne_from_state;
+    int update_te, write_diag;
+    double min_spec, ele_mob, ele_diff, min_te, charge_e;
+    int ghost;  // stencil half width H (1, 2 or 3)
+};
+
+// Arguments of the per-cell prep kernel: N = sum_s n_s over the grown box, and
+// rxn (chemistry) over the valid box.
+struct PrepArgs {
+    A4 sb, rxn, Nv;
+    int glo[3], ghi[3];     // grown box
+    int lo[3], hi[3];       // valid box
+    double Tg;
+    int do_reactions, write_n;
+};
+
+int upload_mech(const VdMechDev* h, cudaStream_t st);
+
+cudaError_t launch_reaction_source(const BoxIdx& b, const A4& sb, const A4& rxn, double Tg, int prec,
+                                   cudaStream_t st);
+cudaError_t launch_face_flux(const BoxIdx& fb, int dir, int specid, const A4& phi, const A4& fx,
+                             const int8_t zlo[3], const int8_t zhi[3], const int domlo[3], const int domhi[3],
+                             double Tg, double dxmin, double dt, int hyp_order, int udv, int weno,
+                             const double uvel[3], int vel_sp, int ns, cudaStream_t st);
+cudaError_t launch_dsdt(const BoxIdx& b, int dim, int specid, const A4 flux[3], const A4& rxn, const A4& dsdt,
+                        const double dx[3], cudaStream_t st);
+cudaError_t launch_joule(const BoxIdx& b, int dim, const A4& sb, const A4& rxn, const A4 ef[3], const A4 gne[3],
+                         const A4& dsdt, const A4& pn, const TransportArgs& cfg, cudaStream_t st);
+cudaError_t launch_prep(const PrepArgs& a, int prec, cudaStream_t st);
+cudaError_t launch_transport(const TransportArgs& a, int dim, int prec, cudaStream_t st);
+cudaError_t launch_checksums(const BoxIdx& b, const A4& rxn, const A4& pn, double* out, cudaStream_t st);
+
+// Tile shape used by the transport kernel for a given dimension (for host-side tiling).
+void transport_tile(int dim, int tile[3]);
+
+// Launch accounting: every launch increments a counter; when profiling is on it is
+// bracketed by CUDA events on its stream (see vd_profile_* in the header).
+int64_t launch_count();
+void prof_enable(bool on);
+int prof_read(char* names, int names_len, int64_t* counts, double* ms, int max);
+
+struct ProfScope {
+    int slot;
+    cudaStream_t st;
+    ProfScope(const char* name, cudaStream_t s);
+    ~ProfScope();
+};
+
+}  // namespace vd
