@@ -107,6 +107,7 @@ class Port(_Base):
             L.orc_compute_dsdt.argtypes = [BOXP, C.c_int, A4P, A4P, A4P, DP]
             L.orc_elecenergy_source.argtypes = [MECHP, BOXP, A4P, A4P, A4P, A4P, A4P, A4P, PRMP]
             L.orc_explicit_update_all.argtypes = [MECHP, BOXP, A4P, A4P, A4P, A4P, A4P, A4P, A4P, PRMP]
+            L.orc_update_scale.argtypes = [MECHP, BOXP, A4P, A4P, A4P, A4P, A4P, PRMP]
             L.orc_fill_ghosts.argtypes = [BOXP, A4P, C.c_int, I32P]
             L.orc_fill_ghosts.restype = None
             L.orc_specmob.argtypes = [MECHP, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double]
@@ -164,6 +165,23 @@ class Port(_Base):
                                 C.byref(np_a4(np.ascontiguousarray(rxn), (0, 0, 0))),
                                 C.byref(np_a4(out, (0, 0, 0))), _d3(case.dx))
         return out
+
+    def update_scale(self, case: BoxCase, prm: abi.VdParams):
+        """Per cell and component (NS+1): the gross magnitude of the terms summed into
+        dsdt (sum of |face fluxes|/dx, of |chemistry terms| and of |Joule terms|).
+        rxn errors are measured against the chemistry part, dsdt errors against the
+        whole, and n + dt*dsdt errors against |n| + dt*scale."""
+        _, scale, _ = self.new_outputs(case)
+        ws, wsa = self.flux_ws(case)
+        ef = (A4 * 3)(*[np_a4(case.efield[d], (0, 0, 0)) for d in range(3)])
+        gn = (A4 * 3)(*[np_a4(case.gradne[d], (0, 0, 0)) for d in range(3)])
+        self.L.orc_update_scale(C.byref(self.cm), C.byref(self._box(case)), C.byref(self._sb(case)), ef, gn,
+                                C.byref(np_a4(scale, (0, 0, 0))), wsa, C.byref(prm))
+        return scale
+
+    def rxn_scale(self, case: BoxCase, Tg=300.0):
+        """gross magnitude of the chemistry terms only (transport switched off)"""
+        return self.update_scale(case, case.vd_params(do_transport=0, elecenergy_solve=0, Tg=Tg))
 
     def specmob(self, s, Te, N, Tg=300.0):
         return self.L.orc_specmob(C.byref(self.cm), s, Te, N, 0.0, Tg)

@@ -344,6 +344,30 @@ static double orc_face_flux(const vd_mech *m, int i, int j, int k, int sweepdir,
     return fx;
 }
 
+/* Magnitude of the values one face flux is built from (test error scale): for
+ * WENO, 10/3 (the largest sum of |candidate-polynomial coefficients|) times
+ * max|f| + lambda*max|u| over the six stencil cells; for the first/second-order
+ * fluxes |f_L| + |f_R| (+ the WAF limiter's |f_R - f_L|).                      */
+static double orc_face_scale(const vd_mech *m, int i, int j, int k, int sweepdir, int specid,
+                             const vd_array4 *phi, double Tg, int hyp_order, int udv, const double *uvel,
+                             int vel_species)
+{
+    int H = (hyp_order == 5) ? 3 : hyp_order;
+    double fmax = 0.0, umax = 0.0, vL = 0.0, vR = 0.0, fL = 0.0, fR = 0.0;
+    for (int q = -H; q < H; q++) {
+        int c[3] = {i, j, k};
+        c[sweepdir] += q;
+        double u = A4(phi, c[0], c[1], c[2], specid);
+        double v = orc_vel(m, phi, c, sweepdir, specid, Tg, udv, uvel, vel_species);
+        if (fabs(u * v) > fmax) fmax = fabs(u * v);
+        if (fabs(u) > umax) umax = fabs(u);
+        if (q == -1) { vL = v; fL = u * v; }
+        if (q == 0) { vR = v; fR = u * v; }
+    }
+    if (hyp_order == 5) return (10.0 / 3.0) * (fmax + fabs(0.5 * (vL + vR)) * umax);
+    return 2.0 * (fabs(fL) + fabs(fR));
+}
+
 /* The ParallelFor over convert(bx, dir) (Source/ScalarSolve.cpp:208-250). */
 int orc_compute_explicit_flux(const vd_mech *m, const vd_box *bx, int dir, int specid,
                               const vd_array4 *phi, const int32_t *bclo, const int32_t *bchi,
@@ -562,4 +586,128 @@ void orc_fill_ghosts(const vd_box *bx, const vd_array4 *a, int ng, const int *pe
                             A4(a, gh[0], gh[1], gh[2], c) = A4(a, sh[0], sh[1], sh[2], c);
                         }
     }
+}
+
+/* ------------------------------------------------------------------------- */
+/* Error scales (test infrastructure).  Every output of the update is a sum of
+ * terms; a last-bit change of any term (for instance exp/pow of one library
+ * against another) moves the sum by about eps times the sum of the absolute
+ * terms, not eps times the sum.  These functions return that gross magnitude per
+ * cell so that tests measure errors relative to it.                            */
+
+/* gross magnitude of productionRate: gw[s] = sum |coef*qdot|, *ge = sum of the
+ * absolute energy-exchange terms (same order and units as orc_production_rate). */
+static void orc_production_gross(const vd_mech *m, double *gw, const double *sc, double T, double Te,
+                                 double *ge)
+{
+    int ns = m->nspecies;
+    for (int i = 0; i < ns; ++i) gw[i] = 0.0;
+    *ge = 0.0;
+    double ne = sc[m->e_id] * 6.02214085774e23;
+    double Ue = 1.5 * Te * ne * 1.380649e-23;
+    for (int ir = 0; ir < m->nreactions; ++ir) {
+        const vd_reaction *r = &m->rxn[ir];
+        double k_f = orc_rate(r, T, Te);
+        double prod = sc[r->reac[0]];
+        for (int t = 1; t < r->nreac; ++t) prod = prod * sc[r->reac[t]];
+        double q = k_f * prod;
+        for (int t = 0; t < r->nterms; ++t) gw[r->term_sp[t]] += fabs(r->term_coef[t] * q);
+        if (r->rxntype != VD_RXN_NONE) {
+            double e = 0.0;
+            orc_comp_ener_exch(m, q, 0.0, sc, k_f, r->rxntype, r->eexci, r->elidx, &e, Ue, T, Te);
+            *ge += fabs(e);
+        }
+    }
+    if (m->elastic_loss) {
+        double ndens = 0.0;
+        for (int sp = 0; sp < ns; sp++) ndens += sc[sp] * N_A;
+        double mu = orc_specmob(m, m->e_id, Te, ndens, 0.0, T);
+        double nu = -ECHARGE / ME / mu;
+        *ge += fabs(3.0 / 2.0 * K_B * sc[m->e_id] * N_A * (Te - T) * nu * (2.0 * ME / m->elastic_mass));
+    }
+}
+
+/* dsdt scale of every species and the energy (NS+1 components over bx):
+ * sum_d (S_lo + S_hi)/dx_d + gross(rxn_s) (+ the Joule terms for the energy), with
+ * S the face scale of orc_face_scale. */
+int orc_update_scale(const vd_mech *m, const vd_box *bx, const vd_array4 *sb, const vd_array4 *ef,
+                     const vd_array4 *gne, const vd_array4 *scale, const vd_array4 *flux_ws,
+                     const vd_params *p)
+{
+    int ns = m->nspecies, dim = bx->dim;
+    for (int k = bx->lo[2]; k <= bx->hi[2]; ++k)
+        for (int j = bx->lo[1]; j <= bx->hi[1]; ++j)
+            for (int i = bx->lo[0]; i <= bx->hi[0]; ++i) {
+                double sc[VD_MAX_SPECIES], gw[VD_MAX_SPECIES], ge = 0.0;
+                for (int sp = 0; sp < ns; sp++) sc[sp] = A4(sb, i, j, k, sp) * 1.0e-6 / N_A * 1.0e6;
+                if (p->do_reactions)
+                    orc_production_gross(m, gw, sc, p->Tg, A4(sb, i, j, k, VD_ETEMP(ns)), &ge);
+                else
+                    for (int sp = 0; sp < ns; sp++) gw[sp] = 0.0;
+                for (int sp = 0; sp < ns; sp++) A4(scale, i, j, k, sp) = gw[sp] * 1.0e-6 * N_A * 1.0e6;
+                A4(scale, i, j, k, ns) = ge;
+            }
+    for (int s = 0; s <= ns; s++) {
+        int is_energy = (s == ns);
+        if (is_energy && !p->elecenergy_solve) continue;
+        if (!is_energy && ((p->bg_mask >> s) & 1ull)) continue;
+        if (!p->do_transport) continue;
+        int cls = orc_class(m, s);
+        for (int d = 0; d < dim; d++) {
+            int fhi[3] = {bx->hi[0], bx->hi[1], bx->hi[2]};
+            fhi[d] += 1;
+            for (int k = bx->lo[2]; k <= fhi[2]; ++k)
+                for (int j = bx->lo[1]; j <= fhi[1]; ++j)
+                    for (int i = bx->lo[0]; i <= fhi[0]; ++i)
+                        A4(&flux_ws[d], i, j, k, 0) = orc_face_scale(m, i, j, k, d, s, sb, p->Tg, p->hyp_order,
+                                                                     p->user_defined_vel, p->user_vel,
+                                                                     p->vel_species);
+            (void)cls;
+            for (int k = bx->lo[2]; k <= bx->hi[2]; ++k)
+                for (int j = bx->lo[1]; j <= bx->hi[1]; ++j)
+                    for (int i = bx->lo[0]; i <= bx->hi[0]; ++i) {
+                        int h[3] = {i, j, k};
+                        h[d] += 1;
+                        A4(scale, i, j, k, s) += (fabs(A4(&flux_ws[d], i, j, k, 0)) +
+                                                  fabs(A4(&flux_ws[d], h[0], h[1], h[2], 0))) / p->dx[d];
+                    }
+        }
+    }
+    if (p->elecenergy_solve) {
+        /* Joule: 0.5 * sum over faces |q mu ne E^2| + |q D grad(ne) E| */
+        int eidx = m->e_id;
+        double charge = fabs((double)m->charge[eidx] * ECHARGE);
+        for (int k = bx->lo[2]; k <= bx->hi[2]; ++k)
+            for (int j = bx->lo[1]; j <= bx->hi[1]; ++j)
+                for (int i = bx->lo[0]; i <= bx->hi[0]; ++i) {
+                    double g = 0.0;
+                    for (int idim = 0; idim < dim; idim++)
+                        for (int f = 0; f < 2; f++) {
+                            int face[3] = {i, j, k};
+                            face[idim] += f;
+                            if (face[idim] == p->domlo[idim]) face[idim] += 1;
+                            if (face[idim] == (p->domhi[idim] + 1)) face[idim] -= 1;
+                            int l[3] = {face[0], face[1], face[2]};
+                            l[idim] -= 1;
+                            double etemp = 0.5 * (A4(sb, l[0], l[1], l[2], VD_ETEMP(ns)) +
+                                                  A4(sb, face[0], face[1], face[2], VD_ETEMP(ns)));
+                            double ne = 0.5 * (A4(sb, l[0], l[1], l[2], eidx) + A4(sb, face[0], face[1], face[2], eidx));
+                            double ndens = 0.0;
+                            for (int sp = 0; sp < ns; sp++)
+                                ndens += 0.5 * (A4(sb, l[0], l[1], l[2], sp) + A4(sb, face[0], face[1], face[2], sp));
+                            double efc = p->cs_technique
+                                             ? 0.5 * (A4(sb, l[0], l[1], l[2], VD_EFX(ns) + idim) +
+                                                      A4(sb, face[0], face[1], face[2], VD_EFX(ns) + idim))
+                                             : A4(&ef[idim], face[0], face[1], face[2], 0);
+                            double gn = A4(&gne[idim], face[0], face[1], face[2], 0);
+                            double mu = p->const_ele_trans ? p->ele_mob / ndens
+                                                           : orc_specmob(m, eidx, etemp, ndens, 0.0, p->Tg);
+                            double dc = p->const_ele_trans ? p->ele_diff / ndens
+                                                           : orc_specdiff(m, eidx, etemp, ndens, 0.0, p->Tg);
+                            g += charge * (fabs(mu * ne * efc * efc) + fabs(dc * gn * efc));
+                        }
+                    A4(scale, i, j, k, ns) += 0.5 * g;
+                }
+    }
+    return 0;
 }

@@ -46,3 +46,22 @@ def max_elem_rel(a: np.ndarray, b: np.ndarray, floor: float = 0.0) -> float:
     with np.errstate(divide="ignore", invalid="ignore"):
         r = np.where(den > 0, np.abs(a - b) / den, np.abs(a - b))
     return float(np.max(r))
+
+
+def scaled_err(a: np.ndarray, b: np.ndarray, scale: np.ndarray) -> float:
+    """max over cells of |a - b| / scale: the error relative to the gross magnitude
+    of the terms summed into the value (cells with zero scale must agree exactly)."""
+    d = np.abs(a - b)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r = np.where(scale > 0, d / scale, np.where(d > 0, np.inf, 0.0))
+    return float(np.max(r))
+
+
+def update_scales(port, case, prm):
+    """(rxn scale, dsdt scale, n_new scale) from the oracle, NS+1 components each."""
+    ns = case.mech.ns
+    g = case.gvec
+    n_old = case.state[:ns + 1, g[2]:g[2] + case.n[2], g[1]:g[1] + case.n[1], g[0]:g[0] + case.n[0]]
+    rs = port.rxn_scale(case, prm.Tg)
+    ds = port.update_scale(case, prm)
+    return rs, ds, np.abs(n_old) + prm.dt * ds

@@ -376,7 +376,7 @@ int vd_reaction_source(const vd_box* bx, vd_array4 sborder, vd_array4 rxn, doubl
     std::string why;
     if (!covers(sborder, bx->lo, bx->hi, VD_NVAR(ns), &why)) return fail(VD_ERR_ARG, "sborder: %s", why.c_str());
     if (!covers(rxn, bx->lo, bx->hi, ns + 1, &why)) return fail(VD_ERR_ARG, "rxn: %s", why.c_str());
-    cudaError_t e = launch_reaction_source(box_idx(bx->lo, bx->hi), A4(sborder), A4(rxn), Tg, PREC_FP64, st);
+    cudaError_t e = launch_reaction_source(box_idx(bx->lo, bx->hi), A4(sborder), A4(rxn), Tg, PREC_FP64, ns, st);
     if (e != cudaSuccess) return cuda_fail(e, "k_reaction_source launch");
     return VD_OK;
 }
@@ -400,6 +400,7 @@ static void fill_cfg(TransportArgs& a, const vd_box* bx, const vd_params* p, con
         a.lo[d] = bx->lo[d];
         a.hi[d] = bx->hi[d];
         a.dx[d] = (d < bx->dim) ? p->dx[d] : 1.0;
+        a.idx[d] = 1.0 / a.dx[d];
         a.domlo[d] = p->domlo[d];
         a.domhi[d] = p->domhi[d];
         a.uvel[d] = p->user_vel[d];
@@ -610,7 +611,7 @@ int vd_explicit_update_all(const vd_box* bx, vd_array4 sborder, const vd_array4 
     pa.Tg = prm->Tg;
     pa.do_reactions = prm->do_reactions;
     pa.write_n = 1;
-    e = launch_prep(pa, prm->precision, st);
+    e = launch_prep(pa, prm->precision, ns, st);
     if (e == cudaSuccess) e = launch_transport(a, dim, prm->precision, st);
     cudaError_t e2 = cudaFreeAsync(scratch, st);
     if (e != cudaSuccess) return cuda_fail(e, "fused update launch");

@@ -19,6 +19,15 @@ namespace vd {
 // The loaded mechanism (one translation unit: vd_kernels.cu includes this header).
 __constant__ VdMechDev c_mech;
 
+// Approximate reciprocal on the special-function unit (rcp.approx.ftz.f32,
+// ~1 ulp); arguments are normal positive numbers wherever it is used.
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // ---------------------------------------------------------------------------
 // Mobility (specMob, test/models/Ar_DC_1d/Chemistry.H:177-202) by model kind.
 // FP64: mob_c = -e/me / sqrt(8 kB/(pi me)) (electron) or e/M / sqrt(8 kB/(pi M))
@@ -42,9 +51,9 @@ __device__ __forceinline__ double mob_fp64(int s, double Te, double N, double Tg
 __device__ __forceinline__ float mob_base_f32(int s, float Te, float N, float Tg)
 {
     switch (c_mech.mob_kind[s]) {
-    case VD_MOB_ELECTRON: return (float)c_mech.mob_c[s] * rsqrtf(Te) / (N * (float)c_mech.mob_p0[s]);
-    case VD_MOB_ION_TG: return (float)c_mech.mob_c[s] * rsqrtf(Tg) / (N * (float)c_mech.mob_p0[s]);
-    case VD_MOB_CONST_N: return (float)c_mech.mob_p0[s] / N;
+    case VD_MOB_ELECTRON: return (float)c_mech.mob_c[s] * rsqrtf(Te) * rcp_approx(N * (float)c_mech.mob_p0[s]);
+    case VD_MOB_ION_TG: return (float)c_mech.mob_c[s] * rsqrtf(Tg) * rcp_approx(N * (float)c_mech.mob_p0[s]);
+    case VD_MOB_CONST_N: return (float)c_mech.mob_p0[s] * rcp_approx(N);
     case VD_MOB_CONST: return (float)c_mech.mob_p0[s];
     default: return 0.0f;
     }
@@ -112,10 +121,14 @@ __device__ __forceinline__ double weno_fp64(double a, double b, double c, double
     return (a1 / s) * p1 + (a2 / s) * p2 + (a3 / s) * p3;
 }
 
-// FP32 reconstruction of values already scaled to O(1).  The nonlinear weights
-// use one reciprocal: with B_k = beta_k + eps normalised by max_k B_k,
-// w_k is proportional to gamma_k (B_k^2 + tau^2) prod_{j!=k} B_j^2 (WENO-Z) or
-// gamma_k prod_{j!=k} B_j^2 (WENO-JS); WENO-M keeps its explicit map.
+// FP32 reconstruction of values already scaled to O(1).  The nonlinear weights are
+// rescaled so that no term can overflow and the smoothest stencil always keeps a
+// weight of order gamma (the sum never underflows to zero, whatever the spread of
+// the smoothness indicators): with q_k = beta_k + eps and m = min_k q_k,
+//   WENO-JS  alpha_k ~ gamma_k (m/q_k)^2
+//   WENO-Z   alpha_k ~ gamma_k (1 + (tau/q_k)^2)              if tau <= m
+//            alpha_k ~ gamma_k ((m/tau)^2 + (m/q_k)^2)        otherwise
+// (each a positive multiple of the reference's alpha_k); WENO-M keeps its map.
 __device__ __forceinline__ float weno_f32(float a, float b, float c, float d, float e, int scheme,
                                           float eps)
 {
@@ -128,37 +141,33 @@ __device__ __forceinline__ float weno_f32(float a, float b, float c, float d, fl
     float b2 = fmaf(13.0f / 12.0f, t3 * t3, 0.25f * (t4 * t4));
     float t5 = fmaf(-2.0f, d, c) + e, t6 = fmaf(3.0f, c, fmaf(-4.0f, d, e));
     float b3 = fmaf(13.0f / 12.0f, t5 * t5, 0.25f * (t6 * t6));
-    float q1 = b1 + eps, q2 = b2 + eps, q3 = b3 + eps;
+    const float q1 = b1 + eps, q2 = b2 + eps, q3 = b3 + eps;
+    const float m = fminf(q1, fminf(q2, q3));
+    const float r1 = rcp_approx(q1), r2 = rcp_approx(q2), r3 = rcp_approx(q3);
     float a1, a2, a3;
-    if (scheme == 2) {
-        float i1 = __frcp_rn(q1 * q1), i2 = __frcp_rn(q2 * q2), i3 = __frcp_rn(q3 * q3);
-        a1 = 0.1f * i1;
-        a2 = 0.6f * i2;
-        a3 = 0.3f * i3;
-        float is = __frcp_rn(a1 + a2 + a3);
-        a1 = gk_map(a1 * is, 0.1f);
-        a2 = gk_map(a2 * is, 0.6f);
-        a3 = gk_map(a3 * is, 0.3f);
+    if (scheme == 3) {
+        const float tau = fabsf(b1 - b3);
+        const bool big = tau > m;
+        const float cr = big ? m * rcp_approx(tau) : 1.0f;
+        const float t = big ? m : tau;
+        const float B1 = t * r1, B2 = t * r2, B3 = t * r3;
+        const float c2 = cr * cr;
+        a1 = 0.1f * fmaf(B1, B1, c2);
+        a2 = 0.6f * fmaf(B2, B2, c2);
+        a3 = 0.3f * fmaf(B3, B3, c2);
     } else {
-        float mx = fmaxf(q1, fmaxf(q2, q3));
-        float im = __frcp_rn(mx);
-        q1 *= im;
-        q2 *= im;
-        q3 *= im;
-        float s1 = q1 * q1, s2 = q2 * q2, s3 = q3 * q3;
-        if (scheme == 3) {
-            float tau = fabsf(b1 - b3) * im;
-            float tt = tau * tau;
-            a1 = 0.1f * (s1 + tt) * (s2 * s3);
-            a2 = 0.6f * (s2 + tt) * (s1 * s3);
-            a3 = 0.3f * (s3 + tt) * (s1 * s2);
-        } else {
-            a1 = 0.1f * (s2 * s3);
-            a2 = 0.6f * (s1 * s3);
-            a3 = 0.3f * (s1 * s2);
+        const float B1 = m * r1, B2 = m * r2, B3 = m * r3;
+        a1 = 0.1f * (B1 * B1);
+        a2 = 0.6f * (B2 * B2);
+        a3 = 0.3f * (B3 * B3);
+        if (scheme == 2) {
+            const float is = rcp_approx(a1 + a2 + a3);
+            a1 = gk_map(a1 * is, 0.1f);
+            a2 = gk_map(a2 * is, 0.6f);
+            a3 = gk_map(a3 * is, 0.3f);
         }
     }
-    float is = __frcp_rn(a1 + a2 + a3);
+    float is = rcp_approx(a1 + a2 + a3);
     return fmaf(a1, p1, fmaf(a2, p2, a3 * p3)) * is;
 }
 
@@ -231,31 +240,33 @@ __device__ __forceinline__ double face_flux_mixed(const double* u, const float* 
     float up = weno_f32(us[0], us[1], us[2], us[3], us[4], scheme, eps);
     float um = weno_f32(us[5], us[4], us[3], us[2], us[1], scheme, eps);
     float F = 0.5f * (fmaf(lam, up, fp) + fmaf(-lam, um, fm));
-    return (double)F / s;
+    return (double)F * (1.0 / s);  // s is a power of two: exact
 }
 
 // ---------------------------------------------------------------------------
 // CKWC for one cell (Source/ScalarSolve.cpp:143-157 + the generated productionRate,
-// test/models/Ar_DC_1d/Chemistry.H:315-506).  n: number densities [1/m^3] of all
-// species; out[0..NS-1] = rxn [1/m^3/s]; out[NS] = energy exchange [W/m^3].
-// sc and wdot live in thread-local arrays indexed by the table.
+// test/models/Ar_DC_1d/Chemistry.H:315-506).  The thread's species arrays live in
+// shared memory with a stride of the block size ([species][thread]): every thread
+// of a warp works on the same reaction at the same time, so sc[reac*st + tid] and
+// wd[sp*st + tid] are conflict-free rows, and nothing spills to local memory.
+// On entry sc[s*st] holds the number density of species s [1/m^3]; on exit
+// wd[s*st] holds rxn_s [1/m^3/s]; returns the energy exchange [W/m^3].
 template <int PREC>
-__device__ __forceinline__ void chem_cell(const double* n, double Te, double Tg, double* out)
+__device__ __forceinline__ double chem_cell(double* sc, double* wd, const int st, double Te, double Tg)
 {
     const int ns = c_mech.ns;
     const int eid = c_mech.e_id;
-    double sc[VD_MAX_SPECIES];
-    double wdot[VD_MAX_SPECIES];
     for (int s = 0; s < ns; s++) {
-        sc[s] = n[s] * 1.0e-6 / N_A * 1.0e6;
-        wdot[s] = 0.0;
+        sc[s * st] = sc[s * st] * 1.0e-6 / N_A * 1.0e6;
+        wd[s * st] = 0.0;
     }
-    const double ne = sc[eid] * NA_CE;
+    const double sce = sc[eid * st];
+    const double ne = sce * NA_CE;
     const double Ue = 1.5 * Te * ne * KB_CE;
     const double mee_na = Ue / ne * NA_CE;
     const double sefact = (tanh((Te - Tg) / 0.5) + 1.0) / 2.0;
     const double dT = Te - Tg;
-    double lnTe, invTe, lnTg, invTg;
+    double lnTe, lnTg;
     if (PREC == PREC_FP64) {
         lnTe = log(Te);
         lnTg = log(Tg);
@@ -263,8 +274,7 @@ __device__ __forceinline__ void chem_cell(const double* n, double Te, double Tg,
         lnTe = log2(Te);
         lnTg = log2(Tg);
     }
-    invTe = 1.0 / Te;
-    invTg = 1.0 / Tg;
+    const double invTe = 1.0 / Te, invTg = 1.0 / Tg;
     double ee = 0.0;
     const int nr = c_mech.nr;
     for (int r = 0; r < nr; r++) {
@@ -290,27 +300,30 @@ __device__ __forceinline__ void chem_cell(const double* n, double Te, double Tg,
                 }
             }
         }
-        double prod = sc[R.reac[0]];
-        for (int t = 1; t < R.nreac; t++) prod *= sc[R.reac[t]];
+        double prod = sc[R.reac[0] * st];
+        for (int t = 1; t < R.nreac; t++) prod *= sc[R.reac[t] * st];
         const double q = k * prod;
-        for (int t = 0; t < R.nterms; t++) wdot[R.sp[t]] = fma(R.coef[t], q, wdot[R.sp[t]]);
+        for (int t = 0; t < R.nterms; t++) {
+            double* w = wd + R.sp[t] * st;
+            *w = fma(R.coef[t], q, *w);
+        }
         if (R.rxntype == VD_RXN_EXCITATION || R.rxntype == VD_RXN_IONIZATION) {
             ee -= R.ex * q * sefact;
         } else if (R.rxntype == VD_RXN_RECOMB) {
             ee -= mee_na * q;
         } else if (R.rxntype == VD_RXN_ELASTIC) {
-            ee -= R.ex * dT * (sc[eid] * sc[R.elidx] * k) * NA_CE;
+            ee -= R.ex * dT * (sce * sc[R.elidx * st] * k) * NA_CE;
         }
     }
     if (c_mech.elastic_loss) {
         double nd = 0.0;
-        for (int s = 0; s < ns; s++) nd += sc[s] * N_A;
+        for (int s = 0; s < ns; s++) nd += sc[s * st] * N_A;
         double mu = mob_fp64(eid, Te, nd, Tg);
         double nu = -ECHARGE / ME / mu;
-        ee -= 1.5 * K_B * sc[eid] * N_A * dT * nu * c_mech.elastic_coef;
+        ee -= 1.5 * K_B * sce * N_A * dT * nu * c_mech.elastic_coef;
     }
-    for (int s = 0; s < ns; s++) out[s] = wdot[s] * 1.0e-6 * N_A * 1.0e6;
-    out[ns] = ee;
+    for (int s = 0; s < ns; s++) wd[s * st] = wd[s * st] * 1.0e-6 * N_A * 1.0e6;
+    return ee;
 }
 
 }  // namespace vd

@@ -139,28 +139,46 @@ static inline unsigned grid_for(int64_t n, int bs)
 template <int PREC>
 __global__ void __launch_bounds__(128) k_reaction_source(BoxIdx b, A4 sb, A4 rxn, double Tg)
 {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int ns = c_mech.ns;
+    const int st = blockDim.x;
+    double* sc = reinterpret_cast<double*>(smem_raw) + threadIdx.x;
+    double* wd = sc + ns * st;
     for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < b.ncell;
          idx += (int64_t)gridDim.x * blockDim.x) {
         int i, j, k;
         cell_of(b, idx, i, j, k);
-        double n[VD_MAX_SPECIES], out[VD_MAX_SPECIES + 1];
         const int64_t o = sb.off(i, j, k);
-        for (int s = 0; s < ns; s++) n[s] = sb.p[o + s * sb.ns];
+        for (int s = 0; s < ns; s++) sc[s * st] = sb.p[o + s * sb.ns];
         double Te = sb.p[o + (int64_t)VD_ETEMP(ns) * sb.ns];
-        chem_cell<PREC>(n, Te, Tg, out);
+        double ee = chem_cell<PREC>(sc, wd, st, Te, Tg);
         const int64_t r = rxn.off(i, j, k);
-        for (int s = 0; s <= ns; s++) rxn.p[r + s * rxn.ns] = out[s];
+        for (int s = 0; s < ns; s++) rxn.p[r + s * rxn.ns] = wd[s * st];
+        rxn.p[r + (int64_t)ns * rxn.ns] = ee;
     }
 }
 
-cudaError_t launch_reaction_source(const BoxIdx& b, const A4& sb, const A4& rxn, double Tg, int prec,
+// dynamic shared memory of the chemistry kernels: sc and wd, ns doubles per thread each
+static cudaError_t chem_smem(const void* fn, int ns, int threads, size_t* bytes)
+{
+    *bytes = (size_t)2 * ns * threads * sizeof(double);
+    if (*bytes > 48 * 1024)
+        return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*bytes);
+    return cudaSuccess;
+}
+
+cudaError_t launch_reaction_source(const BoxIdx& b, const A4& sb, const A4& rxn, double Tg, int prec, int ns,
                                    cudaStream_t st)
 {
     unsigned g = grid_for(b.ncell, 128);
+    size_t sm = 0;
+    const void* fn = prec == PREC_MIXED ? (const void*)k_reaction_source<PREC_MIXED>
+                                        : (const void*)k_reaction_source<PREC_FP64>;
+    cudaError_t e = chem_smem(fn, ns, 128, &sm);
+    if (e != cudaSuccess) return e;
     ProfScope ps("k_reaction_source", st);
-    if (prec == PREC_MIXED) k_reaction_source<PREC_MIXED><<<g, 128, 0, st>>>(b, sb, rxn, Tg);
-    else k_reaction_source<PREC_FP64><<<g, 128, 0, st>>>(b, sb, rxn, Tg);
+    if (prec == PREC_MIXED) k_reaction_source<PREC_MIXED><<<g, 128, sm, st>>>(b, sb, rxn, Tg);
+    else k_reaction_source<PREC_FP64><<<g, 128, sm, st>>>(b, sb, rxn, Tg);
     return cudaGetLastError();
 }
 
@@ -357,7 +375,11 @@ cudaError_t launch_joule(const BoxIdx& b, int dim, const A4& sb, const A4& rxn, 
 template <int PREC>
 __global__ void __launch_bounds__(128) k_prep(const __grid_constant__ PrepArgs a)
 {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int ns = c_mech.ns;
+    const int st = blockDim.x;
+    double* sc = reinterpret_cast<double*>(smem_raw) + threadIdx.x;
+    double* wd = sc + ns * st;
     const int gx = a.ghi[0] - a.glo[0] + 1, gy = a.ghi[1] - a.glo[1] + 1, gz = a.ghi[2] - a.glo[2] + 1;
     const int64_t ntot = (int64_t)gx * gy * gz;
     for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < ntot;
@@ -370,43 +392,54 @@ __global__ void __launch_bounds__(128) k_prep(const __grid_constant__ PrepArgs a
         j += a.glo[1];
         k += a.glo[2];
         const int64_t o = a.sb.off(i, j, k);
-        double n[VD_MAX_SPECIES];
         double N = 0.0;
         for (int s = 0; s < ns; s++) {
-            n[s] = a.sb.p[o + s * a.sb.ns];
-            N += n[s];
+            const double v = a.sb.p[o + s * a.sb.ns];
+            sc[s * st] = v;
+            N += v;
         }
         if (a.write_n) a.Nv(i, j, k) = N;
         bool inside = i >= a.lo[0] && i <= a.hi[0] && j >= a.lo[1] && j <= a.hi[1] && k >= a.lo[2] && k <= a.hi[2];
         if (!inside) continue;
         const int64_t ro = a.rxn.off(i, j, k);
         if (a.do_reactions) {
-            double out[VD_MAX_SPECIES + 1];
             double Te = a.sb.p[o + (int64_t)VD_ETEMP(ns) * a.sb.ns];
-            chem_cell<PREC>(n, Te, a.Tg, out);
-            for (int s = 0; s <= ns; s++) a.rxn.p[ro + s * a.rxn.ns] = out[s];
+            double ee = chem_cell<PREC>(sc, wd, st, Te, a.Tg);
+            for (int s = 0; s < ns; s++) a.rxn.p[ro + s * a.rxn.ns] = wd[s * st];
+            a.rxn.p[ro + (int64_t)ns * a.rxn.ns] = ee;
         } else {
             for (int s = 0; s <= ns; s++) a.rxn.p[ro + s * a.rxn.ns] = 0.0;
         }
     }
 }
 
-cudaError_t launch_prep(const PrepArgs& a, int prec, cudaStream_t st)
+cudaError_t launch_prep(const PrepArgs& a, int prec, int ns, cudaStream_t st)
 {
     int64_t n = (int64_t)(a.ghi[0] - a.glo[0] + 1) * (a.ghi[1] - a.glo[1] + 1) * (a.ghi[2] - a.glo[2] + 1);
     unsigned g = grid_for(n, 128);
+    size_t sm = 0;
+    const void* fn = prec == PREC_MIXED ? (const void*)k_prep<PREC_MIXED> : (const void*)k_prep<PREC_FP64>;
+    cudaError_t e = chem_smem(fn, ns, 128, &sm);
+    if (e != cudaSuccess) return e;
     ProfScope ps("k_prep", st);
-    if (prec == PREC_MIXED) k_prep<PREC_MIXED><<<g, 128, 0, st>>>(a);
-    else k_prep<PREC_FP64><<<g, 128, 0, st>>>(a);
+    if (prec == PREC_MIXED) k_prep<PREC_MIXED><<<g, 128, sm, st>>>(a);
+    else k_prep<PREC_FP64><<<g, 128, sm, st>>>(a);
     return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
-// Fused transport kernel.  One CTA per TX x TY x TZ tile, NTH threads.
+// Fused transport kernel.  One CTA per TX x TY x TZ tile, NTH threads.  Per
+// transported species: (1) stage the stencil lines of every sweep direction in
+// shared memory -- for direction d the cells rel -3 .. T_d+2 along d of each tile
+// row, with the density and the drift velocity mu(Te, N) E_d computed once per
+// staged cell; (2) compute every face flux of the tile once (all directions in one
+// pass, faces spread evenly over the threads); (3) each thread takes the
+// divergence of its own cell, adds rxn (and the Joule term for the electron
+// energy) and writes n + dt*dsdt in FP64.  Two barriers per species.
 template <int DIM> struct Tile;
 template <> struct Tile<1> { static constexpr int X = 256, Y = 1, Z = 1, NTH = 256; };
-template <> struct Tile<2> { static constexpr int X = 32, Y = 7, Z = 1, NTH = 256; };
-template <> struct Tile<3> { static constexpr int X = 8, Y = 8, Z = 7, NTH = 512; };
+template <> struct Tile<2> { static constexpr int X = 32, Y = 8, Z = 1, NTH = 256; };
+template <> struct Tile<3> { static constexpr int X = 8, Y = 8, Z = 8, NTH = 512; };
 
 void transport_tile(int dim, int t[3])
 {
@@ -417,20 +450,95 @@ void transport_tile(int dim, int t[3])
 
 template <int DIM>
 struct TileGeom {
-    static constexpr int TX = Tile<DIM>::X, TY = Tile<DIM>::Y, TZ = Tile<DIM>::Z;
-    static constexpr int NCELL = TX * TY * TZ;
-    static constexpr int SX = (TX + 6) * TY * TZ;
-    static constexpr int SY = TX * (TY + 6) * TZ;
-    static constexpr int SZ = TX * TY * (TZ + 6);
-    static constexpr int SMAX = (DIM == 1) ? SX : ((DIM == 2) ? (SX > SY ? SX : SY) : (SX > SY ? (SX > SZ ? SX : SZ) : (SY > SZ ? SY : SZ)));
-    static constexpr int FX = (TX + 1) * TY * TZ;
-    static constexpr int FY = TX * (TY + 1) * TZ;
-    static constexpr int FZ = TX * TY * (TZ + 1);
-    static constexpr int FMAX = (DIM == 1) ? FX : ((DIM == 2) ? (FX > FY ? FX : FY) : (FX > FY ? (FX > FZ ? FX : FZ) : (FY > FZ ? FY : FZ)));
+    static constexpr int T[3] = {Tile<DIM>::X, Tile<DIM>::Y, Tile<DIM>::Z};
+    static constexpr int NCELL = T[0] * T[1] * T[2];
+    // staged line set of direction d: extent T_d + 6 along d
+    template <int D> static constexpr int SE(int e) { return T[e] + (e == D ? 6 : 0); }
+    template <int D> static constexpr int NS() { return D < DIM ? SE<D>(0) * SE<D>(1) * SE<D>(2) : 0; }
+    template <int D> static constexpr int FE(int e) { return T[e] + (e == D ? 1 : 0); }
+    template <int D> static constexpr int NF() { return D < DIM ? FE<D>(0) * FE<D>(1) * FE<D>(2) : 0; }
+    static constexpr int SOFF1 = NS<0>(), SOFF2 = NS<0>() + NS<1>(), STOT = NS<0>() + NS<1>() + NS<2>();
+    static constexpr int FOFF1 = NF<0>(), FOFF2 = NF<0>() + NF<1>(), FTOT = NF<0>() + NF<1>() + NF<2>();
 };
 
 template <int PREC> struct VelT { using T = double; };
 template <> struct VelT<PREC_MIXED> { using T = float; };
+
+// stage staged-cell cc of direction D's line set: density and drift velocity
+template <int DIM, int PREC, int D>
+__device__ __forceinline__ void stage_cell(const TransportArgs& a, int cc, int s, const int* org, double* sU,
+                                           typename VelT<PREC>::T* sV)
+{
+    using G = TileGeom<DIM>;
+    using VT = typename VelT<PREC>::T;
+    constexpr int E0 = G::template SE<D>(0), E1 = G::template SE<D>(1);
+    int l[3];
+    l[0] = cc % E0;
+    l[1] = (cc / E0) % E1;
+    l[2] = cc / (E0 * E1);
+    int g[3] = {org[0] + l[0], org[1] + l[1], org[2] + l[2]};
+    g[D] -= 3;
+    bool ok = (g[D] >= a.lo[D] - a.ghost) && (g[D] <= a.hi[D] + a.ghost);
+#pragma unroll
+    for (int e = 0; e < DIM; e++)
+        if (e != D) ok = ok && (g[e] <= a.hi[e]);
+    double u = 0.0;
+    VT v = VT(0);
+    if (ok) {
+        const int ns = a.ns;
+        const int64_t cs = a.sb.ns;
+        const double* p = a.sb.p + a.sb.off(g[0], g[1], g[2]);
+        u = p[s * cs];
+        if (a.udv) {
+            v = (s == a.vel_sp) ? VT(a.uvel[D]) : VT(0);
+        } else {
+            const double Te = p[VD_ETEMP(ns) * cs];
+            const double E = p[(VD_EFX(ns) + D) * cs];
+            const double N = a.Nv(g[0], g[1], g[2]);
+            if constexpr (PREC == PREC_FP64) v = mob_fp64(s, Te, N, a.Tg) * E;
+            else v = mob_f32(s, (float)Te, (float)N, (float)a.Tg) * (float)E;
+        }
+    }
+    sU[cc] = u;
+    sV[cc] = v;
+}
+
+// flux of face ff of direction D from the staged lines
+template <int DIM, int PREC, int D>
+__device__ __forceinline__ double face_of(const TransportArgs& a, int ff, int cls, const int* org, const double* sU,
+                                          const typename VelT<PREC>::T* sV)
+{
+    using G = TileGeom<DIM>;
+    using VT = typename VelT<PREC>::T;
+    constexpr int F0 = G::template FE<D>(0), F1 = G::template FE<D>(1);
+    constexpr int S0 = G::template SE<D>(0), S1 = G::template SE<D>(1);
+    constexpr int STR = (D == 0) ? 1 : ((D == 1) ? S0 : S0 * S1);
+    int l[3];
+    l[0] = ff % F0;
+    l[1] = (ff / F0) % F1;
+    l[2] = ff / (F0 * F1);
+    int g[3] = {org[0] + l[0], org[1] + l[1], org[2] + l[2]};
+    bool ok = g[D] <= a.hi[D] + 1;
+#pragma unroll
+    for (int e = 0; e < DIM; e++)
+        if (e != D) ok = ok && (g[e] <= a.hi[e]);
+    if (!ok) return 0.0;
+    // staged index of rel cell (f_d - 3 + q) is f_d + q along d
+    const int base = l[0] + S0 * (l[1] + S1 * l[2]);
+    double u[6];
+    VT v[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        u[q] = sU[base + q * STR];
+        v[q] = sV[base + q * STR];
+    }
+    double F;
+    if constexpr (PREC == PREC_FP64) F = face_flux_fp64(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
+    else F = face_flux_mixed(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
+    if (g[D] == a.domlo[D] && a.zlo[cls][D]) F = 0.0;
+    if (g[D] == a.domhi[D] + 1 && a.zhi[cls][D]) F = 0.0;
+    return F;
+}
 
 template <int DIM, int PREC>
 __global__ void __launch_bounds__(Tile<DIM>::NTH) k_transport(const __grid_constant__ TransportArgs a)
@@ -438,9 +546,10 @@ __global__ void __launch_bounds__(Tile<DIM>::NTH) k_transport(const __grid_const
     using G = TileGeom<DIM>;
     using VT = typename VelT<PREC>::T;
     constexpr int NTH = Tile<DIM>::NTH;
-    __shared__ double sU[G::SMAX];
-    __shared__ VT sV[G::SMAX];
-    __shared__ double sF[G::FMAX];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sU = reinterpret_cast<double*>(smem_raw);
+    double* sF = sU + G::STOT;
+    VT* sV = reinterpret_cast<VT*>(sF + G::FTOT);
 
     const int tid = threadIdx.x;
     int tb = blockIdx.x;
@@ -448,10 +557,10 @@ __global__ void __launch_bounds__(Tile<DIM>::NTH) k_transport(const __grid_const
     tb /= a.ntile[0];
     const int tiy = tb % a.ntile[1];
     const int tiz = tb / a.ntile[1];
-    const int org[3] = {a.lo[0] + tix * G::TX, a.lo[1] + tiy * G::TY, a.lo[2] + tiz * G::TZ};
+    const int org[3] = {a.lo[0] + tix * G::T[0], a.lo[1] + tiy * G::T[1], a.lo[2] + tiz * G::T[2]};
 
     // own cell
-    const int cx = tid % G::TX, cy = (tid / G::TX) % G::TY, cz = tid / (G::TX * G::TY);
+    const int cx = tid % G::T[0], cy = (tid / G::T[0]) % G::T[1], cz = tid / (G::T[0] * G::T[1]);
     const int gi = org[0] + cx, gj = org[1] + cy, gk = org[2] + cz;
     const bool own = (tid < G::NCELL) && gi <= a.hi[0] && gj <= a.hi[1] && gk <= a.hi[2];
     const int ns = a.ns;
@@ -459,95 +568,45 @@ __global__ void __launch_bounds__(Tile<DIM>::NTH) k_transport(const __grid_const
     const int64_t own_o = own ? a.sb.off(gi, gj, gk) : 0;
 
     double ne_new = 0.0, een_new = 0.0;
-    const int H = a.ghost;
-
     for (int it = 0; it < a.ntr; it++) {
         const int s = a.tr_sp[it];
         const int cls = a.tr_cls[it];
         double acc = own ? a.rxn(gi, gj, gk, s) : 0.0;
         if (a.tr_flux[it]) {
-            for (int d = 0; d < DIM; d++) {
-                // ---- stage the d-lines of the tile: cells rel -3 .. T_d+2 along d
-                int SE[3] = {G::TX, G::TY, G::TZ};
-                SE[d] += 6;
-                const int nst = SE[0] * SE[1] * SE[2];
-                for (int c = tid; c < nst; c += NTH) {
-                    int l[3];
-                    l[0] = c % SE[0];
-                    l[1] = (c / SE[0]) % SE[1];
-                    l[2] = c / (SE[0] * SE[1]);
-                    int g[3] = {org[0] + l[0], org[1] + l[1], org[2] + l[2]};
-                    g[d] -= 3;
-                    bool ok = (g[d] >= a.lo[d] - H) && (g[d] <= a.hi[d] + H);
-#pragma unroll
-                    for (int e = 0; e < DIM; e++)
-                        if (e != d) ok = ok && (g[e] <= a.hi[e]);
-                    double u = 0.0;
-                    VT v = VT(0);
-                    if (ok) {
-                        const int64_t o = a.sb.off(g[0], g[1], g[2]);
-                        u = a.sb.p[o + s * cs];
-                        if (a.udv) {
-                            v = (s == a.vel_sp) ? VT(a.uvel[d]) : VT(0);
-                        } else {
-                            double Te = a.sb.p[o + VD_ETEMP(ns) * cs];
-                            double E = a.sb.p[o + (VD_EFX(ns) + d) * cs];
-                            double N = a.Nv(g[0], g[1], g[2]);
-                            if (PREC == PREC_FP64) v = (VT)(mob_fp64(s, Te, N, a.Tg) * E);
-                            else v = (VT)(mob_f32(s, (float)Te, (float)N, (float)a.Tg) * (float)E);
-                        }
-                    }
-                    sU[c] = u;
-                    sV[c] = v;
+            for (int c = tid; c < G::STOT; c += NTH) {
+                if (c < G::SOFF1) stage_cell<DIM, PREC, 0>(a, c, s, org, sU, sV);
+                else if (DIM > 1 && c < G::SOFF2)
+                    stage_cell<DIM, PREC, (DIM > 1 ? 1 : 0)>(a, c - G::SOFF1, s, org, sU + G::SOFF1, sV + G::SOFF1);
+                else if (DIM > 2)
+                    stage_cell<DIM, PREC, (DIM > 2 ? 2 : 0)>(a, c - G::SOFF2, s, org, sU + G::SOFF2, sV + G::SOFF2);
+            }
+            __syncthreads();
+            for (int f = tid; f < G::FTOT; f += NTH) {
+                double F;
+                if (f < G::FOFF1) F = face_of<DIM, PREC, 0>(a, f, cls, org, sU, sV);
+                else if (DIM > 1 && f < G::FOFF2)
+                    F = face_of<DIM, PREC, (DIM > 1 ? 1 : 0)>(a, f - G::FOFF1, cls, org, sU + G::SOFF1, sV + G::SOFF1);
+                else
+                    F = face_of<DIM, PREC, (DIM > 2 ? 2 : 0)>(a, f - G::FOFF2, cls, org, sU + G::SOFF2, sV + G::SOFF2);
+                sF[f] = F;
+            }
+            __syncthreads();
+            if (own) {
+                // dsdt = (Fx_lo - Fx_hi)/dx + rxn, then += y and z terms (ScalarSolve.cpp:45-51)
+                {
+                    constexpr int F0 = G::template FE<0>(0), F1 = G::template FE<0>(1);
+                    const int lo_f = cx + F0 * (cy + F1 * cz);
+                    acc = (sF[lo_f] - sF[lo_f + 1]) * a.idx[0] + acc;
                 }
-                __syncthreads();
-                // ---- faces: f_d in [0, T_d], between rel cells f_d-1 and f_d
-                int FE[3] = {G::TX, G::TY, G::TZ};
-                FE[d] += 1;
-                const int nf = FE[0] * FE[1] * FE[2];
-                for (int f = tid; f < nf; f += NTH) {
-                    int l[3];
-                    l[0] = f % FE[0];
-                    l[1] = (f / FE[0]) % FE[1];
-                    l[2] = f / (FE[0] * FE[1]);
-                    int g[3] = {org[0] + l[0], org[1] + l[1], org[2] + l[2]};
-                    bool ok = g[d] <= a.hi[d] + 1;
-#pragma unroll
-                    for (int e = 0; e < DIM; e++)
-                        if (e != d) ok = ok && (g[e] <= a.hi[e]);
-                    double F = 0.0;
-                    if (ok) {
-                        // staged index of rel cell (f_d - 3 + q) is f_d + q
-                        int base;
-                        int strd;
-                        if (d == 0) { base = l[0] + SE[0] * (l[1] + SE[1] * l[2]); strd = 1; }
-                        else if (d == 1) { base = l[0] + SE[0] * (l[1] + SE[1] * l[2]); strd = SE[0]; }
-                        else { base = l[0] + SE[0] * (l[1] + SE[1] * l[2]); strd = SE[0] * SE[1]; }
-                        double u[6];
-                        VT v[6];
-#pragma unroll
-                        for (int q = 0; q < 6; q++) {
-                            u[q] = sU[base + q * strd];
-                            v[q] = sV[base + q * strd];
-                        }
-                        if (PREC == PREC_FP64) {
-                            F = face_flux_fp64(u, (const double*)v, a.hyp_order, a.weno, a.dxmin, a.dt);
-                        } else {
-                            F = face_flux_mixed(u, (const float*)v, a.hyp_order, a.weno, a.dxmin, a.dt);
-                        }
-                        if (g[d] == a.domlo[d] && a.zlo[cls][d]) F = 0.0;
-                        if (g[d] == a.domhi[d] + 1 && a.zhi[cls][d]) F = 0.0;
-                    }
-                    sF[f] = F;
+                if constexpr (DIM > 1) {
+                    constexpr int F0 = G::template FE<1>(0), F1 = G::template FE<1>(1);
+                    const int lo_f = G::FOFF1 + cx + F0 * (cy + F1 * cz);
+                    acc += (sF[lo_f] - sF[lo_f + F0]) * a.idx[1];
                 }
-                __syncthreads();
-                if (own) {
-                    int lo_f, hi_f;
-                    if (d == 0) { lo_f = cx + FE[0] * (cy + FE[1] * cz); hi_f = lo_f + 1; }
-                    else if (d == 1) { lo_f = cx + FE[0] * (cy + FE[1] * cz); hi_f = lo_f + FE[0]; }
-                    else { lo_f = cx + FE[0] * (cy + FE[1] * cz); hi_f = lo_f + FE[0] * FE[1]; }
-                    double term = (sF[lo_f] - sF[hi_f]) / a.dx[d];
-                    acc = (d == 0) ? term + acc : acc + term;
+                if constexpr (DIM > 2) {
+                    constexpr int F0 = G::template FE<2>(0), F1 = G::template FE<2>(1);
+                    const int lo_f = G::FOFF2 + cx + F0 * (cy + F1 * cz);
+                    acc += (sF[lo_f] - sF[lo_f + F0 * F1]) * a.idx[2];
                 }
             }
         }
@@ -593,9 +652,21 @@ __global__ void __launch_bounds__(Tile<DIM>::NTH) k_transport(const __grid_const
 template <int DIM, int PREC>
 static cudaError_t launch_tr(const TransportArgs& a, cudaStream_t st)
 {
+    using G = TileGeom<DIM>;
+    using VT = typename VelT<PREC>::T;
+    constexpr size_t smem = (size_t)G::STOT * (sizeof(double) + sizeof(VT)) + (size_t)G::FTOT * sizeof(double);
+    static unsigned attr_set = 0;  // one bit per device
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(attr_set & (1u << (dev & 31)))) {
+        cudaError_t e = cudaFuncSetAttribute(k_transport<DIM, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_set |= 1u << (dev & 31);
+    }
     unsigned nt = (unsigned)a.ntile[0] * a.ntile[1] * a.ntile[2];
     ProfScope ps("k_transport", st);
-    k_transport<DIM, PREC><<<nt, Tile<DIM>::NTH, 0, st>>>(a);
+    k_transport<DIM, PREC><<<nt, Tile<DIM>::NTH, smem, st>>>(a);
     return cudaGetLastError();
 }
 

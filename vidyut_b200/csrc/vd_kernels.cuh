@@ -19,7 +19,7 @@ struct TransportArgs {
     A4 ef[3], gne[3];
     int lo[3], hi[3];
     int ntile[3];
-    double dx[3], dt, Tg, dxmin;
+    double dx[3], idx[3], dt, Tg, dxmin;
     int domlo[3], domhi[3];
     int8_t zlo[4][3], zhi[4][3];  // 1: IHNEUBC zero flux on that domain face, per class
     int ntr, nbg;
@@ -45,7 +45,7 @@ struct PrepArgs {
 
 int upload_mech(const VdMechDev* h, cudaStream_t st);
 
-cudaError_t launch_reaction_source(const BoxIdx& b, const A4& sb, const A4& rxn, double Tg, int prec,
+cudaError_t launch_reaction_source(const BoxIdx& b, const A4& sb, const A4& rxn, double Tg, int prec, int ns,
                                    cudaStream_t st);
 cudaError_t launch_face_flux(const BoxIdx& fb, int dir, int specid, const A4& phi, const A4& fx,
                              const int8_t zlo[3], const int8_t zhi[3], const int domlo[3], const int domhi[3],
@@ -55,7 +55,7 @@ cudaError_t launch_dsdt(const BoxIdx& b, int dim, int specid, const A4 flux[3], 
                         const double dx[3], cudaStream_t st);
 cudaError_t launch_joule(const BoxIdx& b, int dim, const A4& sb, const A4& rxn, const A4 ef[3], const A4 gne[3],
                          const A4& dsdt, const A4& pn, const TransportArgs& cfg, cudaStream_t st);
-cudaError_t launch_prep(const PrepArgs& a, int prec, cudaStream_t st);
+cudaError_t launch_prep(const PrepArgs& a, int prec, int ns, cudaStream_t st);
 cudaError_t launch_transport(const TransportArgs& a, int dim, int prec, cudaStream_t st);
 cudaError_t launch_checksums(const BoxIdx& b, const A4& rxn, const A4& pn, double* out, cudaStream_t st);
 

@@ -140,13 +140,44 @@ def _coords(n, dx, g, dim):
     return out
 
 
+def smooth_uniform_field(rng, n, dim: int, n_modes: int = 12, kmax: int = 2) -> np.ndarray:
+    """Spatially correlated field with a uniform [0, 1) marginal: a sum of n_modes
+    random cosines (at most kmax periods across the box), normalised to unit
+    variance and mapped through the normal CDF.  Shape (nz, ny, nx)."""
+    from math import erf, sqrt
+    axes = [(np.arange(n[d]) + 0.5) / n[d] if d < dim else np.zeros(1) for d in range(3)]
+    g = np.zeros((len(axes[2]), len(axes[1]), len(axes[0])))
+    var = 0.0
+    for _ in range(n_modes):
+        k = [int(rng.integers(-kmax, kmax + 1)) if d < dim else 0 for d in range(3)]
+        if not any(k):
+            k[0] = 1
+        a = rng.normal()
+        ph = rng.uniform(0.0, 2.0 * np.pi)
+        # separable evaluation: cos(A+B+C+ph) through complex exponentials
+        ex = np.exp(2j * np.pi * k[0] * axes[0])
+        ey = np.exp(2j * np.pi * k[1] * axes[1])
+        ez = np.exp(2j * np.pi * k[2] * axes[2])
+        g += a * np.real(np.exp(1j * ph) * ez[:, None, None] * ey[None, :, None] * ex[None, None, :])
+        var += 0.5 * a * a
+    g /= np.sqrt(max(var, 1e-30))
+    try:
+        from scipy.special import ndtr
+        u = ndtr(g)
+    except ImportError:  # pragma: no cover
+        u = 0.5 * (1.0 + np.vectorize(erf, otypes=[float])(g / sqrt(2.0)))
+    return np.clip(u, 0.0, 1.0 - 1e-15)
+
+
 def build_case(mech: Mechanism, dim: int, n, dx, seed: int, *, density="loguniform",
                dens_range=(1e8, 1e22), blob_peak_exp=(14.0, 18.0), floor=1e10, bg_density=2.4e25,
                te_range_ev=(0.5, 5.0), voltage=1000.0, noise=0.05, ghost=3, periodic=(0, 0, 0),
                params: dict | None = None) -> BoxCase:
-    """Seeded box: species densities (``loguniform`` per cell and species, or the
-    ``blob`` of the 2-D argon config: a Gaussian electron blob with ions matching
-    and the other species at the floor), background species at ``bg_density``,
+    """Seeded box: species densities (``loguniform``: independent per cell and
+    species; ``loguniform_smooth``: the same log-uniform marginal but spatially
+    correlated over about half the box; ``blob``: the 2-D argon config's
+    Gaussian electron blob with ions matching and the other species at the
+    floor), background species at ``bg_density``,
     per-cell Te uniform in te_range_ev, potential phi = V x/L (1 + noise*xi) with
     xi uniform in [-1, 1]."""
     n = tuple(int(v) for v in n) + (1,) * (3 - len(n))
@@ -181,6 +212,13 @@ def build_case(mech: Mechanism, dim: int, n, dx, seed: int, *, density="logunifo
                 st[(s,) + inner] = ne
             else:
                 st[(s,) + inner] = floor
+    elif density == "loguniform_smooth":
+        lo, hi = np.log10(dens_range[0]), np.log10(dens_range[1])
+        for s in range(ns):
+            if s in bg:
+                st[(s,) + inner] = bg_density
+            else:
+                st[(s,) + inner] = 10.0 ** (lo + (hi - lo) * smooth_uniform_field(rng, n, dim))
     else:
         lo, hi = np.log10(dens_range[0]), np.log10(dens_range[1])
         for s in range(ns):
@@ -260,8 +298,9 @@ def config_argon2d(seed: int = BASE_SEED, n=(256, 256), n_reactions: int = 10) -
 def config_precision3d(seed: int = BASE_SEED, n=(128, 128, 128), n_species: int = 24,
                        n_reactions: int = 150) -> BoxCase:
     """3-D single box: 24 species / 150 reactions, densities log-uniform 1e8-1e22
-    (background gas 2.4e25), Te 0.3-10 eV, potential ramp + noise; one step."""
+    (spatially correlated; background gas 2.4e25), Te 0.3-10 eV per cell,
+    potential ramp + noise; one step."""
     mech = synthetic(n_species, n_reactions, seed + 11)
-    return build_case(mech, 3, n, (1e-5, 1e-5, 1e-5), seed + 12, density="loguniform",
+    return build_case(mech, 3, n, (1e-5, 1e-5, 1e-5), seed + 12, density="loguniform_smooth",
                       dens_range=(1e8, 1e22), te_range_ev=(0.3, 10.0), voltage=1000.0,
                       params=dict(dt=1e-12))
