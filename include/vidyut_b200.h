@@ -241,7 +241,7 @@ int vd_explicit_update_all(const vd_box* bx, vd_array4 sborder,
                            vd_array4 phi_new, vd_array4 dsdt, vd_array4 rxn,
                            const vd_params* prm, void* stream);
 
-/* Per-box FP64 checksums of an update (conservation checks, north_star):
+/* Per-box FP64 checksums of an update (conservation checks; no reference counterpart):
  * out[0] = sum over cells of sum_s charge_s * rxn_s   (charge production; 0 up to rounding)
  * out[1] = sum over cells of sum_s |charge_s * rxn_s| (scale for out[0])
  * out[2] = sum over cells of rxn(NS)                  (energy exchange)
