@@ -241,6 +241,28 @@ int vd_explicit_update_all(const vd_box* bx, vd_array4 sborder,
                            vd_array4 phi_new, vd_array4 dsdt, vd_array4 rxn,
                            const vd_params* prm, void* stream);
 
+/* Allocation-free form of vd_explicit_update_all (no counterpart in the reference).
+ * For hosts that cannot let a library allocate device memory during a step: an
+ * AMReX application normally hands most of the GPU to its own memory arena at
+ * start-up, and some callers forbid any allocation inside their time-step loop.
+ * Same arguments, work and results as vd_explicit_update_all, but the per-call
+ * scratch (per-cell density sums on the stencil-grown box, plus the reaction
+ * source when rxn.p is NULL) comes from one fixed array compiled into the library:
+ * VD_NOALLOC_SCRATCH_BYTES on every GPU that loads the library, held until the
+ * process exits.  A box whose scratch would not fit is rejected with
+ * VD_ERR_NOMEM before anything is launched (pass rxn to need less scratch).
+ * The first call on a device does that device's set-up (it looks up the array's
+ * device address and, if needed, uploads the mechanism table, which synchronises
+ * the stream); make that first call before any stream capture.  All calls share
+ * the one array: calls that overlap on the GPU (different streams, or another
+ * host thread) race on it, so order them on one stream.  Nothing in the array
+ * needs clearing between calls: each call writes every scratch value it reads. */
+#define VD_NOALLOC_SCRATCH_BYTES (64u << 20)
+int vd_explicit_update_all_noalloc(const vd_box* bx, vd_array4 sborder,
+                                   const vd_array4 efield_ec[3], const vd_array4 gradne_fc[3],
+                                   vd_array4 phi_new, vd_array4 dsdt, vd_array4 rxn,
+                                   const vd_params* prm, void* stream);
+
 /* Per-box FP64 checksums of an update (conservation checks; no reference counterpart):
  * out[0] = sum over cells of sum_s charge_s * rxn_s   (charge production; 0 up to rounding)
  * out[1] = sum over cells of sum_s |charge_s * rxn_s| (scale for out[0])

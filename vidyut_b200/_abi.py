@@ -28,6 +28,7 @@ RXN_NONE, RXN_EXCITATION, RXN_IONIZATION, RXN_RECOMB, RXN_ELASTIC = 0, 1, 2, 3, 
 MOB_ZERO, MOB_ELECTRON, MOB_ION_TG, MOB_SCALED, MOB_CONST_N, MOB_CONST = 0, 1, 2, 3, 4, 5
 DIFF_ZERO, DIFF_TE_ABSMOB, DIFF_TG_MOB = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
+NOALLOC_SCRATCH_BYTES = 64 << 20
 
 
 def EEN(ns): return ns
@@ -112,6 +113,7 @@ PROTOTYPES = {
     "vd_elecenergy_source": (C.c_int, [BOXP, A4, A4, A4P, A4P, A4, A4, PRMP, C.c_void_p]),
     "vd_explicit_update_all": (C.c_int, [BOXP, A4, A4P, A4P, A4, A4, A4, PRMP, C.c_void_p]),
     "vd_box_checksums": (C.c_int, [BOXP, A4, A4, C.c_void_p, C.c_void_p]),
+    "vd_explicit_update_all_noalloc": (C.c_int, [BOXP, A4, A4P, A4P, A4, A4, A4, PRMP, C.c_void_p]),
     "vd_launch_count": (C.c_int64, []),
     "vd_profile_enable": (C.c_int, [C.c_int]),
     "vd_profile_read": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_double), C.c_int]),

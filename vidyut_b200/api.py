@@ -149,3 +149,19 @@ def box_checksums(dc: DeviceCase, rxn: torch.Tensor, phi_new: torch.Tensor, stre
                             _stream(stream))
     abi.check(rc, "vd_box_checksums")
     return out.cpu().numpy()
+
+
+def explicit_update_all_noalloc(dc: DeviceCase, prm: abi.VdParams, phi_new: torch.Tensor,
+                                dsdt: torch.Tensor | None = None, rxn: torch.Tensor | None = None,
+                                stream=None) -> None:
+    """explicit_update_all for callers that must not have the library allocate
+    device memory during a step (for example a host whose memory arena owns the
+    GPU): its scratch comes from a fixed VD_NOALLOC_SCRATCH_BYTES array in the
+    library.  Boxes whose scratch would not fit raise VidyutError(ERR_NOMEM)."""
+    L = abi.lib()
+    rc = L.vd_explicit_update_all_noalloc(C.byref(dc.box()), dc.sb(), dc.face_a4s("efield"),
+                                          dc.face_a4s("gradne"), t_a4(phi_new, (0, 0, 0)),
+                                          t_a4(dsdt, (0, 0, 0)) if dsdt is not None else abi.null_array4(),
+                                          t_a4(rxn, (0, 0, 0)) if rxn is not None else abi.null_array4(),
+                                          C.byref(prm), _stream(stream))
+    abi.check(rc, "vd_explicit_update_all_noalloc")

@@ -651,3 +651,174 @@ int vd_box_checksums(const vd_box* bx, vd_array4 rxn, vd_array4 phi_new, double*
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free explicit update.
+//
+// Some hosts cannot let this library allocate device memory while they step: an
+// AMReX application usually gives most of the GPU to its own arena when it
+// starts, and some callers allow no allocation inside the time-step loop at all.
+// For them the scratch of the fused update lives in this fixed array instead of
+// coming from the stream-ordered allocator.  Every GPU that loads the library
+// holds the array until the process exits.  In host code the name below is only a
+// host-side stand-in, so its device address is looked up once per device (with
+// that device current) and passed to the kernels.
+namespace {
+
+constexpr size_t kNoallocDoubles = VD_NOALLOC_SCRATCH_BYTES / sizeof(double);
+static __device__ __align__(256) double g_noalloc_scratch[kNoallocDoubles];
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[64] = {nullptr};  // device address of the array, per device
+
+// Once per device: find the array's device address.
+int noalloc_scratch_for_current_device(double** out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if (dev < 0 || dev >= 64) return fail(VD_ERR_ARG, "device ordinal %d not supported", dev);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
+        g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return VD_OK;
+}
+
+}  // namespace
+
+extern "C" int vd_explicit_update_all_noalloc(const vd_box* bx, vd_array4 sborder, const vd_array4 efield_ec[3],
+                                              const vd_array4 gradne_fc[3], vd_array4 phi_new, vd_array4 dsdt,
+                                              vd_array4 rxn, const vd_params* prm, void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = ensure_mech_on_device(st);
+    if (rc) return rc;
+    double* scratch = nullptr;
+    if ((rc = noalloc_scratch_for_current_device(&scratch))) return rc;
+    if ((rc = check_params(bx, prm))) return rc;
+    vd_mech* m;
+    {
+        std::lock_guard<std::mutex> lk(g_mech_mu);
+        m = g_mech;
+    }
+    const int ns = m->nspecies, dim = bx->dim;
+    const int H = stencil_halo(prm->hyp_order);
+    std::string why;
+    int glo[3] = {bx->lo[0], bx->lo[1], bx->lo[2]}, ghi[3] = {bx->hi[0], bx->hi[1], bx->hi[2]};
+    for (int d = 0; d < dim; d++) {
+        glo[d] -= H;
+        ghi[d] += H;
+    }
+    if (!covers(sborder, glo, ghi, VD_NVAR(ns), &why)) return fail(VD_ERR_GHOST, "sborder: %s", why.c_str());
+    if (!covers(phi_new, bx->lo, bx->hi, VD_NVAR(ns), &why)) return fail(VD_ERR_ARG, "phi_new: %s", why.c_str());
+    if (dsdt.p && !covers(dsdt, bx->lo, bx->hi, ns + 1, &why)) return fail(VD_ERR_ARG, "dsdt: %s", why.c_str());
+    if (rxn.p && !covers(rxn, bx->lo, bx->hi, ns + 1, &why)) return fail(VD_ERR_ARG, "rxn: %s", why.c_str());
+    if (prm->bg_mask >> ns) return fail(VD_ERR_ARG, "bg_mask names species >= %d", ns);
+    if (prm->bg_mask & (1ull << m->e_id)) return fail(VD_ERR_ARG, "electrons cannot be a background species");
+    if (prm->user_defined_vel && (prm->vel_species < 0 || prm->vel_species > ns))
+        return fail(VD_ERR_ARG, "vel_species invalid");
+    A4 ef[3], gne[3];
+    if (prm->elecenergy_solve) {
+        for (int d = 0; d < dim; d++) {
+            int fhi[3] = {bx->hi[0], bx->hi[1], bx->hi[2]};
+            fhi[d] += 1;
+            if (!prm->cs_technique) {
+                if (!efield_ec || !covers(efield_ec[d], bx->lo, fhi, 1, &why))
+                    return fail(VD_ERR_ARG, "efield_ec[%d]: %s", d, why.c_str());
+                ef[d] = A4(efield_ec[d]);
+            }
+            if (!prm->gradne_from_state) {
+                if (!gradne_fc || !covers(gradne_fc[d], bx->lo, fhi, 1, &why))
+                    return fail(VD_ERR_ARG, "gradne_fc[%d]: %s", d, why.c_str());
+                gne[d] = A4(gradne_fc[d]);
+            }
+        }
+    }
+    // scratch need, checked against the fixed array before anything is launched
+    const int64_t gn = (int64_t)(ghi[0] - glo[0] + 1) * (ghi[1] - glo[1] + 1) * (ghi[2] - glo[2] + 1);
+    const int64_t vn =
+        (int64_t)(bx->hi[0] - bx->lo[0] + 1) * (bx->hi[1] - bx->lo[1] + 1) * (bx->hi[2] - bx->lo[2] + 1);
+    const int64_t need = gn + (rxn.p ? 0 : vn * (ns + 1));
+    if (need > (int64_t)kNoallocDoubles)
+        return fail(VD_ERR_NOMEM,
+                    "box needs %lld bytes of scratch; the allocation-free update has %zu bytes "
+                    "(pass a rxn array to need %lld bytes, or use vd_explicit_update_all)",
+                    (long long)(need * 8), (size_t)VD_NOALLOC_SCRATCH_BYTES, (long long)(gn * 8));
+
+    TransportArgs a;
+    fill_cfg(a, bx, prm, m);
+    int tile[3];
+    transport_tile(dim, tile);
+    for (int d = 0; d < 3; d++) {
+        int n = bx->hi[d] - bx->lo[d] + 1;
+        a.ntile[d] = (n + tile[d] - 1) / tile[d];
+    }
+    a.sb = A4(sborder);
+    a.pn = A4(phi_new);
+    a.dsdt = dsdt.p ? A4(dsdt) : A4();
+    for (int d = 0; d < 3; d++) {
+        a.ef[d] = ef[d];
+        a.gne[d] = gne[d];
+    }
+    a.ntr = 0;
+    a.nbg = 0;
+    for (int s = 0; s <= ns; s++) {
+        bool energy = (s == ns);
+        if (energy && !prm->elecenergy_solve) continue;
+        if (!energy && ((prm->bg_mask >> s) & 1ull)) {
+            a.bg_sp[a.nbg++] = (int8_t)s;
+            continue;
+        }
+        a.tr_sp[a.ntr] = (int8_t)s;
+        a.tr_cls[a.ntr] = (int8_t)species_class(m, s);
+        bool has_vel = prm->user_defined_vel ? (s == prm->vel_species) : (m->mob_kind[s] != VD_MOB_ZERO);
+        a.tr_flux[a.ntr] = (prm->do_transport && has_vel) ? 1 : 0;
+        a.ntr++;
+    }
+    A4 Nv;
+    Nv.p = scratch;
+    Nv.bx = glo[0];
+    Nv.by = glo[1];
+    Nv.bz = glo[2];
+    Nv.js = ghi[0] - glo[0] + 1;
+    Nv.ks = Nv.js * (ghi[1] - glo[1] + 1);
+    Nv.ns = Nv.ks * (ghi[2] - glo[2] + 1);
+    Nv.ncomp = 1;
+    A4 R;
+    if (rxn.p) {
+        R = A4(rxn);
+    } else {
+        R.p = scratch + gn;
+        R.bx = bx->lo[0];
+        R.by = bx->lo[1];
+        R.bz = bx->lo[2];
+        R.js = bx->hi[0] - bx->lo[0] + 1;
+        R.ks = R.js * (bx->hi[1] - bx->lo[1] + 1);
+        R.ns = R.ks * (bx->hi[2] - bx->lo[2] + 1);
+        R.ncomp = ns + 1;
+    }
+    a.Nv = Nv;
+    a.rxn = R;
+    PrepArgs pa;
+    pa.sb = a.sb;
+    pa.rxn = R;
+    pa.Nv = Nv;
+    for (int d = 0; d < 3; d++) {
+        pa.glo[d] = glo[d];
+        pa.ghi[d] = ghi[d];
+        pa.lo[d] = bx->lo[d];
+        pa.hi[d] = bx->hi[d];
+    }
+    pa.Tg = prm->Tg;
+    pa.do_reactions = prm->do_reactions;
+    pa.write_n = 1;
+    cudaError_t e = launch_prep(pa, prm->precision, ns, st);
+    if (e == cudaSuccess) e = launch_transport(a, dim, prm->precision, st);
+    if (e != cudaSuccess) return cuda_fail(e, "allocation-free update launch");
+    return VD_OK;
+}
