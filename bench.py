@@ -83,7 +83,8 @@ def algorithmic_bytes_per_cell(case) -> dict:
     ns, d = case.mech.ns, case.dim
     reads = ns + 2 + d + 2 * d
     writes = ns + 1
-    return {"step": 8 * (reads + writes), "k_transport": 8 * (reads + writes), "k_prep": 8 * (ns + 1)}
+    return {"step": 8 * (reads + writes), "k_transport": 8 * (reads + writes), "k_prep": 8 * (ns + 1),
+            "k_prep_spec": 8 * (ns + 1)}
 
 
 # ---------------------------------------------------------------------------

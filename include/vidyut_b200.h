@@ -204,6 +204,27 @@ const char* vd_status_string(int status);
  * it into the binary).  Must be called before any compute entry point.           */
 int vd_mech_init(const vd_mech* m);
 
+/* Mechanism-specialised chemistry (no reference counterpart; the reference gets
+ * the same effect by compiling Chemistry.H into each case executable).
+ * vd_mech_init also generates CUDA source for the chemistry with the loaded
+ * mechanism folded in and compiles it with NVRTC; vd_mech_specialized() returns 1
+ * when those kernels run, 0 when the table-driven kernels do (NVRTC missing or
+ * failed, or switched off with vd_set_specialize(0) before vd_mech_init);
+ * vd_mech_specialize_status() says why.                                         */
+int         vd_mech_specialized(void);
+const char* vd_mech_specialize_status(void);
+int         vd_set_specialize(int on);
+/* Kernel-variant knobs (no reference counterpart), chosen by the tuner
+ * (vidyut_b200/tune.py) and settable by hand:
+ *   "transport_minblocks_<1|2|3>d_<fp64|mixed>"  1 or 2 resident transport blocks
+ *                                                 per SM (2 caps registers at 64).
+ * vd_tune_get returns the value or a negative status.                            */
+int         vd_tune_set(const char* key, int value);
+int         vd_tune_get(const char* key);
+/* Generates and compiles (without loading; no GPU needed) the specialised kernels
+ * of a mechanism; VD_OK, or VD_ERR_MECH with the compiler log in vd_last_error(). */
+int         vd_mech_specialize_check(const vd_mech* m, size_t* cubin_bytes);
+
 /* Face fluxes of one species in one sweep direction over the face box
  * convert(bx, dir) (Source/ScalarSolve.cpp:208-250).  phi holds NVAR components
  * with at least 1/2/3 ghost cells for hyp_order 1/2/5; fx is the face array.     */

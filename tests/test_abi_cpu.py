@@ -70,3 +70,18 @@ def test_calls_before_mech_init_fail_cleanly(lib):
     z = abi.null_array4()
     rc = lib.vd_reaction_source(C.byref(b), z, z, 300.0, 0.0, 0.0, None)
     assert rc in (abi.ERR_MECH, abi.ERR_CUDA, abi.ERR_ARG)
+
+
+@pytest.mark.parametrize("mech", [mm.argon(10, 20261204), mm.synthetic(8, 40, 20261224),
+                                  mm.synthetic(24, 150, 20261214)], ids=lambda m: m.name)
+def test_specialised_chemistry_compiles_for_sm100a(lib, mech):
+    """vd_mech_init compiles the mechanism-specialised chemistry with NVRTC; the same
+    source must compile here (no GPU needed) without local-memory spills of note."""
+    lib.vd_mech_specialize_check.argtypes = [C.POINTER(abi.VdMech), C.POINTER(C.c_size_t)]
+    cm = mech.to_c()
+    n = C.c_size_t(0)
+    rc = lib.vd_mech_specialize_check(C.byref(cm), C.byref(n))
+    assert rc == abi.OK, lib.vd_last_error().decode()
+    assert n.value > 0
+    log = lib.vd_last_error().decode()
+    assert "vd_spec_prep_fp64" in log and "vd_spec_prep_mixed" in log

@@ -259,3 +259,33 @@ def test_status_codes_without_launch():
     with pytest.raises(abi.VidyutError) as e:
         api.explicit_update_all(dc, case.vd_params(dim=3), phi_new, dsdt, rxn)
     assert e.value.status == abi.ERR_DIM
+
+
+@pytest.mark.parametrize("name", ["synth24_3d_smooth", "argon2d"])
+def test_specialised_and_table_chemistry_agree(name):
+    """vd_mech_init compiles chemistry specialised to the mechanism (NVRTC); the
+    table-driven kernel (vd_set_specialize(0)) must give the same update."""
+    case = CASES[name]
+    L = abi.lib()
+    outs = {}
+    try:
+        for spec in (1, 0):
+            L.vd_set_specialize(spec)
+            api.mech_init(case.mech)
+            assert L.vd_mech_specialized() == spec, L.vd_mech_specialize_status()
+            dc = api.upload(case)
+            for prec in (abi.PREC_FP64, abi.PREC_MIXED):
+                phi_new, dsdt, rxn = dc.new_outputs()
+                api.explicit_update_all(dc, case.vd_params(precision=prec), phi_new, dsdt, rxn)
+                torch.cuda.synchronize()
+                outs[(spec, prec)] = (phi_new.cpu().numpy(), rxn.cpu().numpy())
+    finally:
+        L.vd_set_specialize(1)
+        api.mech_init(case.mech)
+    port = oracle.Port(case.mech)
+    rs, _, nsc = update_scales(port, case, case.vd_params())
+    ns = case.mech.ns
+    for prec, tol in ((abi.PREC_FP64, TOL64), (abi.PREC_MIXED, 1e-6)):
+        a, b = outs[(1, prec)], outs[(0, prec)]
+        assert scaled_err(a[1], b[1], rs) <= tol
+        assert scaled_err(a[0][:ns + 1], b[0][:ns + 1], nsc) <= tol

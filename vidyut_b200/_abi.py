@@ -115,6 +115,10 @@ PROTOTYPES = {
     "vd_box_checksums": (C.c_int, [BOXP, A4, A4, C.c_void_p, C.c_void_p]),
     "vd_explicit_update_all_noalloc": (C.c_int, [BOXP, A4, A4P, A4P, A4, A4, A4, PRMP, C.c_void_p]),
     "vd_launch_count": (C.c_int64, []),
+    "vd_mech_specialized": (C.c_int, []),
+    "vd_mech_specialize_status": (C.c_char_p, []),
+    "vd_set_specialize": (C.c_int, [C.c_int]),
+    "vd_mech_specialize_check": (C.c_int, [C.POINTER(VdMech), C.POINTER(C.c_size_t)]),
     "vd_profile_enable": (C.c_int, [C.c_int]),
     "vd_profile_read": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_double), C.c_int]),
 }
@@ -202,3 +206,9 @@ def make_array4(ptr: int, shape, begin, ncomp: int | None = None) -> VdArray4:
 
 def null_array4() -> VdArray4:
     return VdArray4()
+
+
+PROTOTYPES.update({
+    "vd_tune_set": (C.c_int, [C.c_char_p, C.c_int]),
+    "vd_tune_get": (C.c_int, [C.c_char_p]),
+})

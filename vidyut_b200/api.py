@@ -30,6 +30,8 @@ _loaded_mech = None
 def mech_init(mech: Mechanism) -> None:
     global _loaded_mech
     L = abi.lib()
+    from . import tune
+    tune.apply()
     cm = mech.to_c()
     abi.check(L.vd_mech_init(C.byref(cm)), "vd_mech_init")
     _loaded_mech = mech

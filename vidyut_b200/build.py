@@ -18,7 +18,7 @@ CSRC = PKG / "csrc"
 LIB = PKG / "libvidyut_b200.so"
 BUILD = PKG / "_build"
 
-SOURCES = ["vd_kernels.cu", "vd_abi.cu"]
+SOURCES = ["vd_kernels.cu", "vd_abi.cu", "vd_spec.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC,-O3", "-Xptxas", "-O3"]
@@ -58,7 +58,9 @@ def build(verbose: bool = False, ptxas_info: bool = False, force: bool = False) 
             if r.returncode != 0:
                 raise RuntimeError(f"nvcc failed on {src}")
     if force or _stale(LIB, objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-cudart", "static"]
+        cuda_lib = Path(nvcc()).resolve().parent.parent / "lib64"
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-cudart", "static",
+               f"-L{cuda_lib}", "-lnvrtc", "-Xlinker", f"-rpath,{cuda_lib}"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -32,7 +32,7 @@ int g_mech_gen = 0;
 int fail(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
 int fail(int code, const char* fmt, ...)
 {
-    char buf[512];
+    char buf[4096];
     va_list ap;
     va_start(ap, fmt);
     vsnprintf(buf, sizeof(buf), fmt, ap);
@@ -193,7 +193,8 @@ const char* vd_status_string(int s)
     }
 }
 
-int vd_mech_init(const vd_mech* m)
+// Validates a mechanism table and builds its device image (no device access).
+static int build_mech_table(const vd_mech* m, VdMechDev** out)
 {
     if (!m) return fail(VD_ERR_ARG, "null mechanism");
     const int ns = m->nspecies, nr = m->nreactions;
@@ -279,6 +280,29 @@ int vd_mech_init(const vd_mech* m)
             D.coef[t] = R.term_coef[t];
         }
     }
+    *out = d;
+    return VD_OK;
+}
+
+int vd_mech_specialize_check(const vd_mech* m, size_t* cubin_bytes)
+{
+    VdMechDev* d = nullptr;
+    int rc = build_mech_table(m, &d);
+    if (rc) return rc;
+    size_t n = 0;
+    rc = spec_compile_only(*d, &n);
+    delete d;
+    if (cubin_bytes) *cubin_bytes = n;
+    if (rc) return fail(VD_ERR_MECH, "%s", spec_error());
+    fail(VD_OK, "%s", spec_error());  // the ptxas resource report, for the caller's information
+    return VD_OK;
+}
+
+int vd_mech_init(const vd_mech* m)
+{
+    VdMechDev* d = nullptr;
+    int brc = build_mech_table(m, &d);
+    if (brc) return brc;
     vd_mech* hm = new vd_mech;
     memcpy(hm, m, sizeof(vd_mech));
     {
@@ -290,7 +314,37 @@ int vd_mech_init(const vd_mech* m)
         g_loaded_dev.clear();
         g_mech_gen++;
     }
-    return ensure_mech_on_device(0);
+    int rc = ensure_mech_on_device(0);
+    if (rc) return rc;
+    spec_build(*d);  // table-driven chemistry stays in use if this fails
+    return VD_OK;
+}
+
+int vd_mech_specialized(void) { return spec_active() ? 1 : 0; }
+
+const char* vd_mech_specialize_status(void) { return spec_active() ? "specialised" : spec_error(); }
+
+int vd_set_specialize(int on)
+{
+    spec_set_enabled(on != 0);
+    return VD_OK;
+}
+
+int vd_tune_set(const char* key, int value)
+{
+    if (!key) return fail(VD_ERR_ARG, "null key");
+    int rc = tune_set(key, value);
+    if (rc == -2) return fail(VD_ERR_ARG, "unknown tuning key %s", key);
+    if (rc) return fail(VD_ERR_ARG, "value %d out of range for %s", value, key);
+    return VD_OK;
+}
+
+int vd_tune_get(const char* key)
+{
+    if (!key) return fail(VD_ERR_ARG, "null key");
+    int v = tune_get(key);
+    if (v == -2) return fail(VD_ERR_ARG, "unknown tuning key %s", key);
+    return v;
 }
 
 // ---------------------------------------------------------------------------

@@ -243,6 +243,66 @@ __device__ __forceinline__ double face_flux_mixed(const double* u, const float* 
     return (double)F * (1.0 / s);  // s is a power of two: exact
 }
 
+// Mixed-precision face flux from densities already staged in FP32 (|n| < 3e38).
+// The six values are scaled by an exact power of two s = 2^-e chosen from the
+// exponent bits of max|u| (so max|u*s| is in [1/2, 1)); eps = 1e-20 is carried
+// into the scaled units as 1e-20 s^2, clamped to [1e-30, 1e30] (for tiny fields
+// eps dominates the smoothness indicators and the weights become the ideal ones,
+// as in FP64).  The flux is unscaled exactly in FP64.
+__device__ __forceinline__ double face_flux_mixed32(const float* u, const float* v, int hyp_order, int scheme,
+                                                    double dxmin, double dt)
+{
+    if (hyp_order != 5) {
+        double ud[6], vd[6];
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            ud[q] = (double)u[q];
+            vd[q] = (double)v[q];
+        }
+        return face_flux_fp64(ud, vd, hyp_order, scheme, dxmin, dt);
+    }
+    const float m = fmaxf(fmaxf(fmaxf(fabsf(u[0]), fabsf(u[1])), fmaxf(fabsf(u[2]), fabsf(u[3]))),
+                          fmaxf(fabsf(u[4]), fabsf(u[5])));
+    const int eb = (__float_as_int(m) >> 23) & 0xff;  // biased exponent of max|u|
+    int e = 0;                                        // scale 2^-e; 0 for zero/denormal/non-finite
+    if (eb > 0 && eb < 255) e = eb - 126;             // m in [2^(e-1), 2^e)
+    int bs = 127 - e;
+    bs = bs < 1 ? 1 : (bs > 254 ? 254 : bs);
+    const float s = __int_as_float(bs << 23);
+    int b2 = 127 - 2 * e;
+    b2 = b2 < 0 ? 0 : (b2 > 255 ? 255 : b2);
+    const float s2 = __int_as_float(b2 << 23);        // 2^-2e, 0 or inf at the ends
+    const float eps = fminf(fmaxf(1e-20f * s2, 1e-30f), 1e30f);
+    float us[6], fs[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        us[q] = u[q] * s;
+        fs[q] = us[q] * v[q];
+    }
+    const float lam = fabsf(0.5f * (v[2] + v[3]));
+    const float fp = weno_f32(fs[0], fs[1], fs[2], fs[3], fs[4], scheme, eps);
+    const float fm = weno_f32(fs[5], fs[4], fs[3], fs[2], fs[1], scheme, eps);
+    const float up = weno_f32(us[0], us[1], us[2], us[3], us[4], scheme, eps);
+    const float um = weno_f32(us[5], us[4], us[3], us[2], us[1], scheme, eps);
+    const float F = 0.5f * (fmaf(lam, up, fp) + fmaf(-lam, um, fm));
+    const double inv_s = __longlong_as_double((long long)(1150 - bs) << 52);  // 2^(127-bs): exact
+    return (double)F * inv_s;
+}
+
+// 2^x for an FP64 exponent x as an FP32 value: x = i + f with i = rint(x) (exact in
+// FP64), 2^f for f in [-1/2, 1/2] on the FP32 special-function unit (exp2f, ~2 ulp)
+// and 2^i through the exponent bits.  Relative error ~2.4e-7 whatever |x|;
+// results below 2^-126 flush to zero, above 2^127 saturate to infinity.
+__device__ __forceinline__ float exp2_split(double x)
+{
+    const double xi = rint(x);
+    const float f = exp2f((float)(x - xi));
+    int i = (int)fmax(fmin(xi, 128.0), -127.0);
+    if (i <= -127) return 0.0f;
+    if (i >= 128) return __int_as_float(0x7f800000);
+    return f * __int_as_float((i + 127) << 23);
+}
+
 // ---------------------------------------------------------------------------
 // CKWC for one cell (Source/ScalarSolve.cpp:143-157 + the generated productionRate,
 // test/models/Ar_DC_1d/Chemistry.H:315-506).  The thread's species arrays live in
@@ -289,15 +349,7 @@ __device__ __forceinline__ double chem_cell(double* sc, double* wd, const int st
             if (PREC == PREC_FP64) {
                 k = exp(fma(R.b, lT, R.lnA) - R.C * iT);
             } else {
-                // x = log2 k assembled in FP64; 2^x = 2^round(x) * 2^frac on the FP32 SFU
-                double x = fma(R.b, lT, R.l2A) - R.Cl2 * iT;
-                if (x < -1000.0) {
-                    k = 0.0;
-                } else {
-                    double xi = rint(x);
-                    float ef = exp2f((float)(x - xi));
-                    k = ldexp((double)ef, (int)xi);
-                }
+                k = (double)exp2_split(fma(R.b, lT, R.l2A) - R.Cl2 * iT);
             }
         }
         double prod = sc[R.reac[0] * st];

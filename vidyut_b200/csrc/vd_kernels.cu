@@ -415,6 +415,10 @@ __global__ void __launch_bounds__(128) k_prep(const __grid_constant__ PrepArgs a
 
 cudaError_t launch_prep(const PrepArgs& a, int prec, int ns, cudaStream_t st)
 {
+    {
+        cudaError_t es = spec_launch_prep(a, prec, st);
+        if (es != cudaErrorNotReady) return es;
+    }
     int64_t n = (int64_t)(a.ghi[0] - a.glo[0] + 1) * (a.ghi[1] - a.glo[1] + 1) * (a.ghi[2] - a.glo[2] + 1);
     unsigned g = grid_for(n, 128);
     size_t sm = 0;
@@ -466,8 +470,8 @@ template <> struct VelT<PREC_MIXED> { using T = float; };
 
 // stage staged-cell cc of direction D's line set: density and drift velocity
 template <int DIM, int PREC, int D>
-__device__ __forceinline__ void stage_cell(const TransportArgs& a, int cc, int s, const int* org, double* sU,
-                                           typename VelT<PREC>::T* sV)
+__device__ __forceinline__ void stage_cell(const TransportArgs& a, int cc, int s, const int* org,
+                                           typename VelT<PREC>::T* sU, typename VelT<PREC>::T* sV)
 {
     using G = TileGeom<DIM>;
     using VT = typename VelT<PREC>::T;
@@ -482,13 +486,13 @@ __device__ __forceinline__ void stage_cell(const TransportArgs& a, int cc, int s
 #pragma unroll
     for (int e = 0; e < DIM; e++)
         if (e != D) ok = ok && (g[e] <= a.hi[e]);
-    double u = 0.0;
+    VT u = VT(0);
     VT v = VT(0);
     if (ok) {
         const int ns = a.ns;
         const int64_t cs = a.sb.ns;
         const double* p = a.sb.p + a.sb.off(g[0], g[1], g[2]);
-        u = p[s * cs];
+        u = (VT)p[s * cs];
         if (a.udv) {
             v = (s == a.vel_sp) ? VT(a.uvel[D]) : VT(0);
         } else {
@@ -505,8 +509,8 @@ __device__ __forceinline__ void stage_cell(const TransportArgs& a, int cc, int s
 
 // flux of face ff of direction D from the staged lines
 template <int DIM, int PREC, int D>
-__device__ __forceinline__ double face_of(const TransportArgs& a, int ff, int cls, const int* org, const double* sU,
-                                          const typename VelT<PREC>::T* sV)
+__device__ __forceinline__ double face_of(const TransportArgs& a, int ff, int cls, const int* org,
+                                          const typename VelT<PREC>::T* sU, const typename VelT<PREC>::T* sV)
 {
     using G = TileGeom<DIM>;
     using VT = typename VelT<PREC>::T;
@@ -525,7 +529,7 @@ __device__ __forceinline__ double face_of(const TransportArgs& a, int ff, int cl
     if (!ok) return 0.0;
     // staged index of rel cell (f_d - 3 + q) is f_d + q along d
     const int base = l[0] + S0 * (l[1] + S1 * l[2]);
-    double u[6];
+    VT u[6];
     VT v[6];
 #pragma unroll
     for (int q = 0; q < 6; q++) {
@@ -534,22 +538,22 @@ __device__ __forceinline__ double face_of(const TransportArgs& a, int ff, int cl
     }
     double F;
     if constexpr (PREC == PREC_FP64) F = face_flux_fp64(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
-    else F = face_flux_mixed(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
+    else F = face_flux_mixed32(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
     if (g[D] == a.domlo[D] && a.zlo[cls][D]) F = 0.0;
     if (g[D] == a.domhi[D] + 1 && a.zhi[cls][D]) F = 0.0;
     return F;
 }
 
-template <int DIM, int PREC>
-__global__ void __launch_bounds__(Tile<DIM>::NTH) k_transport(const __grid_constant__ TransportArgs a)
+template <int DIM, int PREC, int MINB>
+__global__ void __launch_bounds__(Tile<DIM>::NTH, MINB) k_transport(const __grid_constant__ TransportArgs a)
 {
     using G = TileGeom<DIM>;
     using VT = typename VelT<PREC>::T;
     constexpr int NTH = Tile<DIM>::NTH;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* sU = reinterpret_cast<double*>(smem_raw);
-    double* sF = sU + G::STOT;
-    VT* sV = reinterpret_cast<VT*>(sF + G::FTOT);
+    double* sF = reinterpret_cast<double*>(smem_raw);
+    VT* sU = reinterpret_cast<VT*>(sF + G::FTOT);  // staged densities (FP32 in the mixed path)
+    VT* sV = sU + G::STOT;                          // staged drift velocities
 
     const int tid = threadIdx.x;
     int tb = blockIdx.x;
@@ -649,37 +653,85 @@ __global__ void __launch_bounds__(Tile<DIM>::NTH) k_transport(const __grid_const
     }
 }
 
-template <int DIM, int PREC>
+template <int DIM, int PREC, int MINB>
 static cudaError_t launch_tr(const TransportArgs& a, cudaStream_t st)
 {
     using G = TileGeom<DIM>;
     using VT = typename VelT<PREC>::T;
-    constexpr size_t smem = (size_t)G::STOT * (sizeof(double) + sizeof(VT)) + (size_t)G::FTOT * sizeof(double);
+    constexpr size_t smem = (size_t)G::STOT * 2 * sizeof(VT) + (size_t)G::FTOT * sizeof(double);
     static unsigned attr_set = 0;  // one bit per device
     int dev = 0;
     cudaGetDevice(&dev);
     if (!(attr_set & (1u << (dev & 31)))) {
-        cudaError_t e = cudaFuncSetAttribute(k_transport<DIM, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(k_transport<DIM, PREC, MINB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr_set |= 1u << (dev & 31);
     }
     unsigned nt = (unsigned)a.ntile[0] * a.ntile[1] * a.ntile[2];
     ProfScope ps("k_transport", st);
-    k_transport<DIM, PREC><<<nt, Tile<DIM>::NTH, smem, st>>>(a);
+    k_transport<DIM, PREC, MINB><<<nt, Tile<DIM>::NTH, smem, st>>>(a);
     return cudaGetLastError();
+}
+
+// Occupancy variant of the transport kernel per (dimension, precision): resident
+// blocks per SM the compiler must fit (registers capped at 64K / (threads * n)).
+// Set by the tuner (vd_tune_set "transport_minblocks_<dim>d_<fp64|mixed>").
+// Defaults measured on B200 (2 beats 1 for every dimension and precision: the
+// kernels are issue/latency bound and gain more from 2x the resident warps than
+// they lose to the few spills of a 64-register cap in 3-D).
+static int g_tr_minb[4][2] = {{2, 2}, {2, 2}, {2, 2}, {2, 2}};
+
+static int tr_minb_max(int dim) { return dim == 3 ? 2 : 4; }  // 512- vs 256-thread blocks
+
+int tune_set(const char* key, int value)
+{
+    for (int d = 1; d <= 3; d++)
+        for (int p = 0; p < 2; p++) {
+            char k[64];
+            snprintf(k, sizeof(k), "transport_minblocks_%dd_%s", d, p ? "mixed" : "fp64");
+            if (strcmp(k, key) == 0) {
+                if (value < 1 || value > tr_minb_max(d)) return -1;
+                g_tr_minb[d][p] = value;
+                return 0;
+            }
+        }
+    return -2;
+}
+
+int tune_get(const char* key)
+{
+    for (int d = 1; d <= 3; d++)
+        for (int p = 0; p < 2; p++) {
+            char k[64];
+            snprintf(k, sizeof(k), "transport_minblocks_%dd_%s", d, p ? "mixed" : "fp64");
+            if (strcmp(k, key) == 0) return g_tr_minb[d][p];
+        }
+    return -2;
+}
+
+template <int DIM, int PREC>
+static cudaError_t launch_tr_v(const TransportArgs& a, cudaStream_t st)
+{
+    const int mb = g_tr_minb[DIM][PREC];
+    if constexpr (DIM < 3) {
+        if (mb == 4) return launch_tr<DIM, PREC, 4>(a, st);
+        if (mb == 3) return launch_tr<DIM, PREC, 3>(a, st);
+    }
+    if (mb == 2) return launch_tr<DIM, PREC, 2>(a, st);
+    return launch_tr<DIM, PREC, 1>(a, st);
 }
 
 cudaError_t launch_transport(const TransportArgs& a, int dim, int prec, cudaStream_t st)
 {
     if (prec == PREC_MIXED) {
-        if (dim == 1) return launch_tr<1, PREC_MIXED>(a, st);
-        if (dim == 2) return launch_tr<2, PREC_MIXED>(a, st);
-        return launch_tr<3, PREC_MIXED>(a, st);
+        if (dim == 1) return launch_tr_v<1, PREC_MIXED>(a, st);
+        if (dim == 2) return launch_tr_v<2, PREC_MIXED>(a, st);
+        return launch_tr_v<3, PREC_MIXED>(a, st);
     }
-    if (dim == 1) return launch_tr<1, PREC_FP64>(a, st);
-    if (dim == 2) return launch_tr<2, PREC_FP64>(a, st);
-    return launch_tr<3, PREC_FP64>(a, st);
+    if (dim == 1) return launch_tr_v<1, PREC_FP64>(a, st);
+    if (dim == 2) return launch_tr_v<2, PREC_FP64>(a, st);
+    return launch_tr_v<3, PREC_FP64>(a, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -68,6 +68,18 @@ int64_t launch_count();
 void prof_enable(bool on);
 int prof_read(char* names, int names_len, int64_t* counts, double* ms, int max);
 
+// Kernel-variant knobs set by the tuner (vd_tune_set / vd_tune_get).
+int tune_set(const char* key, int value);
+int tune_get(const char* key);
+
+// Mechanism-specialised chemistry compiled at vd_mech_init (vd_spec.cpp).
+int spec_build(const VdMechDev& m);
+bool spec_active();
+void spec_set_enabled(bool on);
+const char* spec_error();
+cudaError_t spec_launch_prep(const PrepArgs& a, int prec, cudaStream_t st);
+int spec_compile_only(const VdMechDev& m, size_t* cubin_bytes);
+
 struct ProfScope {
     int slot;
     cudaStream_t st;
