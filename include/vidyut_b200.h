@@ -293,6 +293,74 @@ int vd_explicit_update_all_noalloc(const vd_box* bx, vd_array4 sborder,
 int vd_box_checksums(const vd_box* bx, vd_array4 rxn, vd_array4 phi_new,
                      double* out_dev, void* stream);
 
+/* Ghost refill of one box (FillPatch with first-order extrapolation on
+ * non-periodic faces, Source/Vidyut.cpp:90-101; periodic wrap elsewhere):
+ * components comps[0..ncomp-1] of the `ghost` layers of face-adjacent ghost cells
+ * are copied from the nearest valid cell (or the periodic image).  Corner and edge
+ * ghosts are not written: no kernel of this library reads them.  periodic may be
+ * NULL (no periodic direction).                                                   */
+int vd_fill_ghosts(const vd_box* bx, vd_array4 state, int ghost, const int32_t* comps, int ncomp,
+                   const int32_t periodic[3], void* stream);
+
+/* ---- batched cases (no single reference counterpart: the reference loops over
+ * boxes with MFIter and calls the per-box functions above for each) -----------
+ * A batch owns a device arena of hbm_budget_bytes and keeps every resident case's
+ * state there (two copies: a step reads one and writes the other), with its
+ * density-sum and reaction-source scratch and its Joule face arrays.  All cases
+ * use the mechanism loaded when the batch was created and the batch's precision;
+ * each has its own box, domain, dt, Tg, scheme and flags (vd_params).
+ * vd_batch_step(n) advances every resident case by min(n, its remaining steps)
+ * explicit steps: per step the density sums + chemistry of all cases, the fused
+ * transport update of all cases (one launch per dimension present) and the ghost
+ * refill of the written state (species, EEN and ETEMP; vd_fill_ghosts), each a
+ * persistent kernel over a work list of (case, chunk-or-tile) items.  The n steps
+ * are captured once as a CUDA graph and replayed while the set of cases stays the
+ * same.  The fields the hot path only reads (E, its face values, the potential)
+ * stay as given; gradne_fc is recomputed from the state when
+ * prm->gradne_from_state, else kept as given.
+ * State layout (add/read): dense, Array4 order (i fastest, component slowest) over
+ * the box grown by the stencil halo H (1, 2 or 3 for hyp_order 1, 2, 5) in each of
+ * its dim directions, VD_NVAR(NS) components; ghosts filled.  efield_ec / gradne_fc:
+ * dense over the face box of direction d, one component; may be NULL when not used
+ * (cs_technique, gradne_from_state, no electron energy).  Pointers may be host or
+ * device memory.  Calls on one batch must come from one host thread at a time;
+ * add/remove/tune wait for the batch's queued work first.                      */
+typedef struct vd_batch vd_batch;
+typedef struct {
+    int32_t  ncases;
+    int32_t  ncases_dim[4];      /* resident cases per dimension (index 1..3)     */
+    int64_t  cells;              /* valid cells over resident cases               */
+    uint64_t bytes_used;         /* arena bytes held by resident cases            */
+    uint64_t bytes_budget;
+    int64_t  steps_run;          /* case-steps completed since creation           */
+    int64_t  graph_builds;       /* CUDA graph captures                           */
+    int32_t  tile_variant[4];    /* transport tile variant per dimension (1..3)   */
+    int32_t  launches_per_step;  /* kernels per step of the current case set      */
+} vd_batch_stats;
+
+int      vd_batch_create(vd_batch** out, int precision, uint64_t hbm_budget_bytes, int max_cases);
+int      vd_batch_destroy(vd_batch* b);
+uint64_t vd_batch_case_bytes(const vd_box* bx, const vd_params* prm);  /* 0 if invalid */
+/* nsteps: steps this case takes in total (< 0: no limit).  VD_ERR_BUDGET when the
+ * case does not fit the arena (or max_cases is reached): nothing is changed. */
+int      vd_batch_add_case(vd_batch* b, const vd_box* bx, const double* state,
+                           const double* const efield_ec[3], const double* const gradne_fc[3],
+                           const vd_params* prm, const int32_t periodic[3], int64_t nsteps,
+                           void* stream, int32_t* case_id);
+int      vd_batch_remove_case(vd_batch* b, int32_t case_id);
+int      vd_batch_step(vd_batch* b, int nsteps, void* stream);
+int      vd_batch_case_info(vd_batch* b, int32_t case_id, int64_t* steps_done, int64_t* steps_left);
+int      vd_batch_read_case(vd_batch* b, int32_t case_id, double* state, void* stream);
+/* autotuner: times the transport kernel of each tile variant on the resident cases
+ * (trials launches each; the state is not advanced), keeps the fastest per
+ * dimension and makes it the default of later batches.  ms_out (16 doubles or
+ * NULL): ms_out[dim*4 + variant], -1 where not timed.                           */
+int      vd_batch_tune(vd_batch* b, int trials, void* stream, double* ms_out);
+int      vd_batch_set_tile_variant(vd_batch* b, int dim, int variant);
+int      vd_batch_tile_shape(int dim, int variant, int32_t tile[3]);  /* returns the variant count */
+int      vd_batch_set_graph(vd_batch* b, int on);  /* 0: launch kernels directly */
+int      vd_batch_get_stats(vd_batch* b, vd_batch_stats* out);
+
 /* ---- measurement (no reference counterpart; the reference only prints the
  * whole-run wall time, Source/main.cpp:45-46) --------------------------------
  * vd_launch_count: kernels launched by this library since load (all entry points).

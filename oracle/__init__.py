@@ -248,3 +248,32 @@ class RefLib(_Base):
         if rc:
             raise RuntimeError(f"reference update aborted (status {rc})")
         return dict(phi_new=phi_new, dsdt=dsdt, rxn=rxn)
+
+
+def run_steps(backend, case: BoxCase, prm: abi.VdParams, nsteps: int) -> np.ndarray:
+    """nsteps explicit steps of one case on the CPU (backend: Port or RefLib).  Each
+    step is the reference's per-box update (update_all) on the current state,
+    followed by the ghost refill of the new state's species, EEN and ETEMP
+    (first-order extrapolation, or periodic wrap; FillPatch before the next step,
+    Source/Vidyut.cpp:90-101).  With prm.gradne_from_state the Joule term's
+    gradne_fc is the face difference of the current electron density.  Returns the
+    final state, laid out like case.state."""
+    from dataclasses import replace
+    from vidyut_b200.inputs import face_gradients, fill_ghosts
+    ns = case.mech.ns
+    g = case.gvec
+    comps = list(range(ns)) + [abi.EEN(ns), abi.ETEMP(ns)]
+    valid = (slice(None), slice(g[2], g[2] + case.n[2]), slice(g[1], g[1] + case.n[1]),
+             slice(g[0], g[0] + case.n[0]))
+    st = case.state.copy()
+    for _ in range(nsteps):
+        gradne = face_gradients(case, st) if prm.gradne_from_state else case.gradne
+        c = replace(case, state=st, gradne=gradne)
+        out = backend.update_all(c, prm)
+        new = st.copy()
+        new[valid] = out["phi_new"]
+        sub = np.ascontiguousarray(new[comps])
+        fill_ghosts(sub, case.dim, case.ghost, case.periodic)
+        new[comps] = sub
+        st = new
+    return st

@@ -294,8 +294,14 @@ int ref_explicit_update_all(const vd_box* bx, vd_array4 sb, const vd_array4* ef,
         if (energy) ref_elecenergy_source(bx, sb, rxn, ef, gne, dv4, phi_new, p);
         for (int k = bx->lo[2]; k <= bx->hi[2]; ++k)
             for (int j = bx->lo[1]; j <= bx->hi[1]; ++j)
-                for (int i = bx->lo[0]; i <= bx->hi[0]; ++i)
+                for (int i = bx->lo[0]; i <= bx->hi[0]; ++i) {
                     pn_arr(i, j, k, s) = sb_arr(i, j, k, s) + p->dt * dv(i, j, k);
+                    /* the species solve's clipping (Source/ScalarSolve.cpp:597-622) */
+                    if (p->bound_specden && !energy) {
+                        double floor_ = (s == E_ID) ? p->min_electron_density : p->min_species_density;
+                        if (pn_arr(i, j, k, s) < floor_) pn_arr(i, j, k, s) = floor_;
+                    }
+                }
     }
     if (p->update_te && p->elecenergy_solve) {
         for (int k = bx->lo[2]; k <= bx->hi[2]; ++k)

@@ -437,7 +437,12 @@ int orc_elecenergy_source(const vd_mech *m, const vd_box *bx, const vd_array4 *s
                         double ne = 0.5 * (A4(sb, l[0], l[1], l[2], eidx) + A4(sb, r[0], r[1], r[2], eidx));
                         double efield_face = p->cs_technique ? evf[idim]
                                                              : A4(&ef[idim], face[0], face[1], face[2], 0);
-                        double gradne_face = A4(&gne[idim], face[0], face[1], face[2], 0);
+                        /* gradne_fc is the face difference of ne (the electron solve's
+                         * gradient); gradne_from_state forms it from the step's state */
+                        double gradne_face =
+                            p->gradne_from_state
+                                ? (A4(sb, r[0], r[1], r[2], eidx) - A4(sb, l[0], l[1], l[2], eidx)) / p->dx[idim]
+                                : A4(&gne[idim], face[0], face[1], face[2], 0);
                         double ndens = 0.0;
                         for (int sp = 0; sp < ns; sp++)
                             ndens += 0.5 * (A4(sb, l[0], l[1], l[2], sp) + A4(sb, r[0], r[1], r[2], sp));
@@ -532,8 +537,15 @@ int orc_explicit_update_all(const vd_mech *m, const vd_box *bx, const vd_array4 
         if (is_energy) orc_elecenergy_source(m, bx, sb, rxn_out, ef, gne, &dv, phi_new, p);
         for (int k = bx->lo[2]; k <= bx->hi[2]; ++k)
             for (int j = bx->lo[1]; j <= bx->hi[1]; ++j)
-                for (int i = bx->lo[0]; i <= bx->hi[0]; ++i)
-                    A4(phi_new, i, j, k, s) = A4(sb, i, j, k, s) + p->dt * A4(&dv, i, j, k, 0);
+                for (int i = bx->lo[0]; i <= bx->hi[0]; ++i) {
+                    double v = A4(sb, i, j, k, s) + p->dt * A4(&dv, i, j, k, 0);
+                    if (p->bound_specden && !is_energy) {
+                        /* solution clipping of the species solve (Source/ScalarSolve.cpp:599-625) */
+                        double lo = (s == m->e_id) ? p->min_electron_density : p->min_species_density;
+                        if (v < lo) v = lo;
+                    }
+                    A4(phi_new, i, j, k, s) = v;
+                }
     }
     if (p->update_te && p->elecenergy_solve) {
         /* Source/ScalarSolve.cpp:659-666: Te from the new energy and the step's input ne */

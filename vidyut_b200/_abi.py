@@ -212,3 +212,29 @@ PROTOTYPES.update({
     "vd_tune_set": (C.c_int, [C.c_char_p, C.c_int]),
     "vd_tune_get": (C.c_int, [C.c_char_p]),
 })
+
+
+class VdBatchStats(C.Structure):
+    _fields_ = [("ncases", C.c_int32), ("ncases_dim", C.c_int32 * 4), ("cells", C.c_int64),
+                ("bytes_used", C.c_uint64), ("bytes_budget", C.c_uint64), ("steps_run", C.c_int64),
+                ("graph_builds", C.c_int64), ("tile_variant", C.c_int32 * 4), ("launches_per_step", C.c_int32)]
+
+
+DPP = C.POINTER(C.c_void_p)  # const double* const[3]
+PROTOTYPES.update({
+    "vd_fill_ghosts": (C.c_int, [BOXP, A4, C.c_int, I32P, C.c_int, I32P, C.c_void_p]),
+    "vd_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_uint64, C.c_int]),
+    "vd_batch_destroy": (C.c_int, [C.c_void_p]),
+    "vd_batch_case_bytes": (C.c_uint64, [BOXP, PRMP]),
+    "vd_batch_add_case": (C.c_int, [C.c_void_p, BOXP, C.c_void_p, DPP, DPP, PRMP, I32P, C.c_int64, C.c_void_p,
+                                    I32P]),
+    "vd_batch_remove_case": (C.c_int, [C.c_void_p, C.c_int32]),
+    "vd_batch_step": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "vd_batch_case_info": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "vd_batch_read_case": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "vd_batch_tune": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, DP]),
+    "vd_batch_set_tile_variant": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "vd_batch_tile_shape": (C.c_int, [C.c_int, C.c_int, I32P]),
+    "vd_batch_set_graph": (C.c_int, [C.c_void_p, C.c_int]),
+    "vd_batch_get_stats": (C.c_int, [C.c_void_p, C.POINTER(VdBatchStats)]),
+})

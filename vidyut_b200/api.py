@@ -167,3 +167,140 @@ def explicit_update_all_noalloc(dc: DeviceCase, prm: abi.VdParams, phi_new: torc
                                           t_a4(rxn, (0, 0, 0)) if rxn is not None else abi.null_array4(),
                                           C.byref(prm), _stream(stream))
     abi.check(rc, "vd_explicit_update_all_noalloc")
+
+
+def fill_ghosts(state: torch.Tensor, case: BoxCase, ghost: int, comps, periodic=(0, 0, 0), stream=None) -> None:
+    """Ghost refill of a device state laid out like case.state (FillPatch with
+    first-order extrapolation / periodic wrap on face-adjacent ghosts)."""
+    L = abi.lib()
+    cl = (C.c_int32 * max(1, len(comps)))(*[int(c) for c in comps])
+    per = (C.c_int32 * 3)(*[int(p) for p in periodic])
+    rc = L.vd_fill_ghosts(C.byref(abi.make_box(case.lo, case.hi, case.dim)), t_a4(state, case.state_begin()),
+                          int(ghost), cl, len(comps), per, _stream(stream))
+    abi.check(rc, "vd_fill_ghosts")
+
+
+def stencil_halo(hyp_order: int) -> int:
+    return 3 if hyp_order == 5 else int(hyp_order)
+
+
+def trim_ghosts(case: BoxCase, state: np.ndarray, H: int) -> np.ndarray:
+    """The state restricted to the box grown by H ghosts (H <= case.ghost)."""
+    g = case.gvec
+    sl = [slice(None)]
+    for d in (2, 1, 0):
+        h = H if d < case.dim else 0
+        sl.append(slice(g[d] - h, g[d] + case.n[d] + h))
+    return np.ascontiguousarray(state[tuple(sl)])
+
+
+class Batch:
+    """Many independent cases resident in one HBM arena and stepped together
+    (vd_batch_* of the C ABI): per step one persistent launch each of the prep
+    (density sums + chemistry), transport (per dimension present) and ghost-refill
+    kernels over a work list of all cases, replayed from a captured CUDA graph."""
+
+    def __init__(self, precision=abi.PREC_MIXED, budget_bytes: int = 4 << 30, max_cases: int = 1024):
+        L = abi.lib()
+        self._h = C.c_void_p()
+        abi.check(L.vd_batch_create(C.byref(self._h), int(precision), int(budget_bytes), int(max_cases)),
+                  "vd_batch_create")
+        self.precision = int(precision)
+        self.cases = {}
+
+    def close(self) -> None:
+        if self._h:
+            abi.lib().vd_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # pragma: no cover
+            pass
+
+    @staticmethod
+    def case_bytes(case: BoxCase, prm: abi.VdParams) -> int:
+        return int(abi.lib().vd_batch_case_bytes(C.byref(abi.make_box(case.lo, case.hi, case.dim)), C.byref(prm)))
+
+    def add(self, case: BoxCase, prm: abi.VdParams, nsteps: int = -1, stream=None) -> int:
+        """Copy the case into the arena; raises VidyutError(ERR_BUDGET) when it does
+        not fit.  Returns the case id."""
+        L = abi.lib()
+        H = stencil_halo(prm.hyp_order)
+        st = trim_ghosts(case, case.state, H)
+        ef = [np.ascontiguousarray(case.efield[d]) for d in range(3)]
+        gn = [np.ascontiguousarray(case.gradne[d]) for d in range(3)]
+        efp = (C.c_void_p * 3)(*[a.ctypes.data for a in ef])
+        gnp = (C.c_void_p * 3)(*[a.ctypes.data for a in gn])
+        per = (C.c_int32 * 3)(*[int(p) for p in case.periodic])
+        cid = C.c_int32()
+        rc = L.vd_batch_add_case(self._h, C.byref(abi.make_box(case.lo, case.hi, case.dim)), st.ctypes.data,
+                                 efp, gnp, C.byref(prm), per, int(nsteps), _stream(stream), C.byref(cid))
+        abi.check(rc, "vd_batch_add_case")
+        self.cases[cid.value] = (case, H)
+        return cid.value
+
+    def remove(self, cid: int) -> None:
+        abi.check(abi.lib().vd_batch_remove_case(self._h, int(cid)), "vd_batch_remove_case")
+        self.cases.pop(cid, None)
+
+    def step(self, nsteps: int, stream=None) -> None:
+        abi.check(abi.lib().vd_batch_step(self._h, int(nsteps), _stream(stream)), "vd_batch_step")
+
+    def info(self, cid: int):
+        done, left = C.c_int64(), C.c_int64()
+        abi.check(abi.lib().vd_batch_case_info(self._h, int(cid), C.byref(done), C.byref(left)),
+                  "vd_batch_case_info")
+        return done.value, left.value
+
+    def read(self, cid: int, stream=None, out: torch.Tensor | None = None) -> torch.Tensor:
+        """The case's current state (ghost-grown box, NVAR components).  Into a
+        device tensor when out is given (asynchronous), else a host array."""
+        case, H = self.cases[cid]
+        ns = case.mech.ns
+        shp = [abi.NVAR(ns)]
+        for d in (2, 1, 0):
+            shp.append(case.n[d] + (2 * H if d < case.dim else 0))
+        if out is None:
+            host = torch.empty(shp, dtype=torch.float64, pin_memory=True)
+            abi.check(abi.lib().vd_batch_read_case(self._h, int(cid), host.data_ptr(), _stream(stream)),
+                      "vd_batch_read_case")
+            (stream or torch.cuda.current_stream()).synchronize()
+            return host
+        assert tuple(out.shape) == tuple(shp) and out.dtype == torch.float64 and out.is_contiguous()
+        abi.check(abi.lib().vd_batch_read_case(self._h, int(cid), out.data_ptr(), _stream(stream)),
+                  "vd_batch_read_case")
+        return out
+
+    def tune(self, trials: int = 5, stream=None) -> dict:
+        ms = (C.c_double * 16)()
+        abi.check(abi.lib().vd_batch_tune(self._h, int(trials), _stream(stream), ms), "vd_batch_tune")
+        return {(d, v): ms[d * 4 + v] for d in range(1, 4) for v in range(4) if ms[d * 4 + v] >= 0}
+
+    def set_tile_variant(self, dim: int, variant: int) -> None:
+        abi.check(abi.lib().vd_batch_set_tile_variant(self._h, int(dim), int(variant)), "vd_batch_set_tile_variant")
+
+    def set_graph(self, on: bool) -> None:
+        abi.check(abi.lib().vd_batch_set_graph(self._h, int(bool(on))), "vd_batch_set_graph")
+
+    def stats(self) -> dict:
+        s = abi.VdBatchStats()
+        abi.check(abi.lib().vd_batch_get_stats(self._h, C.byref(s)), "vd_batch_get_stats")
+        return dict(ncases=s.ncases, ncases_dim=list(s.ncases_dim), cells=s.cells, bytes_used=s.bytes_used,
+                    bytes_budget=s.bytes_budget, steps_run=s.steps_run, graph_builds=s.graph_builds,
+                    tile_variant=list(s.tile_variant), launches_per_step=s.launches_per_step)
+
+
+def batch_tile_shape(dim: int, variant: int):
+    t = (C.c_int32 * 3)()
+    n = abi.lib().vd_batch_tile_shape(int(dim), int(variant), t)
+    if n < 0:
+        abi.check(n, "vd_batch_tile_shape")
+    return tuple(t), n

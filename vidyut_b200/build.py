@@ -18,7 +18,7 @@ CSRC = PKG / "csrc"
 LIB = PKG / "libvidyut_b200.so"
 BUILD = PKG / "_build"
 
-SOURCES = ["vd_kernels.cu", "vd_abi.cu", "vd_spec.cpp"]
+SOURCES = ["vd_kernels.cu", "vd_abi.cu", "vd_spec.cpp", "vd_batch.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC,-O3", "-Xptxas", "-O3"]
@@ -39,9 +39,10 @@ def _stale(out: Path, deps: list[Path]) -> bool:
 
 
 def build(verbose: bool = False, ptxas_info: bool = False, force: bool = False) -> Path:
+    from concurrent.futures import ThreadPoolExecutor
     BUILD.mkdir(exist_ok=True)
-    headers = list(CSRC.glob("*.cuh")) + [PKG.parent / "include" / "vidyut_b200.h"]
-    objs = []
+    headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [PKG.parent / "include" / "vidyut_b200.h"]
+    objs, jobs = [], []
     for src in SOURCES:
         s = CSRC / src
         o = BUILD / (s.stem + ".o")
@@ -50,13 +51,21 @@ def build(verbose: bool = False, ptxas_info: bool = False, force: bool = False) 
             cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", str(s), "-o", str(o)]
             if ptxas_info:
                 cmd += ["-Xptxas", "-v"]
-            if verbose:
-                print(" ".join(cmd), flush=True)
-            r = subprocess.run(cmd, capture_output=True, text=True)
-            if r.returncode != 0 or verbose or ptxas_info:
-                sys.stderr.write(r.stdout + r.stderr)
-            if r.returncode != 0:
-                raise RuntimeError(f"nvcc failed on {src}")
+            jobs.append((src, cmd))
+
+    def run(job):
+        src, cmd = job
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        return src, subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=max(1, len(jobs))) as ex:
+        results = list(ex.map(run, jobs))
+    for src, r in results:
+        if r.returncode != 0 or verbose or ptxas_info:
+            sys.stderr.write(r.stdout + r.stderr)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src}")
     if force or _stale(LIB, objs):
         cuda_lib = Path(nvcc()).resolve().parent.parent / "lib64"
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-cudart", "static",

@@ -479,6 +479,7 @@ static void fill_cfg(TransportArgs& a, const vd_box* bx, const vd_params* p, con
     a.gradne_from_state = p->gradne_from_state;
     a.update_te = p->update_te;
     a.min_spec = p->min_species_density;
+    a.min_elec = p->min_electron_density;
     a.ele_mob = p->ele_mob;
     a.ele_diff = p->ele_diff;
     a.min_te = p->min_electron_temp;
@@ -689,6 +690,50 @@ int vd_profile_read(char* names, int names_len, int64_t* counts, double* ms, int
     return n;
 }
 
+int vd_fill_ghosts(const vd_box* bx, vd_array4 state, int ghost, const int32_t* comps, int ncomp,
+                   const int32_t periodic[3], void* stream)
+{
+    if (!valid_box(bx)) return fail(VD_ERR_ARG, "invalid box");
+    if (ghost < 0 || ghost > 8) return fail(VD_ERR_GHOST, "ghost %d outside [0,8]", ghost);
+    if (ncomp < 0 || ncomp > VD_MAX_SPECIES + 4 || (ncomp && !comps))
+        return fail(VD_ERR_ARG, "ncomp %d outside [0,%d]", ncomp, VD_MAX_SPECIES + 4);
+    int glo[3] = {bx->lo[0], bx->lo[1], bx->lo[2]}, ghi[3] = {bx->hi[0], bx->hi[1], bx->hi[2]};
+    for (int d = 0; d < bx->dim; d++) {
+        glo[d] -= ghost;
+        ghi[d] += ghost;
+    }
+    int maxc = 0;
+    for (int q = 0; q < ncomp; q++) {
+        if (comps[q] < 0 || comps[q] > 127) return fail(VD_ERR_ARG, "component %d out of range", comps[q]);
+        maxc = comps[q] + 1 > maxc ? comps[q] + 1 : maxc;
+    }
+    std::string why;
+    if (!covers(state, glo, ghi, maxc, &why)) return fail(VD_ERR_GHOST, "state: %s", why.c_str());
+    GhostArgs a;
+    memset(&a, 0, sizeof(a));
+    a.st = A4(state);
+    a.ghost = ghost;
+    a.dim = bx->dim;
+    a.count = 0;
+    for (int d = 0; d < 3; d++) {
+        a.lo[d] = bx->lo[d];
+        a.hi[d] = bx->hi[d];
+        a.periodic[d] = (periodic && d < bx->dim) ? (periodic[d] != 0) : 0;
+        if (a.periodic[d] && bx->hi[d] - bx->lo[d] + 1 < 1) return fail(VD_ERR_ARG, "empty periodic direction");
+    }
+    for (int d = 0; d < bx->dim; d++) {
+        int64_t P = 1;
+        for (int e = 0; e < bx->dim; e++)
+            if (e != d) P *= bx->hi[e] - bx->lo[e] + 1;
+        a.count += 2 * (int64_t)ghost * P;
+    }
+    a.ncomp = ncomp;
+    for (int q = 0; q < ncomp; q++) a.comps[q] = (int8_t)comps[q];
+    cudaError_t e = launch_ghost(a, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "k_ghost launch");
+    return VD_OK;
+}
+
 int vd_box_checksums(const vd_box* bx, vd_array4 rxn, vd_array4 phi_new, double* out_dev, void* stream)
 {
     cudaStream_t st = (cudaStream_t)stream;
@@ -876,3 +921,70 @@ extern "C" int vd_explicit_update_all_noalloc(const vd_box* bx, vd_array4 sborde
     if (e != cudaSuccess) return cuda_fail(e, "allocation-free update launch");
     return VD_OK;
 }
+
+// ===========================================================================
+// Host services for the batch layer (vd_host.h).
+#include "vd_host.h"
+
+namespace vd_host {
+
+int set_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
+int ensure_mech(cudaStream_t st) { return ensure_mech_on_device(st); }
+
+int mech_info(MechInfo* out)
+{
+    std::lock_guard<std::mutex> lk(g_mech_mu);
+    if (!g_mech) return fail(VD_ERR_MECH, "no mechanism loaded: call vd_mech_init first");
+    out->ns = g_mech->nspecies;
+    out->e_id = g_mech->e_id;
+    out->generation = g_mech_gen;
+    for (int s = 0; s <= g_mech->nspecies; s++) out->mob_kind[s] = g_mech->mob_kind[s];
+    for (int s = 0; s < g_mech->nspecies; s++) out->charge[s] = g_mech->charge[s];
+    return VD_OK;
+}
+
+int check_update_params(const vd_box* bx, const vd_params* p, const MechInfo& m)
+{
+    int rc = check_params(bx, p);
+    if (rc) return rc;
+    if (p->bg_mask >> m.ns) return fail(VD_ERR_ARG, "bg_mask names species >= %d", m.ns);
+    if (p->bg_mask & (1ull << m.e_id)) return fail(VD_ERR_ARG, "electrons cannot be a background species");
+    if (p->user_defined_vel && (p->vel_species < 0 || p->vel_species > m.ns))
+        return fail(VD_ERR_ARG, "vel_species invalid");
+    if (!(p->dt >= 0.0) || !std::isfinite(p->dt)) return fail(VD_ERR_ARG, "dt must be finite and >= 0");
+    return VD_OK;
+}
+
+void fill_transport_args(TransportArgs& a, const vd_box* bx, const vd_params* p, const MechInfo& m)
+{
+    vd_mech* mm = new vd_mech;  // fill_cfg reads nspecies, e_id and the electron charge
+    memset(mm, 0, sizeof(vd_mech));
+    mm->nspecies = m.ns;
+    mm->e_id = m.e_id;
+    for (int s = 0; s < m.ns; s++) mm->charge[s] = m.charge[s];
+    fill_cfg(a, bx, p, mm);
+    delete mm;
+    const int ns = m.ns;
+    a.ntr = 0;
+    a.nbg = 0;
+    for (int s = 0; s <= ns; s++) {
+        bool energy = (s == ns);
+        if (energy && !p->elecenergy_solve) continue;
+        if (!energy && ((p->bg_mask >> s) & 1ull)) {
+            a.bg_sp[a.nbg++] = (int8_t)s;
+            continue;
+        }
+        a.tr_sp[a.ntr] = (int8_t)s;
+        int cls = energy ? VD_CLASS_ENERGY
+                         : (s == m.e_id ? VD_CLASS_ELECTRON : (m.charge[s] != 0 ? VD_CLASS_ION : VD_CLASS_NEUTRAL));
+        a.tr_cls[a.ntr] = (int8_t)cls;
+        bool has_vel = p->user_defined_vel ? (s == p->vel_species) : (m.mob_kind[s] != VD_MOB_ZERO);
+        a.tr_flux[a.ntr] = (p->do_transport && has_vel) ? 1 : 0;
+        a.ntr++;
+    }
+}
+
+int stencil_halo(int hyp_order) { return ::stencil_halo(hyp_order); }
+
+}  // namespace vd_host

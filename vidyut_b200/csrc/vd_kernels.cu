@@ -34,9 +34,12 @@ struct ProfRec {
     cudaEvent_t a, b;
 };
 std::vector<ProfRec> g_recs;
+thread_local bool t_prof_suspended = false;
 }  // namespace
 
 int64_t launch_count() { return g_launches.load(); }
+void add_launches(int64_t n) { g_launches.fetch_add(n); }
+void prof_suspend(bool on) { t_prof_suspended = on; }
 
 void prof_enable(bool on)
 {
@@ -53,7 +56,7 @@ void prof_enable(bool on)
 ProfScope::ProfScope(const char* name, cudaStream_t s) : slot(-1), st(s)
 {
     g_launches.fetch_add(1);
-    if (!g_prof.load()) return;
+    if (!g_prof.load() || t_prof_suspended) return;
     ProfRec r;
     r.name = name;
     if (cudaEventCreate(&r.a) != cudaSuccess) return;
@@ -372,6 +375,46 @@ cudaError_t launch_joule(const BoxIdx& b, int dim, const A4& sb, const A4& rxn, 
 }
 
 // ---------------------------------------------------------------------------
+// One cell (linear index idx over the grown box) of the prep pass: density sum and,
+// inside the valid box, the reaction source.  sc/wd: this thread's shared rows.
+template <int PREC>
+__device__ __forceinline__ void prep_cell(const PrepArgs& a, int64_t idx, double* sc, double* wd, int st)
+{
+    const int ns = c_mech.ns;
+    const int gx = a.ghi[0] - a.glo[0] + 1, gy = a.ghi[1] - a.glo[1] + 1;
+    int k = (int)(idx / ((int64_t)gx * gy));
+    int64_t r = idx - (int64_t)k * gx * gy;
+    int j = (int)(r / gx);
+    int i = (int)(r - (int64_t)j * gx);
+    i += a.glo[0];
+    j += a.glo[1];
+    k += a.glo[2];
+    const int64_t o = a.sb.off(i, j, k);
+    double N = 0.0;
+    for (int s = 0; s < ns; s++) {
+        const double v = a.sb.p[o + s * a.sb.ns];
+        sc[s * st] = v;
+        N += v;
+    }
+    if (a.write_n) a.Nv(i, j, k) = N;
+    bool inside = i >= a.lo[0] && i <= a.hi[0] && j >= a.lo[1] && j <= a.hi[1] && k >= a.lo[2] && k <= a.hi[2];
+    if (!inside) return;
+    const int64_t ro = a.rxn.off(i, j, k);
+    if (a.do_reactions) {
+        double Te = a.sb.p[o + (int64_t)VD_ETEMP(ns) * a.sb.ns];
+        double ee = chem_cell<PREC>(sc, wd, st, Te, a.Tg);
+        for (int s = 0; s < ns; s++) a.rxn.p[ro + s * a.rxn.ns] = wd[s * st];
+        a.rxn.p[ro + (int64_t)ns * a.rxn.ns] = ee;
+    } else {
+        for (int s = 0; s <= ns; s++) a.rxn.p[ro + s * a.rxn.ns] = 0.0;
+    }
+}
+
+__device__ __forceinline__ int64_t grown_cells(const PrepArgs& a)
+{
+    return (int64_t)(a.ghi[0] - a.glo[0] + 1) * (a.ghi[1] - a.glo[1] + 1) * (a.ghi[2] - a.glo[2] + 1);
+}
+
 template <int PREC>
 __global__ void __launch_bounds__(128) k_prep(const __grid_constant__ PrepArgs a)
 {
@@ -380,37 +423,138 @@ __global__ void __launch_bounds__(128) k_prep(const __grid_constant__ PrepArgs a
     const int st = blockDim.x;
     double* sc = reinterpret_cast<double*>(smem_raw) + threadIdx.x;
     double* wd = sc + ns * st;
-    const int gx = a.ghi[0] - a.glo[0] + 1, gy = a.ghi[1] - a.glo[1] + 1, gz = a.ghi[2] - a.glo[2] + 1;
-    const int64_t ntot = (int64_t)gx * gy * gz;
+    const int64_t ntot = grown_cells(a);
     for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < ntot;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        int k = (int)(idx / ((int64_t)gx * gy));
-        int64_t r = idx - (int64_t)k * gx * gy;
-        int j = (int)(r / gx);
-        int i = (int)(r - (int64_t)j * gx);
-        i += a.glo[0];
-        j += a.glo[1];
-        k += a.glo[2];
-        const int64_t o = a.sb.off(i, j, k);
-        double N = 0.0;
-        for (int s = 0; s < ns; s++) {
-            const double v = a.sb.p[o + s * a.sb.ns];
-            sc[s * st] = v;
-            N += v;
-        }
-        if (a.write_n) a.Nv(i, j, k) = N;
-        bool inside = i >= a.lo[0] && i <= a.hi[0] && j >= a.lo[1] && j <= a.hi[1] && k >= a.lo[2] && k <= a.hi[2];
-        if (!inside) continue;
-        const int64_t ro = a.rxn.off(i, j, k);
-        if (a.do_reactions) {
-            double Te = a.sb.p[o + (int64_t)VD_ETEMP(ns) * a.sb.ns];
-            double ee = chem_cell<PREC>(sc, wd, st, Te, a.Tg);
-            for (int s = 0; s < ns; s++) a.rxn.p[ro + s * a.rxn.ns] = wd[s * st];
-            a.rxn.p[ro + (int64_t)ns * a.rxn.ns] = ee;
-        } else {
-            for (int s = 0; s <= ns; s++) a.rxn.p[ro + s * a.rxn.ns] = 0.0;
+         idx += (int64_t)gridDim.x * blockDim.x)
+        prep_cell<PREC>(a, idx, sc, wd, st);
+}
+
+// batched prep: item (box, chunk) covers grown-box cells [chunk*kPrepChunk, +kPrepChunk)
+template <int PREC>
+__global__ void __launch_bounds__(128) k_prep_batch(const PrepArgs* __restrict__ boxes, const int2* __restrict__ items,
+                                                    int nitems, const BatchCtl ctl)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int ns = c_mech.ns;
+    const int st = blockDim.x;
+    double* sc = reinterpret_cast<double*>(smem_raw) + threadIdx.x;
+    double* wd = sc + ns * st;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int2 w = items[it];
+        const int2 cc = ctl.ctrl[w.x];
+        if (ctl.t >= cc.x) continue;
+        const PrepArgs& a = boxes[((ctl.t + cc.y) & 1) * ctl.nbox + w.x];
+        const int64_t ntot = grown_cells(a);
+        const int64_t base = (int64_t)w.y * kPrepChunk;
+        for (int q = threadIdx.x; q < kPrepChunk; q += blockDim.x) {
+            const int64_t idx = base + q;
+            if (idx < ntot) prep_cell<PREC>(a, idx, sc, wd, st);
         }
     }
+}
+
+cudaError_t launch_prep_batch(const PrepArgs* boxes, const int2* items, int nitems, BatchCtl ctl, int prec, int ns,
+                              cudaStream_t st)
+{
+    if (nitems <= 0) return cudaSuccess;
+    {
+        cudaError_t es = spec_launch_prep_batch(boxes, items, nitems, ctl, prec, st);
+        if (es != cudaErrorNotReady) return es;
+    }
+    size_t sm = 0;
+    const void* fn =
+        prec == PREC_MIXED ? (const void*)k_prep_batch<PREC_MIXED> : (const void*)k_prep_batch<PREC_FP64>;
+    cudaError_t e = chem_smem(fn, ns, 128, &sm);
+    if (e != cudaSuccess) return e;
+    unsigned g = (unsigned)(nitems < 148 * 16 ? nitems : 148 * 16);
+    ProfScope ps("k_prep_batch", st);
+    if (prec == PREC_MIXED) k_prep_batch<PREC_MIXED><<<g, 128, sm, st>>>(boxes, items, nitems, ctl);
+    else k_prep_batch<PREC_FP64><<<g, 128, sm, st>>>(boxes, items, nitems, ctl);
+    return cudaGetLastError();
+}
+
+// ghost cell idx (0 <= idx < a.count) of a box, ordered by direction d, side,
+// layer, then the other coordinates: copy the components in comps[] from the
+// nearest valid cell (first-order extrapolation) or the periodic image
+__device__ __forceinline__ void ghost_cell(const GhostArgs& a, int64_t idx)
+{
+    const int G = a.ghost;
+    int n[3];
+    for (int e = 0; e < 3; e++) n[e] = a.hi[e] - a.lo[e] + 1;
+    int d = 0;
+    int64_t P = 1;
+    for (; d < a.dim; d++) {
+        P = 1;
+        for (int e = 0; e < a.dim; e++)
+            if (e != d) P *= n[e];
+        const int64_t cnt = 2 * (int64_t)G * P;
+        if (idx < cnt) break;
+        idx -= cnt;
+    }
+    if (d >= a.dim) return;
+    const int side = (int)(idx / ((int64_t)G * P));
+    const int g = (int)((idx / P) % G) + 1;
+    int64_t rest = idx % P;
+    int c[3] = {a.lo[0], a.lo[1], a.lo[2]};
+    for (int e = 0; e < a.dim; e++) {
+        if (e == d) continue;
+        c[e] = a.lo[e] + (int)(rest % n[e]);
+        rest /= n[e];
+    }
+    int dst[3] = {c[0], c[1], c[2]}, src[3] = {c[0], c[1], c[2]};
+    if (side == 0) {
+        dst[d] = a.lo[d] - g;
+        src[d] = a.periodic[d] ? a.hi[d] - ((g - 1) % n[d]) : a.lo[d];
+    } else {
+        dst[d] = a.hi[d] + g;
+        src[d] = a.periodic[d] ? a.lo[d] + ((g - 1) % n[d]) : a.hi[d];
+    }
+    const int64_t od = a.st.off(dst[0], dst[1], dst[2]), os = a.st.off(src[0], src[1], src[2]);
+    for (int q = 0; q < a.ncomp; q++) {
+        const int64_t co = (int64_t)a.comps[q] * a.st.ns;
+        a.st.p[od + co] = a.st.p[os + co];
+    }
+}
+
+// batched ghost refill: item (box, chunk) covers ghost cells [chunk*kGhostChunk, +kGhostChunk)
+__global__ void __launch_bounds__(kGhostChunk) k_ghost_batch(const GhostArgs* __restrict__ boxes,
+                                                             const int2* __restrict__ items, int nitems,
+                                                             const BatchCtl ctl)
+{
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int2 w = items[it];
+        const int2 cc = ctl.ctrl[w.x];
+        if (ctl.t >= cc.x) continue;
+        const GhostArgs& a = boxes[((ctl.t + cc.y) & 1) * ctl.nbox + w.x];
+        const int64_t idx = (int64_t)w.y * kGhostChunk + threadIdx.x;
+        if (idx < a.count) ghost_cell(a, idx);
+    }
+}
+
+// single box
+__global__ void __launch_bounds__(256) k_ghost(const __grid_constant__ GhostArgs a)
+{
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < a.count;
+         idx += (int64_t)gridDim.x * blockDim.x)
+        ghost_cell(a, idx);
+}
+
+cudaError_t launch_ghost(const GhostArgs& a, cudaStream_t st)
+{
+    if (a.count <= 0) return cudaSuccess;
+    unsigned g = grid_for(a.count, 256);
+    ProfScope ps("k_ghost", st);
+    k_ghost<<<g, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ghost_batch(const GhostArgs* boxes, const int2* items, int nitems, BatchCtl ctl, cudaStream_t st)
+{
+    if (nitems <= 0) return cudaSuccess;
+    unsigned g = (unsigned)(nitems < 148 * 8 ? nitems : 148 * 8);
+    ProfScope ps("k_ghost_batch", st);
+    k_ghost_batch<<<g, kGhostChunk, 0, st>>>(boxes, items, nitems, ctl);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_prep(const PrepArgs& a, int prec, int ns, cudaStream_t st)
@@ -432,233 +576,22 @@ cudaError_t launch_prep(const PrepArgs& a, int prec, int ns, cudaStream_t st)
 }
 
 // ---------------------------------------------------------------------------
-// Fused transport kernel.  One CTA per TX x TY x TZ tile, NTH threads.  Per
-// transported species: (1) stage the stencil lines of every sweep direction in
-// shared memory -- for direction d the cells rel -3 .. T_d+2 along d of each tile
-// row, with the density and the drift velocity mu(Te, N) E_d computed once per
-// staged cell; (2) compute every face flux of the tile once (all directions in one
-// pass, faces spread evenly over the threads); (3) each thread takes the
-// divergence of its own cell, adds rxn (and the Joule term for the electron
-// energy) and writes n + dt*dsdt in FP64.  Two barriers per species.
-template <int DIM> struct Tile;
-template <> struct Tile<1> { static constexpr int X = 256, Y = 1, Z = 1, NTH = 256; };
-template <> struct Tile<2> { static constexpr int X = 32, Y = 8, Z = 1, NTH = 256; };
-template <> struct Tile<3> { static constexpr int X = 8, Y = 8, Z = 8, NTH = 512; };
+// Fused transport kernel (vd_transport.cuh): tile shapes and the tile update.
+}  // namespace vd
+#include "vd_transport.cuh"
+namespace vd {
 
 void transport_tile(int dim, int t[3])
 {
-    if (dim == 1) { t[0] = Tile<1>::X; t[1] = 1; t[2] = 1; }
-    else if (dim == 2) { t[0] = Tile<2>::X; t[1] = Tile<2>::Y; t[2] = 1; }
-    else { t[0] = Tile<3>::X; t[1] = Tile<3>::Y; t[2] = Tile<3>::Z; }
-}
-
-template <int DIM>
-struct TileGeom {
-    static constexpr int T[3] = {Tile<DIM>::X, Tile<DIM>::Y, Tile<DIM>::Z};
-    static constexpr int NCELL = T[0] * T[1] * T[2];
-    // staged line set of direction d: extent T_d + 6 along d
-    template <int D> static constexpr int SE(int e) { return T[e] + (e == D ? 6 : 0); }
-    template <int D> static constexpr int NS() { return D < DIM ? SE<D>(0) * SE<D>(1) * SE<D>(2) : 0; }
-    template <int D> static constexpr int FE(int e) { return T[e] + (e == D ? 1 : 0); }
-    template <int D> static constexpr int NF() { return D < DIM ? FE<D>(0) * FE<D>(1) * FE<D>(2) : 0; }
-    static constexpr int SOFF1 = NS<0>(), SOFF2 = NS<0>() + NS<1>(), STOT = NS<0>() + NS<1>() + NS<2>();
-    static constexpr int FOFF1 = NF<0>(), FOFF2 = NF<0>() + NF<1>(), FTOT = NF<0>() + NF<1>() + NF<2>();
-};
-
-template <int PREC> struct VelT { using T = double; };
-template <> struct VelT<PREC_MIXED> { using T = float; };
-
-// stage staged-cell cc of direction D's line set: density and drift velocity
-template <int DIM, int PREC, int D>
-__device__ __forceinline__ void stage_cell(const TransportArgs& a, int cc, int s, const int* org,
-                                           typename VelT<PREC>::T* sU, typename VelT<PREC>::T* sV)
-{
-    using G = TileGeom<DIM>;
-    using VT = typename VelT<PREC>::T;
-    constexpr int E0 = G::template SE<D>(0), E1 = G::template SE<D>(1);
-    int l[3];
-    l[0] = cc % E0;
-    l[1] = (cc / E0) % E1;
-    l[2] = cc / (E0 * E1);
-    int g[3] = {org[0] + l[0], org[1] + l[1], org[2] + l[2]};
-    g[D] -= 3;
-    bool ok = (g[D] >= a.lo[D] - a.ghost) && (g[D] <= a.hi[D] + a.ghost);
-#pragma unroll
-    for (int e = 0; e < DIM; e++)
-        if (e != D) ok = ok && (g[e] <= a.hi[e]);
-    VT u = VT(0);
-    VT v = VT(0);
-    if (ok) {
-        const int ns = a.ns;
-        const int64_t cs = a.sb.ns;
-        const double* p = a.sb.p + a.sb.off(g[0], g[1], g[2]);
-        u = (VT)p[s * cs];
-        if (a.udv) {
-            v = (s == a.vel_sp) ? VT(a.uvel[D]) : VT(0);
-        } else {
-            const double Te = p[VD_ETEMP(ns) * cs];
-            const double E = p[(VD_EFX(ns) + D) * cs];
-            const double N = a.Nv(g[0], g[1], g[2]);
-            if constexpr (PREC == PREC_FP64) v = mob_fp64(s, Te, N, a.Tg) * E;
-            else v = mob_f32(s, (float)Te, (float)N, (float)a.Tg) * (float)E;
-        }
-    }
-    sU[cc] = u;
-    sV[cc] = v;
-}
-
-// flux of face ff of direction D from the staged lines
-template <int DIM, int PREC, int D>
-__device__ __forceinline__ double face_of(const TransportArgs& a, int ff, int cls, const int* org,
-                                          const typename VelT<PREC>::T* sU, const typename VelT<PREC>::T* sV)
-{
-    using G = TileGeom<DIM>;
-    using VT = typename VelT<PREC>::T;
-    constexpr int F0 = G::template FE<D>(0), F1 = G::template FE<D>(1);
-    constexpr int S0 = G::template SE<D>(0), S1 = G::template SE<D>(1);
-    constexpr int STR = (D == 0) ? 1 : ((D == 1) ? S0 : S0 * S1);
-    int l[3];
-    l[0] = ff % F0;
-    l[1] = (ff / F0) % F1;
-    l[2] = ff / (F0 * F1);
-    int g[3] = {org[0] + l[0], org[1] + l[1], org[2] + l[2]};
-    bool ok = g[D] <= a.hi[D] + 1;
-#pragma unroll
-    for (int e = 0; e < DIM; e++)
-        if (e != D) ok = ok && (g[e] <= a.hi[e]);
-    if (!ok) return 0.0;
-    // staged index of rel cell (f_d - 3 + q) is f_d + q along d
-    const int base = l[0] + S0 * (l[1] + S1 * l[2]);
-    VT u[6];
-    VT v[6];
-#pragma unroll
-    for (int q = 0; q < 6; q++) {
-        u[q] = sU[base + q * STR];
-        v[q] = sV[base + q * STR];
-    }
-    double F;
-    if constexpr (PREC == PREC_FP64) F = face_flux_fp64(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
-    else F = face_flux_mixed32(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
-    if (g[D] == a.domlo[D] && a.zlo[cls][D]) F = 0.0;
-    if (g[D] == a.domhi[D] + 1 && a.zhi[cls][D]) F = 0.0;
-    return F;
-}
-
-template <int DIM, int PREC, int MINB>
-__global__ void __launch_bounds__(Tile<DIM>::NTH, MINB) k_transport(const __grid_constant__ TransportArgs a)
-{
-    using G = TileGeom<DIM>;
-    using VT = typename VelT<PREC>::T;
-    constexpr int NTH = Tile<DIM>::NTH;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* sF = reinterpret_cast<double*>(smem_raw);
-    VT* sU = reinterpret_cast<VT*>(sF + G::FTOT);  // staged densities (FP32 in the mixed path)
-    VT* sV = sU + G::STOT;                          // staged drift velocities
-
-    const int tid = threadIdx.x;
-    int tb = blockIdx.x;
-    const int tix = tb % a.ntile[0];
-    tb /= a.ntile[0];
-    const int tiy = tb % a.ntile[1];
-    const int tiz = tb / a.ntile[1];
-    const int org[3] = {a.lo[0] + tix * G::T[0], a.lo[1] + tiy * G::T[1], a.lo[2] + tiz * G::T[2]};
-
-    // own cell
-    const int cx = tid % G::T[0], cy = (tid / G::T[0]) % G::T[1], cz = tid / (G::T[0] * G::T[1]);
-    const int gi = org[0] + cx, gj = org[1] + cy, gk = org[2] + cz;
-    const bool own = (tid < G::NCELL) && gi <= a.hi[0] && gj <= a.hi[1] && gk <= a.hi[2];
-    const int ns = a.ns;
-    const int64_t cs = a.sb.ns;
-    const int64_t own_o = own ? a.sb.off(gi, gj, gk) : 0;
-
-    double ne_new = 0.0, een_new = 0.0;
-    for (int it = 0; it < a.ntr; it++) {
-        const int s = a.tr_sp[it];
-        const int cls = a.tr_cls[it];
-        double acc = own ? a.rxn(gi, gj, gk, s) : 0.0;
-        if (a.tr_flux[it]) {
-            for (int c = tid; c < G::STOT; c += NTH) {
-                if (c < G::SOFF1) stage_cell<DIM, PREC, 0>(a, c, s, org, sU, sV);
-                else if (DIM > 1 && c < G::SOFF2)
-                    stage_cell<DIM, PREC, (DIM > 1 ? 1 : 0)>(a, c - G::SOFF1, s, org, sU + G::SOFF1, sV + G::SOFF1);
-                else if (DIM > 2)
-                    stage_cell<DIM, PREC, (DIM > 2 ? 2 : 0)>(a, c - G::SOFF2, s, org, sU + G::SOFF2, sV + G::SOFF2);
-            }
-            __syncthreads();
-            for (int f = tid; f < G::FTOT; f += NTH) {
-                double F;
-                if (f < G::FOFF1) F = face_of<DIM, PREC, 0>(a, f, cls, org, sU, sV);
-                else if (DIM > 1 && f < G::FOFF2)
-                    F = face_of<DIM, PREC, (DIM > 1 ? 1 : 0)>(a, f - G::FOFF1, cls, org, sU + G::SOFF1, sV + G::SOFF1);
-                else
-                    F = face_of<DIM, PREC, (DIM > 2 ? 2 : 0)>(a, f - G::FOFF2, cls, org, sU + G::SOFF2, sV + G::SOFF2);
-                sF[f] = F;
-            }
-            __syncthreads();
-            if (own) {
-                // dsdt = (Fx_lo - Fx_hi)/dx + rxn, then += y and z terms (ScalarSolve.cpp:45-51)
-                {
-                    constexpr int F0 = G::template FE<0>(0), F1 = G::template FE<0>(1);
-                    const int lo_f = cx + F0 * (cy + F1 * cz);
-                    acc = (sF[lo_f] - sF[lo_f + 1]) * a.idx[0] + acc;
-                }
-                if constexpr (DIM > 1) {
-                    constexpr int F0 = G::template FE<1>(0), F1 = G::template FE<1>(1);
-                    const int lo_f = G::FOFF1 + cx + F0 * (cy + F1 * cz);
-                    acc += (sF[lo_f] - sF[lo_f + F0]) * a.idx[1];
-                }
-                if constexpr (DIM > 2) {
-                    constexpr int F0 = G::template FE<2>(0), F1 = G::template FE<2>(1);
-                    const int lo_f = G::FOFF2 + cx + F0 * (cy + F1 * cz);
-                    acc += (sF[lo_f] - sF[lo_f + F0 * F1]) * a.idx[2];
-                }
-            }
-        }
-        if (own) {
-            if (s == ns) {
-                double jh = joule_cell<true>(a, DIM, gi, gj, gk);
-                acc += jh;
-                if (a.write_diag) {
-                    a.pn(gi, gj, gk, VD_EJH(ns)) = jh;
-                    a.pn(gi, gj, gk, VD_EIH(ns)) = a.rxn(gi, gj, gk, ns);
-                }
-            }
-            double nn = a.sb.p[own_o + s * cs] + a.dt * acc;
-            a.pn(gi, gj, gk, s) = nn;
-            if (a.dsdt.p) a.dsdt(gi, gj, gk, s) = acc;
-            if (s == a.e_id) ne_new = nn;
-            if (s == ns) een_new = nn;
-        }
-    }
-    if (!own) return;
-    for (int ib = 0; ib < a.nbg; ib++) {
-        const int s = a.bg_sp[ib];
-        double v = a.sb.p[own_o + s * cs];
-        double r = a.rxn(gi, gj, gk, s);
-        if (a.do_bg) {
-            v += r * a.dt;
-            if (v < a.min_spec && a.bound_specden) v = a.min_spec;
-        }
-        a.pn(gi, gj, gk, s) = v;
-        if (a.dsdt.p) a.dsdt(gi, gj, gk, s) = r;
-    }
-    if (a.update_te && a.elecenergy) {
-        // Source/ScalarSolve.cpp:659-666
-        double te = (2.0 / 3.0) / K_B * een_new / a.sb.p[own_o + a.e_id * cs];
-        if (te < a.min_te) {
-            te = a.min_te;
-            a.pn(gi, gj, gk, VD_EEN(ns)) = 1.5 * K_B * ne_new * te;
-        }
-        a.pn(gi, gj, gk, VD_ETEMP(ns)) = te;
-    }
+    if (dim == 1) { t[0] = DefaultTile<1>::T::X; t[1] = 1; t[2] = 1; }
+    else if (dim == 2) { t[0] = DefaultTile<2>::T::X; t[1] = DefaultTile<2>::T::Y; t[2] = 1; }
+    else { t[0] = DefaultTile<3>::T::X; t[1] = DefaultTile<3>::T::Y; t[2] = DefaultTile<3>::T::Z; }
 }
 
 template <int DIM, int PREC, int MINB>
 static cudaError_t launch_tr(const TransportArgs& a, cudaStream_t st)
 {
-    using G = TileGeom<DIM>;
-    using VT = typename VelT<PREC>::T;
-    constexpr size_t smem = (size_t)G::STOT * 2 * sizeof(VT) + (size_t)G::FTOT * sizeof(double);
+    constexpr size_t smem = transport_smem<DIM, PREC, typename DefaultTile<DIM>::T>();
     static unsigned attr_set = 0;  // one bit per device
     int dev = 0;
     cudaGetDevice(&dev);
@@ -670,7 +603,7 @@ static cudaError_t launch_tr(const TransportArgs& a, cudaStream_t st)
     }
     unsigned nt = (unsigned)a.ntile[0] * a.ntile[1] * a.ntile[2];
     ProfScope ps("k_transport", st);
-    k_transport<DIM, PREC, MINB><<<nt, Tile<DIM>::NTH, smem, st>>>(a);
+    k_transport<DIM, PREC, MINB><<<nt, DefaultTile<DIM>::T::NTH, smem, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -684,6 +617,12 @@ static int g_tr_minb[4][2] = {{2, 2}, {2, 2}, {2, 2}, {2, 2}};
 
 static int tr_minb_max(int dim) { return dim == 3 ? 2 : 4; }  // 512- vs 256-thread blocks
 
+// Tile-shape variant of the batched transport kernel per (dimension, precision),
+// the default for new batches ("batch_tile_<dim>d_<fp64|mixed>"; vd_batch_tune
+// stores its choice here).
+static int g_batch_tile[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+int batch_tile_variants(int dim);
+
 int tune_set(const char* key, int value)
 {
     for (int d = 1; d <= 3; d++)
@@ -693,6 +632,12 @@ int tune_set(const char* key, int value)
             if (strcmp(k, key) == 0) {
                 if (value < 1 || value > tr_minb_max(d)) return -1;
                 g_tr_minb[d][p] = value;
+                return 0;
+            }
+            snprintf(k, sizeof(k), "batch_tile_%dd_%s", d, p ? "mixed" : "fp64");
+            if (strcmp(k, key) == 0) {
+                if (value < 0 || value >= batch_tile_variants(d)) return -1;
+                g_batch_tile[d][p] = value;
                 return 0;
             }
         }
@@ -706,6 +651,8 @@ int tune_get(const char* key)
             char k[64];
             snprintf(k, sizeof(k), "transport_minblocks_%dd_%s", d, p ? "mixed" : "fp64");
             if (strcmp(k, key) == 0) return g_tr_minb[d][p];
+            snprintf(k, sizeof(k), "batch_tile_%dd_%s", d, p ? "mixed" : "fp64");
+            if (strcmp(k, key) == 0) return g_batch_tile[d][p];
         }
     return -2;
 }
@@ -732,6 +679,94 @@ cudaError_t launch_transport(const TransportArgs& a, int dim, int prec, cudaStre
     if (dim == 1) return launch_tr_v<1, PREC_FP64>(a, st);
     if (dim == 2) return launch_tr_v<2, PREC_FP64>(a, st);
     return launch_tr_v<3, PREC_FP64>(a, st);
+}
+
+// ---------------------------------------------------------------------------
+// Batched transport: tile-shape variants per dimension (chosen by the batch tuner).
+template <int DIM> struct BatchTiles;
+template <> struct BatchTiles<1> {
+    static constexpr int N = 2;
+    using V0 = TileShape<256, 1, 1, 256>;
+    using V1 = TileShape<128, 1, 1, 128>;
+    using V2 = V1;
+};
+template <> struct BatchTiles<2> {
+    static constexpr int N = 3;
+    using V0 = TileShape<32, 8, 1, 256>;
+    using V1 = TileShape<16, 16, 1, 256>;
+    using V2 = TileShape<64, 4, 1, 256>;
+};
+template <> struct BatchTiles<3> {
+    static constexpr int N = 2;
+    using V0 = TileShape<8, 8, 8, 512>;
+    using V1 = TileShape<16, 8, 4, 512>;
+    using V2 = V1;
+};
+
+int batch_tile_variants(int dim) { return dim == 1 ? BatchTiles<1>::N : dim == 2 ? BatchTiles<2>::N : BatchTiles<3>::N; }
+
+template <class TS> static void tile_of(int t[3]) { t[0] = TS::X; t[1] = TS::Y; t[2] = TS::Z; }
+
+template <int DIM> static void batch_tile_shape_d(int v, int t[3])
+{
+    if (v == 0) tile_of<typename BatchTiles<DIM>::V0>(t);
+    else if (v == 1) tile_of<typename BatchTiles<DIM>::V1>(t);
+    else tile_of<typename BatchTiles<DIM>::V2>(t);
+}
+
+void batch_tile_shape(int dim, int v, int t[3])
+{
+    if (dim == 1) batch_tile_shape_d<1>(v, t);
+    else if (dim == 2) batch_tile_shape_d<2>(v, t);
+    else batch_tile_shape_d<3>(v, t);
+}
+
+template <int DIM, int PREC, class TS>
+static cudaError_t launch_trb(const TransportArgs* boxes, const int2* items, int nitems, BatchCtl ctl, cudaStream_t st)
+{
+    constexpr int MINB = 2;
+    constexpr size_t smem = transport_smem<DIM, PREC, TS>();
+    auto fn = k_transport_batch<DIM, PREC, TS, MINB>;
+    static int grid_of[32] = {0};  // persistent grid (SMs x resident CTAs), per device
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int& grid = grid_of[dev & 31];
+    if (!grid) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        int nsm = 148, per_sm = 1;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, TS::NTH, smem);
+        if (e != cudaSuccess) return e;
+        grid = nsm * (per_sm < 1 ? 1 : per_sm);
+    }
+    int g = grid < nitems ? grid : nitems;
+    ProfScope ps("k_transport_batch", st);
+    fn<<<g, TS::NTH, smem, st>>>(boxes, items, nitems, ctl);
+    return cudaGetLastError();
+}
+
+template <int DIM, int PREC>
+static cudaError_t launch_trb_v(const TransportArgs* boxes, const int2* items, int nitems, BatchCtl ctl, int v,
+                                cudaStream_t st)
+{
+    if (v == 1) return launch_trb<DIM, PREC, typename BatchTiles<DIM>::V1>(boxes, items, nitems, ctl, st);
+    if (v == 2) return launch_trb<DIM, PREC, typename BatchTiles<DIM>::V2>(boxes, items, nitems, ctl, st);
+    return launch_trb<DIM, PREC, typename BatchTiles<DIM>::V0>(boxes, items, nitems, ctl, st);
+}
+
+cudaError_t launch_transport_batch(const TransportArgs* boxes, const int2* items, int nitems, BatchCtl ctl, int dim,
+                                   int prec, int variant, cudaStream_t st)
+{
+    if (nitems <= 0) return cudaSuccess;
+    if (prec == PREC_MIXED) {
+        if (dim == 1) return launch_trb_v<1, PREC_MIXED>(boxes, items, nitems, ctl, variant, st);
+        if (dim == 2) return launch_trb_v<2, PREC_MIXED>(boxes, items, nitems, ctl, variant, st);
+        return launch_trb_v<3, PREC_MIXED>(boxes, items, nitems, ctl, variant, st);
+    }
+    if (dim == 1) return launch_trb_v<1, PREC_FP64>(boxes, items, nitems, ctl, variant, st);
+    if (dim == 2) return launch_trb_v<2, PREC_FP64>(boxes, items, nitems, ctl, variant, st);
+    return launch_trb_v<3, PREC_FP64>(boxes, items, nitems, ctl, variant, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -29,7 +29,7 @@ struct TransportArgs {
     double uvel[3];
     int elecenergy, do_bg, bound_specden, floor_jh, const_ele_trans, cs_technique, gradne_from_state;
     int update_te, write_diag;
-    double min_spec, ele_mob, ele_diff, min_te, charge_e;
+    double min_spec, min_elec, ele_mob, ele_diff, min_te, charge_e;
     int ghost;  // stencil half width H (1, 2 or 3)
 };
 
@@ -43,7 +43,45 @@ struct PrepArgs {
     int do_reactions, write_n;
 };
 
+// Ghost refill of one box after a step: the components in comps[] of every
+// face-adjacent ghost cell (first-order extrapolation, or periodic wrap) --
+// what FillPatch does before the next step (Source/GridWork.cpp:112-140).
+struct GhostArgs {
+    A4 st;
+    int lo[3], hi[3];
+    int ghost, dim;
+    int periodic[3];
+    int ncomp;
+    int8_t comps[VD_MAX_SPECIES + 4];
+    int64_t count;  // number of ghost cells to fill
+};
+
 int upload_mech(const VdMechDev* h, cudaStream_t st);
+
+// Step control of a batched launch.  ctrl[c] = {steps case c takes in this call,
+// index (0/1) of the buffer holding its current state}.  At step t a work item of
+// case c is skipped when t >= ctrl[c].x; otherwise it uses the argument record
+// boxes[((t + ctrl[c].y) & 1) * nbox + c] (records of both buffer parities are
+// stored, so a captured graph replays unchanged while the per-case counts vary).
+struct BatchCtl {
+    const int2* ctrl;
+    int nbox;
+    int t;
+};
+
+// Batched launches over a work list of int2 items (box index, chunk or tile index).
+constexpr int kPrepChunk = 512;   // cells of the grown box per prep work item
+constexpr int kGhostChunk = 256;  // ghost cells per ghost work item
+cudaError_t launch_prep_batch(const PrepArgs* boxes, const int2* items, int nitems, BatchCtl ctl, int prec, int ns,
+                              cudaStream_t st);
+cudaError_t launch_transport_batch(const TransportArgs* boxes, const int2* items, int nitems, BatchCtl ctl, int dim,
+                                   int prec, int variant, cudaStream_t st);
+cudaError_t launch_ghost_batch(const GhostArgs* boxes, const int2* items, int nitems, BatchCtl ctl,
+                               cudaStream_t st);
+cudaError_t launch_ghost(const GhostArgs& a, cudaStream_t st);
+// tile shapes of the batched transport kernel: variant v of dimension dim
+int batch_tile_variants(int dim);
+void batch_tile_shape(int dim, int variant, int t[3]);
 
 cudaError_t launch_reaction_source(const BoxIdx& b, const A4& sb, const A4& rxn, double Tg, int prec, int ns,
                                    cudaStream_t st);
@@ -65,6 +103,8 @@ void transport_tile(int dim, int tile[3]);
 // Launch accounting: every launch increments a counter; when profiling is on it is
 // bracketed by CUDA events on its stream (see vd_profile_* in the header).
 int64_t launch_count();
+void add_launches(int64_t n);     // kernels run by a graph replay
+void prof_suspend(bool on);       // this thread: no event pairs (stream capture)
 void prof_enable(bool on);
 int prof_read(char* names, int names_len, int64_t* counts, double* ms, int max);
 
@@ -78,6 +118,8 @@ bool spec_active();
 void spec_set_enabled(bool on);
 const char* spec_error();
 cudaError_t spec_launch_prep(const PrepArgs& a, int prec, cudaStream_t st);
+cudaError_t spec_launch_prep_batch(const PrepArgs* boxes, const int2* items, int nitems, BatchCtl ctl, int prec,
+                                   cudaStream_t st);
 int spec_compile_only(const VdMechDev& m, size_t* cubin_bytes);
 
 struct ProfScope {

@@ -57,7 +57,16 @@ struct PrepArgs {
     double Tg;
     int do_reactions, write_n;
 };
-extern "C" __global__ void vd_spec_sizeof(unsigned long long* out) { out[0] = sizeof(PrepArgs); }
+struct BatchCtl {
+    const int2* ctrl;
+    int nbox;
+    int t;
+};
+extern "C" __global__ void vd_spec_sizeof(unsigned long long* out)
+{
+    out[0] = sizeof(PrepArgs);
+    out[1] = sizeof(BatchCtl);
+}
 // 2^x as FP32 from an FP64 exponent (same as exp2_split in vd_device.cuh)
 __device__ __forceinline__ float exp2_split(double x)
 {
@@ -110,14 +119,33 @@ std::string gen_prep_kernel(const VdMechDev& m, int prec)
     int minb = 65536 / (128 * (4 * ns + 48));
     minb = minb < 1 ? 1 : (minb > 8 ? 8 : minb);
     if (const char* e = getenv("VD_SPEC_MINBLOCKS")) minb = atoi(e);
-    o << "extern \"C\" __global__ void __launch_bounds__(128" << (minb > 0 ? ", " + std::to_string(minb) : "")
-      << ") vd_spec_prep_" << (prec == PREC_MIXED ? "mixed" : "fp64") << "(const PrepArgs a)\n{\n";
+    const std::string sfx = prec == PREC_MIXED ? "mixed" : "fp64";
+    const std::string lb = "__launch_bounds__(128" + (minb > 0 ? ", " + std::to_string(minb) : std::string()) + ")";
+    // per-box kernel (grid-stride over the grown box) and batched kernel (work list
+    // of (box, chunk of kPrepChunk cells)), both around one per-cell function
+    o << "__device__ __forceinline__ void vd_spec_cell_" << sfx << "(const PrepArgs& a, i64 idx);\n";
+    o << "extern \"C\" __global__ void " << lb << " vd_spec_prep_" << sfx << "(const PrepArgs a)\n{\n"
+      << "  const i64 ntot = (i64)(a.ghi[0] - a.glo[0] + 1) * (a.ghi[1] - a.glo[1] + 1) * (a.ghi[2] - a.glo[2] + 1);\n"
+      << "  for (i64 idx = blockIdx.x * (i64)blockDim.x + threadIdx.x; idx < ntot; idx += (i64)gridDim.x * blockDim.x)\n"
+      << "    vd_spec_cell_" << sfx << "(a, idx);\n}\n";
+    o << "extern \"C\" __global__ void " << lb << " vd_spec_prep_batch_" << sfx
+      << "(const PrepArgs* __restrict__ boxes, const int2* __restrict__ items, int nitems, const BatchCtl ctl)\n{\n"
+      << "  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {\n"
+      << "    const int2 w = items[it];\n"
+      << "    const int2 cc = ctl.ctrl[w.x];\n"
+      << "    if (ctl.t >= cc.x) continue;\n"
+      << "    const PrepArgs& a = boxes[((ctl.t + cc.y) & 1) * ctl.nbox + w.x];\n"
+      << "    const i64 ntot = (i64)(a.ghi[0] - a.glo[0] + 1) * (a.ghi[1] - a.glo[1] + 1) * (a.ghi[2] - a.glo[2] + 1);\n"
+      << "    for (int q = threadIdx.x; q < " << kPrepChunk << "; q += blockDim.x) {\n"
+      << "      const i64 idx = (i64)w.y * " << kPrepChunk << " + q;\n"
+      << "      if (idx < ntot) vd_spec_cell_" << sfx << "(a, idx);\n"
+      << "    }\n  }\n}\n";
+    o << "__device__ __forceinline__ void vd_spec_cell_" << sfx << "(const PrepArgs& a, i64 idx)\n{\n";
     o << "  const double N_A = " << hexd(N_A) << ", NA_CE = " << hexd(NA_CE) << ", KB_CE = " << hexd(KB_CE)
       << ", K_B = " << hexd(K_B) << ";\n";
-    o << "  const int gx = a.ghi[0] - a.glo[0] + 1, gy = a.ghi[1] - a.glo[1] + 1, gz = a.ghi[2] - a.glo[2] + 1;\n"
-         "  const i64 ntot = (i64)gx * gy * gz;\n"
+    o << "  const int gx = a.ghi[0] - a.glo[0] + 1, gy = a.ghi[1] - a.glo[1] + 1;\n"
          "  const i64 cs = a.sb.ns, rs = a.rxn.ns;\n"
-         "  for (i64 idx = blockIdx.x * (i64)blockDim.x + threadIdx.x; idx < ntot; idx += (i64)gridDim.x * blockDim.x) {\n"
+         "  {\n"
          "    int k = (int)(idx / ((i64)gx * gy));\n"
          "    i64 r = idx - (i64)k * gx * gy;\n"
          "    int j = (int)(r / gx);\n"
@@ -128,11 +156,11 @@ std::string gen_prep_kernel(const VdMechDev& m, int prec)
     o << "    double N = 0.0;\n";
     for (int s = 0; s < ns; s++) o << "    N += n" << s << ";\n";
     o << "    if (a.write_n) a.Nv.p[a.Nv.off(i, j, k)] = N;\n"
-         "    if (i < a.lo[0] || i > a.hi[0] || j < a.lo[1] || j > a.hi[1] || k < a.lo[2] || k > a.hi[2]) continue;\n"
+         "    if (i < a.lo[0] || i > a.hi[0] || j < a.lo[1] || j > a.hi[1] || k < a.lo[2] || k > a.hi[2]) return;\n"
          "    double* rx = a.rxn.p + a.rxn.off(i, j, k);\n"
          "    if (!a.do_reactions) {\n";
     for (int s = 0; s <= ns; s++) o << "      rx[" << s << " * rs] = 0.0;\n";
-    o << "      continue;\n    }\n";
+    o << "      return;\n    }\n";
     o << "    const double Te = p[" << (ns + 1) << " * cs];\n    const double Tg = a.Tg;\n";
     for (int s = 0; s < ns; s++) o << "    const double sc" << s << " = n" << s << " * 1.0e-6 / N_A * 1.0e6;\n";
     for (int s = 0; s < ns; s++) o << "    double w" << s << " = 0.0;\n";
@@ -191,6 +219,7 @@ std::string gen_prep_kernel(const VdMechDev& m, int prec)
 struct SpecModule {
     cudaLibrary_t lib = nullptr;
     cudaKernel_t prep[2] = {nullptr, nullptr};
+    cudaKernel_t batch[2] = {nullptr, nullptr};
 };
 
 std::mutex g_spec_mu;
@@ -259,19 +288,21 @@ int spec_build(const VdMechDev& m)
     cudaError_t e = cudaLibraryLoadData(&mod->lib, bin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
     if (e == cudaSuccess) e = cudaLibraryGetKernel(&mod->prep[PREC_FP64], mod->lib, "vd_spec_prep_fp64");
     if (e == cudaSuccess) e = cudaLibraryGetKernel(&mod->prep[PREC_MIXED], mod->lib, "vd_spec_prep_mixed");
+    if (e == cudaSuccess) e = cudaLibraryGetKernel(&mod->batch[PREC_FP64], mod->lib, "vd_spec_prep_batch_fp64");
+    if (e == cudaSuccess) e = cudaLibraryGetKernel(&mod->batch[PREC_MIXED], mod->lib, "vd_spec_prep_batch_mixed");
     if (e == cudaSuccess) {
         // layout check of the kernel argument struct
         cudaKernel_t sz;
         unsigned long long* d = nullptr;
-        unsigned long long h = 0;
+        unsigned long long h[2] = {0, 0};
         e = cudaLibraryGetKernel(&sz, mod->lib, "vd_spec_sizeof");
         if (e == cudaSuccess) e = cudaMalloc(&d, sizeof(h));
         if (e == cudaSuccess) {
             void* args[] = {&d};
             e = cudaLaunchKernel((const void*)sz, dim3(1), dim3(1), args, 0, 0);
-            if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
+            if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
             cudaFree(d);
-            if (e == cudaSuccess && h != sizeof(PrepArgs)) {
+            if (e == cudaSuccess && (h[0] != sizeof(PrepArgs) || h[1] != sizeof(BatchCtl))) {
                 g_spec_err = "specialised kernel argument layout differs";
                 return 4;
             }
@@ -333,6 +364,22 @@ cudaError_t spec_launch_prep(const PrepArgs& a, int prec, cudaStream_t st)
     void* args[] = {&copy};
     ProfScope ps("k_prep_spec", st);
     return cudaLaunchKernel((const void*)k, dim3((unsigned)g), dim3(128), args, 0, st);
+}
+
+// Batched form: boxes and items are device arrays; one CTA per work item (grid-stride).
+cudaError_t spec_launch_prep_batch(const PrepArgs* boxes, const int2* items, int nitems, BatchCtl ctl, int prec,
+                                   cudaStream_t st)
+{
+    cudaKernel_t k;
+    {
+        std::lock_guard<std::mutex> lk(g_spec_mu);
+        if (!g_active) return cudaErrorNotReady;
+        k = g_active->batch[prec == PREC_MIXED ? PREC_MIXED : PREC_FP64];
+    }
+    unsigned g = (unsigned)(nitems < 148 * 16 ? nitems : 148 * 16);
+    void* args[] = {(void*)&boxes, (void*)&items, &nitems, &ctl};
+    ProfScope ps("k_prep_batch_spec", st);
+    return cudaLaunchKernel((const void*)k, dim3(g), dim3(128), args, 0, st);
 }
 
 }  // namespace vd

@@ -304,3 +304,51 @@ def config_precision3d(seed: int = BASE_SEED, n=(128, 128, 128), n_species: int 
     return build_case(mech, 3, n, (1e-5, 1e-5, 1e-5), seed + 12, density="loguniform_smooth",
                       dens_range=(1e8, 1e22), te_range_ev=(0.3, 10.0), voltage=1000.0,
                       params=dict(dt=1e-12))
+
+
+def face_gradients(case: BoxCase, state: np.ndarray) -> list:
+    """gradne_fc[d] = (ne_i - ne_{i-1}) / dx_d on the face box of direction d, from
+    the electron density of `state` (laid out like case.state)."""
+    g = case.gvec
+    n = case.n
+    ne = state[case.mech.e_id]
+    out = []
+    for d in range(3):
+        if d >= case.dim:
+            out.append(np.zeros((1, n[2], n[1], n[0])))
+            continue
+        ax = 2 - d
+        fn = [n[2], n[1], n[0]]
+        fn[ax] += 1
+        sl_r = [slice(g[2], g[2] + n[2]), slice(g[1], g[1] + n[1]), slice(g[0], g[0] + n[0])]
+        sl_r[ax] = slice(sl_r[ax].start, sl_r[ax].stop + 1)
+        sl_l = list(sl_r)
+        sl_l[ax] = slice(sl_r[ax].start - 1, sl_r[ax].stop - 1)
+        out.append(np.ascontiguousarray(((ne[tuple(sl_r)] - ne[tuple(sl_l)]) / case.dx[d]).reshape((1,) + tuple(fn))))
+    return out
+
+
+# parameters of a case that takes many steps: the state evolves, so the Joule
+# term's density gradient is taken from it, Te follows the energy, and densities
+# are clipped at the floors as the species solve does
+MULTISTEP_PARAMS = dict(dt=1e-12, gradne_from_state=1, update_te=1, bound_specden=1)
+
+
+def config_batched(seed: int = BASE_SEED, n_cases: int = 64, side=(64, 512), n_species: int = 8,
+                   n_reactions: int = 40, dens_range=(1e10, 1e18)):
+    """Batched workload: n_cases independent 2-D cases, each side length drawn
+    log-uniform in `side` (uneven boxes), one shared 8-species / 40-reaction
+    synthetic mechanism, densities log-uniform (spatially correlated) in
+    dens_range, Te 0.3-10 eV, 1 kV ramp + 5 % noise, dx = 1e-5 m.  Returns
+    (mechanism, [BoxCase])."""
+    mech = synthetic(n_species, n_reactions, seed + 21)
+    rng = np.random.default_rng(seed + 22)
+    lo, hi = np.log(side[0]), np.log(side[1])
+    cases = []
+    for i in range(n_cases):
+        nx = int(round(float(np.exp(rng.uniform(lo, hi)))))
+        ny = int(round(float(np.exp(rng.uniform(lo, hi)))))
+        cases.append(build_case(mech, 2, (nx, ny), (1e-5, 1e-5), seed + 1000 + i, density="loguniform_smooth",
+                                dens_range=dens_range, te_range_ev=(0.3, 10.0), voltage=1000.0,
+                                params=dict(MULTISTEP_PARAMS)))
+    return mech, cases
