@@ -42,6 +42,8 @@ sys.path.insert(0, str(ROOT))
 WORKLOADS = {
     "precision3d": "3-D 128^3 box, 24 species / 150 reactions, WENO-Z, one explicit step",
     "argon2d": "2-D 256^2 box, E/Ar+/Ar*/Ar, 10 reactions, WENO-Z, one explicit step",
+    "batched": "64 independent 2-D cases, sides log-uniform 64-512, 8 species / 40 reactions, "
+               "WENO-Z, 20 explicit steps per case per solve",
 }
 
 
@@ -59,6 +61,8 @@ def parse():
                     help="run W+K mixed-precision updates and nothing else (the command ncu profiles)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="precision of the --only-update run")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched-workload measurement added to the default line")
     return ap.parse_args()
 
 
@@ -174,6 +178,8 @@ def run_reference(args):
         return 0
     threads = os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(threads)
+    if args.workload == "batched":
+        return run_reference_batched(args, threads)
     case = make_case(args.workload)
     lib, kind, run, nplanes, cpp = cpu_reference_rate(case, max(1.0, args.cpu_seconds / max(1, args.steps)))
     for _ in range(args.warmup):
@@ -191,6 +197,50 @@ def run_reference(args):
                        "reactions": len(case.mech.reactions)},
             "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": kind,
                              "sample": sample},
+            "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_batched(args, threads: int):
+    """The reference's own code on the batched workload: each step updates a
+    bounded sample of the cases (smallest first) by one explicit step."""
+    import oracle
+    from vidyut_b200 import inputs
+    mech, cases = inputs.config_batched()
+    try:
+        lib, kind = oracle.RefLib(mech.name, 2), "reference"
+    except FileNotFoundError:
+        lib, kind = oracle.Port(mech), "port"
+    budget = max(1.0, args.cpu_seconds / max(1, args.steps))
+    order = sorted(cases, key=lambda c: c.ncell)
+    sample, t = [], 0.0
+    for c in order:  # choose the sample once, by timing one step of each
+        t0 = time.perf_counter()
+        lib.update_all(c, c.vd_params())
+        t += time.perf_counter() - t0
+        sample.append(c)
+        if t >= budget:
+            break
+    for _ in range(args.warmup):
+        for c in sample:
+            lib.update_all(c, c.vd_params())
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for c in sample:
+            lib.update_all(c, c.vd_params())
+    t = time.perf_counter() - t0
+    cells = sum(c.ncell for c in sample)
+    value = cells * args.steps / t
+    line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": WORKLOADS["batched"], "cases": len(cases),
+                       "cells": sum(c.ncell for c in cases)},
+            "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": kind,
+                             "sample": f"one explicit step of {len(sample)} of {len(cases)} cases "
+                                       f"({cells} cells) per step"},
             "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -378,6 +428,19 @@ def run_ours(args):
                 "kernel_share": kms / sum(v[1] for v in prof.values()),
                 "step_achieved_gbs": alg["step"] * cells / (ms_mixed * 1e-3) / 1e9}
 
+    batched = None
+    if not args.no_batched and world == 1 and args.workload == "precision3d":
+        dc = phi_new = None  # free the 3-D case's device memory
+        torch.cuda.empty_cache()
+        r = measure_batched(args.steps, args.warmup, e2e=not args.no_e2e)
+        api.mech_init(case.mech)
+        batched = {k: r[k] for k in ("value", "ms_per_solve", "solves_per_s", "cases", "cells", "steps_per_solve",
+                                     "speedup_vs_plain_fp64", "plain_fp64", "batched_fp64",
+                                     "mixed_vs_fp64_max_rel", "roofline", "tile_2d", "gpu_launches", "e2e",
+                                     "kernels_ms_per_launch") if k in r}
+        batched["unit"] = "cell-updates/s"
+        batched["workload"] = WORKLOADS["batched"]
+
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         threads = os.cpu_count() or 1
@@ -411,7 +474,216 @@ def run_ours(args):
                                 "max_rel_to_step_scale_per_species": [float(x) for x in err_scaled],
                                 "max_rel": float(np.max(err_max)),
                                 "max_rel_to_step_scale": float(np.max(err_scaled))},
+        "batched": batched,
     }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+BATCH_STEPS = 20  # explicit steps per case in one batched solve
+
+
+def measure_batched(steps: int, warmup: int, *, cpu_seconds: float = 0.0, e2e: bool = True,
+                    plain_fp64: bool = True) -> dict:
+    """The batched workload on one GPU.  One bench step = one solve of every case:
+    its state is re-loaded from a device-resident copy of its initial state and the
+    batch takes BATCH_STEPS steps (one graph replay).  Returns the measurements."""
+    import numpy as np
+    import torch
+
+    from vidyut_b200 import _abi as abi
+    from vidyut_b200 import api, inputs
+
+    L = abi.lib()
+    mech, cases = inputs.config_batched()
+    api.mech_init(mech)
+    stream = torch.cuda.current_stream()
+    cells = sum(c.ncell for c in cases)
+    H = 3
+    init_host = [torch.from_numpy(api.trim_ghosts(c, c.state, H)).pin_memory() for c in cases]
+    init_dev = [h.cuda() for h in init_host]
+
+    def make_batch(prec):
+        need = sum(api.Batch.case_bytes(c, c.vd_params(precision=prec)) for c in cases)
+        b = api.Batch(prec, budget_bytes=int(need * 1.05) + (64 << 20), max_cases=len(cases))
+        ids = [b.add(c, c.vd_params(precision=prec), nsteps=BATCH_STEPS) for c in cases]
+        return b, ids
+
+    def solve(b, ids, src):
+        for i, cid in enumerate(ids):
+            b.load(cid, src[i], nsteps=BATCH_STEPS)
+        b.step(BATCH_STEPS)
+
+    def timed(fn, k, w):
+        for _ in range(w):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n0 = L.vd_launch_count()
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k, L.vd_launch_count() - n0
+
+    out = {"cases": len(cases), "cells": cells, "steps_per_solve": BATCH_STEPS,
+           "sides": [list(c.n[:2]) for c in cases]}
+    bm, idm = make_batch(abi.PREC_MIXED)
+    tune_ms = bm.tune(trials=3)
+    out["tuner_ms"] = {f"{d}d_v{v}": round(ms, 4) for (d, v), ms in tune_ms.items()}
+    out["tile_variant_2d"] = bm.stats()["tile_variant"][2]
+    out["tile_2d"] = list(api.batch_tile_shape(2, out["tile_variant_2d"])[0][:2])
+    clock = ClockSampler(torch.cuda.current_device())
+    clock.start()
+    ms, launches = timed(lambda: solve(bm, idm, init_dev), steps, warmup)
+    out["clocks"] = clock.stop()
+    out["ms_per_solve"] = ms
+    out["value"] = cells * BATCH_STEPS / (ms * 1e-3)
+    out["solves_per_s"] = len(cases) / (ms * 1e-3)
+    out["gpu_launches"] = int(launches)
+    out["graph_builds"] = bm.stats()["graph_builds"]
+
+    # per-kernel device time (direct launches so that every launch has its events)
+    bm.set_graph(False)
+    L.vd_profile_enable(1)
+    solve(bm, idm, init_dev)
+    torch.cuda.synchronize()
+    prof = abi.profile_read()
+    L.vd_profile_enable(0)
+    bm.set_graph(True)
+    out["kernels_ms_per_launch"] = {k: v[1] / v[0] for k, v in prof.items()}
+    out["kernels_launches"] = {k: v[0] for k, v in prof.items()}
+    mixed_final = [bm.read(i, out=torch.empty_like(init_dev[n])) for n, i in enumerate(idm)]
+
+    # the same batch machinery in FP64, and the mixed result's error against it
+    b64, id64 = make_batch(abi.PREC_FP64)
+    ms64, _ = timed(lambda: solve(b64, id64, init_dev), max(2, steps // 2), 1)
+    out["batched_fp64"] = {"ms_per_solve": ms64, "value": cells * BATCH_STEPS / (ms64 * 1e-3)}
+    solve(b64, id64, init_dev)
+    solve(bm, idm, init_dev)
+    ns = mech.ns
+    comps = list(range(ns)) + [abi.EEN(ns), abi.ETEMP(ns)]
+    errs = np.zeros(len(comps))
+    for n, (i64, im) in enumerate(zip(id64, idm)):
+        c = cases[n]
+        a = bm.read(im, out=torch.empty_like(init_dev[n]))
+        r = b64.read(i64, out=torch.empty_like(init_dev[n]))
+        sl = (comps, slice(None), slice(H, H + c.n[1]), slice(H, H + c.n[0]))
+        e = ((a[sl] - r[sl]).abs() / r[sl].abs().clamp_min(1e-300)).reshape(len(comps), -1).max(1).values
+        errs = np.maximum(errs, e.cpu().numpy())
+    out["mixed_vs_fp64_max_rel"] = {"per_component": [float(x) for x in errs], "max": float(errs.max()),
+                                    "components": "species 0..NS-1, EEN, ETEMP; all cells of all cases "
+                                                  f"after {BATCH_STEPS} steps"}
+    b64.close()
+    del mixed_final
+
+    # plain FP64 per-box path, case by case (vd_explicit_update_all + vd_fill_ghosts)
+    if plain_fp64:
+        dcs = [api.upload(c) for c in cases]
+        outs = [dc.new_outputs()[0] for dc in dcs]
+        init_full = [dc.state.clone() for dc in dcs]
+        g = H
+
+        def plain_solve():
+            for dc, pn, st0, c in zip(dcs, outs, init_full, cases):
+                dc.state.copy_(st0, non_blocking=True)
+                prm = c.vd_params(precision=abi.PREC_FP64)
+                v = dc.state[:, :, g:g + c.n[1], g:g + c.n[0]]
+                for _ in range(BATCH_STEPS):
+                    api.explicit_update_all(dc, prm, pn)
+                    v.copy_(pn)
+                    api.fill_ghosts(dc.state, c, H, comps, c.periodic)
+
+        msp, _ = timed(plain_solve, 2, 1)
+        out["plain_fp64"] = {"ms_per_solve": msp, "value": cells * BATCH_STEPS / (msp * 1e-3),
+                             "path": "per case: 20 x (vd_explicit_update_all FP64 + vd_fill_ghosts)"}
+        out["speedup_vs_plain_fp64"] = msp / ms
+        del dcs, outs, init_full
+
+    # end to end: states from pinned host memory, results back to pinned host memory
+    if e2e:
+        res_host = [torch.empty_like(h).pin_memory() for h in init_host]
+
+        def e2e_solve():
+            solve(bm, idm, init_host)
+            for n, i in enumerate(idm):
+                bm.read(i, out=res_host[n])
+
+        mse, _ = timed(e2e_solve, max(3, steps // 2), 1)
+        nbytes = sum(h.numel() * 8 for h in init_host)
+        out["e2e"] = {"value": cells * BATCH_STEPS / (mse * 1e-3), "unit": "cell-updates/s", "ms_per_solve": mse,
+                      "h2d_bytes_per_step": int(nbytes), "d2h_bytes_per_step": int(nbytes),
+                      "path": "vd_batch_load_case from pinned host, vd_batch_step, vd_batch_read_case "
+                              "to pinned host, inside the timing"}
+    bm.close()
+
+    # roofline of the dominant batched kernel: algorithmic bytes per cell-update
+    dom = max(prof.items(), key=lambda kv: kv[1][1])
+    kname, (kcount, kms) = dom
+    per_launch = kms / kcount
+    alg = algorithmic_bytes_per_cell(cases[0])
+    abytes = {"k_transport_batch": alg["step"], "k_prep_batch": alg["k_prep"],
+              "k_prep_batch_spec": alg["k_prep"]}.get(kname, alg["step"])
+    achieved = abytes * cells / (per_launch * 1e-3) / 1e9
+    out["roofline"] = {"kernel": kname, "achieved": achieved, "unit": "GB/s", "kernel_ms": per_launch,
+                       "kernel_share": kms / sum(v[1] for v in prof.values()),
+                       "alg_bytes_per_cell": abytes}
+
+    if cpu_seconds > 0:
+        import oracle
+        name = mech.name
+        threads = os.cpu_count() or 1
+        try:
+            lib = oracle.RefLib(name, 2)
+            kind = "reference"
+        except FileNotFoundError:
+            lib = oracle.Port(mech)
+            kind = "port"
+        done_cells, t = 0, 0.0
+        for c in sorted(cases, key=lambda c: c.ncell):
+            t0 = time.perf_counter()
+            lib.update_all(c, c.vd_params())
+            t += time.perf_counter() - t0
+            done_cells += c.ncell
+            if t >= cpu_seconds:
+                break
+        out["cpu_baseline"] = {"value": done_cells / t, "unit": "cell-updates/s", "cores": threads, "kind": kind,
+                               "sample": f"one step of {done_cells} cells (smallest cases first), {t:.1f} s"}
+    return out
+
+
+def run_batched_line(args):
+    import torch
+    from vidyut_b200 import _abi as abi
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1 and int(os.environ.get("RANK", "0")) != 0:
+        return 0  # replicas only: the batched workload is measured on one GPU
+    r = measure_batched(args.steps, args.warmup, cpu_seconds=0.0 if args.no_cpu_baseline else args.cpu_seconds,
+                        e2e=not args.no_e2e)
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    roof = dict(r["roofline"])
+    roof.update({"bound": "hbm", "peak": hbm, "frac": roof["achieved"] / hbm,
+                 "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback",
+                 "traffic": read_profile_traffic(roof["kernel"], "batched")})
+    line = {"metric": "cell-updates/s", "value": r["value"], "unit": "cell-updates/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_solve"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32/f64 (mixed: FP32 WENO, rates, fluxes; FP64 accumulate)", "data": "synthetic",
+            "config": {"workload": WORKLOADS["batched"], "cases": r["cases"], "cells": r["cells"],
+                       "steps_per_solve": BATCH_STEPS, "species": 8, "reactions": 40,
+                       "l2": "inputs larger than L2 (two state copies of 3M cells x 18 comps)"},
+            "roofline": roof, "cpu_baseline": r.get("cpu_baseline"), "e2e": r.get("e2e"),
+            "gpu_launches": r["gpu_launches"], "clocks": r["clocks"],
+            "solves_per_s": r["solves_per_s"], "speedup_vs_plain_fp64": r.get("speedup_vs_plain_fp64"),
+            "plain_fp64": r.get("plain_fp64"), "batched_fp64": r["batched_fp64"],
+            "mixed_vs_fp64_max_rel": r["mixed_vs_fp64_max_rel"], "tuner_ms": r["tuner_ms"],
+            "tile_2d": r["tile_2d"], "kernels_ms_per_launch": r["kernels_ms_per_launch"]}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -420,6 +692,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batched" and not args.only_update:
+        return run_batched_line(args)
     return run_ours(args)
 
 

@@ -351,6 +351,11 @@ int      vd_batch_remove_case(vd_batch* b, int32_t case_id);
 int      vd_batch_step(vd_batch* b, int nsteps, void* stream);
 int      vd_batch_case_info(vd_batch* b, int32_t case_id, int64_t* steps_done, int64_t* steps_left);
 int      vd_batch_read_case(vd_batch* b, int32_t case_id, double* state, void* stream);
+/* replaces a resident case's state (same layout as add; both copies are written)
+ * and restarts its step count with nsteps; the arena region and the captured
+ * graph are kept, so this is the cheap way to start a new solve of the same shape */
+int      vd_batch_load_case(vd_batch* b, int32_t case_id, const double* state, int64_t nsteps,
+                            void* stream);
 /* autotuner: times the transport kernel of each tile variant on the resident cases
  * (trials launches each; the state is not advanced), keeps the fastest per
  * dimension and makes it the default of later batches.  ms_out (16 doubles or

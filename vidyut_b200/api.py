@@ -279,6 +279,14 @@ class Batch:
                   "vd_batch_read_case")
         return out
 
+    def load(self, cid: int, state, nsteps: int = -1, stream=None) -> None:
+        """Replace the case's state (a device tensor or host array in the batch
+        layout, see read) and restart its step count."""
+        src = state if isinstance(state, torch.Tensor) else np.ascontiguousarray(state)
+        ptr = src.data_ptr() if isinstance(src, torch.Tensor) else src.ctypes.data
+        abi.check(abi.lib().vd_batch_load_case(self._h, int(cid), ptr, int(nsteps), _stream(stream)),
+                  "vd_batch_load_case")
+
     def tune(self, trials: int = 5, stream=None) -> dict:
         ms = (C.c_double * 16)()
         abi.check(abi.lib().vd_batch_tune(self._h, int(trials), _stream(stream), ms), "vd_batch_tune")

@@ -732,6 +732,31 @@ int vd_batch_read_case(vd_batch* b, int32_t case_id, double* state, void* stream
     return VD_OK;
 }
 
+int vd_batch_load_case(vd_batch* b, int32_t case_id, const double* state, int64_t nsteps, void* stream)
+{
+    if (!b || !state) return err(VD_ERR_ARG, "null argument");
+    int rc = check_device(b);
+    if (rc) return rc;
+    int c = slot_of(b, case_id);
+    if (c < 0) return err(VD_ERR_ARG, "no case %d in the batch", case_id);
+    Case& k = b->cases[c];
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = b->pending ? cudaStreamWaitEvent(st, b->last_done, 0) : cudaSuccess;
+    const size_t sbytes = (size_t)k.L.gcells * VD_NVAR(b->mech.ns) * sizeof(double);
+    // both copies: the fields a step only reads (E, potential, ...) are read from
+    // whichever copy is current
+    char* cur = b->arena_base + k.off + k.L.st[k.cur];
+    char* oth = b->arena_base + k.off + k.L.st[k.cur ^ 1];
+    if (e == cudaSuccess) e = cudaMemcpyAsync(cur, state, sbytes, cudaMemcpyDefault, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(oth, cur, sbytes, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaEventRecord(b->last_done, st);
+    if (e != cudaSuccess) return cuda_err(e, "loading the case");
+    b->pending = true;
+    k.steps_done = 0;
+    k.steps_left = nsteps;
+    return VD_OK;
+}
+
 int vd_batch_set_tile_variant(vd_batch* b, int dim, int variant)
 {
     if (!b) return err(VD_ERR_ARG, "null batch");
