@@ -692,9 +692,39 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
-    if args.workload == "batched" and not args.only_update:
+    if args.workload == "batched":
+        if args.only_update:
+            return run_batched_only(args)
         return run_batched_line(args)
     return run_ours(args)
+
+
+def run_batched_only(args):
+    """W + K batched solves and nothing else (the command ncu profiles); graph
+    replay off so that every kernel is a separate launch."""
+    import torch
+    from vidyut_b200 import _abi as abi
+    from vidyut_b200 import api, inputs
+    mech, cases = inputs.config_batched()
+    api.mech_init(mech)
+    prec = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
+    need = sum(api.Batch.case_bytes(c, c.vd_params(precision=prec)) for c in cases)
+    with api.Batch(prec, budget_bytes=int(need * 1.05) + (64 << 20), max_cases=len(cases)) as b:
+        b.set_graph(False)
+        ids = [b.add(c, c.vd_params(precision=prec), nsteps=-1) for c in cases]
+        for _ in range(args.warmup):
+            b.step(1)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            b.step(1)
+        e1.record()
+        torch.cuda.synchronize()
+        print(json.dumps({"only_update": True, "workload": "batched", "precision": args.precision,
+                          "ms_per_batch_step": e0.elapsed_time(e1) / max(1, args.steps),
+                          "cells": sum(c.ncell for c in cases), "cases": len(ids)}), flush=True)
+    return 0
 
 
 if __name__ == "__main__":

@@ -146,6 +146,13 @@ void fill_class_flags(const vd_params* p, int8_t zlo[4][3], int8_t zhi[4][3])
         }
 }
 
+// fluxed / unfluxed species lists and velocity bases of a transport record
+void finish_lists(TransportArgs& a)
+{
+    std::lock_guard<std::mutex> lk(g_mech_mu);
+    finish_species_lists(a, *g_mech_dev);
+}
+
 int species_class(const vd_mech* m, int s)
 {
     if (s == m->nspecies) return VD_CLASS_ENERGY;
@@ -619,6 +626,7 @@ int vd_explicit_update_all(const vd_box* bx, vd_array4 sborder, const vd_array4 
         a.tr_flux[a.ntr] = (prm->do_transport && has_vel) ? 1 : 0;
         a.ntr++;
     }
+    finish_lists(a);
 
     // scratch: N on the grown box, rxn on the valid box when the caller does not keep it
     const int64_t gn = (int64_t)(ghi[0] - glo[0] + 1) * (ghi[1] - glo[1] + 1) * (ghi[2] - glo[2] + 1);
@@ -879,6 +887,7 @@ extern "C" int vd_explicit_update_all_noalloc(const vd_box* bx, vd_array4 sborde
         a.tr_flux[a.ntr] = (prm->do_transport && has_vel) ? 1 : 0;
         a.ntr++;
     }
+    finish_lists(a);
     A4 Nv;
     Nv.p = scratch;
     Nv.bx = glo[0];
@@ -983,6 +992,7 @@ void fill_transport_args(TransportArgs& a, const vd_box* bx, const vd_params* p,
         a.tr_flux[a.ntr] = (p->do_transport && has_vel) ? 1 : 0;
         a.ntr++;
     }
+    finish_lists(a);
 }
 
 int stencil_halo(int hyp_order) { return ::stencil_halo(hyp_order); }

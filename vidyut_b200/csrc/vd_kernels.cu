@@ -581,6 +581,63 @@ cudaError_t launch_prep(const PrepArgs& a, int prec, int ns, cudaStream_t st)
 #include "vd_transport.cuh"
 namespace vd {
 
+// The mobility models of specMob (test/models/Ar_DC_1d/Chemistry.H:177-202) as a
+// species constant K times a per-cell basis: electron-type mu = c/(sqrt(Te) N s0)
+// gives K = c/s0 on E/(sqrt(Te) N); ion-type mu = c/(sqrt(Tg) N s0) gives
+// K = c/(sqrt(Tg) s0) on E/N; mu = p0/N gives K = p0 on E/N; a constant mu gives
+// K = p0 on E; a scaled model multiplies its reference's K.
+static bool velocity_basis(const VdMechDev& m, int s, double Tg, int* kind, double* K)
+{
+    double scale = 1.0;
+    int k = m.mob_kind[s];
+    if (k == VD_MOB_SCALED) {
+        scale = m.mob_p0[s];
+        s = m.mob_ref[s];
+        k = m.mob_kind[s];
+    }
+    switch (k) {
+    case VD_MOB_ELECTRON: *kind = 0; *K = scale * (m.mob_c[s] / m.mob_p0[s]); return true;
+    case VD_MOB_ION_TG: *kind = 1; *K = scale * (m.mob_c[s] / (std::sqrt(Tg) * m.mob_p0[s])); return true;
+    case VD_MOB_CONST_N: *kind = 1; *K = scale * m.mob_p0[s]; return true;
+    case VD_MOB_CONST: *kind = 2; *K = scale * m.mob_p0[s]; return true;
+    default: return false;
+    }
+}
+
+void finish_species_lists(TransportArgs& a, const VdMechDev& m)
+{
+    a.nfl = a.nnf = a.nb = 0;
+    int slot_of_kind[3] = {-1, -1, -1};
+    for (int it = 0; it < a.ntr; it++) {
+        const int s = a.tr_sp[it];
+        if (!a.tr_flux[it]) {
+            a.nf_sp[a.nnf++] = (int8_t)s;
+            continue;
+        }
+        int kind = 0;
+        double K = 0.0;
+        int slot = -1;
+        if (a.udv) {
+            K = 1.0;  // v = the user velocity of the sweep direction
+        } else {
+            if (!velocity_basis(m, s, a.Tg, &kind, &K)) {
+                a.nf_sp[a.nnf++] = (int8_t)s;
+                continue;
+            }
+            if (slot_of_kind[kind] < 0) {
+                slot_of_kind[kind] = a.nb;
+                a.bkind[a.nb++] = (int8_t)kind;
+            }
+            slot = slot_of_kind[kind];
+        }
+        a.fl_sp[a.nfl] = (int8_t)s;
+        a.fl_cls[a.nfl] = a.tr_cls[it];
+        a.fl_slot[a.nfl] = (int8_t)slot;
+        a.fl_K[a.nfl] = K;
+        a.nfl++;
+    }
+}
+
 void transport_tile(int dim, int t[3])
 {
     if (dim == 1) { t[0] = DefaultTile<1>::T::X; t[1] = 1; t[2] = 1; }
@@ -591,13 +648,14 @@ void transport_tile(int dim, int t[3])
 template <int DIM, int PREC, int MINB>
 static cudaError_t launch_tr(const TransportArgs& a, cudaStream_t st)
 {
-    constexpr size_t smem = transport_smem<DIM, PREC, typename DefaultTile<DIM>::T>();
+    using TS = typename DefaultTile<DIM>::T;
+    const size_t smem = transport_smem<DIM, PREC, TS>(a.nb);
     static unsigned attr_set = 0;  // one bit per device
     int dev = 0;
     cudaGetDevice(&dev);
     if (!(attr_set & (1u << (dev & 31)))) {
-        cudaError_t e = cudaFuncSetAttribute(k_transport<DIM, PREC, MINB>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(k_transport<DIM, PREC, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)transport_smem_max<DIM, PREC, TS>());
         if (e != cudaSuccess) return e;
         attr_set |= 1u << (dev & 31);
     }
@@ -725,7 +783,7 @@ template <int DIM, int PREC, class TS>
 static cudaError_t launch_trb(const TransportArgs* boxes, const int2* items, int nitems, BatchCtl ctl, cudaStream_t st)
 {
     constexpr int MINB = 2;
-    constexpr size_t smem = transport_smem<DIM, PREC, TS>();
+    constexpr size_t smem = transport_smem_max<DIM, PREC, TS>();  // boxes differ in basis count
     auto fn = k_transport_batch<DIM, PREC, TS, MINB>;
     static int grid_of[32] = {0};  // persistent grid (SMs x resident CTAs), per device
     int dev = 0;

@@ -31,7 +31,21 @@ struct TransportArgs {
     int update_te, write_diag;
     double min_spec, min_elec, ele_mob, ele_diff, min_te, charge_e;
     int ghost;  // stencil half width H (1, 2 or 3)
+    // Derived from the lists above (finish_species_lists): the transported species
+    // with a drift flux, in update order, and those without.  A fluxed species'
+    // face velocity is fl_K * (velocity basis fl_slot of the cell): the mobility
+    // models of specMob factor into a species constant and a per-cell basis
+    // (bkind 0: E/(sqrt(Te) N), 1: E/N, 2: E); fl_slot < 0 means the user velocity.
+    int nfl, nnf, nb;
+    int8_t fl_sp[VD_MAX_SPECIES + 1], fl_cls[VD_MAX_SPECIES + 1], fl_slot[VD_MAX_SPECIES + 1];
+    int8_t nf_sp[VD_MAX_SPECIES + 1];
+    int8_t bkind[4];
+    double fl_K[VD_MAX_SPECIES + 1];
 };
+
+// Fills the derived fluxed / unfluxed lists and velocity bases of a from its tr_*
+// lists and the mechanism table m (host).
+void finish_species_lists(TransportArgs& a, const VdMechDev& m);
 
 // Arguments of the per-cell prep kernel: N = sum_s n_s over the grown box, and
 // rxn (chemistry) over the valid box.

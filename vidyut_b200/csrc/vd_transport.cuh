@@ -1,16 +1,23 @@
 // vd_transport.cuh -- the fused transport update of one tile (included by vd_kernels.cu).
 //
-// One CTA updates a TX x TY x TZ tile of one box.  Per transported species:
-// (1) stage the stencil lines of every sweep direction in shared memory -- for
-//     direction d the cells rel -3 .. T_d+2 along d of each tile row, with the
-//     density and the drift velocity mu(Te, N) E_d computed once per staged cell;
-// (2) compute every face flux of the tile once (all directions in one pass,
-//     faces spread evenly over the threads);
-// (3) each thread takes the divergence of its own cell, adds rxn (and the Joule
-//     term for the electron energy) and writes n + dt*dsdt in FP64.
-// Two barriers per species.  The tile body is a device function so that the
-// per-box kernel (one CTA per tile) and the batched persistent kernel (CTAs loop
-// over a work list of (box, tile) items of many boxes) share it.
+// One CTA updates a TX x TY x TZ tile of one box.
+// (0) Once per tile, for every cell of the stencil lines of each sweep direction d
+//     (cells rel -3 .. T_d+2 along d of each tile row), the velocity bases of the
+//     mobility models -- E_d/(sqrt(Te) N), E_d/N, E_d, as the mechanism needs --
+//     are computed from Te, E and the density sum and kept in shared memory.  A
+//     species' face velocity is then its constant times one basis (specMob).
+// (1) The transported species with a drift flux go in groups of up to GRP: the
+//     densities of the whole group on all staged lines are loaded at once (many
+//     independent loads in flight), then every face flux of every species of the
+//     group is computed once (all directions, faces spread over the threads), then
+//     each thread takes the divergence of its own cell, adds rxn (and the Joule
+//     term for the electron energy) and writes n + dt*dsdt in FP64.  Two barriers
+//     per group.
+// (2) Transported species without a drift flux, background species and the Te
+//     update need no neighbours and no barrier.
+// The tile body is a device function so that the per-box kernel (one CTA per
+// tile) and the batched persistent kernel (CTAs loop over a work list of
+// (box, tile) items of many boxes) share it.
 #pragma once
 
 namespace vd {
@@ -24,6 +31,10 @@ template <> struct DefaultTile<1> { using T = TileShape<256, 1, 1, 256>; };
 template <> struct DefaultTile<2> { using T = TileShape<32, 8, 1, 256>; };
 template <> struct DefaultTile<3> { using T = TileShape<8, 8, 8, 512>; };
 template <int DIM> constexpr int default_nth() { return DIM == 3 ? 512 : 256; }
+// species per group: all fluxed species of a small mechanism in one group in 1-D
+// and 2-D; in 3-D the staged lines are 5x the tile, so groups of 2 (FP32 staging)
+// or 1 (FP64) keep two CTAs of 512 threads resident
+template <int DIM, int PREC> constexpr int group_size() { return DIM == 3 ? (PREC == PREC_MIXED ? 2 : 1) : 8; }
 
 template <int DIM, class TS>
 struct TileGeom {
@@ -41,58 +52,92 @@ struct TileGeom {
 template <int PREC> struct VelT { using T = double; };
 template <> struct VelT<PREC_MIXED> { using T = float; };
 
-// dynamic shared memory of one tile: face fluxes (FP64), staged densities and
-// velocities (FP32 in the mixed path)
+// dynamic shared memory of one tile with nb velocity bases: the group's face
+// fluxes (FP64), then the bases and the group's staged densities (FP32 in the
+// mixed path)
 template <int DIM, int PREC, class TS>
-constexpr size_t transport_smem()
+__host__ __device__ constexpr size_t transport_smem(int nb)
 {
     using G = TileGeom<DIM, TS>;
-    return (size_t)G::FTOT * sizeof(double) + (size_t)G::STOT * 2 * sizeof(typename VelT<PREC>::T);
+    constexpr int GRP = group_size<DIM, PREC>();
+    return (size_t)GRP * G::FTOT * sizeof(double) +
+           (size_t)(nb + GRP) * G::STOT * sizeof(typename VelT<PREC>::T);
 }
+template <int DIM, int PREC, class TS>
+constexpr size_t transport_smem_max() { return transport_smem<DIM, PREC, TS>(3); }
 
-// stage staged-cell cc of direction D's line set: density and drift velocity
-template <int DIM, int PREC, int D, class TS>
-__device__ __forceinline__ void stage_cell(const TransportArgs& a, int cc, int s, const int* org,
-                                           typename VelT<PREC>::T* sU, typename VelT<PREC>::T* sV)
+// global cell of staged position cc of direction D's line set; false when the
+// position lies outside what the box's stencil may read (those stage as zero)
+template <int DIM, int D, class TS>
+__device__ __forceinline__ bool staged_cell(const TransportArgs& a, int cc, const int* org, int* g)
 {
     using G = TileGeom<DIM, TS>;
-    using VT = typename VelT<PREC>::T;
     constexpr int E0 = G::template SE<D>(0), E1 = G::template SE<D>(1);
     int l[3];
     l[0] = cc % E0;
     l[1] = (cc / E0) % E1;
     l[2] = cc / (E0 * E1);
-    int g[3] = {org[0] + l[0], org[1] + l[1], org[2] + l[2]};
+    g[0] = org[0] + l[0];
+    g[1] = org[1] + l[1];
+    g[2] = org[2] + l[2];
     g[D] -= 3;
     bool ok = (g[D] >= a.lo[D] - a.ghost) && (g[D] <= a.hi[D] + a.ghost);
 #pragma unroll
     for (int e = 0; e < DIM; e++)
         if (e != D) ok = ok && (g[e] <= a.hi[e]);
-    VT u = VT(0);
-    VT v = VT(0);
+    return ok;
+}
+
+// velocity bases of staged position cc of direction D: sB[k*STOT + cc] for slot k
+template <int DIM, int PREC, int D, class TS>
+__device__ __forceinline__ void stage_basis(const TransportArgs& a, int cc, const int* org,
+                                            typename VelT<PREC>::T* sB)
+{
+    using G = TileGeom<DIM, TS>;
+    using VT = typename VelT<PREC>::T;
+    int g[3];
+    const bool ok = staged_cell<DIM, D, TS>(a, cc, org, g);
+    VT b[3] = {VT(0), VT(0), VT(0)};
     if (ok) {
         const int ns = a.ns;
         const int64_t cs = a.sb.ns;
         const double* p = a.sb.p + a.sb.off(g[0], g[1], g[2]);
-        u = (VT)p[s * cs];
-        if (a.udv) {
-            v = (s == a.vel_sp) ? VT(a.uvel[D]) : VT(0);
-        } else {
-            const double Te = p[VD_ETEMP(ns) * cs];
-            const double E = p[(VD_EFX(ns) + D) * cs];
-            const double N = a.Nv(g[0], g[1], g[2]);
-            if constexpr (PREC == PREC_FP64) v = mob_fp64(s, Te, N, a.Tg) * E;
-            else v = mob_f32(s, (float)Te, (float)N, (float)a.Tg) * (float)E;
+        const double E = p[(VD_EFX(ns) + D) * cs];
+        const double N = a.Nv(g[0], g[1], g[2]);
+        for (int k = 0; k < a.nb; k++) {
+            const int kind = a.bkind[k];
+            if constexpr (PREC == PREC_FP64) {
+                if (kind == 0) b[k] = E / (sqrt(p[VD_ETEMP(ns) * cs]) * N);
+                else if (kind == 1) b[k] = E / N;
+                else b[k] = E;
+            } else {
+                const float Ef = (float)E, rN = rcp_approx((float)N);
+                if (kind == 0) b[k] = Ef * rsqrtf((float)p[VD_ETEMP(ns) * cs]) * rN;
+                else if (kind == 1) b[k] = Ef * rN;
+                else b[k] = Ef;
+            }
         }
     }
-    sU[cc] = u;
-    sV[cc] = v;
+    for (int k = 0; k < a.nb; k++) sB[k * G::STOT + cc] = b[k];
 }
 
-// flux of face ff of direction D from the staged lines
+// density of species s at staged position cc of direction D
+template <int DIM, int PREC, int D, class TS>
+__device__ __forceinline__ typename VelT<PREC>::T stage_density(const TransportArgs& a, int cc, int s,
+                                                                  const int* org)
+{
+    using VT = typename VelT<PREC>::T;
+    int g[3];
+    if (!staged_cell<DIM, D, TS>(a, cc, org, g)) return VT(0);
+    return (VT)a.sb.p[a.sb.off(g[0], g[1], g[2]) + (int64_t)s * a.sb.ns];
+}
+
+// flux of face ff of direction D: sU / sB point at direction D's staged lines of
+// the species and of its basis (sB null: constant velocity K)
 template <int DIM, int PREC, int D, class TS>
 __device__ __forceinline__ double face_of(const TransportArgs& a, int ff, int cls, const int* org,
-                                          const typename VelT<PREC>::T* sU, const typename VelT<PREC>::T* sV)
+                                          const typename VelT<PREC>::T* sU, const typename VelT<PREC>::T* sB,
+                                          typename VelT<PREC>::T K)
 {
     using G = TileGeom<DIM, TS>;
     using VT = typename VelT<PREC>::T;
@@ -116,7 +161,7 @@ __device__ __forceinline__ double face_of(const TransportArgs& a, int ff, int cl
 #pragma unroll
     for (int q = 0; q < 6; q++) {
         u[q] = sU[base + q * STR];
-        v[q] = sV[base + q * STR];
+        v[q] = sB ? K * sB[base + q * STR] : K;
     }
     double F;
     if constexpr (PREC == PREC_FP64) F = face_flux_fp64(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
@@ -127,13 +172,16 @@ __device__ __forceinline__ double face_of(const TransportArgs& a, int ff, int cl
 }
 
 // Update tile `tile` (index over a.ntile) of the box described by a.  Every thread
-// of the CTA must call it; it returns with all shared memory reads finished.
+// of the CTA must call it; it returns with all shared memory reads finished
+// except those of the last group's divergence (callers that reuse the shared
+// memory for another tile synchronise first).
 template <int DIM, int PREC, class TS>
-__device__ __forceinline__ void transport_tile_update(const TransportArgs& a, int tile, double* sF,
-                                               typename VelT<PREC>::T* sU, typename VelT<PREC>::T* sV)
+__device__ __forceinline__ void transport_tile_update(const TransportArgs& a, int tile, unsigned char* smem)
 {
     using G = TileGeom<DIM, TS>;
+    using VT = typename VelT<PREC>::T;
     constexpr int NTH = TS::NTH;
+    constexpr int GRP = group_size<DIM, PREC>();
     const int tid = threadIdx.x;
     int tb = tile;
     const int tix = tb % a.ntile[0];
@@ -141,6 +189,9 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     const int tiy = tb % a.ntile[1];
     const int tiz = tb / a.ntile[1];
     const int org[3] = {a.lo[0] + tix * G::T[0], a.lo[1] + tiy * G::T[1], a.lo[2] + tiz * G::T[2]};
+    double* sF = reinterpret_cast<double*>(smem);
+    VT* sB = reinterpret_cast<VT*>(sF + GRP * G::FTOT);
+    VT* sU = sB + a.nb * G::STOT;
 
     // own cell
     const int cx = tid % G::T[0], cy = (tid / G::T[0]) % G::T[1], cz = tid / (G::T[0] * G::T[1]);
@@ -149,80 +200,116 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     const int ns = a.ns;
     const int64_t cs = a.sb.ns;
     const int64_t own_o = own ? a.sb.off(gi, gj, gk) : 0;
-
     double ne_new = 0.0, een_new = 0.0;
-    const int ntr = a.ntr;
-    for (int it = 0; it < ntr; it++) {
-        const int s = a.tr_sp[it];
-        const int cls = a.tr_cls[it];
-        double acc = own ? a.rxn(gi, gj, gk, s) : 0.0;
-        if (a.tr_flux[it]) {
-            for (int c = tid; c < G::STOT; c += NTH) {
-                if (c < G::SOFF1) stage_cell<DIM, PREC, 0, TS>(a, c, s, org, sU, sV);
-                else if (DIM > 1 && c < G::SOFF2)
-                    stage_cell<DIM, PREC, (DIM > 1 ? 1 : 0), TS>(a, c - G::SOFF1, s, org, sU + G::SOFF1,
-                                                                 sV + G::SOFF1);
-                else if (DIM > 2)
-                    stage_cell<DIM, PREC, (DIM > 2 ? 2 : 0), TS>(a, c - G::SOFF2, s, org, sU + G::SOFF2,
-                                                                 sV + G::SOFF2);
+
+    // one species' own-cell result
+    auto finish = [&](int s, double acc) {
+        if (s == ns) {
+            const double jh = joule_cell<true>(a, DIM, gi, gj, gk);
+            acc += jh;
+            if (a.write_diag) {
+                a.pn(gi, gj, gk, VD_EJH(ns)) = jh;
+                a.pn(gi, gj, gk, VD_EIH(ns)) = a.rxn(gi, gj, gk, ns);
             }
-            __syncthreads();
-            for (int f = tid; f < G::FTOT; f += NTH) {
-                double F;
-                if (f < G::FOFF1) F = face_of<DIM, PREC, 0, TS>(a, f, cls, org, sU, sV);
-                else if (DIM > 1 && f < G::FOFF2)
-                    F = face_of<DIM, PREC, (DIM > 1 ? 1 : 0), TS>(a, f - G::FOFF1, cls, org, sU + G::SOFF1,
-                                                                  sV + G::SOFF1);
-                else
-                    F = face_of<DIM, PREC, (DIM > 2 ? 2 : 0), TS>(a, f - G::FOFF2, cls, org, sU + G::SOFF2,
-                                                                  sV + G::SOFF2);
-                sF[f] = F;
+        }
+        double nn = a.sb.p[own_o + s * cs] + a.dt * acc;
+        if (a.bound_specden && s != ns) {
+            // solution clipping of the species solve (Source/ScalarSolve.cpp:597-622)
+            const double lo = (s == a.e_id) ? a.min_elec : a.min_spec;
+            if (nn < lo) nn = lo;
+        }
+        a.pn(gi, gj, gk, s) = nn;
+        if (a.dsdt.p) a.dsdt(gi, gj, gk, s) = acc;
+        if (s == a.e_id) ne_new = nn;
+        if (s == ns) een_new = nn;
+    };
+
+    const int nfl = a.nfl;
+    if (nfl > 0) {
+        // (0) velocity bases of every staged position
+        for (int c = tid; c < G::STOT; c += NTH) {
+            if (c < G::SOFF1) stage_basis<DIM, PREC, 0, TS>(a, c, org, sB);
+            else if (DIM > 1 && c < G::SOFF2)
+                stage_basis<DIM, PREC, (DIM > 1 ? 1 : 0), TS>(a, c - G::SOFF1, org, sB + G::SOFF1);
+            else if (DIM > 2)
+                stage_basis<DIM, PREC, (DIM > 2 ? 2 : 0), TS>(a, c - G::SOFF2, org, sB + G::SOFF2);
+        }
+    }
+    for (int g0 = 0; g0 < nfl; g0 += GRP) {
+        const int gn = nfl - g0 < GRP ? nfl - g0 : GRP;
+        // own-cell inputs of the group, loaded with the staging
+        double rx[GRP];
+#pragma unroll
+        for (int j = 0; j < GRP; j++) rx[j] = (own && j < gn) ? a.rxn(gi, gj, gk, a.fl_sp[g0 + j]) : 0.0;
+        // (1) densities of the group on the staged lines
+        for (int q = tid; q < gn * G::STOT; q += NTH) {
+            const int j = q / G::STOT, c = q - j * G::STOT;
+            const int s = a.fl_sp[g0 + j];
+            VT u;
+            if (c < G::SOFF1) u = stage_density<DIM, PREC, 0, TS>(a, c, s, org);
+            else if (DIM > 1 && c < G::SOFF2) u = stage_density<DIM, PREC, (DIM > 1 ? 1 : 0), TS>(a, c - G::SOFF1, s, org);
+            else u = stage_density<DIM, PREC, (DIM > 2 ? 2 : 0), TS>(a, c - G::SOFF2, s, org);
+            sU[q] = u;
+        }
+        __syncthreads();
+        // (2) every face flux of the group
+        for (int q = tid; q < gn * G::FTOT; q += NTH) {
+            const int j = q / G::FTOT, f = q - j * G::FTOT;
+            const int sl = a.fl_slot[g0 + j];
+            const int cls = a.fl_cls[g0 + j];
+            const VT* uj = sU + j * G::STOT;
+            const VT* bj = sl >= 0 ? sB + sl * G::STOT : nullptr;
+            const double K = a.fl_K[g0 + j];
+            double F;
+            if (f < G::FOFF1) {
+                F = face_of<DIM, PREC, 0, TS>(a, f, cls, org, uj, bj, (VT)(sl >= 0 ? K : a.uvel[0]));
+            } else if (DIM > 1 && f < G::FOFF2) {
+                constexpr int D1 = DIM > 1 ? 1 : 0;
+                F = face_of<DIM, PREC, D1, TS>(a, f - G::FOFF1, cls, org, uj + G::SOFF1,
+                                               bj ? bj + G::SOFF1 : nullptr, (VT)(sl >= 0 ? K : a.uvel[D1]));
+            } else {
+                constexpr int D2 = DIM > 2 ? 2 : 0;
+                F = face_of<DIM, PREC, D2, TS>(a, f - G::FOFF2, cls, org, uj + G::SOFF2,
+                                               bj ? bj + G::SOFF2 : nullptr, (VT)(sl >= 0 ? K : a.uvel[D2]));
             }
-            __syncthreads();
-            if (own) {
-                // dsdt = (Fx_lo - Fx_hi)/dx + rxn, then += y and z terms (ScalarSolve.cpp:45-51)
+            sF[q] = F;
+        }
+        __syncthreads();
+        // (3) divergence + sources of the own cell: dsdt = (Fx_lo - Fx_hi)/dx + rxn,
+        // then += y and z terms (Source/ScalarSolve.cpp:45-51)
+        if (own) {
+#pragma unroll
+            for (int j = 0; j < GRP; j++) {
+                if (j >= gn) break;
+                const double* Fj = sF + j * G::FTOT;
+                double acc;
                 {
                     constexpr int F0 = G::template FE<0>(0), F1 = G::template FE<0>(1);
                     const int lo_f = cx + F0 * (cy + F1 * cz);
-                    acc = (sF[lo_f] - sF[lo_f + 1]) * a.idx[0] + acc;
+                    acc = (Fj[lo_f] - Fj[lo_f + 1]) * a.idx[0] + rx[j];
                 }
                 if constexpr (DIM > 1) {
                     constexpr int F0 = G::template FE<1>(0), F1 = G::template FE<1>(1);
                     const int lo_f = G::FOFF1 + cx + F0 * (cy + F1 * cz);
-                    acc += (sF[lo_f] - sF[lo_f + F0]) * a.idx[1];
+                    acc += (Fj[lo_f] - Fj[lo_f + F0]) * a.idx[1];
                 }
                 if constexpr (DIM > 2) {
                     constexpr int F0 = G::template FE<2>(0), F1 = G::template FE<2>(1);
                     const int lo_f = G::FOFF2 + cx + F0 * (cy + F1 * cz);
-                    acc += (sF[lo_f] - sF[lo_f + F0 * F1]) * a.idx[2];
+                    acc += (Fj[lo_f] - Fj[lo_f + F0 * F1]) * a.idx[2];
                 }
+                finish(a.fl_sp[g0 + j], acc);
             }
-            // the next species' staging overwrites sU/sV only after every thread has
-            // passed the barrier above; sF is rewritten only after the next staging
-            // barrier, by which time every divergence read of this species is done
         }
-        if (own) {
-            if (s == ns) {
-                double jh = joule_cell<true>(a, DIM, gi, gj, gk);
-                acc += jh;
-                if (a.write_diag) {
-                    a.pn(gi, gj, gk, VD_EJH(ns)) = jh;
-                    a.pn(gi, gj, gk, VD_EIH(ns)) = a.rxn(gi, gj, gk, ns);
-                }
-            }
-            double nn = a.sb.p[own_o + s * cs] + a.dt * acc;
-            if (a.bound_specden && s != ns) {
-                // solution clipping of the species solve (Source/ScalarSolve.cpp:599-625)
-                const double lo = (s == a.e_id) ? a.min_elec : a.min_spec;
-                if (nn < lo) nn = lo;
-            }
-            a.pn(gi, gj, gk, s) = nn;
-            if (a.dsdt.p) a.dsdt(gi, gj, gk, s) = acc;
-            if (s == a.e_id) ne_new = nn;
-            if (s == ns) een_new = nn;
-        }
+        // the next group's staging overwrites sU only after every thread has passed
+        // the barrier above; sF is rewritten only after the next staging barrier,
+        // by which time every divergence read of this group is done
     }
     if (own) {
+        for (int j = 0; j < a.nnf; j++) {
+            const int s = a.nf_sp[j];
+            finish(s, a.rxn(gi, gj, gk, s));
+        }
         for (int ib = 0; ib < a.nbg; ib++) {
             const int s = a.bg_sp[ib];
             double v = a.sb.p[own_o + s * cs];
@@ -250,14 +337,8 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
 template <int DIM, int PREC, int MINB>
 __global__ void __launch_bounds__(default_nth<DIM>(), MINB) k_transport(const __grid_constant__ TransportArgs a)
 {
-    using TS = typename DefaultTile<DIM>::T;
-    using G = TileGeom<DIM, TS>;
-    using VT = typename VelT<PREC>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* sF = reinterpret_cast<double*>(smem_raw);
-    VT* sU = reinterpret_cast<VT*>(sF + G::FTOT);
-    VT* sV = sU + G::STOT;
-    transport_tile_update<DIM, PREC, TS>(a, blockIdx.x, sF, sU, sV);
+    transport_tile_update<DIM, PREC, typename DefaultTile<DIM>::T>(a, blockIdx.x, smem_raw);
 }
 
 // batched persistent kernel: each CTA walks the work list of (box, tile) items
@@ -267,17 +348,12 @@ __global__ void __launch_bounds__(TS::NTH, MINB)
     k_transport_batch(const TransportArgs* __restrict__ boxes, const int2* __restrict__ items, int nitems,
                       const BatchCtl ctl)
 {
-    using G = TileGeom<DIM, TS>;
-    using VT = typename VelT<PREC>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* sF = reinterpret_cast<double*>(smem_raw);
-    VT* sU = reinterpret_cast<VT*>(sF + G::FTOT);
-    VT* sV = sU + G::STOT;
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const int2 w = items[it];
         const int2 cc = ctl.ctrl[w.x];
         if (ctl.t >= cc.x) continue;  // uniform over the CTA
-        transport_tile_update<DIM, PREC, TS>(boxes[((ctl.t + cc.y) & 1) * ctl.nbox + w.x], w.y, sF, sU, sV);
+        transport_tile_update<DIM, PREC, TS>(boxes[((ctl.t + cc.y) & 1) * ctl.nbox + w.x], w.y, smem_raw);
         __syncthreads();  // the next item's staging must not overwrite a slow thread's reads
     }
 }
