@@ -439,16 +439,28 @@ __global__ void __launch_bounds__(128) k_prep_batch(const PrepArgs* __restrict__
     const int st = blockDim.x;
     double* sc = reinterpret_cast<double*>(smem_raw) + threadIdx.x;
     double* wd = sc + ns * st;
+    __shared__ long long sA_raw[sizeof(PrepArgs) / 8];  // the item's record, read from shared memory
+    static_assert(sizeof(PrepArgs) % 8 == 0, "record copied in 8-byte words");
+    const PrepArgs& sA = *reinterpret_cast<const PrepArgs*>(sA_raw);
+    int cur = -1;
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const int2 w = items[it];
         const int2 cc = ctl.ctrl[w.x];
         if (ctl.t >= cc.x) continue;
-        const PrepArgs& a = boxes[((ctl.t + cc.y) & 1) * ctl.nbox + w.x];
-        const int64_t ntot = grown_cells(a);
+        const int rec = ((ctl.t + cc.y) & 1) * ctl.nbox + w.x;
+        if (rec != cur) {
+            __syncthreads();  // every thread is done with the previous record
+            const long long* src = reinterpret_cast<const long long*>(boxes + rec);
+            long long* dst = sA_raw;
+            for (int q = threadIdx.x; q < (int)(sizeof(PrepArgs) / 8); q += blockDim.x) dst[q] = src[q];
+            cur = rec;
+            __syncthreads();
+        }
+        const int64_t ntot = grown_cells(sA);
         const int64_t base = (int64_t)w.y * kPrepChunk;
         for (int q = threadIdx.x; q < kPrepChunk; q += blockDim.x) {
             const int64_t idx = base + q;
-            if (idx < ntot) prep_cell<PREC>(a, idx, sc, wd, st);
+            if (idx < ntot) prep_cell<PREC>(sA, idx, sc, wd, st);
         }
     }
 }

@@ -130,11 +130,21 @@ std::string gen_prep_kernel(const VdMechDev& m, int prec)
       << "    vd_spec_cell_" << sfx << "(a, idx);\n}\n";
     o << "extern \"C\" __global__ void " << lb << " vd_spec_prep_batch_" << sfx
       << "(const PrepArgs* __restrict__ boxes, const int2* __restrict__ items, int nitems, const BatchCtl ctl)\n{\n"
+      << "  __shared__ PrepArgs a;  // the item's record\n"
+      << "  int cur = -1;\n"
       << "  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {\n"
       << "    const int2 w = items[it];\n"
       << "    const int2 cc = ctl.ctrl[w.x];\n"
       << "    if (ctl.t >= cc.x) continue;\n"
-      << "    const PrepArgs& a = boxes[((ctl.t + cc.y) & 1) * ctl.nbox + w.x];\n"
+      << "    const int rec = ((ctl.t + cc.y) & 1) * ctl.nbox + w.x;\n"
+      << "    if (rec != cur) {\n"
+      << "      __syncthreads();\n"
+      << "      const long long* src = reinterpret_cast<const long long*>(boxes + rec);\n"
+      << "      long long* dst = reinterpret_cast<long long*>(&a);\n"
+      << "      for (int q = threadIdx.x; q < (int)(sizeof(PrepArgs) / 8); q += blockDim.x) dst[q] = src[q];\n"
+      << "      cur = rec;\n"
+      << "      __syncthreads();\n"
+      << "    }\n"
       << "    const i64 ntot = (i64)(a.ghi[0] - a.glo[0] + 1) * (a.ghi[1] - a.glo[1] + 1) * (a.ghi[2] - a.glo[2] + 1);\n"
       << "    for (int q = threadIdx.x; q < " << kPrepChunk << "; q += blockDim.x) {\n"
       << "      const i64 idx = (i64)w.y * " << kPrepChunk << " + q;\n"

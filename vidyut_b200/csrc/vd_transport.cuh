@@ -53,15 +53,51 @@ template <int PREC> struct VelT { using T = double; };
 template <> struct VelT<PREC_MIXED> { using T = float; };
 
 // dynamic shared memory of one tile with nb velocity bases: the group's face
-// fluxes (FP64), then the bases and the group's staged densities (FP32 in the
-// mixed path)
+// fluxes and the Joule term of every face (FP64), then the bases and the group's
+// staged densities (FP32 in the mixed path)
 template <int DIM, int PREC, class TS>
 __host__ __device__ constexpr size_t transport_smem(int nb)
 {
     using G = TileGeom<DIM, TS>;
     constexpr int GRP = group_size<DIM, PREC>();
-    return (size_t)GRP * G::FTOT * sizeof(double) +
+    return (size_t)(GRP + 1) * G::FTOT * sizeof(double) +
            (size_t)(nb + GRP) * G::STOT * sizeof(typename VelT<PREC>::T);
+}
+
+// Joule heating carried by face g of direction D (the face between cells g - e_D
+// and g): q (mu ne E_f - D grad ne) E_f with face averages of Te, ne and the density
+// sum (Source/ElecEnergySource.cpp:86-160, one face of the per-cell loop).  Each
+// cell adds half of its faces' values, after the domain-face substitution.
+__device__ __forceinline__ double joule_face(const TransportArgs& a, int D, const int* g)
+{
+    const int ns = a.ns, eidx = a.e_id;
+    int l[3] = {g[0], g[1], g[2]};
+    l[D] -= 1;
+    const int64_t ol = a.sb.off(l[0], l[1], l[2]);
+    const int64_t orr = a.sb.off(g[0], g[1], g[2]);
+    const double* p = a.sb.p;
+    const int64_t cs = a.sb.ns;
+    const double etemp = 0.5 * (p[ol + VD_ETEMP(ns) * cs] + p[orr + VD_ETEMP(ns) * cs]);
+    const double evf_d = 0.5 * (p[ol + (VD_EFX(ns) + D) * cs] + p[orr + (VD_EFX(ns) + D) * cs]);
+    const double nel = p[ol + eidx * cs], ner = p[orr + eidx * cs];
+    const double ne = 0.5 * (nel + ner);
+    const double ef = a.cs_technique ? evf_d : a.ef[D](g[0], g[1], g[2]);
+    const double gn = a.gradne_from_state ? (ner - nel) / a.dx[D] : a.gne[D](g[0], g[1], g[2]);
+    const double ndens = 0.5 * (a.Nv.p[a.Nv.off(l[0], l[1], l[2])] + a.Nv.p[a.Nv.off(g[0], g[1], g[2])]);
+    double mu, dc;
+    if (a.const_ele_trans) {
+        mu = a.ele_mob / ndens;
+        dc = a.ele_diff / ndens;
+    } else {
+        mu = mob_fp64(eidx, etemp, ndens, a.Tg);
+        // the usual electron diffusion model refers to the electron mobility itself
+        if (c_mech.diff_kind[eidx] == VD_DIFF_TE_ABSMOB && c_mech.diff_ref[eidx] == eidx)
+            dc = c_mech.diff_factor[eidx] * (etemp / EV) * fabs(mu);
+        else
+            dc = diff_fp64(eidx, etemp, ndens, a.Tg);
+    }
+    const double cur = a.charge_e * (mu * ne * ef - dc * gn);
+    return cur * ef;
 }
 template <int DIM, int PREC, class TS>
 constexpr size_t transport_smem_max() { return transport_smem<DIM, PREC, TS>(3); }
@@ -190,7 +226,8 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     const int tiz = tb / a.ntile[1];
     const int org[3] = {a.lo[0] + tix * G::T[0], a.lo[1] + tiy * G::T[1], a.lo[2] + tiz * G::T[2]};
     double* sF = reinterpret_cast<double*>(smem);
-    VT* sB = reinterpret_cast<VT*>(sF + GRP * G::FTOT);
+    double* sJ = sF + GRP * G::FTOT;
+    VT* sB = reinterpret_cast<VT*>(sJ + G::FTOT);
     VT* sU = sB + a.nb * G::STOT;
 
     // own cell
@@ -201,11 +238,39 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     const int64_t cs = a.sb.ns;
     const int64_t own_o = own ? a.sb.off(gi, gj, gk) : 0;
     double ne_new = 0.0, een_new = 0.0;
+    const int nfl = a.nfl;
+    // Joule faces of the tile are computed once (phase 0) when a barrier follows
+    const bool jfaces = a.elecenergy && nfl > 0;
+
+    // Joule term of the own cell: half the sum of its faces, each domain face
+    // replaced as the reference does (Source/ElecEnergySource.cpp:95-99)
+    auto joule_own = [&]() -> double {
+        if (!jfaces) return joule_cell<true>(a, DIM, gi, gj, gk);
+        const int gc[3] = {gi, gj, gk}, lc[3] = {cx, cy, cz};
+        double jheat = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            const int foff = d == 0 ? 0 : (d == 1 ? G::FOFF1 : G::FOFF2);
+            const int F0 = G::T[0] + (d == 0), F1 = G::T[1] + (d == 1);
+            const int str = d == 0 ? 1 : (d == 1 ? F0 : F0 * F1);
+            const int base = foff + lc[0] + F0 * (lc[1] + F1 * lc[2]);
+#pragma unroll
+            for (int f = 0; f < 2; f++) {
+                int fe = gc[d] + f;
+                if (fe == a.domlo[d]) fe += 1;
+                if (fe == a.domhi[d] + 1) fe -= 1;
+                jheat += sJ[base + (fe - gc[d]) * str];
+            }
+        }
+        jheat *= 0.5;
+        if (a.floor_jh && jheat < 0.0) jheat = 0.0;
+        return jheat;
+    };
 
     // one species' own-cell result
     auto finish = [&](int s, double acc) {
         if (s == ns) {
-            const double jh = joule_cell<true>(a, DIM, gi, gj, gk);
+            const double jh = joule_own();
             acc += jh;
             if (a.write_diag) {
                 a.pn(gi, gj, gk, VD_EJH(ns)) = jh;
@@ -224,7 +289,6 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
         if (s == ns) een_new = nn;
     };
 
-    const int nfl = a.nfl;
     if (nfl > 0) {
         // (0) velocity bases of every staged position
         for (int c = tid; c < G::STOT; c += NTH) {
@@ -233,6 +297,22 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
                 stage_basis<DIM, PREC, (DIM > 1 ? 1 : 0), TS>(a, c - G::SOFF1, org, sB + G::SOFF1);
             else if (DIM > 2)
                 stage_basis<DIM, PREC, (DIM > 2 ? 2 : 0), TS>(a, c - G::SOFF2, org, sB + G::SOFF2);
+        }
+    }
+    if (jfaces) {
+        // (0') the Joule term of every face of the tile, once
+        for (int f = tid; f < G::FTOT; f += NTH) {
+            int d = 0, ff = f;
+            if (DIM > 1 && f >= G::FOFF1) {
+                d = (DIM > 2 && f >= G::FOFF2) ? 2 : 1;
+                ff = f - (d == 1 ? G::FOFF1 : G::FOFF2);
+            }
+            const int F0 = G::T[0] + (d == 0), F1 = G::T[1] + (d == 1);
+            int g[3] = {org[0] + ff % F0, org[1] + (ff / F0) % F1, org[2] + ff / (F0 * F1)};
+            bool ok = g[d] <= a.hi[d] + 1;
+            for (int e = 0; e < DIM; e++)
+                if (e != d) ok = ok && g[e] <= a.hi[e];
+            sJ[f] = ok ? joule_face(a, d, g) : 0.0;
         }
     }
     for (int g0 = 0; g0 < nfl; g0 += GRP) {
@@ -342,19 +422,33 @@ __global__ void __launch_bounds__(default_nth<DIM>(), MINB) k_transport(const __
 }
 
 // batched persistent kernel: each CTA walks the work list of (box, tile) items
-// with a grid stride; boxes are described by TransportArgs records in global memory
+// with a grid stride.  Boxes are described by TransportArgs records in global
+// memory; the item's record is first copied to shared memory, so that the tile
+// body's many reads of it are shared-memory loads rather than global ones.
 template <int DIM, int PREC, class TS, int MINB>
 __global__ void __launch_bounds__(TS::NTH, MINB)
     k_transport_batch(const TransportArgs* __restrict__ boxes, const int2* __restrict__ items, int nitems,
                       const BatchCtl ctl)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ long long sA_raw[sizeof(TransportArgs) / 8];
+    static_assert(sizeof(TransportArgs) % 8 == 0, "record copied in 8-byte words");
+    const TransportArgs& sA = *reinterpret_cast<const TransportArgs*>(sA_raw);
+    int cur = -1;  // record held in sA
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const int2 w = items[it];
         const int2 cc = ctl.ctrl[w.x];
         if (ctl.t >= cc.x) continue;  // uniform over the CTA
-        transport_tile_update<DIM, PREC, TS>(boxes[((ctl.t + cc.y) & 1) * ctl.nbox + w.x], w.y, smem_raw);
-        __syncthreads();  // the next item's staging must not overwrite a slow thread's reads
+        const int rec = ((ctl.t + cc.y) & 1) * ctl.nbox + w.x;
+        if (rec != cur) {
+            const long long* src = reinterpret_cast<const long long*>(boxes + rec);
+            long long* dst = sA_raw;
+            for (int q = threadIdx.x; q < (int)(sizeof(TransportArgs) / 8); q += TS::NTH) dst[q] = src[q];
+            cur = rec;
+            __syncthreads();
+        }
+        transport_tile_update<DIM, PREC, TS>(sA, w.y, smem_raw);
+        __syncthreads();  // the next item's staging (or record) must not overwrite a slow thread's reads
     }
 }
 
