@@ -168,36 +168,56 @@ __device__ __forceinline__ typename VelT<PREC>::T stage_density(const TransportA
     return (VT)a.sb.p[a.sb.off(g[0], g[1], g[2]) + (int64_t)s * a.sb.ns];
 }
 
-// flux of face ff of direction D: sU / sB point at direction D's staged lines of
-// the species and of its basis (sB null: constant velocity K)
-template <int DIM, int PREC, int D, class TS>
-__device__ __forceinline__ double face_of(const TransportArgs& a, int ff, int cls, const int* org,
-                                          const typename VelT<PREC>::T* sU, const typename VelT<PREC>::T* sB,
-                                          typename VelT<PREC>::T K)
+// local coordinates of face ff of direction D's face set
+template <int DIM, int D, class TS>
+__device__ __forceinline__ void face_local(int ff, int* l)
 {
     using G = TileGeom<DIM, TS>;
-    using VT = typename VelT<PREC>::T;
     constexpr int F0 = G::template FE<D>(0), F1 = G::template FE<D>(1);
-    constexpr int S0 = G::template SE<D>(0), S1 = G::template SE<D>(1);
-    constexpr int STR = (D == 0) ? 1 : ((D == 1) ? S0 : S0 * S1);
-    int l[3];
     l[0] = ff % F0;
     l[1] = (ff / F0) % F1;
     l[2] = ff / (F0 * F1);
-    int g[3] = {org[0] + l[0], org[1] + l[1], org[2] + l[2]};
+}
+
+// flux of face f of the tile (the faces of all directions in one index range) of
+// one species: sU / sB are the species' staged densities and its velocity basis
+// over all line sets (sB null: the user velocity of the face's direction).  One
+// copy of the flux arithmetic serves every direction.
+template <int DIM, int PREC, class TS>
+__device__ __forceinline__ double face_any(const TransportArgs& a, int f, int cls, const int* org,
+                                           const typename VelT<PREC>::T* sU, const typename VelT<PREC>::T* sB,
+                                           double K)
+{
+    using G = TileGeom<DIM, TS>;
+    using VT = typename VelT<PREC>::T;
+    int D = 0, l[3];
+    if (DIM > 2 && f >= G::FOFF2) {
+        D = 2;
+        face_local<DIM, (DIM > 2 ? 2 : 0), TS>(f - G::FOFF2, l);
+    } else if (DIM > 1 && f >= G::FOFF1) {
+        D = 1;
+        face_local<DIM, (DIM > 1 ? 1 : 0), TS>(f - G::FOFF1, l);
+    } else {
+        face_local<DIM, 0, TS>(f, l);
+    }
+    const int S0 = G::T[0] + (D == 0 ? 6 : 0), S1 = G::T[1] + (D == 1 ? 6 : 0);
+    const int STR = D == 0 ? 1 : (D == 1 ? S0 : S0 * S1);
+    const int soff = D == 0 ? 0 : (D == 1 ? G::SOFF1 : G::SOFF2);
+    const int g[3] = {org[0] + l[0], org[1] + l[1], org[2] + l[2]};
     bool ok = g[D] <= a.hi[D] + 1;
 #pragma unroll
     for (int e = 0; e < DIM; e++)
         if (e != D) ok = ok && (g[e] <= a.hi[e]);
     if (!ok) return 0.0;
     // staged index of rel cell (f_d - 3 + q) is f_d + q along d
-    const int base = l[0] + S0 * (l[1] + S1 * l[2]);
+    const int base = soff + l[0] + S0 * (l[1] + S1 * l[2]);
+    const VT k = (VT)(sB ? K : a.uvel[D]);
     VT u[6];
     VT v[6];
 #pragma unroll
     for (int q = 0; q < 6; q++) {
         u[q] = sU[base + q * STR];
-        v[q] = sB ? K * sB[base + q * STR] : K;
+        v[q] = sB ? k * sB[base + q * STR] : k;
     }
     double F;
     if constexpr (PREC == PREC_FP64) F = face_flux_fp64(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
@@ -317,10 +337,6 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     }
     for (int g0 = 0; g0 < nfl; g0 += GRP) {
         const int gn = nfl - g0 < GRP ? nfl - g0 : GRP;
-        // own-cell inputs of the group, loaded with the staging
-        double rx[GRP];
-#pragma unroll
-        for (int j = 0; j < GRP; j++) rx[j] = (own && j < gn) ? a.rxn(gi, gj, gk, a.fl_sp[g0 + j]) : 0.0;
         // (1) densities of the group on the staged lines
         for (int q = tid; q < gn * G::STOT; q += NTH) {
             const int j = q / G::STOT, c = q - j * G::STOT;
@@ -336,37 +352,21 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
         for (int q = tid; q < gn * G::FTOT; q += NTH) {
             const int j = q / G::FTOT, f = q - j * G::FTOT;
             const int sl = a.fl_slot[g0 + j];
-            const int cls = a.fl_cls[g0 + j];
-            const VT* uj = sU + j * G::STOT;
-            const VT* bj = sl >= 0 ? sB + sl * G::STOT : nullptr;
-            const double K = a.fl_K[g0 + j];
-            double F;
-            if (f < G::FOFF1) {
-                F = face_of<DIM, PREC, 0, TS>(a, f, cls, org, uj, bj, (VT)(sl >= 0 ? K : a.uvel[0]));
-            } else if (DIM > 1 && f < G::FOFF2) {
-                constexpr int D1 = DIM > 1 ? 1 : 0;
-                F = face_of<DIM, PREC, D1, TS>(a, f - G::FOFF1, cls, org, uj + G::SOFF1,
-                                               bj ? bj + G::SOFF1 : nullptr, (VT)(sl >= 0 ? K : a.uvel[D1]));
-            } else {
-                constexpr int D2 = DIM > 2 ? 2 : 0;
-                F = face_of<DIM, PREC, D2, TS>(a, f - G::FOFF2, cls, org, uj + G::SOFF2,
-                                               bj ? bj + G::SOFF2 : nullptr, (VT)(sl >= 0 ? K : a.uvel[D2]));
-            }
-            sF[q] = F;
+            sF[q] = face_any<DIM, PREC, TS>(a, f, a.fl_cls[g0 + j], org, sU + j * G::STOT,
+                                            sl >= 0 ? sB + sl * G::STOT : nullptr, a.fl_K[g0 + j]);
         }
         __syncthreads();
         // (3) divergence + sources of the own cell: dsdt = (Fx_lo - Fx_hi)/dx + rxn,
         // then += y and z terms (Source/ScalarSolve.cpp:45-51)
         if (own) {
-#pragma unroll
-            for (int j = 0; j < GRP; j++) {
-                if (j >= gn) break;
+#pragma unroll 1
+            for (int j = 0; j < gn; j++) {
                 const double* Fj = sF + j * G::FTOT;
                 double acc;
                 {
                     constexpr int F0 = G::template FE<0>(0), F1 = G::template FE<0>(1);
                     const int lo_f = cx + F0 * (cy + F1 * cz);
-                    acc = (Fj[lo_f] - Fj[lo_f + 1]) * a.idx[0] + rx[j];
+                    acc = (Fj[lo_f] - Fj[lo_f + 1]) * a.idx[0] + a.rxn(gi, gj, gk, a.fl_sp[g0 + j]);
                 }
                 if constexpr (DIM > 1) {
                     constexpr int F0 = G::template FE<1>(0), F1 = G::template FE<1>(1);
