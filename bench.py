@@ -44,6 +44,8 @@ WORKLOADS = {
     "argon2d": "2-D 256^2 box, E/Ar+/Ar*/Ar, 10 reactions, WENO-Z, one explicit step",
     "batched": "64 independent 2-D cases, sides log-uniform 64-512, 8 species / 40 reactions, "
                "WENO-Z, 20 explicit steps per case per solve",
+    "serving": "Poisson stream at 500 req/s of 1-D/2-D discharge cases, sides log-uniform 256-1024, "
+               "0.5-5 kV, 0.1-10 bar, 50-2000 explicit steps, 8 species / 40 reactions, fixed HBM budget",
 }
 
 
@@ -63,6 +65,10 @@ def parse():
                     help="precision of the --only-update run")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-workload measurement added to the default line")
+    ap.add_argument("--no-serving", action="store_true",
+                    help="skip the serving-workload measurement added to the default line")
+    ap.add_argument("--requests", type=int, default=48, help="requests of the serving stream")
+    ap.add_argument("--budget-gb", type=float, default=8.0, help="HBM budget of the serving loop")
     return ap.parse_args()
 
 
@@ -180,6 +186,8 @@ def run_reference(args):
     os.environ["OMP_NUM_THREADS"] = str(threads)
     if args.workload == "batched":
         return run_reference_batched(args, threads)
+    if args.workload == "serving":
+        return run_reference_serving(args, threads)
     case = make_case(args.workload)
     lib, kind, run, nplanes, cpp = cpu_reference_rate(case, max(1.0, args.cpu_seconds / max(1, args.steps)))
     for _ in range(args.warmup):
@@ -242,6 +250,55 @@ def run_reference_batched(args, threads: int):
                              "sample": f"one explicit step of {len(sample)} of {len(cases)} cases "
                                        f"({cells} cells) per step"},
             "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_serving(args, threads: int):
+    """The reference's own code on the serving stream, one request at a time (the
+    reference runs one case per process): each step of the bench times one
+    explicit step of every request of a bounded sample and extrapolates each
+    request's service time to its step count; solves/s = requests / total service."""
+    import oracle
+    from vidyut_b200 import inputs
+    mech, reqs = inputs.config_serving(n_requests=args.requests)
+    try:
+        lib, kind = oracle.RefLib(mech.name, 2), "reference"
+        lib1 = oracle.RefLib(mech.name, 1)
+    except FileNotFoundError:
+        lib = lib1 = oracle.Port(mech)
+        kind = "port"
+    budget = max(1.0, args.cpu_seconds / max(1, args.steps))
+    sample, t = [], 0.0
+    for _, c, n in reqs:  # choose the sample once, in arrival order
+        t0 = time.perf_counter()
+        (lib if c.dim == 2 else lib1).update_all(c, c.vd_params())
+        t += time.perf_counter() - t0
+        sample.append((c, n))
+        if t >= budget:
+            break
+    for _ in range(args.warmup):
+        for c, _ in sample:
+            (lib if c.dim == 2 else lib1).update_all(c, c.vd_params())
+    service = 0.0
+    t_all = time.perf_counter()
+    for _ in range(args.steps):
+        for c, n in sample:
+            t0 = time.perf_counter()
+            (lib if c.dim == 2 else lib1).update_all(c, c.vd_params())
+            service += (time.perf_counter() - t0) * n
+    t_all = time.perf_counter() - t_all
+    service /= args.steps
+    value = len(sample) / service
+    line = {"metric": "solves/s", "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_all / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": WORKLOADS["serving"], "requests": len(reqs)},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": kind,
+                             "sample": f"one timed explicit step of each of the first {len(sample)} of {len(reqs)} "
+                                       "requests, times its step count"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -441,6 +498,15 @@ def run_ours(args):
         batched["unit"] = "cell-updates/s"
         batched["workload"] = WORKLOADS["batched"]
 
+    serving = None
+    if not args.no_serving and world == 1 and args.workload == "precision3d":
+        dc = phi_new = None
+        torch.cuda.empty_cache()
+        serving = measure_serving(args.requests, args.budget_gb)
+        serving.pop("clocks", None)
+        serving["workload"] = WORKLOADS["serving"]
+        api.mech_init(case.mech)
+
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         threads = os.cpu_count() or 1
@@ -475,6 +541,7 @@ def run_ours(args):
                                 "max_rel": float(np.max(err_max)),
                                 "max_rel_to_step_scale": float(np.max(err_scaled))},
         "batched": batched,
+        "serving": serving,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -653,6 +720,125 @@ def measure_batched(steps: int, warmup: int, *, cpu_seconds: float = 0.0, e2e: b
     return out
 
 
+def measure_serving(n_requests: int = 48, budget_gb: float = 8.0, quantum: int = 25, plain_fp64: bool = True,
+                    warmup: bool = True) -> dict:
+    """The serving workload on one GPU: the seeded Poisson stream is submitted to
+    the continuous-batching server at its arrival times (host inputs in, final
+    states back to host memory), then every result is collected.  The baseline is
+    the same stream served first-come-first-served one case at a time on the plain
+    FP64 per-box path (a queue alone): each request's service time is measured on
+    the GPU and its latency follows from the queue, finish_i = max(arrival_i,
+    finish_(i-1)) + service_i."""
+    import threading
+
+    import torch
+
+    from vidyut_b200 import _abi as abi
+    from vidyut_b200 import api, inputs
+
+    L = abi.lib()
+    mech, reqs = inputs.config_serving(n_requests=n_requests)
+    api.mech_init(mech)
+    budget = int(budget_gb * (1 << 30))
+    if warmup:  # graph capture paths, NVRTC module load, pinned pools
+        with api.Server(abi.PREC_MIXED, budget_bytes=budget, max_cases=256, quantum_steps=quantum) as s:
+            ids = [s.submit(c, c.vd_params(precision=abi.PREC_MIXED), 30) for _, c, _ in reqs[:4]]
+            for i in ids:
+                s.wait(i)
+    clock = ClockSampler(torch.cuda.current_device())
+    n0 = L.vd_launch_count()
+    clock.start()
+    with api.Server(abi.PREC_MIXED, budget_bytes=budget, max_cases=256, quantum_steps=quantum) as s:
+        ids = [None] * len(reqs)
+
+        def feeder():
+            t0 = time.perf_counter()
+            for k, (t_arr, c, n) in enumerate(reqs):
+                dt = t_arr - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                ids[k] = s.submit(c, c.vd_params(precision=abi.PREC_MIXED), n)
+
+        th = threading.Thread(target=feeder)
+        t_start = time.perf_counter()
+        th.start()
+        th.join()
+        lat = [s.wait(i)[1] for i in ids]
+        wall = time.perf_counter() - t_start
+        st = s.stats()
+    clocks = clock.stop()
+    launches = L.vd_launch_count() - n0
+    cells_steps = sum(c.ncell * n for _, c, n in reqs)
+    nbytes = sum(c.state.nbytes for _, c, _ in reqs)
+    out = {"requests": len(reqs), "offered_rate_per_s": len(reqs) / reqs[-1][0], "n_2d": sum(c.dim == 2 for _, c, _ in reqs),
+           "cell_updates": cells_steps, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
+           "solves_per_s": st["solves_per_s"], "cell_updates_per_s": st["cell_updates_per_s"], "span_s": st["span_s"],
+           "wall_s": wall, "peak_bytes_used": st["peak_bytes_used"], "budget_bytes": budget, "quanta": st["quanta"],
+           "graph_builds": st["graph_builds"], "quantum_steps": quantum, "gpu_launches": int(launches),
+           "h2d_bytes": int(nbytes), "d2h_bytes": int(nbytes), "clocks": clocks,
+           "lat_mean_ms": float(sum(lat) / len(lat))}
+    if plain_fp64:
+        import numpy as np
+        service = []
+        for t_arr, c, n in reqs:
+            ns = c.mech.ns
+            comps = list(range(ns)) + [abi.EEN(ns), abi.ETEMP(ns)]
+            prm = c.vd_params(precision=abi.PREC_FP64)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            dc = api.upload(c)
+            pn, _, _ = dc.new_outputs()
+            g = c.gvec
+            v = dc.state[:, g[2]:g[2] + c.n[2], g[1]:g[1] + c.n[1], g[0]:g[0] + c.n[0]]
+            for _ in range(n):
+                api.explicit_update_all(dc, prm, pn)
+                v.copy_(pn)
+                api.fill_ghosts(dc.state, c, c.ghost, comps, c.periodic)
+            res = dc.state.cpu()
+            torch.cuda.synchronize()
+            service.append(time.perf_counter() - t0)
+            del dc, pn, res
+        fin, lats = 0.0, []
+        for (t_arr, _, _), sv in zip(reqs, service):
+            fin = max(t_arr, fin) + sv
+            lats.append(1e3 * (fin - t_arr))
+        span = fin - reqs[0][0]
+        out["plain_fp64_fifo"] = {"p50_ms": float(np.percentile(lats, 50)), "p99_ms": float(np.percentile(lats, 99)),
+                                  "solves_per_s": len(reqs) / span, "cell_updates_per_s": cells_steps / span,
+                                  "service_s_total": float(sum(service)),
+                                  "path": "one request at a time: upload, n x (vd_explicit_update_all FP64 + "
+                                          "vd_fill_ghosts), result to host"}
+        out["speedup_solves_vs_plain_fp64"] = out["solves_per_s"] / out["plain_fp64_fifo"]["solves_per_s"]
+        out["p99_ratio_vs_plain_fp64"] = out["plain_fp64_fifo"]["p99_ms"] / max(out["p99_ms"], 1e-9)
+    return out
+
+
+def run_serving_line(args):
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1 and int(os.environ.get("RANK", "0")) != 0:
+        return 0  # replicas only: the serving workload is measured on one GPU
+    r = measure_serving(args.requests, args.budget_gb)
+    line = {"metric": "solves/s", "value": r["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
+            "steps": r["requests"], "warmup": 4, "ms_per_step": 1e3 * r["span_s"] / max(1, r["requests"]),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32/f64 (mixed: FP32 WENO, rates, fluxes; FP64 accumulate)", "data": "synthetic",
+            "config": {"workload": WORKLOADS["serving"], "requests": r["requests"],
+                       "budget_bytes": r["budget_bytes"], "quantum_steps": r["quantum_steps"],
+                       "l2": "inputs larger than L2 (resident cases of up to 1M cells x 18 comps, two copies)"},
+            "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "max_ms": r["max_ms"],
+            "cell_updates_per_s": r["cell_updates_per_s"],
+            "e2e": {"value": r["solves_per_s"], "unit": "solves/s", "h2d_bytes_per_step": r["h2d_bytes"] // r["requests"],
+                    "d2h_bytes_per_step": r["d2h_bytes"] // r["requests"],
+                    "path": "vd_server_submit with host inputs .. vd_server_wait with host results; every "
+                            "request's copies are inside its latency"},
+            "roofline": None, "cpu_baseline": None, "gpu_launches": r["gpu_launches"], "clocks": r["clocks"],
+            "serving": r}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_batched_line(args):
     import torch
     from vidyut_b200 import _abi as abi
@@ -696,6 +882,8 @@ def main():
         if args.only_update:
             return run_batched_only(args)
         return run_batched_line(args)
+    if args.workload == "serving":
+        return run_serving_line(args)
     return run_ours(args)
 
 

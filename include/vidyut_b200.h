@@ -54,7 +54,7 @@ extern "C" {
 #define VD_ERR_DIM       -4   /* dim not 1, 2 or 3                                          */
 #define VD_ERR_MECH      -5   /* no mechanism loaded, or the mechanism table is invalid     */
 #define VD_ERR_CUDA      -6   /* a CUDA runtime call failed (vd_last_error has the text)    */
-#define VD_ERR_TIMEOUT   -7   /* a persistent kernel gave up waiting (bounded spin)         */
+#define VD_ERR_TIMEOUT   -7   /* a bounded wait ran out (vd_server_wait)                    */
 #define VD_ERR_NOMEM     -8   /* device scratch could not be obtained                       */
 #define VD_ERR_NONFINITE -9   /* input scan found NaN/Inf                                   */
 #define VD_ERR_BUDGET   -10   /* serving: case does not fit the HBM budget                  */
@@ -365,6 +365,42 @@ int      vd_batch_set_tile_variant(vd_batch* b, int dim, int variant);
 int      vd_batch_tile_shape(int dim, int variant, int32_t tile[3]);  /* returns the variant count */
 int      vd_batch_set_graph(vd_batch* b, int on);  /* 0: launch kernels directly */
 int      vd_batch_get_stats(vd_batch* b, vd_batch_stats* out);
+
+/* ---- serving (no reference counterpart: the reference runs one case per process)
+ * A continuous-batching request loop on one GPU over a vd_batch of
+ * hbm_budget_bytes.  vd_server_submit copies the request's inputs (layouts as for
+ * vd_batch_add_case) into host memory the server owns and queues it; a worker
+ * thread admits queued requests oldest first as arena room frees up (smaller
+ * ones may backfill past a request that does not fit until it has waited 200 ms),
+ * steps all resident cases together quantum_steps explicit steps at a time,
+ * and retires finished cases to host memory.  vd_server_wait blocks until the
+ * request is done (timeout_s < 0: no limit; VD_ERR_TIMEOUT otherwise), copies its
+ * final state (the ghost-grown layout) to state_out when not NULL, gives its
+ * latency (submission to result in host memory) and forgets the request.
+ * A request larger than the whole budget is rejected at submission with
+ * VD_ERR_BUDGET.  The server uses the device current at creation and the
+ * mechanism loaded then.                                                         */
+typedef struct vd_server vd_server;
+typedef struct {
+    int64_t  submitted, completed, failed, queued;
+    double   p50_ms, p99_ms, max_ms;    /* latency of completed requests            */
+    double   span_s;                    /* first submission to last completion      */
+    double   solves_per_s;              /* completed / span_s                       */
+    double   cell_updates_per_s;        /* sum of cells x steps completed / span_s  */
+    uint64_t bytes_budget, peak_bytes_used;
+    int64_t  quanta, graph_builds;
+} vd_server_stats;
+
+int vd_server_create(vd_server** out, int precision, uint64_t hbm_budget_bytes, int max_cases,
+                     int quantum_steps);
+int vd_server_destroy(vd_server* s);   /* stops the worker; unfinished requests fail */
+int vd_server_submit(vd_server* s, const vd_box* bx, const double* state,
+                     const double* const efield_ec[3], const double* const gradne_fc[3],
+                     const vd_params* prm, const int32_t periodic[3], int64_t nsteps,
+                     int64_t* request_id);
+int vd_server_wait(vd_server* s, int64_t request_id, double* state_out, double timeout_s,
+                   double* latency_ms);
+int vd_server_get_stats(vd_server* s, vd_server_stats* out);
 
 /* ---- measurement (no reference counterpart; the reference only prints the
  * whole-run wall time, Source/main.cpp:45-46) --------------------------------

@@ -239,3 +239,20 @@ PROTOTYPES.update({
     "vd_batch_set_graph": (C.c_int, [C.c_void_p, C.c_int]),
     "vd_batch_get_stats": (C.c_int, [C.c_void_p, C.POINTER(VdBatchStats)]),
 })
+
+
+class VdServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64), ("queued", C.c_int64),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double), ("span_s", C.c_double),
+                ("solves_per_s", C.c_double), ("cell_updates_per_s", C.c_double), ("bytes_budget", C.c_uint64),
+                ("peak_bytes_used", C.c_uint64), ("quanta", C.c_int64), ("graph_builds", C.c_int64)]
+
+
+PROTOTYPES.update({
+    "vd_server_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_uint64, C.c_int, C.c_int]),
+    "vd_server_destroy": (C.c_int, [C.c_void_p]),
+    "vd_server_submit": (C.c_int, [C.c_void_p, BOXP, C.c_void_p, DPP, DPP, PRMP, I32P, C.c_int64,
+                                   C.POINTER(C.c_int64)]),
+    "vd_server_wait": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_double, C.POINTER(C.c_double)]),
+    "vd_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(VdServerStats)]),
+})

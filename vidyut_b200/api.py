@@ -312,3 +312,66 @@ def batch_tile_shape(dim: int, variant: int):
     if n < 0:
         abi.check(n, "vd_batch_tile_shape")
     return tuple(t), n
+
+
+class Server:
+    """Continuous-batching request loop on one GPU (vd_server_* of the C ABI).
+    submit() queues a case and returns at once; the library's worker thread admits
+    it when the HBM budget has room, steps it together with every other resident
+    case and brings its final state back; wait() blocks for it."""
+
+    def __init__(self, precision=abi.PREC_MIXED, budget_bytes: int = 4 << 30, max_cases: int = 1024,
+                 quantum_steps: int = 25):
+        self._h = C.c_void_p()
+        abi.check(abi.lib().vd_server_create(C.byref(self._h), int(precision), int(budget_bytes), int(max_cases),
+                                             int(quantum_steps)), "vd_server_create")
+        self.precision = int(precision)
+        self.requests = {}
+
+    def close(self) -> None:
+        if self._h:
+            abi.lib().vd_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # pragma: no cover
+            pass
+
+    def submit(self, case: BoxCase, prm: abi.VdParams, nsteps: int) -> int:
+        H = stencil_halo(prm.hyp_order)
+        st = trim_ghosts(case, case.state, H)
+        ef = [np.ascontiguousarray(case.efield[d]) for d in range(3)]
+        gn = [np.ascontiguousarray(case.gradne[d]) for d in range(3)]
+        efp = (C.c_void_p * 3)(*[a.ctypes.data for a in ef])
+        gnp = (C.c_void_p * 3)(*[a.ctypes.data for a in gn])
+        per = (C.c_int32 * 3)(*[int(p) for p in case.periodic])
+        rid = C.c_int64()
+        rc = abi.lib().vd_server_submit(self._h, C.byref(abi.make_box(case.lo, case.hi, case.dim)), st.ctypes.data,
+                                        efp, gnp, C.byref(prm), per, int(nsteps), C.byref(rid))
+        abi.check(rc, "vd_server_submit")
+        self.requests[rid.value] = st.shape
+        return rid.value
+
+    def wait(self, rid: int, timeout_s: float = -1.0):
+        """(final state in the ghost-grown layout, latency in ms)"""
+        shape = self.requests.get(rid)
+        out = np.empty(shape, dtype=np.float64) if shape is not None else None
+        lat = C.c_double()
+        rc = abi.lib().vd_server_wait(self._h, int(rid), out.ctypes.data if out is not None else None,
+                                      float(timeout_s), C.byref(lat))
+        abi.check(rc, "vd_server_wait")
+        del self.requests[rid]
+        return out, lat.value
+
+    def stats(self) -> dict:
+        s = abi.VdServerStats()
+        abi.check(abi.lib().vd_server_get_stats(self._h, C.byref(s)), "vd_server_get_stats")
+        return {k: getattr(s, k) for k, _ in abi.VdServerStats._fields_}

@@ -172,7 +172,7 @@ def smooth_uniform_field(rng, n, dim: int, n_modes: int = 12, kmax: int = 2) -> 
 def build_case(mech: Mechanism, dim: int, n, dx, seed: int, *, density="loguniform",
                dens_range=(1e8, 1e22), blob_peak_exp=(14.0, 18.0), floor=1e10, bg_density=2.4e25,
                te_range_ev=(0.5, 5.0), voltage=1000.0, noise=0.05, ghost=3, periodic=(0, 0, 0),
-               params: dict | None = None) -> BoxCase:
+               params: dict | None = None, n_modes: int = 12) -> BoxCase:
     """Seeded box: species densities (``loguniform``: independent per cell and
     species; ``loguniform_smooth``: the same log-uniform marginal but spatially
     correlated over about half the box; ``blob``: the 2-D argon config's
@@ -218,7 +218,7 @@ def build_case(mech: Mechanism, dim: int, n, dx, seed: int, *, density="logunifo
             if s in bg:
                 st[(s,) + inner] = bg_density
             else:
-                st[(s,) + inner] = 10.0 ** (lo + (hi - lo) * smooth_uniform_field(rng, n, dim))
+                st[(s,) + inner] = 10.0 ** (lo + (hi - lo) * smooth_uniform_field(rng, n, dim, n_modes))
     else:
         lo, hi = np.log10(dens_range[0]), np.log10(dens_range[1])
         for s in range(ns):
@@ -352,3 +352,31 @@ def config_batched(seed: int = BASE_SEED, n_cases: int = 64, side=(64, 512), n_s
                                 dens_range=dens_range, te_range_ev=(0.3, 10.0), voltage=1000.0,
                                 params=dict(MULTISTEP_PARAMS)))
     return mech, cases
+
+
+def config_serving(seed: int = BASE_SEED, n_requests: int = 48, rate_per_s: float = 500.0,
+                   side=(256, 1024), steps=(50, 2000), voltage_kv=(0.5, 5.0), pressure_bar=(0.1, 10.0),
+                   frac_2d: float = 0.5):
+    """Serving workload: a Poisson request stream at rate_per_s of 1-D and 2-D
+    discharge cases (2-D with probability frac_2d).  Each case: sides log-uniform
+    in `side` cells, applied voltage uniform in voltage_kv (the potential ramp's
+    amplitude), pressure log-uniform in pressure_bar scaling the background gas
+    (2.4e25 m^-3 at 1 bar), step count log-uniform in `steps`, the batched
+    workload's 8-species / 40-reaction mechanism.  Returns (mechanism, [(arrival
+    time [s], BoxCase, nsteps)])."""
+    mech = synthetic(8, 40, seed + 21)
+    rng = np.random.default_rng(seed + 31)
+    t = 0.0
+    out = []
+    for i in range(n_requests):
+        t += float(rng.exponential(1.0 / rate_per_s))
+        dim = 2 if rng.uniform() < frac_2d else 1
+        n = tuple(int(round(float(np.exp(rng.uniform(np.log(side[0]), np.log(side[1])))))) for _ in range(dim))
+        v = float(rng.uniform(*voltage_kv)) * 1e3
+        p = float(np.exp(rng.uniform(np.log(pressure_bar[0]), np.log(pressure_bar[1]))))
+        ns = int(round(float(np.exp(rng.uniform(np.log(steps[0]), np.log(steps[1]))))))
+        case = build_case(mech, dim, n, (1e-5,) * dim, seed + 5000 + i, density="loguniform_smooth",
+                          dens_range=(1e10, 1e18), te_range_ev=(0.3, 10.0), voltage=v, bg_density=2.4e25 * p,
+                          params=dict(MULTISTEP_PARAMS), n_modes=4)
+        out.append((t, case, ns))
+    return mech, out
