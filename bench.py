@@ -600,7 +600,8 @@ def measure_batched(steps: int, warmup: int, *, cpu_seconds: float = 0.0, e2e: b
     tune_ms = bm.tune(trials=3)
     out["tuner_ms"] = {f"{d}d_v{v}": round(ms, 4) for (d, v), ms in tune_ms.items()}
     out["tile_variant_2d"] = bm.stats()["tile_variant"][2]
-    out["tile_2d"] = list(api.batch_tile_shape(2, out["tile_variant_2d"])[0][:2])
+    shp, _, minb = api.batch_tile_shape(2, out["tile_variant_2d"])
+    out["tile_2d"] = list(shp[:2]) + [f"{minb} CTAs/SM"]
     clock = ClockSampler(torch.cuda.current_device())
     clock.start()
     ms, launches = timed(lambda: solve(bm, idm, init_dev), steps, warmup)

@@ -358,11 +358,13 @@ int      vd_batch_load_case(vd_batch* b, int32_t case_id, const double* state, i
                             void* stream);
 /* autotuner: times the transport kernel of each tile variant on the resident cases
  * (trials launches each; the state is not advanced), keeps the fastest per
- * dimension and makes it the default of later batches.  ms_out (16 doubles or
- * NULL): ms_out[dim*4 + variant], -1 where not timed.                           */
+ * dimension and makes it the default of later batches.  ms_out (32 doubles or
+ * NULL): ms_out[dim*8 + variant], -1 where not timed.                           */
 int      vd_batch_tune(vd_batch* b, int trials, void* stream, double* ms_out);
 int      vd_batch_set_tile_variant(vd_batch* b, int dim, int variant);
-int      vd_batch_tile_shape(int dim, int variant, int32_t tile[3]);  /* returns the variant count */
+/* tile shape and target resident CTAs per SM of a transport variant (min_blocks may
+ * be NULL); returns the number of variants of that dimension                    */
+int      vd_batch_tile_shape(int dim, int variant, int32_t tile[3], int32_t* min_blocks);
 int      vd_batch_set_graph(vd_batch* b, int on);  /* 0: launch kernels directly */
 int      vd_batch_get_stats(vd_batch* b, vd_batch_stats* out);
 

@@ -189,7 +189,7 @@ def test_graph_and_direct_launches_agree(mech):
     assert sa["graph_builds"] >= 1 and sb["graph_builds"] == 0
 
 
-@pytest.mark.parametrize("variant", [1, 2])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 6])
 def test_tile_variants_agree(mech, variant):
     cases = make_cases(mech, [(37, 29), (90,)], seed=11)
     a, _ = run_batch(cases, abi.PREC_FP64, 3, variant=0)

@@ -235,7 +235,7 @@ PROTOTYPES.update({
     "vd_batch_load_case": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p]),
     "vd_batch_tune": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, DP]),
     "vd_batch_set_tile_variant": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
-    "vd_batch_tile_shape": (C.c_int, [C.c_int, C.c_int, I32P]),
+    "vd_batch_tile_shape": (C.c_int, [C.c_int, C.c_int, I32P, I32P]),
     "vd_batch_set_graph": (C.c_int, [C.c_void_p, C.c_int]),
     "vd_batch_get_stats": (C.c_int, [C.c_void_p, C.POINTER(VdBatchStats)]),
 })

@@ -288,9 +288,9 @@ class Batch:
                   "vd_batch_load_case")
 
     def tune(self, trials: int = 5, stream=None) -> dict:
-        ms = (C.c_double * 16)()
+        ms = (C.c_double * 32)()
         abi.check(abi.lib().vd_batch_tune(self._h, int(trials), _stream(stream), ms), "vd_batch_tune")
-        return {(d, v): ms[d * 4 + v] for d in range(1, 4) for v in range(4) if ms[d * 4 + v] >= 0}
+        return {(d, v): ms[d * 8 + v] for d in range(1, 4) for v in range(8) if ms[d * 8 + v] >= 0}
 
     def set_tile_variant(self, dim: int, variant: int) -> None:
         abi.check(abi.lib().vd_batch_set_tile_variant(self._h, int(dim), int(variant)), "vd_batch_set_tile_variant")
@@ -307,11 +307,13 @@ class Batch:
 
 
 def batch_tile_shape(dim: int, variant: int):
+    """(tile shape, number of variants of dim, target resident CTAs per SM)"""
     t = (C.c_int32 * 3)()
-    n = abi.lib().vd_batch_tile_shape(int(dim), int(variant), t)
+    mb = C.c_int32()
+    n = abi.lib().vd_batch_tile_shape(int(dim), int(variant), t, C.byref(mb))
     if n < 0:
         abi.check(n, "vd_batch_tile_shape")
-    return tuple(t), n
+    return tuple(t), n, mb.value
 
 
 class Server:

@@ -772,13 +772,14 @@ int vd_batch_set_tile_variant(vd_batch* b, int dim, int variant)
     return VD_OK;
 }
 
-int vd_batch_tile_shape(int dim, int variant, int32_t tile[3])
+int vd_batch_tile_shape(int dim, int variant, int32_t tile[3], int32_t* min_blocks)
 {
     if (dim < 1 || dim > 3) return err(VD_ERR_DIM, "dim %d", dim);
     if (variant < 0 || variant >= batch_tile_variants(dim)) return err(VD_ERR_ARG, "variant %d", variant);
     int t[3];
     batch_tile_shape(dim, variant, t);
     for (int d = 0; d < 3; d++) tile[d] = t[d];
+    if (min_blocks) *min_blocks = batch_variant_minblocks(dim, variant);
     return batch_tile_variants(dim);
 }
 
@@ -800,7 +801,7 @@ int vd_batch_tune(vd_batch* b, int trials, void* stream, double* ms_out)
     if ((rc = check_device(b)) || (rc = check_mech(b))) return rc;
     const int nb = (int)b->cases.size();
     if (ms_out)
-        for (int i = 0; i < 16; i++) ms_out[i] = -1.0;
+        for (int i = 0; i < 32; i++) ms_out[i] = -1.0;
     if (nb == 0) return VD_OK;
     cudaStream_t st = (cudaStream_t)stream;
     std::vector<int> one(nb, 1);
@@ -836,7 +837,7 @@ int vd_batch_tune(vd_batch* b, int trials, void* stream, double* ms_out)
                 break;
             }
             ms /= trials;
-            if (ms_out && v < 4) ms_out[d * 4 + v] = ms;
+            if (ms_out && v < 8) ms_out[d * 8 + v] = ms;
             if (ms < best_ms) {
                 best_ms = ms;
                 best = v;

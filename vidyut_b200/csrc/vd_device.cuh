@@ -16,8 +16,11 @@
 
 namespace vd {
 
-// The loaded mechanism (one translation unit: vd_kernels.cu includes this header).
-__constant__ VdMechDev c_mech;
+// The loaded mechanism.  Every translation unit that includes this header has its
+// own copy (internal linkage; the library is compiled without relocatable device
+// code) and uploads it through its own upload function (upload_mech in
+// vd_kernels.cu, upload_mech_batch in vd_batch_kernels.cu).
+static __constant__ VdMechDev c_mech;
 
 // Approximate reciprocal on the special-function unit (rcp.approx.ftz.f32,
 // ~1 ulp); arguments are normal positive numbers wherever it is used.

@@ -20,6 +20,7 @@
 #include <vector>
 #include "vd_device.cuh"
 #include "vd_kernels.cuh"
+#include "vd_transport.cuh"
 
 namespace vd {
 
@@ -113,6 +114,8 @@ int prof_read(char* names, int names_len, int64_t* counts, double* ms, int max)
 int upload_mech(const VdMechDev* h, cudaStream_t st)
 {
     cudaError_t e = cudaMemcpyToSymbolAsync(c_mech, h, sizeof(VdMechDev), 0, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return (int)e;
+    e = upload_mech_batch(h, st);  // the batched transport kernels' copy
     if (e != cudaSuccess) return (int)e;
     e = cudaStreamSynchronize(st);
     return (int)e;
@@ -291,56 +294,6 @@ cudaError_t launch_dsdt(const BoxIdx& b, int dim, int specid, const A4 flux[3], 
     k_dsdt<<<grid_for(b.ncell, 256), 256, 0, st>>>(b, dim, specid, flux[0], flux[1], flux[2], rxn, dsdt, dx[0],
                                                     dx[1], dx[2]);
     return cudaGetLastError();
-}
-
-// ---------------------------------------------------------------------------
-// Joule heating at one cell (Source/ElecEnergySource.cpp:76-153).  sumN: use the
-// per-cell density sums Nv (fused path) instead of re-summing the species.
-template <bool USE_N>
-__device__ __forceinline__ double joule_cell(const TransportArgs& a, int dim, int i, int j, int k)
-{
-    const int ns = a.ns, eidx = a.e_id;
-    double jheat = 0.0;
-    for (int idim = 0; idim < dim; idim++) {
-        for (int f = 0; f < 2; f++) {
-            int face[3] = {i, j, k};
-            face[idim] += f;
-            if (face[idim] == a.domlo[idim]) face[idim] += 1;
-            if (face[idim] == a.domhi[idim] + 1) face[idim] -= 1;
-            int l[3] = {face[0], face[1], face[2]};
-            l[idim] -= 1;
-            const int64_t ol = a.sb.off(l[0], l[1], l[2]);
-            const int64_t orr = a.sb.off(face[0], face[1], face[2]);
-            const double* p = a.sb.p;
-            const int64_t cs = a.sb.ns;
-            double etemp = 0.5 * (p[ol + VD_ETEMP(ns) * cs] + p[orr + VD_ETEMP(ns) * cs]);
-            double Esum = 0.0, evf_d = 0.0;
-            for (int d = 0; d < dim; d++) {
-                double e = 0.5 * (p[ol + (VD_EFX(ns) + d) * cs] + p[orr + (VD_EFX(ns) + d) * cs]);
-                Esum += e * e;
-                if (d == idim) evf_d = e;
-            }
-            (void)Esum;
-            double nel = p[ol + eidx * cs], ner = p[orr + eidx * cs];
-            double ne = 0.5 * (nel + ner);
-            double ef = a.cs_technique ? evf_d : a.ef[idim](face[0], face[1], face[2]);
-            double gn = a.gradne_from_state ? (ner - nel) / a.dx[idim] : a.gne[idim](face[0], face[1], face[2]);
-            double ndens;
-            if (USE_N) {
-                ndens = 0.5 * (a.Nv(l[0], l[1], l[2]) + a.Nv(face[0], face[1], face[2]));
-            } else {
-                ndens = 0.0;
-                for (int s = 0; s < ns; s++) ndens += 0.5 * (p[ol + s * cs] + p[orr + s * cs]);
-            }
-            double mu = a.const_ele_trans ? a.ele_mob / ndens : mob_fp64(eidx, etemp, ndens, a.Tg);
-            double dc = a.const_ele_trans ? a.ele_diff / ndens : diff_fp64(eidx, etemp, ndens, a.Tg);
-            double cur = a.charge_e * (mu * ne * ef - dc * gn);
-            jheat += cur * ef;
-        }
-    }
-    jheat *= 0.5;
-    if (a.floor_jh && jheat < 0.0) jheat = 0.0;
-    return jheat;
 }
 
 __global__ void __launch_bounds__(128) k_joule(BoxIdx b, int dim, const __grid_constant__ TransportArgs a)
@@ -589,9 +542,6 @@ cudaError_t launch_prep(const PrepArgs& a, int prec, int ns, cudaStream_t st)
 
 // ---------------------------------------------------------------------------
 // Fused transport kernel (vd_transport.cuh): tile shapes and the tile update.
-}  // namespace vd
-#include "vd_transport.cuh"
-namespace vd {
 
 // The mobility models of specMob (test/models/Ar_DC_1d/Chemistry.H:177-202) as a
 // species constant K times a per-cell basis: electron-type mu = c/(sqrt(Te) N s0)
@@ -661,13 +611,14 @@ template <int DIM, int PREC, int MINB>
 static cudaError_t launch_tr(const TransportArgs& a, cudaStream_t st)
 {
     using TS = typename DefaultTile<DIM>::T;
-    const size_t smem = transport_smem<DIM, PREC, TS>(a.nb);
+    constexpr int GRP = group_fit<DIM, PREC, TS, MINB>();
+    const size_t smem = transport_smem<DIM, PREC, TS, GRP>(a.nb);
     static unsigned attr_set = 0;  // one bit per device
     int dev = 0;
     cudaGetDevice(&dev);
     if (!(attr_set & (1u << (dev & 31)))) {
         cudaError_t e = cudaFuncSetAttribute(k_transport<DIM, PREC, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)transport_smem_max<DIM, PREC, TS>());
+                                             (int)transport_smem_max<DIM, PREC, TS, GRP>());
         if (e != cudaSuccess) return e;
         attr_set |= 1u << (dev & 31);
     }
@@ -751,93 +702,6 @@ cudaError_t launch_transport(const TransportArgs& a, int dim, int prec, cudaStre
     return launch_tr_v<3, PREC_FP64>(a, st);
 }
 
-// ---------------------------------------------------------------------------
-// Batched transport: tile-shape variants per dimension (chosen by the batch tuner).
-template <int DIM> struct BatchTiles;
-template <> struct BatchTiles<1> {
-    static constexpr int N = 2;
-    using V0 = TileShape<256, 1, 1, 256>;
-    using V1 = TileShape<128, 1, 1, 128>;
-    using V2 = V1;
-};
-template <> struct BatchTiles<2> {
-    static constexpr int N = 3;
-    using V0 = TileShape<32, 8, 1, 256>;
-    using V1 = TileShape<16, 16, 1, 256>;
-    using V2 = TileShape<64, 4, 1, 256>;
-};
-template <> struct BatchTiles<3> {
-    static constexpr int N = 2;
-    using V0 = TileShape<8, 8, 8, 512>;
-    using V1 = TileShape<16, 8, 4, 512>;
-    using V2 = V1;
-};
-
-int batch_tile_variants(int dim) { return dim == 1 ? BatchTiles<1>::N : dim == 2 ? BatchTiles<2>::N : BatchTiles<3>::N; }
-
-template <class TS> static void tile_of(int t[3]) { t[0] = TS::X; t[1] = TS::Y; t[2] = TS::Z; }
-
-template <int DIM> static void batch_tile_shape_d(int v, int t[3])
-{
-    if (v == 0) tile_of<typename BatchTiles<DIM>::V0>(t);
-    else if (v == 1) tile_of<typename BatchTiles<DIM>::V1>(t);
-    else tile_of<typename BatchTiles<DIM>::V2>(t);
-}
-
-void batch_tile_shape(int dim, int v, int t[3])
-{
-    if (dim == 1) batch_tile_shape_d<1>(v, t);
-    else if (dim == 2) batch_tile_shape_d<2>(v, t);
-    else batch_tile_shape_d<3>(v, t);
-}
-
-template <int DIM, int PREC, class TS>
-static cudaError_t launch_trb(const TransportArgs* boxes, const int2* items, int nitems, BatchCtl ctl, cudaStream_t st)
-{
-    constexpr int MINB = 2;
-    constexpr size_t smem = transport_smem_max<DIM, PREC, TS>();  // boxes differ in basis count
-    auto fn = k_transport_batch<DIM, PREC, TS, MINB>;
-    static int grid_of[32] = {0};  // persistent grid (SMs x resident CTAs), per device
-    int dev = 0;
-    cudaGetDevice(&dev);
-    int& grid = grid_of[dev & 31];
-    if (!grid) {
-        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        int nsm = 148, per_sm = 1;
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, TS::NTH, smem);
-        if (e != cudaSuccess) return e;
-        grid = nsm * (per_sm < 1 ? 1 : per_sm);
-    }
-    int g = grid < nitems ? grid : nitems;
-    ProfScope ps("k_transport_batch", st);
-    fn<<<g, TS::NTH, smem, st>>>(boxes, items, nitems, ctl);
-    return cudaGetLastError();
-}
-
-template <int DIM, int PREC>
-static cudaError_t launch_trb_v(const TransportArgs* boxes, const int2* items, int nitems, BatchCtl ctl, int v,
-                                cudaStream_t st)
-{
-    if (v == 1) return launch_trb<DIM, PREC, typename BatchTiles<DIM>::V1>(boxes, items, nitems, ctl, st);
-    if (v == 2) return launch_trb<DIM, PREC, typename BatchTiles<DIM>::V2>(boxes, items, nitems, ctl, st);
-    return launch_trb<DIM, PREC, typename BatchTiles<DIM>::V0>(boxes, items, nitems, ctl, st);
-}
-
-cudaError_t launch_transport_batch(const TransportArgs* boxes, const int2* items, int nitems, BatchCtl ctl, int dim,
-                                   int prec, int variant, cudaStream_t st)
-{
-    if (nitems <= 0) return cudaSuccess;
-    if (prec == PREC_MIXED) {
-        if (dim == 1) return launch_trb_v<1, PREC_MIXED>(boxes, items, nitems, ctl, variant, st);
-        if (dim == 2) return launch_trb_v<2, PREC_MIXED>(boxes, items, nitems, ctl, variant, st);
-        return launch_trb_v<3, PREC_MIXED>(boxes, items, nitems, ctl, variant, st);
-    }
-    if (dim == 1) return launch_trb_v<1, PREC_FP64>(boxes, items, nitems, ctl, variant, st);
-    if (dim == 2) return launch_trb_v<2, PREC_FP64>(boxes, items, nitems, ctl, variant, st);
-    return launch_trb_v<3, PREC_FP64>(boxes, items, nitems, ctl, variant, st);
-}
 
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_checksums(BoxIdx b, A4 rxn, A4 pn, double* out)

@@ -71,6 +71,7 @@ struct GhostArgs {
 };
 
 int upload_mech(const VdMechDev* h, cudaStream_t st);
+cudaError_t upload_mech_batch(const VdMechDev* h, cudaStream_t st);  // vd_batch_kernels.cu
 
 // Step control of a batched launch.  ctrl[c] = {steps case c takes in this call,
 // index (0/1) of the buffer holding its current state}.  At step t a work item of
@@ -96,6 +97,7 @@ cudaError_t launch_ghost(const GhostArgs& a, cudaStream_t st);
 // tile shapes of the batched transport kernel: variant v of dimension dim
 int batch_tile_variants(int dim);
 void batch_tile_shape(int dim, int variant, int t[3]);
+int batch_variant_minblocks(int dim, int variant);  // resident CTAs per SM the variant targets
 
 cudaError_t launch_reaction_source(const BoxIdx& b, const A4& sb, const A4& rxn, double Tg, int prec, int ns,
                                    cudaStream_t st);

@@ -19,8 +19,60 @@
 // tile) and the batched persistent kernel (CTAs loop over a work list of
 // (box, tile) items of many boxes) share it.
 #pragma once
+#include "vd_device.cuh"
+#include "vd_kernels.cuh"
 
 namespace vd {
+
+// ---------------------------------------------------------------------------
+// Joule heating at one cell (Source/ElecEnergySource.cpp:76-153).  USE_N: use the
+// per-cell density sums Nv (fused path) instead of re-summing the species.
+template <bool USE_N>
+__device__ __forceinline__ double joule_cell(const TransportArgs& a, int dim, int i, int j, int k)
+{
+    const int ns = a.ns, eidx = a.e_id;
+    double jheat = 0.0;
+    for (int idim = 0; idim < dim; idim++) {
+        for (int f = 0; f < 2; f++) {
+            int face[3] = {i, j, k};
+            face[idim] += f;
+            if (face[idim] == a.domlo[idim]) face[idim] += 1;
+            if (face[idim] == a.domhi[idim] + 1) face[idim] -= 1;
+            int l[3] = {face[0], face[1], face[2]};
+            l[idim] -= 1;
+            const int64_t ol = a.sb.off(l[0], l[1], l[2]);
+            const int64_t orr = a.sb.off(face[0], face[1], face[2]);
+            const double* p = a.sb.p;
+            const int64_t cs = a.sb.ns;
+            double etemp = 0.5 * (p[ol + VD_ETEMP(ns) * cs] + p[orr + VD_ETEMP(ns) * cs]);
+            double Esum = 0.0, evf_d = 0.0;
+            for (int d = 0; d < dim; d++) {
+                double e = 0.5 * (p[ol + (VD_EFX(ns) + d) * cs] + p[orr + (VD_EFX(ns) + d) * cs]);
+                Esum += e * e;
+                if (d == idim) evf_d = e;
+            }
+            (void)Esum;
+            double nel = p[ol + eidx * cs], ner = p[orr + eidx * cs];
+            double ne = 0.5 * (nel + ner);
+            double ef = a.cs_technique ? evf_d : a.ef[idim](face[0], face[1], face[2]);
+            double gn = a.gradne_from_state ? (ner - nel) / a.dx[idim] : a.gne[idim](face[0], face[1], face[2]);
+            double ndens;
+            if (USE_N) {
+                ndens = 0.5 * (a.Nv(l[0], l[1], l[2]) + a.Nv(face[0], face[1], face[2]));
+            } else {
+                ndens = 0.0;
+                for (int s = 0; s < ns; s++) ndens += 0.5 * (p[ol + s * cs] + p[orr + s * cs]);
+            }
+            double mu = a.const_ele_trans ? a.ele_mob / ndens : mob_fp64(eidx, etemp, ndens, a.Tg);
+            double dc = a.const_ele_trans ? a.ele_diff / ndens : diff_fp64(eidx, etemp, ndens, a.Tg);
+            double cur = a.charge_e * (mu * ne * ef - dc * gn);
+            jheat += cur * ef;
+        }
+    }
+    jheat *= 0.5;
+    if (a.floor_jh && jheat < 0.0) jheat = 0.0;
+    return jheat;
+}
 
 template <int X_, int Y_, int Z_, int NTH_>
 struct TileShape {
@@ -31,10 +83,6 @@ template <> struct DefaultTile<1> { using T = TileShape<256, 1, 1, 256>; };
 template <> struct DefaultTile<2> { using T = TileShape<32, 8, 1, 256>; };
 template <> struct DefaultTile<3> { using T = TileShape<8, 8, 8, 512>; };
 template <int DIM> constexpr int default_nth() { return DIM == 3 ? 512 : 256; }
-// species per group: all fluxed species of a small mechanism in one group in 1-D
-// and 2-D; in 3-D the staged lines are 5x the tile, so groups of 2 (FP32 staging)
-// or 1 (FP64) keep two CTAs of 512 threads resident
-template <int DIM, int PREC> constexpr int group_size() { return DIM == 3 ? (PREC == PREC_MIXED ? 2 : 1) : 8; }
 
 template <int DIM, class TS>
 struct TileGeom {
@@ -52,16 +100,30 @@ struct TileGeom {
 template <int PREC> struct VelT { using T = double; };
 template <> struct VelT<PREC_MIXED> { using T = float; };
 
-// dynamic shared memory of one tile with nb velocity bases: the group's face
-// fluxes and the Joule term of every face (FP64), then the bases and the group's
-// staged densities (FP32 in the mixed path)
-template <int DIM, int PREC, class TS>
+// dynamic shared memory of one tile with nb velocity bases and species groups of
+// GRP: the group's face fluxes and the Joule term of every face (FP64), then the
+// bases and the group's staged densities (FP32 in the mixed path)
+template <int DIM, int PREC, class TS, int GRP>
 __host__ __device__ constexpr size_t transport_smem(int nb)
 {
     using G = TileGeom<DIM, TS>;
-    constexpr int GRP = group_size<DIM, PREC>();
     return (size_t)(GRP + 1) * G::FTOT * sizeof(double) +
            (size_t)(nb + GRP) * G::STOT * sizeof(typename VelT<PREC>::T);
+}
+
+// Species per group for a kernel that must keep MINB CTAs resident per SM: the
+// largest of 8, 4, 2, 1 whose tile (with up to three velocity bases, the batched
+// kernel's copy of its record and the driver's reserve) fits MINB times into the
+// SM's 228 KB of shared memory.  Larger groups mean fewer barriers and more loads
+// in flight; smaller ones leave room for more resident CTAs.
+template <int DIM, int PREC, class TS, int MINB>
+constexpr int group_fit()
+{
+    constexpr size_t per_sm = 228 * 1024, extra = 3 * 1024;
+    if ((transport_smem<DIM, PREC, TS, 8>(3) + extra) * MINB <= per_sm) return 8;
+    if ((transport_smem<DIM, PREC, TS, 4>(3) + extra) * MINB <= per_sm) return 4;
+    if ((transport_smem<DIM, PREC, TS, 2>(3) + extra) * MINB <= per_sm) return 2;
+    return 1;
 }
 
 // Joule heating carried by face g of direction D (the face between cells g - e_D
@@ -99,8 +161,8 @@ __device__ __forceinline__ double joule_face(const TransportArgs& a, int D, cons
     const double cur = a.charge_e * (mu * ne * ef - dc * gn);
     return cur * ef;
 }
-template <int DIM, int PREC, class TS>
-constexpr size_t transport_smem_max() { return transport_smem<DIM, PREC, TS>(3); }
+template <int DIM, int PREC, class TS, int GRP>
+constexpr size_t transport_smem_max() { return transport_smem<DIM, PREC, TS, GRP>(3); }
 
 // global cell of staged position cc of direction D's line set; false when the
 // position lies outside what the box's stencil may read (those stage as zero)
@@ -231,13 +293,12 @@ __device__ __forceinline__ double face_any(const TransportArgs& a, int f, int cl
 // of the CTA must call it; it returns with all shared memory reads finished
 // except those of the last group's divergence (callers that reuse the shared
 // memory for another tile synchronise first).
-template <int DIM, int PREC, class TS>
+template <int DIM, int PREC, class TS, int GRP>
 __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, int tile, unsigned char* smem)
 {
     using G = TileGeom<DIM, TS>;
     using VT = typename VelT<PREC>::T;
     constexpr int NTH = TS::NTH;
-    constexpr int GRP = group_size<DIM, PREC>();
     const int tid = threadIdx.x;
     int tb = tile;
     const int tix = tb % a.ntile[0];
@@ -418,7 +479,8 @@ template <int DIM, int PREC, int MINB>
 __global__ void __launch_bounds__(default_nth<DIM>(), MINB) k_transport(const __grid_constant__ TransportArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    transport_tile_update<DIM, PREC, typename DefaultTile<DIM>::T>(a, blockIdx.x, smem_raw);
+    using TS = typename DefaultTile<DIM>::T;
+    transport_tile_update<DIM, PREC, TS, group_fit<DIM, PREC, TS, MINB>()>(a, blockIdx.x, smem_raw);
 }
 
 // batched persistent kernel: each CTA walks the work list of (box, tile) items
@@ -447,7 +509,7 @@ __global__ void __launch_bounds__(TS::NTH, MINB)
             cur = rec;
             __syncthreads();
         }
-        transport_tile_update<DIM, PREC, TS>(sA, w.y, smem_raw);
+        transport_tile_update<DIM, PREC, TS, group_fit<DIM, PREC, TS, MINB>()>(sA, w.y, smem_raw);
         __syncthreads();  // the next item's staging (or record) must not overwrite a slow thread's reads
     }
 }
