@@ -90,14 +90,45 @@ def apply(path: Path = TUNING_FILE, force: bool = False) -> dict:
     return rec
 
 
+def tune_batch(mech, cases, precisions=(abi.PREC_MIXED, abi.PREC_FP64), trials: int = 5) -> dict:
+    """Fastest batched transport variant per dimension and precision on `cases`."""
+    from . import api
+    api.mech_init(mech)
+    out = {}
+    for prec in precisions:
+        pname = "mixed" if prec == abi.PREC_MIXED else "fp64"
+        need = sum(api.Batch.case_bytes(c, c.vd_params(precision=prec)) for c in cases)
+        with api.Batch(prec, budget_bytes=int(need * 1.05) + (64 << 20), max_cases=len(cases)) as b:
+            for c in cases:
+                b.add(c, c.vd_params(precision=prec))
+            b.step(1)
+            ms = b.tune(trials=trials)
+            st = b.stats()
+        dims = sorted({d for d, _ in ms})
+        for d in dims:
+            times = {v: t for (dd, v), t in ms.items() if dd == d}
+            out[f"batch_tile_{d}d_{pname}"] = {
+                "best": int(st["tile_variant"][d]), "ms": {str(k): round(v, 5) for k, v in times.items()},
+                "workload": f"{mech.name} batch of {len(cases)} {d}-D cases"}
+    return out
+
+
 def main() -> int:
     from . import inputs
     res = {}
-    for case in (inputs.config_argon2d(), inputs.config_precision3d()):
+    mech_b, cases_b = inputs.config_batched()
+    one_d = inputs.build_case(mech_b, 1, (1000,), (1e-5,), inputs.BASE_SEED + 77, density="loguniform_smooth",
+                              dens_range=(1e10, 1e18), te_range_ev=(0.3, 10.0), n_modes=4,
+                              params=dict(inputs.MULTISTEP_PARAMS))
+    for case in (max(cases_b, key=lambda c: c.ncell), one_d, inputs.config_precision3d()):
         r = tune_transport(case)
         res.update(r)
         for k, v in r.items():
             print(k, v, flush=True)
+    r = tune_batch(mech_b, cases_b)
+    res.update(r)
+    for k, v in r.items():
+        print(k, v, flush=True)
     save(res)
     print("wrote", TUNING_FILE)
     return 0
