@@ -302,6 +302,31 @@ int vd_box_checksums(const vd_box* bx, vd_array4 rxn, vd_array4 phi_new,
 int vd_fill_ghosts(const vd_box* bx, vd_array4 state, int ghost, const int32_t* comps, int ncomp,
                    const int32_t periodic[3], void* stream);
 
+/* Potential and electric field of one box that is the whole domain, before the
+ * update (replaces the MLMG solve of Source/PotentialSolve.cpp:188-378 with the
+ * same discrete problem, and Vidyut::update_cc_efields,
+ * Source/PotentialSolve.cpp:391-430): del^2 phi = -(e/eps0) sum_k z_k n_k on the
+ * cell-centred grid, faces with bc_* == VD_BC_DIRC hold phi = value_* at the face,
+ * the others zero normal gradient.  Geometric multigrid in FP64 from the state's
+ * POT component as initial guess, V(2,2) cycles until max|residual| <=
+ * tol_rel * max|rhs| (tol_rel > 0; one host synchronisation per cycle) or
+ * max_vcycles (tol_rel == 0: exactly max_vcycles, no synchronisation).  Writes POT,
+ * EFX..EFZ (centred differences, one-sided at domain faces), REF (|E|/N in Td) in
+ * the valid cells and refills their ghosts, and efield_ec[d] = -dphi/dx_d on the
+ * face boxes (Dirichlet faces: to the face value over half a cell; unless
+ * prm->cs_technique).  Scratch (3 doubles per cell over the hierarchy) comes from
+ * the stream-ordered allocator. */
+typedef struct {
+    int32_t bc_lo[3], bc_hi[3];
+    double  value_lo[3], value_hi[3];
+    int32_t max_vcycles;
+    int32_t pad0;
+    double  tol_rel;
+} vd_poisson_params;
+int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_array4 efield_ec[3],
+                     const vd_params* prm, const vd_poisson_params* pp,
+                     int32_t* vcycles_done, double* rel_residual, void* stream);
+
 /* ---- batched cases (no single reference counterpart: the reference loops over
  * boxes with MFIter and calls the per-box functions above for each) -----------
  * A batch owns a device arena of hbm_budget_bytes and keeps every resident case's

@@ -256,3 +256,14 @@ PROTOTYPES.update({
     "vd_server_wait": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_double, C.POINTER(C.c_double)]),
     "vd_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(VdServerStats)]),
 })
+
+
+class VdPoissonParams(C.Structure):
+    _fields_ = [("bc_lo", C.c_int32 * 3), ("bc_hi", C.c_int32 * 3), ("value_lo", C.c_double * 3),
+                ("value_hi", C.c_double * 3), ("max_vcycles", C.c_int32), ("pad0", C.c_int32),
+                ("tol_rel", C.c_double)]
+
+
+PROTOTYPES.update({
+    "vd_poisson_solve": (C.c_int, [BOXP, A4, A4P, PRMP, C.POINTER(VdPoissonParams), I32P, DP, C.c_void_p]),
+})

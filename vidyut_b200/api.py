@@ -377,3 +377,32 @@ class Server:
         s = abi.VdServerStats()
         abi.check(abi.lib().vd_server_get_stats(self._h, C.byref(s)), "vd_server_get_stats")
         return {k: getattr(s, k) for k, _ in abi.VdServerStats._fields_}
+
+
+def poisson_params(dim: int, v_lo: float, v_hi: float = 0.0, max_vcycles: int = 30, tol_rel: float = 1e-12,
+                   dirichlet_dir: int = 0) -> abi.VdPoissonParams:
+    """Applied potential v_lo at the low face and v_hi at the high face of
+    direction dirichlet_dir (the electrodes), zero normal gradient elsewhere."""
+    pp = abi.VdPoissonParams()
+    for d in range(3):
+        pp.bc_lo[d] = abi.BC_DIRC if d == dirichlet_dir else abi.BC_HNEU
+        pp.bc_hi[d] = abi.BC_DIRC if d == dirichlet_dir else abi.BC_HNEU
+    pp.value_lo[dirichlet_dir] = v_lo
+    pp.value_hi[dirichlet_dir] = v_hi
+    pp.max_vcycles = max_vcycles
+    pp.tol_rel = tol_rel
+    return pp
+
+
+def poisson_solve(dc: DeviceCase, prm: abi.VdParams, pp: abi.VdPoissonParams, state: torch.Tensor | None = None,
+                  stream=None):
+    """Potential and fields of dc (or of `state`, laid out like dc.state): writes
+    POT, EFX..EFZ, REF into the state and the face fields into dc.efield.
+    Returns (V-cycles done, relative residual or -1 when not checked)."""
+    st = state if state is not None else dc.state
+    nv = C.c_int32()
+    rr = C.c_double()
+    rc = abi.lib().vd_poisson_solve(C.byref(dc.box()), t_a4(st, dc.case.state_begin()), dc.face_a4s("efield"),
+                                    C.byref(prm), C.byref(pp), C.byref(nv), C.byref(rr), _stream(stream))
+    abi.check(rc, "vd_poisson_solve")
+    return nv.value, rr.value

@@ -1,0 +1,547 @@
+// vd_poisson.cu -- the potential / electric-field step before the explicit update
+// (vd_poisson_solve in vidyut_b200.h).
+//
+// The reference solves del^2 phi = -(e/eps0) sum_k z_k n_k with AMReX's MLMG
+// (Source/PotentialSolve.cpp:188-378), takes the face field -grad phi from the
+// solver and the cell field by centred (one-sided at domain faces) differences of
+// phi, and the reduced field |E|/N (Source/PotentialSolve.cpp:391-430,
+// Source/HelperFuncs.H:14-70).  AMReX is not part of this library, so this file
+// carries a self-contained geometric multigrid for the same discrete problem on
+// one box that is the whole domain: cell-centred 2D+1-point Laplacian, Dirichlet
+// faces (the applied potential at the face) or zero-gradient faces, V(2,2) cycles
+// of red-black Gauss-Seidel, full-weighting restriction, linear prolongation, a
+// 64-sweep bottom solve on the coarsest grid.  All in FP64.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+#include "vd_host.h"
+
+namespace vd {
+namespace {
+
+constexpr double EPS0 = 8.854187817e-12;  // Source/UnivConstants.H:12
+
+struct Level {
+    int n[3];          // cells per direction (1 beyond dim)
+    double idx2[3];    // 1/dx^2 (0 beyond dim)
+    double* phi;
+    double* rhs;
+    double* res;
+    __host__ __device__ int64_t cells() const { return (int64_t)n[0] * n[1] * n[2]; }
+};
+
+struct BcInfo {
+    int dir_lo[3], dir_hi[3];    // 1: Dirichlet face
+    double val_lo[3], val_hi[3]; // its value (0 on the correction levels)
+};
+
+__device__ __forceinline__ void cell3(const Level& L, int64_t c, int& i, int& j, int& k)
+{
+    k = (int)(c / ((int64_t)L.n[0] * L.n[1]));
+    int64_t r = c - (int64_t)k * L.n[0] * L.n[1];
+    j = (int)(r / L.n[0]);
+    i = (int)(r - (int64_t)j * L.n[0]);
+}
+
+__device__ __forceinline__ int64_t lin(const Level& L, int i, int j, int k)
+{
+    return (int64_t)i + (int64_t)L.n[0] * (j + (int64_t)L.n[1] * k);
+}
+
+// Off-diagonal sum and diagonal of the Laplacian at cell (i,j,k), with the domain
+// faces folded in.  Each face of the cell contributes (phi_out - phi_c)/dx^2: an
+// inside neighbour adds phi_nb and -phi_c; a Dirichlet face holds phi = V at the
+// face, so phi_out = 2V - phi_c (constant 2V/dx^2, diagonal -2/dx^2); a
+// zero-gradient face has phi_out = phi_c and adds nothing.
+__device__ __forceinline__ void stencil(const Level& L, const BcInfo& bc, int dim, int i, int j, int k,
+                                        const double* phi, double& off, double& diag)
+{
+    const int c[3] = {i, j, k};
+    off = 0.0;
+    diag = 0.0;
+    for (int d = 0; d < dim; d++) {
+        const double w = L.idx2[d];
+        int m[3] = {i, j, k}, p[3] = {i, j, k};
+        m[d] -= 1;
+        p[d] += 1;
+        if (c[d] > 0) {
+            off += w * phi[lin(L, m[0], m[1], m[2])];
+            diag -= w;
+        } else if (bc.dir_lo[d]) {
+            off += 2.0 * w * bc.val_lo[d];
+            diag -= 2.0 * w;
+        }
+        if (c[d] < L.n[d] - 1) {
+            off += w * phi[lin(L, p[0], p[1], p[2])];
+            diag -= w;
+        } else if (bc.dir_hi[d]) {
+            off += 2.0 * w * bc.val_hi[d];
+            diag -= 2.0 * w;
+        }
+    }
+}
+
+__global__ void k_mg_rbgs(Level L, BcInfo bc, int dim, int color)
+{
+    const int64_t nc = L.cells();
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell3(L, c, i, j, k);
+        if (((i + j + k) & 1) != color) continue;
+        double off, diag;
+        stencil(L, bc, dim, i, j, k, L.phi, off, diag);
+        // L phi = off + diag phi = rhs  ->  phi = (rhs - off) / diag
+        L.phi[c] = (L.rhs[c] - off) / diag;
+    }
+}
+
+__global__ void k_mg_residual(Level L, BcInfo bc, int dim, unsigned long long* maxabs)
+{
+    const int64_t nc = L.cells();
+    double m = 0.0;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell3(L, c, i, j, k);
+        double off, diag;
+        stencil(L, bc, dim, i, j, k, L.phi, off, diag);
+        const double r = L.rhs[c] - (off + diag * L.phi[c]);
+        L.res[c] = r;
+        m = fmax(m, fabs(r));
+    }
+    if (maxabs) {
+        // non-negative doubles order like their bit patterns
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((threadIdx.x & 31) == 0) atomicMax(maxabs, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+// coarse rhs = average of the 2^dim fine residuals (full weighting for cell centres)
+__global__ void k_mg_restrict(Level F, Level C, int dim)
+{
+    const int64_t nc = C.cells();
+    const double w = 1.0 / (double)(1 << dim);
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell3(C, c, i, j, k);
+        double s = 0.0;
+        for (int dz = 0; dz < (dim > 2 ? 2 : 1); dz++)
+            for (int dy = 0; dy < (dim > 1 ? 2 : 1); dy++)
+                for (int dx = 0; dx < 2; dx++)
+                    s += F.res[lin(F, (dim > 0 ? 2 * i + dx : i), (dim > 1 ? 2 * j + dy : j), (dim > 2 ? 2 * k + dz : k))];
+        C.rhs[c] = w * s;
+        C.phi[c] = 0.0;
+    }
+}
+
+// fine phi += linear interpolation of the coarse correction (weights 3/4, 1/4 per
+// direction; at a domain face the outside coarse value is the correction's
+// boundary value: -c for a Dirichlet face (zero at the face), c for zero gradient)
+__global__ void k_mg_prolong(Level F, Level C, BcInfo bc, int dim)
+{
+    const int64_t nf = F.cells();
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nf; c += (int64_t)gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell3(F, c, i, j, k);
+        const int f[3] = {i, j, k};
+        int ci[3] = {0, 0, 0}, nb[3] = {0, 0, 0};
+        for (int d = 0; d < 3; d++) {
+            if (d < dim) {
+                ci[d] = f[d] >> 1;
+                nb[d] = (f[d] & 1) ? 1 : -1;  // the other coarse cell this fine cell leans towards
+            } else {
+                ci[d] = f[d];
+            }
+        }
+        double acc = 0.0;
+        for (int mz = 0; mz < (dim > 2 ? 2 : 1); mz++)
+            for (int my = 0; my < (dim > 1 ? 2 : 1); my++)
+                for (int mx = 0; mx < 2; mx++) {
+                    const int m[3] = {mx, my, mz};
+                    double w = 1.0;
+                    int q[3] = {ci[0], ci[1], ci[2]};
+                    double sign = 1.0;
+                    for (int d = 0; d < dim; d++) {
+                        w *= m[d] ? 0.25 : 0.75;
+                        if (m[d]) {
+                            q[d] += nb[d];
+                            if (q[d] < 0) {
+                                q[d] = 0;
+                                if (bc.dir_lo[d]) sign = -sign;
+                            } else if (q[d] >= C.n[d]) {
+                                q[d] = C.n[d] - 1;
+                                if (bc.dir_hi[d]) sign = -sign;
+                            }
+                        }
+                    }
+                    acc += w * sign * C.phi[lin(C, q[0], q[1], q[2])];
+                }
+        F.phi[c] += acc;
+    }
+}
+
+__global__ void k_maxabs(const double* x, int64_t n, unsigned long long* out)
+{
+    double m = 0.0;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(x[c]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+struct PoisArgs {
+    A4 st;
+    int lo[3], hi[3];
+    int ns, dim;
+    int8_t charge[VD_MAX_SPECIES];
+};
+
+// rhs = -(e/eps0) sum_k z_k n_k (Source/PotentialSolve.cpp:199-215); initial guess
+// phi = the state's potential
+__global__ void k_pois_rhs(PoisArgs a, Level L)
+{
+    const int64_t nc = L.cells();
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell3(L, c, i, j, k);
+        const int64_t o = a.st.off(a.lo[0] + i, a.lo[1] + j, a.lo[2] + k);
+        double r = 0.0;
+        for (int s = 0; s < a.ns; s++)
+            if (a.charge[s] != 0) r += (double)a.charge[s] * a.st.p[o + (int64_t)s * a.st.ns];
+        L.rhs[c] = r * (-ECHARGE / EPS0);
+        L.phi[c] = a.st.p[o + (int64_t)VD_POT(a.ns) * a.st.ns];
+    }
+}
+
+// potential, cell field (Source/HelperFuncs.H:14-70) and reduced field
+// (Source/PotentialSolve.cpp:419-424) of the valid cells
+struct D3 {
+    double v[3];
+};
+
+__global__ void k_pois_cell_fields(PoisArgs a, Level L, D3 dxs)
+{
+    const int64_t nc = L.cells();
+    const int ns = a.ns;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell3(L, c, i, j, k);
+        const int cc[3] = {i, j, k};
+        double E[3] = {0.0, 0.0, 0.0};
+        for (int d = 0; d < a.dim; d++) {
+            const int n = L.n[d];
+            int p1[3] = {i, j, k}, p2[3] = {i, j, k}, m1[3] = {i, j, k}, m2[3] = {i, j, k};
+            p1[d] += 1;
+            p2[d] += 2;
+            m1[d] -= 1;
+            m2[d] -= 2;
+            const double dx = dxs.v[d];
+            if (cc[d] > 0 && cc[d] < n - 1) {
+                E[d] = -0.5 * (L.phi[lin(L, p1[0], p1[1], p1[2])] - L.phi[lin(L, m1[0], m1[1], m1[2])]) / dx;
+            } else if (cc[d] == 0 && n > 1) {
+                if (n - 1 > 2)
+                    E[d] = -0.5 * (-L.phi[lin(L, p2[0], p2[1], p2[2])] + 4.0 * L.phi[lin(L, p1[0], p1[1], p1[2])] -
+                                   3.0 * L.phi[c]) / dx;
+                else
+                    E[d] = -(L.phi[lin(L, p1[0], p1[1], p1[2])] - L.phi[c]) / dx;
+            } else if (cc[d] == n - 1 && n > 1) {
+                if (n - 1 > 2)
+                    E[d] = -0.5 * (L.phi[lin(L, m2[0], m2[1], m2[2])] - 4.0 * L.phi[lin(L, m1[0], m1[1], m1[2])] +
+                                   3.0 * L.phi[c]) / dx;
+                else
+                    E[d] = -(L.phi[c] - L.phi[lin(L, m1[0], m1[1], m1[2])]) / dx;
+            }
+        }
+        const int64_t o = a.st.off(a.lo[0] + i, a.lo[1] + j, a.lo[2] + k);
+        const int64_t cs = a.st.ns;
+        double nd = 0.0, es = 0.0;
+        for (int s = 0; s < ns; s++) nd += a.st.p[o + (int64_t)s * cs];
+        for (int d = 0; d < a.dim; d++) es += E[d] * E[d];
+        a.st.p[o + (int64_t)VD_POT(ns) * cs] = L.phi[c];
+        a.st.p[o + (int64_t)VD_EFX(ns) * cs] = E[0];
+        a.st.p[o + (int64_t)VD_EFY(ns) * cs] = E[1];
+        a.st.p[o + (int64_t)VD_EFZ(ns) * cs] = E[2];
+        a.st.p[o + (int64_t)VD_REF(ns) * cs] = (pow(es, 0.5) / nd) / 1.0e-21;
+    }
+}
+
+// face field -dphi/dx_d on the face box of direction d; at a Dirichlet domain face
+// the gradient to the face value over half a cell, at a zero-gradient face 0
+// (what MLMG's getGradSolution returns, negated)
+__global__ void k_pois_face_field(Level L, BcInfo bc, A4 ef, int d, double dx)
+{
+    int nf[3] = {L.n[0], L.n[1], L.n[2]};
+    nf[d] += 1;
+    const int64_t tot = (int64_t)nf[0] * nf[1] * nf[2];
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < tot; c += (int64_t)gridDim.x * blockDim.x) {
+        const int k = (int)(c / ((int64_t)nf[0] * nf[1]));
+        const int64_t r = c - (int64_t)k * nf[0] * nf[1];
+        const int j = (int)(r / nf[0]);
+        const int i = (int)(r - (int64_t)j * nf[0]);
+        const int f[3] = {i, j, k};
+        int m[3] = {i, j, k};
+        m[d] -= 1;
+        double e;
+        if (f[d] == 0) e = bc.dir_lo[d] ? -(L.phi[lin(L, i, j, k)] - bc.val_lo[d]) / (0.5 * dx) : 0.0;
+        else if (f[d] == L.n[d]) e = bc.dir_hi[d] ? -(bc.val_hi[d] - L.phi[lin(L, m[0], m[1], m[2])]) / (0.5 * dx) : 0.0;
+        else e = -(L.phi[lin(L, i, j, k)] - L.phi[lin(L, m[0], m[1], m[2])]) / dx;
+        ef.p[ef.off(ef.bx + i, ef.by + j, ef.bz + k)] = e;
+    }
+}
+
+unsigned grid_of(int64_t n)
+{
+    int64_t g = (n + 255) / 256;
+    if (g > 148LL * 32) g = 148LL * 32;
+    return (unsigned)(g < 1 ? 1 : g);
+}
+
+int err(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+int err(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    return vd_host::set_error(code, buf);
+}
+
+}  // namespace
+}  // namespace vd
+
+using namespace vd;
+
+extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_array4 efield_ec[3], const vd_params* prm,
+                                const vd_poisson_params* pp, int32_t* vcycles_done, double* rel_residual,
+                                void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    vd_host::MechInfo m;
+    int rc = vd_host::mech_info(&m);
+    if (rc) return rc;
+    if (!bx || !prm || !pp) return err(VD_ERR_ARG, "null argument");
+    if ((rc = vd_host::check_update_params(bx, prm, m))) return rc;
+    const int dim = bx->dim, ns = m.ns;
+    for (int d = 0; d < dim; d++)
+        if (prm->domlo[d] != bx->lo[d] || prm->domhi[d] != bx->hi[d])
+            return err(VD_ERR_ARG, "the potential solve needs the box to be the whole domain (direction %d)", d);
+    if (pp->max_vcycles < 1 || pp->max_vcycles > 1000) return err(VD_ERR_ARG, "max_vcycles %d", pp->max_vcycles);
+    // ghost layers of the state (refilled for the potential and the fields)
+    int n[3], glo[3], ghi[3];
+    for (int d = 0; d < 3; d++) {
+        n[d] = bx->hi[d] - bx->lo[d] + 1;
+        glo[d] = bx->lo[d];
+        ghi[d] = bx->hi[d];
+    }
+    int G = 0;  // ghost layers available in every active direction
+    {
+        G = 1 << 20;
+        for (int d = 0; d < dim; d++) {
+            G = std::min(G, bx->lo[d] - state.begin[d]);
+            G = std::min(G, state.end[d] - 1 - bx->hi[d]);
+        }
+        if (G < 0) G = 0;
+        if (G > 8) G = 8;
+    }
+    for (int d = 0; d < dim; d++) {
+        glo[d] -= G;
+        ghi[d] += G;
+    }
+    if (!state.p || state.ncomp < VD_NVAR(ns) || state.begin[0] > glo[0] || state.end[0] <= ghi[0])
+        return err(VD_ERR_ARG, "state does not cover the box with NVAR components");
+    if (!prm->cs_technique)
+        for (int d = 0; d < dim; d++) {
+            if (!efield_ec || !efield_ec[d].p) return err(VD_ERR_ARG, "efield_ec[%d] is null", d);
+            int fhi[3] = {bx->hi[0], bx->hi[1], bx->hi[2]};
+            fhi[d] += 1;
+            for (int e = 0; e < 3; e++)
+                if (efield_ec[d].begin[e] > bx->lo[e] || efield_ec[d].end[e] <= fhi[e])
+                    return err(VD_ERR_ARG, "efield_ec[%d] does not cover the face box", d);
+        }
+    BcInfo bc;
+    memset(&bc, 0, sizeof(bc));
+    for (int d = 0; d < dim; d++) {
+        bc.dir_lo[d] = pp->bc_lo[d] == VD_BC_DIRC;
+        bc.dir_hi[d] = pp->bc_hi[d] == VD_BC_DIRC;
+        bc.val_lo[d] = pp->value_lo[d];
+        bc.val_hi[d] = pp->value_hi[d];
+    }
+    bool any_dir = false;
+    for (int d = 0; d < dim; d++) any_dir = any_dir || bc.dir_lo[d] || bc.dir_hi[d];
+    if (!any_dir) return err(VD_ERR_ARG, "the potential needs at least one Dirichlet face");
+
+    // hierarchy: halve every active direction while all stay even and above 2
+    std::vector<Level> lv;
+    {
+        Level L0;
+        for (int d = 0; d < 3; d++) {
+            L0.n[d] = n[d];
+            L0.idx2[d] = d < dim ? 1.0 / (prm->dx[d] * prm->dx[d]) : 0.0;
+        }
+        lv.push_back(L0);
+        for (;;) {
+            const Level& f = lv.back();
+            bool ok = true;
+            for (int d = 0; d < dim; d++) ok = ok && (f.n[d] % 2 == 0) && f.n[d] > 2;
+            if (!ok || lv.size() >= 24) break;
+            Level c;
+            for (int d = 0; d < 3; d++) {
+                c.n[d] = d < dim ? f.n[d] / 2 : f.n[d];
+                c.idx2[d] = f.idx2[d] * 0.25;
+            }
+            lv.push_back(c);
+        }
+    }
+    size_t total = 0;
+    for (auto& L : lv) total += 3 * (size_t)L.cells();
+    double* buf = nullptr;
+    cudaError_t e = cudaMallocAsync(&buf, (total + 1) * sizeof(double) + 64, st);
+    if (e != cudaSuccess) return err(VD_ERR_NOMEM, "multigrid scratch of %zu bytes: %s", total * 8, cudaGetErrorString(e));
+    {
+        double* p = buf;
+        for (auto& L : lv) {
+            L.phi = p;
+            p += L.cells();
+            L.rhs = p;
+            p += L.cells();
+            L.res = p;
+            p += L.cells();
+        }
+    }
+    unsigned long long* d_max = reinterpret_cast<unsigned long long*>(buf + total);
+    BcInfo bc0;  // homogeneous version for the correction levels
+    bc0 = bc;
+    for (int d = 0; d < 3; d++) bc0.val_lo[d] = bc0.val_hi[d] = 0.0;
+
+    PoisArgs pa;
+    memset(&pa, 0, sizeof(pa));
+    pa.st = A4(state);
+    for (int d = 0; d < 3; d++) {
+        pa.lo[d] = bx->lo[d];
+        pa.hi[d] = bx->hi[d];
+    }
+    pa.ns = ns;
+    pa.dim = dim;
+    for (int s = 0; s < ns; s++) pa.charge[s] = (int8_t)m.charge[s];
+
+    auto launch_check = [&](const char* what) -> int {
+        cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess) {
+            cudaFreeAsync(buf, st);
+            return err(VD_ERR_CUDA, "%s: %s", what, cudaGetErrorString(le));
+        }
+        return VD_OK;
+    };
+
+    k_pois_rhs<<<grid_of(lv[0].cells()), 256, 0, st>>>(pa, lv[0]);
+    if ((rc = launch_check("k_pois_rhs"))) return rc;
+    add_launches(1);
+    // |rhs| scale for the relative residual: residual of phi = 0 would be rhs; use
+    // the residual of the initial guess when nothing better is known
+    double rhs_scale = 0.0;
+    const bool check = pp->tol_rel > 0.0;
+    int64_t launches = 0;
+    auto vcycle = [&]() {
+        const int nl = (int)lv.size();
+        for (int l = 0; l < nl; l++) {
+            const BcInfo& b = l == 0 ? bc : bc0;
+            const int sweeps = (l == nl - 1) ? 64 : 2;
+            for (int s = 0; s < sweeps; s++) {
+                k_mg_rbgs<<<grid_of(lv[l].cells()), 256, 0, st>>>(lv[l], b, dim, 0);
+                k_mg_rbgs<<<grid_of(lv[l].cells()), 256, 0, st>>>(lv[l], b, dim, 1);
+                launches += 2;
+            }
+            if (l < nl - 1) {
+                k_mg_residual<<<grid_of(lv[l].cells()), 256, 0, st>>>(lv[l], b, dim, nullptr);
+                k_mg_restrict<<<grid_of(lv[l + 1].cells()), 256, 0, st>>>(lv[l], lv[l + 1], dim);
+                launches += 2;
+            }
+        }
+        for (int l = nl - 2; l >= 0; l--) {
+            const BcInfo& b = l == 0 ? bc : bc0;
+            k_mg_prolong<<<grid_of(lv[l].cells()), 256, 0, st>>>(lv[l], lv[l + 1], bc0, dim);
+            launches++;
+            for (int s = 0; s < 2; s++) {
+                k_mg_rbgs<<<grid_of(lv[l].cells()), 256, 0, st>>>(lv[l], b, dim, 0);
+                k_mg_rbgs<<<grid_of(lv[l].cells()), 256, 0, st>>>(lv[l], b, dim, 1);
+                launches += 2;
+            }
+        }
+    };
+    auto resid_max = [&](double* out) -> int {
+        cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), st);
+        k_mg_residual<<<grid_of(lv[0].cells()), 256, 0, st>>>(lv[0], bc, dim, d_max);
+        launches++;
+        unsigned long long h = 0;
+        cudaError_t ce = cudaMemcpyAsync(&h, d_max, sizeof(h), cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+        if (ce != cudaSuccess) return err(VD_ERR_CUDA, "residual norm: %s", cudaGetErrorString(ce));
+        double v;
+        memcpy(&v, &h, sizeof(v));
+        *out = v;
+        return VD_OK;
+    };
+    int done = 0;
+    double rel = -1.0;
+    if (check) {
+        // scale of the relative residual: max |rhs|
+        cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), st);
+        k_maxabs<<<grid_of(lv[0].cells()), 256, 0, st>>>(lv[0].rhs, lv[0].cells(), d_max);
+        launches++;
+        unsigned long long h = 0;
+        cudaError_t ce = cudaMemcpyAsync(&h, d_max, sizeof(h), cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+        if (ce != cudaSuccess) {
+            cudaFreeAsync(buf, st);
+            return err(VD_ERR_CUDA, "rhs norm: %s", cudaGetErrorString(ce));
+        }
+        memcpy(&rhs_scale, &h, sizeof(rhs_scale));
+        if (rhs_scale == 0.0) rhs_scale = 1.0;
+    }
+    for (done = 0; done < pp->max_vcycles;) {
+        vcycle();
+        done++;
+        if (check) {
+            double r = 0.0;
+            if ((rc = resid_max(&r))) {
+                cudaFreeAsync(buf, st);
+                return rc;
+            }
+            rel = r / rhs_scale;
+            if (rel <= pp->tol_rel) break;
+        }
+    }
+    if ((rc = launch_check("multigrid"))) return rc;
+    D3 dxs{{prm->dx[0], prm->dx[1], prm->dx[2]}};
+    k_pois_cell_fields<<<grid_of(lv[0].cells()), 256, 0, st>>>(pa, lv[0], dxs);
+    launches++;
+    if (!prm->cs_technique)
+        for (int d = 0; d < dim; d++) {
+            Level L = lv[0];
+            int nf[3] = {L.n[0], L.n[1], L.n[2]};
+            nf[d] += 1;
+            k_pois_face_field<<<grid_of((int64_t)nf[0] * nf[1] * nf[2]), 256, 0, st>>>(lv[0], bc, A4(efield_ec[d]), d,
+                                                                                        prm->dx[d]);
+            launches++;
+        }
+    if ((rc = launch_check("potential fields"))) return rc;
+    add_launches(launches);
+    // ghosts of the potential, the cell field and the reduced field
+    if (G > 0) {
+        const int32_t comps[5] = {VD_POT(ns), VD_EFX(ns), VD_EFY(ns), VD_EFZ(ns), VD_REF(ns)};
+        const int32_t per[3] = {0, 0, 0};
+        rc = vd_fill_ghosts(bx, state, G, comps, 5, per, stream);
+        if (rc) {
+            cudaFreeAsync(buf, st);
+            return rc;
+        }
+    }
+    e = cudaFreeAsync(buf, st);
+    if (e != cudaSuccess) return err(VD_ERR_CUDA, "scratch release: %s", cudaGetErrorString(e));
+    if (vcycles_done) *vcycles_done = done;
+    if (rel_residual) *rel_residual = rel;
+    return VD_OK;
+}
