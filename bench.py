@@ -46,6 +46,8 @@ WORKLOADS = {
                "WENO-Z, 20 explicit steps per case per solve",
     "serving": "Poisson stream at 500 req/s of 1-D/2-D discharge cases, sides log-uniform 256-1024, "
                "0.5-5 kV, 0.1-10 bar, 50-2000 explicit steps, 8 species / 40 reactions, fixed HBM budget",
+    "large": "3-D 384^3 single box, 12 species / 60 reactions, WENO-Z, potential solve (multigrid) + explicit "
+             "step every step, 100 steps",
 }
 
 
@@ -69,6 +71,7 @@ def parse():
                     help="skip the serving-workload measurement added to the default line")
     ap.add_argument("--requests", type=int, default=48, help="requests of the serving stream")
     ap.add_argument("--budget-gb", type=float, default=8.0, help="HBM budget of the serving loop")
+    ap.add_argument("--large-n", type=int, default=384, help="cells per side of the large workload")
     return ap.parse_args()
 
 
@@ -814,6 +817,141 @@ def measure_serving(n_requests: int = 48, budget_gb: float = 8.0, quantum: int =
     return out
 
 
+def measure_large(steps: int = 100, warmup: int = 3, n: int = 384, fp64_compare: bool = True) -> dict:
+    """The large single case: every step solves the potential (multigrid, warm
+    started, to 1e-8 relative residual) and takes one explicit step (prep +
+    transport), then refills the ghosts.  Mixed precision timed; the same steps in
+    FP64 from the same initial state give the error of the mixed run."""
+    import ctypes as C
+
+    import torch
+
+    from vidyut_b200 import _abi as abi
+    from vidyut_b200 import api, inputs
+
+    L = abi.lib()
+    mech, case, st_init = inputs.config_large_device(n=(n, n, n))
+    api.mech_init(mech)
+    ns = mech.ns
+    cells = case.ncell
+    ef = [torch.zeros((1, n + (d == 2), n + (d == 1), n + (d == 0)), dtype=torch.float64, device="cuda")
+          for d in range(3)]
+    gn = [torch.zeros((1, 1, 1, 1), dtype=torch.float64, device="cuda") for _ in range(3)]  # not read
+    comps = list(range(ns)) + [abi.EEN(ns), abi.ETEMP(ns)]
+    stream = torch.cuda.current_stream()
+    pp = api.poisson_params(3, 1000.0, 0.0, max_vcycles=40, tol_rel=1e-8)
+    box = abi.make_box(case.lo, case.hi, 3)
+    null = abi.null_array4()
+    cyc = []
+
+    def run(prec, nsteps, bufs, profile=False):
+        prm = case.vd_params(precision=prec)
+        cur, nxt = bufs
+        dc = api.DeviceCase(case, cur, ef, gn)
+        for _ in range(nsteps):
+            dc.state = cur
+            nv, _ = api.poisson_solve(dc, prm, pp)
+            cyc.append(nv)
+            rc = L.vd_explicit_update_all(C.byref(box), api.t_a4(cur, case.state_begin()), dc.face_a4s("efield"),
+                                          dc.face_a4s("gradne"), api.t_a4(nxt, case.state_begin()), null, null,
+                                          C.byref(prm), stream.cuda_stream)
+            abi.check(rc, "vd_explicit_update_all")
+            api.fill_ghosts(nxt, case, case.ghost, comps)
+            cur, nxt = nxt, cur
+        return cur, nxt
+
+    # mixed precision
+    a, b = st_init.clone(), st_init.clone()
+    a, b = run(abi.PREC_MIXED, warmup, (a, b))
+    a.copy_(st_init)
+    b.copy_(st_init)
+    cyc.clear()
+    torch.cuda.synchronize()
+    clock = ClockSampler(torch.cuda.current_device())
+    clock.start()
+    n0 = L.vd_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fin_mixed, spare = run(abi.PREC_MIXED, steps, (a, b))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clock.stop()
+    ms = e0.elapsed_time(e1) / steps
+    launches = L.vd_launch_count() - n0
+    vcycles = sum(cyc) / max(1, len(cyc))
+    # per-kernel device time of a few more steps (from the final state)
+    L.vd_profile_enable(1)
+    run(abi.PREC_MIXED, 2, (fin_mixed, spare))
+    torch.cuda.synchronize()
+    prof = abi.profile_read()
+    L.vd_profile_enable(0)
+    out = {"cells": cells, "steps": steps, "ms_per_step": ms, "value": cells / (ms * 1e-3),
+           "vcycles_per_step": vcycles, "gpu_launches": int(launches), "clocks": clocks,
+           "kernels_ms_per_launch": {k: v[1] / v[0] for k, v in prof.items()},
+           "kernels_launches_2_steps": {k: v[0] for k, v in prof.items()}}
+    del spare
+    if fp64_compare:
+        # the mixed final state was advanced 2 more profiled steps: redo it cleanly
+        fin_mixed = spare = None
+        torch.cuda.empty_cache()
+        a, b = st_init.clone(), st_init.clone()
+        fm, other = run(abi.PREC_MIXED, steps, (a, b))
+        del a, b, other
+        torch.cuda.empty_cache()
+        c64, d64 = st_init.clone(), st_init
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fin64, _ = run(abi.PREC_FP64, steps, (c64, d64))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = e0.elapsed_time(e1) / steps
+        g = case.ghost
+        errs = []
+        for q in comps:
+            x = fm[q, g:g + n, g:g + n, g:g + n]
+            r = fin64[q, g:g + n, g:g + n, g:g + n]
+            errs.append(float(((x - r).abs() / r.abs().clamp_min(1e-300)).max()))
+        out["fp64"] = {"ms_per_step": ms64, "value": cells / (ms64 * 1e-3), "mixed_speedup": ms64 / ms}
+        out["mixed_vs_fp64_max_rel"] = {"per_component": errs, "max": max(errs),
+                                        "components": f"species 0..{ns - 1}, EEN, ETEMP after {steps} steps"}
+    return out
+
+
+def run_large_line(args):
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1 and int(os.environ.get("RANK", "0")) != 0:
+        return 0  # one resident domain on one GPU
+    steps = args.steps if args.steps != 10 else 100
+    r = measure_large(steps, max(3, args.warmup), n=args.large_n)
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    kt = r["kernels_ms_per_launch"].get("k_transport")
+    alg = 8 * (12 + 2 + 3 + 6 + 12 + 1)  # reads NS+2+D+2D, writes NS+1 (FP64)
+    roof = None
+    if kt:
+        ach = alg * r["cells"] / (kt * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": "k_transport", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                "frac": ach / hbm, "traffic": read_profile_traffic("k_transport", "large"), "kernel_ms": kt,
+                "alg_bytes_per_cell": alg, "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback"}
+    line = {"metric": "cell-updates/s", "value": r["value"], "unit": "cell-updates/s", "n_gpus": 1,
+            "steps": r["steps"], "warmup": max(3, args.warmup), "ms_per_step": r["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32/f64 (mixed: FP32 WENO, rates, fluxes; FP64 accumulate; FP64 potential solve)",
+            "data": "synthetic",
+            "config": {"workload": WORKLOADS["large"].replace("384^3", f"{args.large_n}^3"), "cells": r["cells"],
+                       "species": 12, "reactions": 60,
+                       "l2": "inputs larger than L2 (10.4 GB state per copy)"},
+            "roofline": roof, "cpu_baseline": None, "e2e": None, "gpu_launches": r["gpu_launches"],
+            "clocks": r["clocks"], "large": r}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_serving_line(args):
     import torch
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
@@ -885,6 +1023,8 @@ def main():
         return run_batched_line(args)
     if args.workload == "serving":
         return run_serving_line(args)
+    if args.workload == "large":
+        return run_large_line(args)
     return run_ours(args)
 
 

@@ -380,3 +380,71 @@ def config_serving(seed: int = BASE_SEED, n_requests: int = 48, rate_per_s: floa
                           params=dict(MULTISTEP_PARAMS), n_modes=4)
         out.append((t, case, ns))
     return mech, out
+
+
+def config_large_device(device="cuda", seed: int = BASE_SEED, n=(384, 384, 384), n_species: int = 12,
+                        n_reactions: int = 60, dens_range=(1e10, 1e18), te_range_ev=(0.3, 10.0),
+                        voltage: float = 1000.0, n_modes: int = 4, ghost: int = 3):
+    """Large single case, built on the GPU (a 384^3 state is 10 GB; numpy would take
+    minutes): 3-D box, synthetic 12-species / 60-reaction mechanism, every
+    non-background species log-uniform in dens_range and spatially correlated (a
+    sum of n_modes random cosines mapped through the normal CDF, as
+    smooth_uniform_field), background gas 2.4e25, Te uniform in te_range_ev per
+    cell, potential initialised to the ramp V (1 - x/L) (the potential step
+    replaces it), dx = 1e-5 m.  Returns (mechanism, BoxCase without host arrays,
+    device state tensor of shape (NVAR, nz+2g, ny+2g, nx+2g))."""
+    import torch
+    mech = synthetic(n_species, n_reactions, seed + 31)
+    gen = torch.Generator(device="cpu").manual_seed(seed + 32)
+    ns = mech.ns
+    dim = 3
+    n = tuple(int(v) for v in n)
+    shp = (mech.nvar, n[2] + 2 * ghost, n[1] + 2 * ghost, n[0] + 2 * ghost)
+    st = torch.zeros(shp, dtype=torch.float64, device=device)
+    inner = (slice(ghost, ghost + n[2]), slice(ghost, ghost + n[1]), slice(ghost, ghost + n[0]))
+    axes = [(torch.arange(n[d], device=device, dtype=torch.float64) + 0.5) / n[d] for d in range(3)]
+    lo, hi = np.log10(dens_range[0]), np.log10(dens_range[1])
+    bg = set(mech.bg_species)
+    for s in range(ns):
+        if s in bg:
+            st[(s,) + inner] = 2.4e25
+            continue
+        g = torch.zeros((n[2], n[1], n[0]), dtype=torch.float64, device=device)
+        var = 0.0
+        for _ in range(n_modes):
+            k = [int(torch.randint(-2, 3, (1,), generator=gen)) for _ in range(3)]
+            if not any(k):
+                k[0] = 1
+            a = float(torch.randn(1, generator=gen))
+            ph = float(torch.rand(1, generator=gen)) * 2.0 * np.pi
+            cz = torch.cos(2 * np.pi * k[2] * axes[2])[:, None, None]
+            sz = torch.sin(2 * np.pi * k[2] * axes[2])[:, None, None]
+            xy = 2 * np.pi * (k[0] * axes[0][None, None, :] + k[1] * axes[1][None, :, None]) + ph
+            g += a * (torch.cos(xy) * cz - torch.sin(xy) * sz)  # cos(xy + z)
+            var += 0.5 * a * a
+        g /= max(var, 1e-30) ** 0.5
+        u = torch.special.ndtr(g).clamp(0.0, 1.0 - 1e-15)
+        st[(s,) + inner] = torch.pow(10.0, lo + (hi - lo) * u)
+        del g, u
+    te = torch.rand((n[2], n[1], n[0]), generator=gen, dtype=torch.float64).to(device)
+    st[(abi.ETEMP(ns),) + inner] = (te_range_ev[0] + (te_range_ev[1] - te_range_ev[0]) * te) * EV
+    del te
+    x = (torch.arange(n[0], device=device, dtype=torch.float64) + 0.5) / n[0]
+    st[(abi.POT(ns),) + inner] = (voltage * (1.0 - x))[None, None, :]
+    # ghosts by first-order extrapolation, then the energy density from ne and Te
+    for d in range(3):
+        ax = 3 - d
+        for q in range(1, ghost + 1):
+            lo_idx = [slice(None)] * 4
+            src = [slice(None)] * 4
+            lo_idx[ax] = ghost - q
+            src[ax] = ghost
+            st[tuple(lo_idx)] = st[tuple(src)]
+            lo_idx[ax] = ghost + n[d] - 1 + q
+            src[ax] = ghost + n[d] - 1
+            st[tuple(lo_idx)] = st[tuple(src)]
+    st[abi.EEN(ns)] = 1.5 * st[mech.e_id] * K_B * st[abi.ETEMP(ns)]
+    prm = dict(dim=dim, dx=(1e-5,) * 3, n=n, bg_mask=mech.bg_mask(), **MULTISTEP_PARAMS)
+    case = BoxCase(mech=mech, dim=dim, n=n, ghost=ghost, dx=(1e-5,) * 3, state=None, efield=[], gradne=[],
+                   params=prm, seed=seed)
+    return mech, case, st
