@@ -885,7 +885,11 @@ def measure_large(steps: int = 100, warmup: int = 3, n: int = 384, fp64_compare:
     torch.cuda.synchronize()
     prof = abi.profile_read()
     L.vd_profile_enable(0)
+    kms = {k: v[1] / v[0] for k, v in prof.items()}
+    update_ms = kms.get("k_transport", 0.0) + kms.get("k_prep_spec", kms.get("k_prep", 0.0)) + \
+        2 * kms.get("k_ghost", 0.0)
     out = {"cells": cells, "steps": steps, "ms_per_step": ms, "value": cells / (ms * 1e-3),
+           "update_ms_per_step": update_ms, "potential_ms_per_step": ms - update_ms,
            "vcycles_per_step": vcycles, "gpu_launches": int(launches), "clocks": clocks,
            "kernels_ms_per_launch": {k: v[1] / v[0] for k, v in prof.items()},
            "kernels_launches_2_steps": {k: v[0] for k, v in prof.items()}}
@@ -914,6 +918,21 @@ def measure_large(steps: int = 100, warmup: int = 3, n: int = 384, fp64_compare:
         out["fp64"] = {"ms_per_step": ms64, "value": cells / (ms64 * 1e-3), "mixed_speedup": ms64 / ms}
         out["mixed_vs_fp64_max_rel"] = {"per_component": errs, "max": max(errs),
                                         "components": f"species 0..{ns - 1}, EEN, ETEMP after {steps} steps"}
+        # the trajectory's own sensitivity: FP64 again from the same initial state
+        # with every density scaled by (1 + 1e-15), against the FP64 run above
+        keep = fin64
+        del fm, c64, d64, st_init, fin64
+        torch.cuda.empty_cache()
+        a = inputs.config_large_device(n=(n, n, n))[2]
+        a[:ns] *= 1.0 + 1e-15
+        b = a.clone()
+        finp, _ = run(abi.PREC_FP64, steps, (a, b))
+        errs_p = []
+        for q in comps:
+            x = finp[q, g:g + n, g:g + n, g:g + n]
+            r = keep[q, g:g + n, g:g + n, g:g + n]
+            errs_p.append(float(((x - r).abs() / r.abs().clamp_min(1e-300)).max()))
+        out["fp64_vs_fp64_perturbed_1e-15"] = {"per_component": errs_p, "max": max(errs_p)}
     return out
 
 

@@ -84,32 +84,36 @@ __device__ __forceinline__ void stencil(const Level& L, const BcInfo& bc, int di
     }
 }
 
-__global__ void k_mg_rbgs(Level L, BcInfo bc, int dim, int color)
+// Multigrid kernels: one thread per cell (or per cell of one colour) with i over
+// the x threads and j, k from the y and z block indices, so no index division.
+
+// one red-black Gauss-Seidel half sweep: cells with (i + j + k) % 2 == color
+template <int DIM>
+__global__ void __launch_bounds__(128) k_mg_rbgs(Level L, BcInfo bc, int color)
 {
-    const int64_t nc = L.cells();
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
-        int i, j, k;
-        cell3(L, c, i, j, k);
-        if (((i + j + k) & 1) != color) continue;
-        double off, diag;
-        stencil(L, bc, dim, i, j, k, L.phi, off, diag);
-        // L phi = off + diag phi = rhs  ->  phi = (rhs - off) / diag
-        L.phi[c] = (L.rhs[c] - off) / diag;
-    }
+    const int j = blockIdx.y, k = blockIdx.z;
+    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((j + k + color) & 1);
+    if (i >= L.n[0]) return;
+    double off, diag;
+    stencil(L, bc, DIM, i, j, k, L.phi, off, diag);
+    // L phi = off + diag phi = rhs  ->  phi = (rhs - off) / diag
+    const int64_t c = lin(L, i, j, k);
+    L.phi[c] = (L.rhs[c] - off) / diag;
 }
 
-__global__ void k_mg_residual(Level L, BcInfo bc, int dim, unsigned long long* maxabs)
+template <int DIM>
+__global__ void __launch_bounds__(128) k_mg_residual(Level L, BcInfo bc, unsigned long long* maxabs)
 {
-    const int64_t nc = L.cells();
+    const int j = blockIdx.y, k = blockIdx.z;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double m = 0.0;
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
-        int i, j, k;
-        cell3(L, c, i, j, k);
+    if (i < L.n[0]) {
         double off, diag;
-        stencil(L, bc, dim, i, j, k, L.phi, off, diag);
+        stencil(L, bc, DIM, i, j, k, L.phi, off, diag);
+        const int64_t c = lin(L, i, j, k);
         const double r = L.rhs[c] - (off + diag * L.phi[c]);
         L.res[c] = r;
-        m = fmax(m, fabs(r));
+        m = fabs(r);
     }
     if (maxabs) {
         // non-negative doubles order like their bit patterns
@@ -119,67 +123,109 @@ __global__ void k_mg_residual(Level L, BcInfo bc, int dim, unsigned long long* m
 }
 
 // coarse rhs = average of the 2^dim fine residuals (full weighting for cell centres)
-__global__ void k_mg_restrict(Level F, Level C, int dim)
+template <int DIM>
+__global__ void __launch_bounds__(128) k_mg_restrict(Level F, Level C)
 {
-    const int64_t nc = C.cells();
-    const double w = 1.0 / (double)(1 << dim);
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
-        int i, j, k;
-        cell3(C, c, i, j, k);
-        double s = 0.0;
-        for (int dz = 0; dz < (dim > 2 ? 2 : 1); dz++)
-            for (int dy = 0; dy < (dim > 1 ? 2 : 1); dy++)
-                for (int dx = 0; dx < 2; dx++)
-                    s += F.res[lin(F, (dim > 0 ? 2 * i + dx : i), (dim > 1 ? 2 * j + dy : j), (dim > 2 ? 2 * k + dz : k))];
-        C.rhs[c] = w * s;
-        C.phi[c] = 0.0;
-    }
+    const int j = blockIdx.y, k = blockIdx.z;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C.n[0]) return;
+    double s = 0.0;
+#pragma unroll
+    for (int dz = 0; dz < (DIM > 2 ? 2 : 1); dz++)
+#pragma unroll
+        for (int dy = 0; dy < (DIM > 1 ? 2 : 1); dy++)
+#pragma unroll
+            for (int dx = 0; dx < 2; dx++)
+                s += F.res[lin(F, 2 * i + dx, DIM > 1 ? 2 * j + dy : j, DIM > 2 ? 2 * k + dz : k)];
+    const int64_t c = lin(C, i, j, k);
+    C.rhs[c] = s * (1.0 / (double)(1 << DIM));
+    C.phi[c] = 0.0;
 }
 
 // fine phi += linear interpolation of the coarse correction (weights 3/4, 1/4 per
 // direction; at a domain face the outside coarse value is the correction's
 // boundary value: -c for a Dirichlet face (zero at the face), c for zero gradient)
-__global__ void k_mg_prolong(Level F, Level C, BcInfo bc, int dim)
+template <int DIM>
+__global__ void __launch_bounds__(128) k_mg_prolong(Level F, Level C, BcInfo bc)
 {
-    const int64_t nf = F.cells();
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nf; c += (int64_t)gridDim.x * blockDim.x) {
-        int i, j, k;
-        cell3(F, c, i, j, k);
-        const int f[3] = {i, j, k};
-        int ci[3] = {0, 0, 0}, nb[3] = {0, 0, 0};
-        for (int d = 0; d < 3; d++) {
-            if (d < dim) {
-                ci[d] = f[d] >> 1;
-                nb[d] = (f[d] & 1) ? 1 : -1;  // the other coarse cell this fine cell leans towards
-            } else {
-                ci[d] = f[d];
-            }
-        }
-        double acc = 0.0;
-        for (int mz = 0; mz < (dim > 2 ? 2 : 1); mz++)
-            for (int my = 0; my < (dim > 1 ? 2 : 1); my++)
-                for (int mx = 0; mx < 2; mx++) {
-                    const int m[3] = {mx, my, mz};
-                    double w = 1.0;
-                    int q[3] = {ci[0], ci[1], ci[2]};
-                    double sign = 1.0;
-                    for (int d = 0; d < dim; d++) {
-                        w *= m[d] ? 0.25 : 0.75;
-                        if (m[d]) {
-                            q[d] += nb[d];
-                            if (q[d] < 0) {
-                                q[d] = 0;
-                                if (bc.dir_lo[d]) sign = -sign;
-                            } else if (q[d] >= C.n[d]) {
-                                q[d] = C.n[d] - 1;
-                                if (bc.dir_hi[d]) sign = -sign;
-                            }
+    const int j = blockIdx.y, k = blockIdx.z;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= F.n[0]) return;
+    const int f[3] = {i, j, k};
+    int ci[3] = {i, j, k}, nb[3] = {0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        ci[d] = f[d] >> 1;
+        nb[d] = (f[d] & 1) ? 1 : -1;  // the other coarse cell this fine cell leans towards
+    }
+    double acc = 0.0;
+#pragma unroll
+    for (int mz = 0; mz < (DIM > 2 ? 2 : 1); mz++)
+#pragma unroll
+        for (int my = 0; my < (DIM > 1 ? 2 : 1); my++)
+#pragma unroll
+            for (int mx = 0; mx < 2; mx++) {
+                const int m[3] = {mx, my, mz};
+                double w = 1.0;
+                int q[3] = {ci[0], ci[1], ci[2]};
+                double sign = 1.0;
+#pragma unroll
+                for (int d = 0; d < DIM; d++) {
+                    w *= m[d] ? 0.25 : 0.75;
+                    if (m[d]) {
+                        q[d] += nb[d];
+                        if (q[d] < 0) {
+                            q[d] = 0;
+                            if (bc.dir_lo[d]) sign = -sign;
+                        } else if (q[d] >= C.n[d]) {
+                            q[d] = C.n[d] - 1;
+                            if (bc.dir_hi[d]) sign = -sign;
                         }
                     }
-                    acc += w * sign * C.phi[lin(C, q[0], q[1], q[2])];
                 }
-        F.phi[c] += acc;
+                acc += w * sign * C.phi[lin(C, q[0], q[1], q[2])];
+            }
+    F.phi[lin(F, i, j, k)] += acc;
+}
+
+dim3 grid_cells(const Level& L, int per_thread = 1)
+{
+    const int nx = (L.n[0] + per_thread - 1) / per_thread;
+    return dim3((unsigned)((nx + 127) / 128), (unsigned)L.n[1], (unsigned)L.n[2]);
+}
+
+template <int DIM>
+struct Mg {
+    static void rbgs(const Level& L, const BcInfo& b, int color, cudaStream_t st)
+    {
+        k_mg_rbgs<DIM><<<grid_cells(L, 2), 128, 0, st>>>(L, b, color);
     }
+    static void residual(const Level& L, const BcInfo& b, unsigned long long* mx, cudaStream_t st)
+    {
+        k_mg_residual<DIM><<<grid_cells(L), 128, 0, st>>>(L, b, mx);
+    }
+    static void restrict_(const Level& F, const Level& C, cudaStream_t st)
+    {
+        k_mg_restrict<DIM><<<grid_cells(C), 128, 0, st>>>(F, C);
+    }
+    static void prolong(const Level& F, const Level& C, const BcInfo& b, cudaStream_t st)
+    {
+        k_mg_prolong<DIM><<<grid_cells(F), 128, 0, st>>>(F, C, b);
+    }
+};
+
+struct MgOps {
+    void (*rbgs)(const Level&, const BcInfo&, int, cudaStream_t);
+    void (*residual)(const Level&, const BcInfo&, unsigned long long*, cudaStream_t);
+    void (*restrict_)(const Level&, const Level&, cudaStream_t);
+    void (*prolong)(const Level&, const Level&, const BcInfo&, cudaStream_t);
+};
+
+MgOps mg_ops(int dim)
+{
+    if (dim == 1) return {Mg<1>::rbgs, Mg<1>::residual, Mg<1>::restrict_, Mg<1>::prolong};
+    if (dim == 2) return {Mg<2>::rbgs, Mg<2>::residual, Mg<2>::restrict_, Mg<2>::prolong};
+    return {Mg<3>::rbgs, Mg<3>::residual, Mg<3>::restrict_, Mg<3>::prolong};
 }
 
 __global__ void k_maxabs(const double* x, int64_t n, unsigned long long* out)
@@ -444,36 +490,37 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
     double rhs_scale = 0.0;
     const bool check = pp->tol_rel > 0.0;
     int64_t launches = 0;
+    const MgOps ops = mg_ops(dim);
     auto vcycle = [&]() {
         const int nl = (int)lv.size();
         for (int l = 0; l < nl; l++) {
             const BcInfo& b = l == 0 ? bc : bc0;
             const int sweeps = (l == nl - 1) ? 64 : 2;
             for (int s = 0; s < sweeps; s++) {
-                k_mg_rbgs<<<grid_of(lv[l].cells()), 256, 0, st>>>(lv[l], b, dim, 0);
-                k_mg_rbgs<<<grid_of(lv[l].cells()), 256, 0, st>>>(lv[l], b, dim, 1);
+                ops.rbgs(lv[l], b, 0, st);
+                ops.rbgs(lv[l], b, 1, st);
                 launches += 2;
             }
             if (l < nl - 1) {
-                k_mg_residual<<<grid_of(lv[l].cells()), 256, 0, st>>>(lv[l], b, dim, nullptr);
-                k_mg_restrict<<<grid_of(lv[l + 1].cells()), 256, 0, st>>>(lv[l], lv[l + 1], dim);
+                ops.residual(lv[l], b, nullptr, st);
+                ops.restrict_(lv[l], lv[l + 1], st);
                 launches += 2;
             }
         }
         for (int l = nl - 2; l >= 0; l--) {
             const BcInfo& b = l == 0 ? bc : bc0;
-            k_mg_prolong<<<grid_of(lv[l].cells()), 256, 0, st>>>(lv[l], lv[l + 1], bc0, dim);
+            ops.prolong(lv[l], lv[l + 1], bc0, st);
             launches++;
             for (int s = 0; s < 2; s++) {
-                k_mg_rbgs<<<grid_of(lv[l].cells()), 256, 0, st>>>(lv[l], b, dim, 0);
-                k_mg_rbgs<<<grid_of(lv[l].cells()), 256, 0, st>>>(lv[l], b, dim, 1);
+                ops.rbgs(lv[l], b, 0, st);
+                ops.rbgs(lv[l], b, 1, st);
                 launches += 2;
             }
         }
     };
     auto resid_max = [&](double* out) -> int {
         cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), st);
-        k_mg_residual<<<grid_of(lv[0].cells()), 256, 0, st>>>(lv[0], bc, dim, d_max);
+        ops.residual(lv[0], bc, d_max, st);
         launches++;
         unsigned long long h = 0;
         cudaError_t ce = cudaMemcpyAsync(&h, d_max, sizeof(h), cudaMemcpyDeviceToHost, st);
