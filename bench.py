@@ -852,6 +852,9 @@ def measure_large(steps: int = 100, warmup: int = 3, n: int = 384, fp64_compare:
             dc.state = cur
             nv, _ = api.poisson_solve(dc, prm, pp)
             cyc.append(nv)
+            # next step's initial guess: 2 phi_n - phi_(n-1) (nxt still holds phi_(n-1))
+            pot = abi.POT(ns)
+            nxt[pot].mul_(-1.0).add_(cur[pot], alpha=2.0)
             rc = L.vd_explicit_update_all(C.byref(box), api.t_a4(cur, case.state_begin()), dc.face_a4s("efield"),
                                           dc.face_a4s("gradne"), api.t_a4(nxt, case.state_begin()), null, null,
                                           C.byref(prm), stream.cuda_stream)

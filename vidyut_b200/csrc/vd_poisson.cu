@@ -38,14 +38,6 @@ struct BcInfo {
     double val_lo[3], val_hi[3]; // its value (0 on the correction levels)
 };
 
-__device__ __forceinline__ void cell3(const Level& L, int64_t c, int& i, int& j, int& k)
-{
-    k = (int)(c / ((int64_t)L.n[0] * L.n[1]));
-    int64_t r = c - (int64_t)k * L.n[0] * L.n[1];
-    j = (int)(r / L.n[0]);
-    i = (int)(r - (int64_t)j * L.n[0]);
-}
-
 __device__ __forceinline__ int64_t lin(const Level& L, int i, int j, int k)
 {
     return (int64_t)i + (int64_t)L.n[0] * (j + (int64_t)L.n[1] * k);
@@ -198,18 +190,22 @@ template <int DIM>
 struct Mg {
     static void rbgs(const Level& L, const BcInfo& b, int color, cudaStream_t st)
     {
+        ProfScope ps("k_mg_rbgs", st);
         k_mg_rbgs<DIM><<<grid_cells(L, 2), 128, 0, st>>>(L, b, color);
     }
     static void residual(const Level& L, const BcInfo& b, unsigned long long* mx, cudaStream_t st)
     {
+        ProfScope ps("k_mg_residual", st);
         k_mg_residual<DIM><<<grid_cells(L), 128, 0, st>>>(L, b, mx);
     }
     static void restrict_(const Level& F, const Level& C, cudaStream_t st)
     {
+        ProfScope ps("k_mg_restrict", st);
         k_mg_restrict<DIM><<<grid_cells(C), 128, 0, st>>>(F, C);
     }
     static void prolong(const Level& F, const Level& C, const BcInfo& b, cudaStream_t st)
     {
+        ProfScope ps("k_mg_prolong", st);
         k_mg_prolong<DIM><<<grid_cells(F), 128, 0, st>>>(F, C, b);
     }
 };
@@ -248,10 +244,10 @@ struct PoisArgs {
 // phi = the state's potential
 __global__ void k_pois_rhs(PoisArgs a, Level L)
 {
-    const int64_t nc = L.cells();
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
-        int i, j, k;
-        cell3(L, c, i, j, k);
+    const int j = blockIdx.y, k = blockIdx.z;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < L.n[0]) {
+        const int64_t c = lin(L, i, j, k);
         const int64_t o = a.st.off(a.lo[0] + i, a.lo[1] + j, a.lo[2] + k);
         double r = 0.0;
         for (int s = 0; s < a.ns; s++)
@@ -269,11 +265,11 @@ struct D3 {
 
 __global__ void k_pois_cell_fields(PoisArgs a, Level L, D3 dxs)
 {
-    const int64_t nc = L.cells();
     const int ns = a.ns;
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
-        int i, j, k;
-        cell3(L, c, i, j, k);
+    const int j = blockIdx.y, k = blockIdx.z;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < L.n[0]) {
+        const int64_t c = lin(L, i, j, k);
         const int cc[3] = {i, j, k};
         double E[3] = {0.0, 0.0, 0.0};
         for (int d = 0; d < a.dim; d++) {
@@ -309,7 +305,8 @@ __global__ void k_pois_cell_fields(PoisArgs a, Level L, D3 dxs)
         a.st.p[o + (int64_t)VD_EFX(ns) * cs] = E[0];
         a.st.p[o + (int64_t)VD_EFY(ns) * cs] = E[1];
         a.st.p[o + (int64_t)VD_EFZ(ns) * cs] = E[2];
-        a.st.p[o + (int64_t)VD_REF(ns) * cs] = (pow(es, 0.5) / nd) / 1.0e-21;
+        // pow(Esum, 0.5) in the reference: the correctly rounded square root
+        a.st.p[o + (int64_t)VD_REF(ns) * cs] = (sqrt(es) / nd) / 1.0e-21;
     }
 }
 
@@ -320,12 +317,9 @@ __global__ void k_pois_face_field(Level L, BcInfo bc, A4 ef, int d, double dx)
 {
     int nf[3] = {L.n[0], L.n[1], L.n[2]};
     nf[d] += 1;
-    const int64_t tot = (int64_t)nf[0] * nf[1] * nf[2];
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < tot; c += (int64_t)gridDim.x * blockDim.x) {
-        const int k = (int)(c / ((int64_t)nf[0] * nf[1]));
-        const int64_t r = c - (int64_t)k * nf[0] * nf[1];
-        const int j = (int)(r / nf[0]);
-        const int i = (int)(r - (int64_t)j * nf[0]);
+    const int j = blockIdx.y, k = blockIdx.z;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nf[0]) {
         const int f[3] = {i, j, k};
         int m[3] = {i, j, k};
         m[d] -= 1;
@@ -482,14 +476,15 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
         return VD_OK;
     };
 
-    k_pois_rhs<<<grid_of(lv[0].cells()), 256, 0, st>>>(pa, lv[0]);
+    {
+        ProfScope ps("k_pois_rhs", st);
+        k_pois_rhs<<<grid_cells(lv[0]), 128, 0, st>>>(pa, lv[0]);
+    }
     if ((rc = launch_check("k_pois_rhs"))) return rc;
-    add_launches(1);
     // |rhs| scale for the relative residual: residual of phi = 0 would be rhs; use
     // the residual of the initial guess when nothing better is known
     double rhs_scale = 0.0;
     const bool check = pp->tol_rel > 0.0;
-    int64_t launches = 0;
     const MgOps ops = mg_ops(dim);
     auto vcycle = [&]() {
         const int nl = (int)lv.size();
@@ -499,29 +494,24 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
             for (int s = 0; s < sweeps; s++) {
                 ops.rbgs(lv[l], b, 0, st);
                 ops.rbgs(lv[l], b, 1, st);
-                launches += 2;
             }
             if (l < nl - 1) {
                 ops.residual(lv[l], b, nullptr, st);
                 ops.restrict_(lv[l], lv[l + 1], st);
-                launches += 2;
             }
         }
         for (int l = nl - 2; l >= 0; l--) {
             const BcInfo& b = l == 0 ? bc : bc0;
             ops.prolong(lv[l], lv[l + 1], bc0, st);
-            launches++;
             for (int s = 0; s < 2; s++) {
                 ops.rbgs(lv[l], b, 0, st);
                 ops.rbgs(lv[l], b, 1, st);
-                launches += 2;
             }
         }
     };
     auto resid_max = [&](double* out) -> int {
         cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), st);
         ops.residual(lv[0], bc, d_max, st);
-        launches++;
         unsigned long long h = 0;
         cudaError_t ce = cudaMemcpyAsync(&h, d_max, sizeof(h), cudaMemcpyDeviceToHost, st);
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
@@ -536,8 +526,10 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
     if (check) {
         // scale of the relative residual: max |rhs|
         cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), st);
-        k_maxabs<<<grid_of(lv[0].cells()), 256, 0, st>>>(lv[0].rhs, lv[0].cells(), d_max);
-        launches++;
+        {
+            ProfScope ps("k_maxabs", st);
+            k_maxabs<<<grid_of(lv[0].cells()), 256, 0, st>>>(lv[0].rhs, lv[0].cells(), d_max);
+        }
         unsigned long long h = 0;
         cudaError_t ce = cudaMemcpyAsync(&h, d_max, sizeof(h), cudaMemcpyDeviceToHost, st);
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
@@ -563,19 +555,20 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
     }
     if ((rc = launch_check("multigrid"))) return rc;
     D3 dxs{{prm->dx[0], prm->dx[1], prm->dx[2]}};
-    k_pois_cell_fields<<<grid_of(lv[0].cells()), 256, 0, st>>>(pa, lv[0], dxs);
-    launches++;
+    {
+        ProfScope ps("k_pois_cell_fields", st);
+        k_pois_cell_fields<<<grid_cells(lv[0]), 128, 0, st>>>(pa, lv[0], dxs);
+    }
     if (!prm->cs_technique)
         for (int d = 0; d < dim; d++) {
             Level L = lv[0];
             int nf[3] = {L.n[0], L.n[1], L.n[2]};
             nf[d] += 1;
-            k_pois_face_field<<<grid_of((int64_t)nf[0] * nf[1] * nf[2]), 256, 0, st>>>(lv[0], bc, A4(efield_ec[d]), d,
+            ProfScope ps("k_pois_face_field", st);
+            k_pois_face_field<<<dim3((unsigned)((nf[0] + 127) / 128), (unsigned)nf[1], (unsigned)nf[2]), 128, 0, st>>>(lv[0], bc, A4(efield_ec[d]), d,
                                                                                         prm->dx[d]);
-            launches++;
         }
     if ((rc = launch_check("potential fields"))) return rc;
-    add_launches(launches);
     // ghosts of the potential, the cell field and the reduced field
     if (G > 0) {
         const int32_t comps[5] = {VD_POT(ns), VD_EFX(ns), VD_EFY(ns), VD_EFZ(ns), VD_REF(ns)};
