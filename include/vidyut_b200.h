@@ -293,6 +293,14 @@ int vd_explicit_update_all_noalloc(const vd_box* bx, vd_array4 sborder,
 int vd_box_checksums(const vd_box* bx, vd_array4 rxn, vd_array4 phi_new,
                      double* out_dev, void* stream);
 
+/* Explicit time scales of one box (Vidyut::find_time_scales, Source/TimeStep.cpp:34-116):
+ * out[0] = min_d dx_d / max(|mu_e| |E|)  (electron drift),
+ * out[1] = min_d dx_d^2 / (2 dim max D_e)  (electron diffusion),
+ * out[2] = eps0 / (e max(|mu_e| n_e))  (dielectric relaxation);
+ * DBL_MAX where the maximum is 0.  Synchronises the stream (the host gets the
+ * numbers).  With several boxes the caller takes the minimum over boxes.          */
+int vd_time_scales(const vd_box* bx, vd_array4 state, const vd_params* prm, double out[3], void* stream);
+
 /* Ghost refill of one box (FillPatch with first-order extrapolation on
  * non-periodic faces, Source/Vidyut.cpp:90-101; periodic wrap elsewhere):
  * components comps[0..ncomp-1] of the `ghost` layers of face-adjacent ghost cells

@@ -112,6 +112,8 @@ class Port(_Base):
             L.orc_fill_ghosts.restype = None
             L.orc_specmob.argtypes = [MECHP, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double]
             L.orc_specmob.restype = C.c_double
+            L.orc_specdiff.argtypes = [MECHP, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double]
+            L.orc_specdiff.restype = C.c_double
             L.orc_weno.argtypes = [C.c_double] * 5 + [C.c_int]
             L.orc_weno.restype = C.c_double
             Port._lib = L
@@ -185,6 +187,9 @@ class Port(_Base):
 
     def specmob(self, s, Te, N, Tg=300.0):
         return self.L.orc_specmob(C.byref(self.cm), s, Te, N, 0.0, Tg)
+
+    def specdiff(self, s, Te, N, Tg=300.0):
+        return self.L.orc_specdiff(C.byref(self.cm), s, Te, N, 0.0, Tg)
 
     def weno(self, a, b, c, d, e, scheme=3):
         return self.L.orc_weno(a, b, c, d, e, scheme)

@@ -109,3 +109,30 @@ def reduced_field(case, E):
     nd = valid[:ns].sum(axis=0)
     es = sum(E[d] * E[d] for d in range(case.dim))
     return (np.sqrt(es) / nd) / 1.0e-21
+
+
+def time_scales(case, prm, port):
+    """Vidyut::find_time_scales (Source/TimeStep.cpp:34-116) on the valid cells of
+    case.state with the C port's specMob/specDiff."""
+    import math
+    from vidyut_b200 import _abi as abi
+    ns, dim = case.mech.ns, case.dim
+    n, g = case.n, case.gvec
+    v = case.state[:, g[2]:g[2] + n[2], g[1]:g[1] + n[1], g[0]:g[0] + n[0]]
+    te = v[abi.ETEMP(ns)].ravel()
+    emag = np.sqrt(sum(v[abi.EFX(ns) + d] ** 2 for d in range(dim))).ravel()
+    nd = v[:ns].sum(axis=0).ravel()
+    ne = v[case.mech.e_id].ravel()
+    mu = np.array([port.specmob(case.mech.e_id, te[q], nd[q], prm.Tg) for q in range(te.size)])
+    dc = np.array([port.specdiff(case.mech.e_id, te[q], nd[q], prm.Tg) for q in range(te.size)])
+    mdrift, mdiff, mmue = np.max(np.abs(mu) * emag), np.max(dc), np.max(np.abs(mu) * ne)
+    big = 1.79769313486231570e308
+    out = [big, big, big]
+    for d in range(dim):
+        if mdrift > 0:
+            out[0] = min(out[0], case.dx[d] / mdrift)
+        if mdiff > 0:
+            out[1] = min(out[1], 0.5 * case.dx[d] * case.dx[d] / mdiff / dim)
+    if mmue > 0:
+        out[2] = EPS0 / ECHARGE / mmue
+    return tuple(out)

@@ -90,3 +90,15 @@ def test_warm_start_converges_faster(mech):
     n1, _ = api.poisson_solve(dc, prm, api.poisson_params(3, 1000.0, max_vcycles=60, tol_rel=1e-11))
     n2, _ = api.poisson_solve(dc, prm, api.poisson_params(3, 1000.0, max_vcycles=60, tol_rel=1e-11))
     assert n2 < n1
+
+
+def test_time_scales_match_reference_formula(mech):
+    import oracle
+    c = inputs.build_case(mech, 2, (30, 20), (1e-5, 2e-5), 14, density="loguniform_smooth", n_modes=4)
+    dc = api.upload(c)
+    prm = c.vd_params()
+    got = api.time_scales(dc, prm)
+    want = poisson.time_scales(c, prm, oracle.Port(mech))
+    for g_, w_ in zip(got, want):
+        assert abs(g_ - w_) <= 1e-12 * abs(w_), (got, want)
+    assert all(0 < x < 1.0 for x in got)

@@ -267,3 +267,7 @@ class VdPoissonParams(C.Structure):
 PROTOTYPES.update({
     "vd_poisson_solve": (C.c_int, [BOXP, A4, A4P, PRMP, C.POINTER(VdPoissonParams), I32P, DP, C.c_void_p]),
 })
+
+PROTOTYPES.update({
+    "vd_time_scales": (C.c_int, [BOXP, A4, PRMP, DP, C.c_void_p]),
+})

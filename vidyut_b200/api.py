@@ -406,3 +406,12 @@ def poisson_solve(dc: DeviceCase, prm: abi.VdParams, pp: abi.VdPoissonParams, st
                                     C.byref(prm), C.byref(pp), C.byref(nv), C.byref(rr), _stream(stream))
     abi.check(rc, "vd_poisson_solve")
     return nv.value, rr.value
+
+
+def time_scales(dc: DeviceCase, prm: abi.VdParams, stream=None):
+    """(dt_edrift, dt_ediff, dt_diel_relax) of the case's current state
+    (Vidyut::find_time_scales)."""
+    out = (C.c_double * 3)()
+    abi.check(abi.lib().vd_time_scales(C.byref(dc.box()), dc.sb(), C.byref(prm), out, _stream(stream)),
+              "vd_time_scales")
+    return tuple(out)

@@ -698,6 +698,46 @@ int vd_profile_read(char* names, int names_len, int64_t* counts, double* ms, int
     return n;
 }
 
+int vd_time_scales(const vd_box* bx, vd_array4 state, const vd_params* prm, double out[3], void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = ensure_mech_on_device(st);
+    if (rc) return rc;
+    if (!out) return fail(VD_ERR_ARG, "null output");
+    if ((rc = check_params(bx, prm))) return rc;
+    vd_mech* m;
+    {
+        std::lock_guard<std::mutex> lk(g_mech_mu);
+        m = g_mech;
+    }
+    const int ns = m->nspecies;
+    std::string why;
+    if (!covers(state, bx->lo, bx->hi, VD_NVAR(ns), &why)) return fail(VD_ERR_ARG, "state: %s", why.c_str());
+    TransportArgs a;
+    fill_cfg(a, bx, prm, m);
+    unsigned long long* d = nullptr;
+    cudaError_t e = cudaMallocAsync(&d, 3 * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return fail(VD_ERR_NOMEM, "3 words of scratch: %s", cudaGetErrorString(e));
+    unsigned long long h[3] = {0, 0, 0};
+    e = cudaMemsetAsync(d, 0, sizeof(h), st);
+    if (e == cudaSuccess) e = launch_time_scales(box_idx(bx->lo, bx->hi), bx->dim, A4(state), a, d, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(d, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "time scales");
+    double mx[3];
+    memcpy(mx, h, sizeof(mx));
+    // Source/TimeStep.cpp:94-110
+    const double big = 1.79769313486231570e308;
+    out[0] = out[1] = out[2] = big;
+    for (int d2 = 0; d2 < bx->dim; d2++) {
+        if (mx[0] > 0) out[0] = std::min(out[0], prm->dx[d2] / mx[0]);
+        if (mx[1] > 0) out[1] = std::min(out[1], 0.5 * prm->dx[d2] * prm->dx[d2] / mx[1] / bx->dim);
+    }
+    if (mx[2] > 0) out[2] = 8.854187817e-12 / ECHARGE / mx[2];
+    return VD_OK;
+}
+
 int vd_fill_ghosts(const vd_box* bx, vd_array4 state, int ghost, const int32_t* comps, int ncomp,
                    const int32_t periodic[3], void* stream)
 {

@@ -745,4 +745,50 @@ cudaError_t launch_checksums(const BoxIdx& b, const A4& rxn, const A4& pn, doubl
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Time-scale maxima (Vidyut::find_time_scales, Source/TimeStep.cpp:34-116): over
+// the valid cells, max |mu_e| |E|, max D_e and max |mu_e| n_e, as the bit patterns
+// of non-negative doubles (which order like the values) in out[0..2].
+__global__ void __launch_bounds__(256) k_time_scales(BoxIdx b, int dim, A4 st, TransportArgs a,
+                                                     unsigned long long* out)
+{
+    const int ns = a.ns, eidx = a.e_id;
+    double m[3] = {0.0, 0.0, 0.0};
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < b.ncell;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell_of(b, idx, i, j, k);
+        const int64_t o = st.off(i, j, k);
+        const double etemp = st.p[o + (int64_t)VD_ETEMP(ns) * st.ns];
+        double esum = 0.0;
+        for (int d = 0; d < dim; d++) {
+            const double e = st.p[o + (int64_t)(VD_EFX(ns) + d) * st.ns];
+            esum += e * e;
+        }
+        const double emag = sqrt(esum);
+        double nd = 0.0;
+        for (int s = 0; s < ns; s++) nd += st.p[o + (int64_t)s * st.ns];
+        const double dc = a.const_ele_trans ? a.ele_diff / nd : diff_fp64(eidx, etemp, nd, a.Tg);
+        const double mu = a.const_ele_trans ? a.ele_mob / nd : mob_fp64(eidx, etemp, nd, a.Tg);
+        m[0] = fmax(m[0], fabs(mu) * emag);
+        m[1] = fmax(m[1], dc);
+        m[2] = fmax(m[2], fabs(mu) * st.p[o + (int64_t)eidx * st.ns]);
+    }
+    for (int q = 0; q < 3; q++) {
+        double v = m[q];
+        for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+        if ((threadIdx.x & 31) == 0) atomicMax(out + q, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+cudaError_t launch_time_scales(const BoxIdx& b, int dim, const A4& st, const TransportArgs& a,
+                               unsigned long long* out, cudaStream_t s)
+{
+    unsigned g = grid_for(b.ncell, 256);
+    if (g > 148 * 8) g = 148 * 8;
+    ProfScope ps("k_time_scales", s);
+    k_time_scales<<<g, 256, 0, s>>>(b, dim, st, a, out);
+    return cudaGetLastError();
+}
+
 }  // namespace vd

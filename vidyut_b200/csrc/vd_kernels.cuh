@@ -112,6 +112,8 @@ cudaError_t launch_joule(const BoxIdx& b, int dim, const A4& sb, const A4& rxn, 
 cudaError_t launch_prep(const PrepArgs& a, int prec, int ns, cudaStream_t st);
 cudaError_t launch_transport(const TransportArgs& a, int dim, int prec, cudaStream_t st);
 cudaError_t launch_checksums(const BoxIdx& b, const A4& rxn, const A4& pn, double* out, cudaStream_t st);
+cudaError_t launch_time_scales(const BoxIdx& b, int dim, const A4& st, const TransportArgs& a,
+                               unsigned long long* out, cudaStream_t s);
 
 // Tile shape used by the transport kernel for a given dimension (for host-side tiling).
 void transport_tile(int dim, int tile[3]);
