@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--requests", type=int, default=48, help="requests of the serving stream")
     ap.add_argument("--budget-gb", type=float, default=8.0, help="HBM budget of the serving loop")
     ap.add_argument("--large-n", type=int, default=384, help="cells per side of the large workload")
+    ap.add_argument("--no-large", action="store_true",
+                    help="skip the large-case measurement added to the default line")
     return ap.parse_args()
 
 
@@ -510,6 +512,16 @@ def run_ours(args):
         serving["workload"] = WORKLOADS["serving"]
         api.mech_init(case.mech)
 
+    large = None
+    if not args.no_large and world == 1 and args.workload == "precision3d":
+        dc = phi_new = None
+        torch.cuda.empty_cache()
+        large = measure_large(100, 3, n=args.large_n)
+        large.pop("clocks", None)
+        large["workload"] = WORKLOADS["large"].replace("384^3", f"{args.large_n}^3")
+        torch.cuda.empty_cache()
+        api.mech_init(case.mech)
+
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         threads = os.cpu_count() or 1
@@ -545,6 +557,7 @@ def run_ours(args):
                                 "max_rel_to_step_scale": float(np.max(err_scaled))},
         "batched": batched,
         "serving": serving,
+        "large": large,
     }
     print(json.dumps(line), flush=True)
     return 0

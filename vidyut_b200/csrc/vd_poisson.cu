@@ -180,6 +180,28 @@ __global__ void __launch_bounds__(128) k_mg_prolong(Level F, Level C, BcInfo bc)
     F.phi[lin(F, i, j, k)] += acc;
 }
 
+// bottom solve of a small coarsest grid: one CTA runs every red-black sweep, with
+// a barrier between half sweeps (cells <= kBottomCells)
+constexpr int kBottomCells = 4096;
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_mg_bottom(Level L, BcInfo bc, int sweeps)
+{
+    const int n0 = L.n[0], n1 = L.n[1];
+    const int nc = (int)L.cells();
+    for (int s = 0; s < sweeps; s++)
+        for (int color = 0; color < 2; color++) {
+            for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+                const int k = c / (n0 * n1), r = c - k * n0 * n1, j = r / n0, i = r - j * n0;
+                if (((i + j + k) & 1) != color) continue;
+                double off, diag;
+                stencil(L, bc, DIM, i, j, k, L.phi, off, diag);
+                L.phi[c] = (L.rhs[c] - off) / diag;
+            }
+            __syncthreads();
+        }
+}
+
 dim3 grid_cells(const Level& L, int per_thread = 1)
 {
     const int nx = (L.n[0] + per_thread - 1) / per_thread;
@@ -203,6 +225,11 @@ struct Mg {
         ProfScope ps("k_mg_restrict", st);
         k_mg_restrict<DIM><<<grid_cells(C), 128, 0, st>>>(F, C);
     }
+    static void bottom(const Level& L, const BcInfo& b, int sweeps, cudaStream_t st)
+    {
+        ProfScope ps("k_mg_bottom", st);
+        k_mg_bottom<DIM><<<1, 256, 0, st>>>(L, b, sweeps);
+    }
     static void prolong(const Level& F, const Level& C, const BcInfo& b, cudaStream_t st)
     {
         ProfScope ps("k_mg_prolong", st);
@@ -215,13 +242,14 @@ struct MgOps {
     void (*residual)(const Level&, const BcInfo&, unsigned long long*, cudaStream_t);
     void (*restrict_)(const Level&, const Level&, cudaStream_t);
     void (*prolong)(const Level&, const Level&, const BcInfo&, cudaStream_t);
+    void (*bottom)(const Level&, const BcInfo&, int, cudaStream_t);
 };
 
 MgOps mg_ops(int dim)
 {
-    if (dim == 1) return {Mg<1>::rbgs, Mg<1>::residual, Mg<1>::restrict_, Mg<1>::prolong};
-    if (dim == 2) return {Mg<2>::rbgs, Mg<2>::residual, Mg<2>::restrict_, Mg<2>::prolong};
-    return {Mg<3>::rbgs, Mg<3>::residual, Mg<3>::restrict_, Mg<3>::prolong};
+    if (dim == 1) return {Mg<1>::rbgs, Mg<1>::residual, Mg<1>::restrict_, Mg<1>::prolong, Mg<1>::bottom};
+    if (dim == 2) return {Mg<2>::rbgs, Mg<2>::residual, Mg<2>::restrict_, Mg<2>::prolong, Mg<2>::bottom};
+    return {Mg<3>::rbgs, Mg<3>::residual, Mg<3>::restrict_, Mg<3>::prolong, Mg<3>::bottom};
 }
 
 __global__ void k_maxabs(const double* x, int64_t n, unsigned long long* out)
@@ -490,10 +518,14 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
         const int nl = (int)lv.size();
         for (int l = 0; l < nl; l++) {
             const BcInfo& b = l == 0 ? bc : bc0;
-            const int sweeps = (l == nl - 1) ? 64 : 2;
-            for (int s = 0; s < sweeps; s++) {
-                ops.rbgs(lv[l], b, 0, st);
-                ops.rbgs(lv[l], b, 1, st);
+            if (l == nl - 1 && lv[l].cells() <= kBottomCells) {
+                ops.bottom(lv[l], b, 64, st);  // one CTA, all sweeps in one launch
+            } else {
+                const int sweeps = (l == nl - 1) ? 64 : 2;
+                for (int s = 0; s < sweeps; s++) {
+                    ops.rbgs(lv[l], b, 0, st);
+                    ops.rbgs(lv[l], b, 1, st);
+                }
             }
             if (l < nl - 1) {
                 ops.residual(lv[l], b, nullptr, st);
