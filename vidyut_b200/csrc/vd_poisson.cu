@@ -291,72 +291,68 @@ struct D3 {
     double v[3];
 };
 
-__global__ void k_pois_cell_fields(PoisArgs a, Level L, D3 dxs)
+__global__ void __launch_bounds__(128) k_pois_cell_fields(PoisArgs a, Level L, D3 dxs)
 {
     const int ns = a.ns;
     const int j = blockIdx.y, k = blockIdx.z;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < L.n[0]) {
-        const int64_t c = lin(L, i, j, k);
-        const int cc[3] = {i, j, k};
-        double E[3] = {0.0, 0.0, 0.0};
-        for (int d = 0; d < a.dim; d++) {
-            const int n = L.n[d];
-            int p1[3] = {i, j, k}, p2[3] = {i, j, k}, m1[3] = {i, j, k}, m2[3] = {i, j, k};
-            p1[d] += 1;
-            p2[d] += 2;
-            m1[d] -= 1;
-            m2[d] -= 2;
-            const double dx = dxs.v[d];
-            if (cc[d] > 0 && cc[d] < n - 1) {
-                E[d] = -0.5 * (L.phi[lin(L, p1[0], p1[1], p1[2])] - L.phi[lin(L, m1[0], m1[1], m1[2])]) / dx;
-            } else if (cc[d] == 0 && n > 1) {
-                if (n - 1 > 2)
-                    E[d] = -0.5 * (-L.phi[lin(L, p2[0], p2[1], p2[2])] + 4.0 * L.phi[lin(L, p1[0], p1[1], p1[2])] -
-                                   3.0 * L.phi[c]) / dx;
-                else
-                    E[d] = -(L.phi[lin(L, p1[0], p1[1], p1[2])] - L.phi[c]) / dx;
-            } else if (cc[d] == n - 1 && n > 1) {
-                if (n - 1 > 2)
-                    E[d] = -0.5 * (L.phi[lin(L, m2[0], m2[1], m2[2])] - 4.0 * L.phi[lin(L, m1[0], m1[1], m1[2])] +
-                                   3.0 * L.phi[c]) / dx;
-                else
-                    E[d] = -(L.phi[c] - L.phi[lin(L, m1[0], m1[1], m1[2])]) / dx;
-            }
+    if (i >= L.n[0]) return;
+    const int64_t c = lin(L, i, j, k);
+    const int cc[3] = {i, j, k};
+    const int64_t str[3] = {1, (int64_t)L.n[0], (int64_t)L.n[0] * L.n[1]};
+    const double* ph = L.phi;
+    double E[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        if (d >= a.dim) break;
+        const int n = L.n[d];
+        const int64_t s1 = str[d];
+        const double dx = dxs.v[d];
+        if (cc[d] > 0 && cc[d] < n - 1) {
+            E[d] = -0.5 * (ph[c + s1] - ph[c - s1]) / dx;
+        } else if (cc[d] == 0 && n > 1) {
+            if (n - 1 > 2) E[d] = -0.5 * (-ph[c + 2 * s1] + 4.0 * ph[c + s1] - 3.0 * ph[c]) / dx;
+            else E[d] = -(ph[c + s1] - ph[c]) / dx;
+        } else if (cc[d] == n - 1 && n > 1) {
+            if (n - 1 > 2) E[d] = -0.5 * (ph[c - 2 * s1] - 4.0 * ph[c - s1] + 3.0 * ph[c]) / dx;
+            else E[d] = -(ph[c] - ph[c - s1]) / dx;
         }
-        const int64_t o = a.st.off(a.lo[0] + i, a.lo[1] + j, a.lo[2] + k);
-        const int64_t cs = a.st.ns;
-        double nd = 0.0, es = 0.0;
-        for (int s = 0; s < ns; s++) nd += a.st.p[o + (int64_t)s * cs];
-        for (int d = 0; d < a.dim; d++) es += E[d] * E[d];
-        a.st.p[o + (int64_t)VD_POT(ns) * cs] = L.phi[c];
-        a.st.p[o + (int64_t)VD_EFX(ns) * cs] = E[0];
-        a.st.p[o + (int64_t)VD_EFY(ns) * cs] = E[1];
-        a.st.p[o + (int64_t)VD_EFZ(ns) * cs] = E[2];
-        // pow(Esum, 0.5) in the reference: the correctly rounded square root
-        a.st.p[o + (int64_t)VD_REF(ns) * cs] = (sqrt(es) / nd) / 1.0e-21;
     }
+    const int64_t o = a.st.off(a.lo[0] + i, a.lo[1] + j, a.lo[2] + k);
+    const int64_t cs = a.st.ns;
+    double nd = 0.0, es = 0.0;
+    for (int s = 0; s < ns; s++) nd += a.st.p[o + (int64_t)s * cs];
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+        if (d < a.dim) es += E[d] * E[d];
+    a.st.p[o + (int64_t)VD_POT(ns) * cs] = ph[c];
+    a.st.p[o + (int64_t)VD_EFX(ns) * cs] = E[0];
+    a.st.p[o + (int64_t)VD_EFY(ns) * cs] = E[1];
+    a.st.p[o + (int64_t)VD_EFZ(ns) * cs] = E[2];
+    // pow(Esum, 0.5) in the reference: the correctly rounded square root
+    a.st.p[o + (int64_t)VD_REF(ns) * cs] = (sqrt(es) / nd) / 1.0e-21;
 }
 
-// face field -dphi/dx_d on the face box of direction d; at a Dirichlet domain face
+// face field -dphi/dx_D on the face box of direction D; at a Dirichlet domain face
 // the gradient to the face value over half a cell, at a zero-gradient face 0
 // (what MLMG's getGradSolution returns, negated)
-__global__ void k_pois_face_field(Level L, BcInfo bc, A4 ef, int d, double dx)
+template <int D>
+__global__ void __launch_bounds__(128) k_pois_face_field(Level L, BcInfo bc, A4 ef, double dx)
 {
-    int nf[3] = {L.n[0], L.n[1], L.n[2]};
-    nf[d] += 1;
     const int j = blockIdx.y, k = blockIdx.z;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nf[0]) {
-        const int f[3] = {i, j, k};
-        int m[3] = {i, j, k};
-        m[d] -= 1;
-        double e;
-        if (f[d] == 0) e = bc.dir_lo[d] ? -(L.phi[lin(L, i, j, k)] - bc.val_lo[d]) / (0.5 * dx) : 0.0;
-        else if (f[d] == L.n[d]) e = bc.dir_hi[d] ? -(bc.val_hi[d] - L.phi[lin(L, m[0], m[1], m[2])]) / (0.5 * dx) : 0.0;
-        else e = -(L.phi[lin(L, i, j, k)] - L.phi[lin(L, m[0], m[1], m[2])]) / dx;
-        ef.p[ef.off(ef.bx + i, ef.by + j, ef.bz + k)] = e;
-    }
+    const int nf0 = L.n[0] + (D == 0);
+    if (i >= nf0) return;
+    const int f[3] = {i, j, k};
+    const int64_t s1 = D == 0 ? 1 : (D == 1 ? (int64_t)L.n[0] : (int64_t)L.n[0] * L.n[1]);
+    // linear index of the cell above the face; the cell below is c - s1 (for
+    // f[D] == n[D] the index runs one past the box and only c - s1 is read)
+    const int64_t c = lin(L, i, j, k);
+    double e;
+    if (f[D] == 0) e = bc.dir_lo[D] ? -(L.phi[c] - bc.val_lo[D]) / (0.5 * dx) : 0.0;
+    else if (f[D] == L.n[D]) e = bc.dir_hi[D] ? -(bc.val_hi[D] - L.phi[c - s1]) / (0.5 * dx) : 0.0;
+    else e = -(L.phi[c] - L.phi[c - s1]) / dx;
+    ef.p[ef.off(ef.bx + i, ef.by + j, ef.bz + k)] = e;
 }
 
 unsigned grid_of(int64_t n)
@@ -597,8 +593,11 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
             int nf[3] = {L.n[0], L.n[1], L.n[2]};
             nf[d] += 1;
             ProfScope ps("k_pois_face_field", st);
-            k_pois_face_field<<<dim3((unsigned)((nf[0] + 127) / 128), (unsigned)nf[1], (unsigned)nf[2]), 128, 0, st>>>(lv[0], bc, A4(efield_ec[d]), d,
-                                                                                        prm->dx[d]);
+            const dim3 g((unsigned)((nf[0] + 127) / 128), (unsigned)nf[1], (unsigned)nf[2]);
+            const A4 efd(efield_ec[d]);
+            if (d == 0) k_pois_face_field<0><<<g, 128, 0, st>>>(lv[0], bc, efd, prm->dx[0]);
+            else if (d == 1) k_pois_face_field<1><<<g, 128, 0, st>>>(lv[0], bc, efd, prm->dx[1]);
+            else k_pois_face_field<2><<<g, 128, 0, st>>>(lv[0], bc, efd, prm->dx[2]);
         }
     if ((rc = launch_check("potential fields"))) return rc;
     // ghosts of the potential, the cell field and the reduced field
