@@ -903,7 +903,7 @@ def measure_large(steps: int = 100, warmup: int = 3, n: int = 384, fp64_compare:
     L.vd_profile_enable(0)
     kms = {k: v[1] / v[0] for k, v in prof.items()}
     update_ms = kms.get("k_transport", 0.0) + kms.get("k_prep_spec", kms.get("k_prep", 0.0)) + \
-        2 * kms.get("k_ghost", 0.0)
+        kms.get("k_joule_pre", 0.0) + 2 * kms.get("k_ghost", 0.0)
     out = {"cells": cells, "steps": steps, "ms_per_step": ms, "value": cells / (ms * 1e-3),
            "update_ms_per_step": update_ms, "potential_ms_per_step": ms - update_ms,
            "vcycles_per_step": vcycles, "gpu_launches": int(launches), "clocks": clocks,

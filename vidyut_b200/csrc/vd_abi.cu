@@ -675,6 +675,8 @@ int vd_explicit_update_all(const vd_box* bx, vd_array4 sborder, const vd_array4 
     pa.do_reactions = prm->do_reactions;
     pa.write_n = 1;
     e = launch_prep(pa, prm->precision, ns, st);
+    if (e == cudaSuccess && a.elecenergy && !joule_in_tile(a, prm->precision))
+        e = launch_joule_pre(a, dim, prm->precision, st);
     if (e == cudaSuccess) e = launch_transport(a, dim, prm->precision, st);
     cudaError_t e2 = cudaFreeAsync(scratch, st);
     if (e != cudaSuccess) return cuda_fail(e, "fused update launch");
@@ -966,6 +968,8 @@ extern "C" int vd_explicit_update_all_noalloc(const vd_box* bx, vd_array4 sborde
     pa.do_reactions = prm->do_reactions;
     pa.write_n = 1;
     cudaError_t e = launch_prep(pa, prm->precision, ns, st);
+    if (e == cudaSuccess && a.elecenergy && !joule_in_tile(a, prm->precision))
+        e = launch_joule_pre(a, dim, prm->precision, st);
     if (e == cudaSuccess) e = launch_transport(a, dim, prm->precision, st);
     if (e != cudaSuccess) return cuda_fail(e, "allocation-free update launch");
     return VD_OK;

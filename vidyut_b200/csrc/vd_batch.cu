@@ -182,8 +182,8 @@ struct vd_batch {
     int2* d_ctrl = nullptr;
     int2* d_items = nullptr;
     size_t items_cap = 0;
-    int n_prep = 0, n_ghost = 0, n_tr[4] = {0, 0, 0, 0};
-    size_t off_prep = 0, off_ghost = 0, off_tr[4] = {0, 0, 0, 0};
+    int n_prep = 0, n_ghost = 0, n_tr[4] = {0, 0, 0, 0}, n_jl[4] = {0, 0, 0, 0};
+    size_t off_prep = 0, off_ghost = 0, off_tr[4] = {0, 0, 0, 0}, off_jl[4] = {0, 0, 0, 0};
     int2* h_ctrl[2] = {nullptr, nullptr};  // pinned staging of the control array
     cudaEvent_t ctrl_done[2] = {nullptr, nullptr};
     int ctrl_slot = 0;
@@ -245,7 +245,7 @@ int rebuild(vd_batch* b)
     std::vector<TransportArgs> tr(2 * (size_t)b->max_cases);
     std::vector<PrepArgs> pr(2 * (size_t)b->max_cases);
     std::vector<GhostArgs> gh(2 * (size_t)b->max_cases);
-    std::vector<int2> prep, ghost, trn[4];
+    std::vector<int2> prep, ghost, trn[4], jl[4];
     for (int c = 0; c < nb; c++) {
         Case& k = b->cases[c];
         const Layout& L = k.L;
@@ -325,11 +325,18 @@ int rebuild(vd_batch* b)
         const int64_t npc = (L.gcells + kPrepChunk - 1) / kPrepChunk;
         for (int64_t q = 0; q < npc; q++) prep.push_back(make_int2(c, (int)q));
         for (int64_t q = 0; q < ntiles; q++) trn[L.dim].push_back(make_int2(c, (int)q));
+        if (a.elecenergy && !joule_in_tile(a, b->prec)) {
+            const int64_t njt = L.dim == 1   ? joule_tile_count<1>(k.box.lo, k.box.hi)
+                                : L.dim == 2 ? joule_tile_count<2>(k.box.lo, k.box.hi)
+                                             : joule_tile_count<3>(k.box.lo, k.box.hi);
+            for (int64_t q = 0; q < njt; q++) jl[L.dim].push_back(make_int2(c, (int)q));
+        }
         const int64_t ngc = (gcount + kGhostChunk - 1) / kGhostChunk;
         for (int64_t q = 0; q < ngc; q++) ghost.push_back(make_int2(c, (int)q));
     }
-    // one items array: prep | ghost | transport 1-D | 2-D | 3-D
-    size_t total = prep.size() + ghost.size() + trn[1].size() + trn[2].size() + trn[3].size();
+    // one items array: prep | ghost | transport 1-D | 2-D | 3-D | Joule 1-D | 2-D | 3-D
+    size_t total = prep.size() + ghost.size();
+    for (int d = 1; d <= 3; d++) total += trn[d].size() + jl[d].size();
     if (total > (size_t)INT32_MAX) return err(VD_ERR_ARG, "too many work items");
     if (total > b->items_cap) {
         if (b->d_items) cudaFree(b->d_items);
@@ -353,6 +360,11 @@ int rebuild(vd_batch* b)
         all.insert(all.end(), trn[d].begin(), trn[d].end());
         b->n_tr[d] = (int)trn[d].size();
     }
+    for (int d = 1; d <= 3; d++) {
+        b->off_jl[d] = all.size();
+        all.insert(all.end(), jl[d].begin(), jl[d].end());
+        b->n_jl[d] = (int)jl[d].size();
+    }
     b->n_prep = (int)prep.size();
     b->n_ghost = (int)ghost.size();
     cudaError_t e = cudaSuccess;
@@ -370,7 +382,7 @@ int rebuild(vd_batch* b)
     }
     if (e != cudaSuccess) return cuda_err(e, "uploading batch tables");
     int ndims = 0;
-    for (int d = 1; d <= 3; d++) ndims += b->n_tr[d] > 0;
+    for (int d = 1; d <= 3; d++) ndims += (b->n_tr[d] > 0) + (b->n_jl[d] > 0);
     b->launches_per_step = (b->n_prep > 0) + ndims + (b->n_ghost > 0);
     drop_graph(b);
     b->dirty = false;
@@ -388,6 +400,9 @@ cudaError_t queue_steps(vd_batch* b, int nsteps, cudaStream_t st)
     for (int t = 0; t < nsteps; t++) {
         BatchCtl ctl{b->d_ctrl, b->max_cases, t};
         cudaError_t e = launch_prep_batch(b->d_pr, b->d_items + b->off_prep, b->n_prep, ctl, b->prec, ns, st);
+        if (e != cudaSuccess) return e;
+        for (int d = 1; d <= 3 && e == cudaSuccess; d++)
+            e = launch_joule_pre_batch(b->d_tr, b->d_items + b->off_jl[d], b->n_jl[d], ctl, d, b->prec, st);
         if (e != cudaSuccess) return e;
         if (nd > 1) {
             // independent dimensions run side by side
@@ -822,6 +837,8 @@ int vd_batch_tune(vd_batch* b, int trials, void* stream, double* ms_out)
             BatchCtl ctl{b->d_ctrl, b->max_cases, 0};
             cudaError_t e =
                 launch_prep_batch(b->d_pr, b->d_items + b->off_prep, b->n_prep, ctl, b->prec, b->mech.ns, st);
+            if (e == cudaSuccess)
+                e = launch_joule_pre_batch(b->d_tr, b->d_items + b->off_jl[d], b->n_jl[d], ctl, d, b->prec, st);
             // one untimed launch, then the timed ones
             if (e == cudaSuccess)
                 e = launch_transport_batch(b->d_tr, b->d_items + b->off_tr[d], b->n_tr[d], ctl, d, b->prec, v, st);

@@ -1,4 +1,5 @@
-// vd_batch_kernels.cu -- launch variants of the batched persistent transport kernel.
+// vd_batch_kernels.cu -- launch variants of the batched persistent transport kernel,
+// and the batched Joule pre-pass that runs before it.
 //
 // A variant is a tile shape and a residency target (CTAs per SM the compiler must
 // fit, which caps registers at 64K / (threads x CTAs)); the species group size
@@ -124,6 +125,56 @@ static cudaError_t launch_trb_v(const TransportArgs* boxes, const int2* items, i
     } else {
         return cudaErrorInvalidValue;
     }
+}
+
+// Joule pre-pass over (box, tile) items: each CTA walks the work list with a grid
+// stride, keeping the item's record in shared memory like the transport kernel.
+template <int DIM, int PREC>
+__global__ void __launch_bounds__(kJouleThreads, 3)
+    k_joule_pre_batch(const TransportArgs* __restrict__ boxes, const int2* __restrict__ items, int nitems,
+                      const BatchCtl ctl)
+{
+    __shared__ long long sA_raw[sizeof(TransportArgs) / 8];
+    __shared__ double sJ[DIM * joule_face_box<DIM>()];
+    const TransportArgs& sA = *reinterpret_cast<const TransportArgs*>(sA_raw);
+    int cur = -1;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int2 w = items[it];
+        const int2 cc = ctl.ctrl[w.x];
+        if (ctl.t >= cc.x) continue;  // uniform over the CTA
+        const int rec = ((ctl.t + cc.y) & 1) * ctl.nbox + w.x;
+        if (rec != cur) {
+            const long long* src = reinterpret_cast<const long long*>(boxes + rec);
+            for (int q = threadIdx.x; q < (int)(sizeof(TransportArgs) / 8); q += kJouleThreads) sA_raw[q] = src[q];
+            cur = rec;
+            __syncthreads();
+        }
+        joule_tile<DIM, PREC>(sA, w.y, sJ);
+        __syncthreads();  // the next item's record and faces must not overwrite a slow thread's reads
+    }
+}
+
+cudaError_t launch_joule_pre_batch(const TransportArgs* boxes, const int2* items, int nitems, BatchCtl ctl, int dim,
+                                   int prec, cudaStream_t st)
+{
+    if (nitems <= 0) return cudaSuccess;
+    static int nsm = 0;
+    if (!nsm) {
+        int dev = 0, n = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        nsm = n;
+    }
+    const int grid = nitems < nsm * 8 ? nitems : nsm * 8;
+    ProfScope ps("k_joule_pre_batch", st);
+    const bool mx = prec == PREC_MIXED;
+    if (dim == 1 && mx) k_joule_pre_batch<1, PREC_MIXED><<<grid, kJouleThreads, 0, st>>>(boxes, items, nitems, ctl);
+    else if (dim == 1) k_joule_pre_batch<1, PREC_FP64><<<grid, kJouleThreads, 0, st>>>(boxes, items, nitems, ctl);
+    else if (dim == 2 && mx) k_joule_pre_batch<2, PREC_MIXED><<<grid, kJouleThreads, 0, st>>>(boxes, items, nitems, ctl);
+    else if (dim == 2) k_joule_pre_batch<2, PREC_FP64><<<grid, kJouleThreads, 0, st>>>(boxes, items, nitems, ctl);
+    else if (mx) k_joule_pre_batch<3, PREC_MIXED><<<grid, kJouleThreads, 0, st>>>(boxes, items, nitems, ctl);
+    else k_joule_pre_batch<3, PREC_FP64><<<grid, kJouleThreads, 0, st>>>(boxes, items, nitems, ctl);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_transport_batch(const TransportArgs* boxes, const int2* items, int nitems, BatchCtl ctl, int dim,

@@ -7,7 +7,8 @@
 //   k_dsdt             Source/ScalarSolve.cpp:44-53
 //   k_joule            Source/ElecEnergySource.cpp:65-171
 //   k_prep             fused path, pass 1: sum_s n_s on the grown box + chemistry
-//   k_transport        fused path, pass 2: for every transported species and sweep
+//   k_joule_pre        fused path, pass 2: the Joule term of every valid cell
+//   k_transport        fused path, pass 3: for every transported species and sweep
 //                      direction, stage the stencil lines of a tile in shared memory,
 //                      compute each face flux once, take the divergence, add rxn and
 //                      the Joule term, and write n + dt*dsdt (FP64 accumulate).
@@ -688,6 +689,40 @@ static cudaError_t launch_tr_v(const TransportArgs& a, cudaStream_t st)
     }
     if (mb == 2) return launch_tr<DIM, PREC, 2>(a, st);
     return launch_tr<DIM, PREC, 1>(a, st);
+}
+
+// one CTA per JouleTile tile of the box
+template <int DIM, int PREC>
+__global__ void __launch_bounds__(kJouleThreads, 3) k_joule_pre(const __grid_constant__ TransportArgs a, int64_t ntiles)
+{
+    __shared__ double sJ[DIM * joule_face_box<DIM>()];
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        joule_tile<DIM, PREC>(a, (int)t, sJ);
+        __syncthreads();  // the next tile rewrites sJ
+    }
+}
+
+template <int DIM, int PREC>
+static cudaError_t launch_jp(const TransportArgs& a, cudaStream_t st)
+{
+    const int64_t nt = joule_tile_count<DIM>(a.lo, a.hi);
+    if (nt <= 0) return cudaSuccess;
+    const unsigned g = (unsigned)(nt < (1 << 30) ? nt : (1 << 30));
+    ProfScope ps("k_joule_pre", st);
+    k_joule_pre<DIM, PREC><<<g, kJouleThreads, 0, st>>>(a, nt);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_joule_pre(const TransportArgs& a, int dim, int prec, cudaStream_t st)
+{
+    if (prec == PREC_MIXED) {
+        if (dim == 1) return launch_jp<1, PREC_MIXED>(a, st);
+        if (dim == 2) return launch_jp<2, PREC_MIXED>(a, st);
+        return launch_jp<3, PREC_MIXED>(a, st);
+    }
+    if (dim == 1) return launch_jp<1, PREC_FP64>(a, st);
+    if (dim == 2) return launch_jp<2, PREC_FP64>(a, st);
+    return launch_jp<3, PREC_FP64>(a, st);
 }
 
 cudaError_t launch_transport(const TransportArgs& a, int dim, int prec, cudaStream_t st)

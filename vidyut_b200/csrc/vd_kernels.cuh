@@ -43,6 +43,14 @@ struct TransportArgs {
     double fl_K[VD_MAX_SPECIES + 1];
 };
 
+// The mixed path evaluates the Joule faces inside the transport tile when the tile
+// has a drift-flux barrier to publish them by; otherwise (and always in FP64) a
+// Joule pass (launch_joule_pre) runs before the transport update.
+__host__ __device__ inline bool joule_in_tile(const TransportArgs& a, int prec)
+{
+    return prec == PREC_MIXED && a.elecenergy && a.nfl > 0;
+}
+
 // Fills the derived fluxed / unfluxed lists and velocity bases of a from its tr_*
 // lists and the mechanism table m (host).
 void finish_species_lists(TransportArgs& a, const VdMechDev& m);
@@ -93,6 +101,10 @@ cudaError_t launch_transport_batch(const TransportArgs* boxes, const int2* items
                                    int prec, int variant, cudaStream_t st);
 cudaError_t launch_ghost_batch(const GhostArgs* boxes, const int2* items, int nitems, BatchCtl ctl,
                                cudaStream_t st);
+// launch_joule_pre over the (box, Joule tile) items of boxes of dimension dim
+// (vd_batch_kernels.cu; tiles as joule_tile_count in vd_transport.cuh)
+cudaError_t launch_joule_pre_batch(const TransportArgs* boxes, const int2* items, int nitems, BatchCtl ctl, int dim,
+                                   int prec, cudaStream_t st);
 cudaError_t launch_ghost(const GhostArgs& a, cudaStream_t st);
 // tile shapes of the batched transport kernel: variant v of dimension dim
 int batch_tile_variants(int dim);
@@ -110,6 +122,11 @@ cudaError_t launch_dsdt(const BoxIdx& b, int dim, int specid, const A4 flux[3], 
 cudaError_t launch_joule(const BoxIdx& b, int dim, const A4& sb, const A4& rxn, const A4 ef[3], const A4 gne[3],
                          const A4& dsdt, const A4& pn, const TransportArgs& cfg, cudaStream_t st);
 cudaError_t launch_prep(const PrepArgs& a, int prec, int ns, cudaStream_t st);
+// The Joule term of every valid cell of the box into the EJH component of a.pn; a
+// transport update with an electron energy equation that does not evaluate it in
+// the tile (joule_in_tile) reads it there, so this runs between launch_prep and
+// launch_transport.
+cudaError_t launch_joule_pre(const TransportArgs& a, int dim, int prec, cudaStream_t st);
 cudaError_t launch_transport(const TransportArgs& a, int dim, int prec, cudaStream_t st);
 cudaError_t launch_checksums(const BoxIdx& b, const A4& rxn, const A4& pn, double* out, cudaStream_t st);
 cudaError_t launch_time_scales(const BoxIdx& b, int dim, const A4& st, const TransportArgs& a,
@@ -125,6 +142,28 @@ void add_launches(int64_t n);     // kernels run by a graph replay
 void prof_suspend(bool on);       // this thread: no event pairs (stream capture)
 void prof_enable(bool on);
 int prof_read(char* names, int names_len, int64_t* counts, double* ms, int max);
+
+// Tiles of the Joule pass: 256 cells, each face of the tile evaluated once.
+template <int DIM> struct JouleTile;
+template <> struct JouleTile<1> { static constexpr int X = 256, Y = 1, Z = 1; };
+template <> struct JouleTile<2> { static constexpr int X = 32, Y = 8, Z = 1; };
+template <> struct JouleTile<3> { static constexpr int X = 8, Y = 8, Z = 4; };
+constexpr int kJouleThreads = 256;
+// faces of one direction, on the tile's box grown by one along every direction
+// of the problem
+template <int DIM> constexpr int joule_face_box()
+{
+    return (JouleTile<DIM>::X + 1) * (JouleTile<DIM>::Y + (DIM > 1)) * (JouleTile<DIM>::Z + (DIM > 2));
+}
+
+// number of JouleTile tiles covering box lo..hi
+template <int DIM>
+__host__ __device__ inline int64_t joule_tile_count(const int* lo, const int* hi)
+{
+    using JT = JouleTile<DIM>;
+    return (int64_t)((hi[0] - lo[0] + JT::X) / JT::X) * ((hi[1] - lo[1] + JT::Y) / JT::Y) *
+           ((hi[2] - lo[2] + JT::Z) / JT::Z);
+}
 
 // Kernel-variant knobs set by the tuner (vd_tune_set / vd_tune_get).
 int tune_set(const char* key, int value);

@@ -12,7 +12,11 @@
 //     group is computed once (all directions, faces spread over the threads), then
 //     each thread takes the divergence of its own cell, adds rxn (and the Joule
 //     term for the electron energy) and writes n + dt*dsdt in FP64.  Two barriers
-//     per group.
+//     per group.  The Joule term: the mixed path evaluates every face of the
+//     tile once in FP32 before the first barrier (joule_face_mixed); the FP64
+//     path reads it from the EJH diagnostic, where a kernel run just before left
+//     it (joule_tile): FP64 face arithmetic inside the tile kernel would raise the
+//     register pressure of every phase.
 // (2) Transported species without a drift flux, background species and the Te
 //     update need no neighbours and no barrier.
 // The tile body is a device function so that the per-box kernel (one CTA per
@@ -101,14 +105,27 @@ template <int PREC> struct VelT { using T = double; };
 template <> struct VelT<PREC_MIXED> { using T = float; };
 
 // dynamic shared memory of one tile with nb velocity bases and species groups of
-// GRP: the group's face fluxes and the Joule term of every face (FP64), then the
-// bases and the group's staged densities (FP32 in the mixed path)
+// GRP: the group's face fluxes (FP64) and, in the mixed path, the Joule term of
+// every face; then the bases and the group's staged densities (FP32 in the mixed
+// path)
+// The mixed path of 1-D and 2-D tiles also stages the Joule inputs of every staged
+// position: ne (FP64: its face differences are the density gradient), Te and the
+// density sum (FP32).  3-D tiles read them from global memory (the staged lines
+// of three directions would not fit).
+template <int DIM, int PREC> constexpr bool joule_staged() { return PREC == PREC_MIXED && DIM < 3; }
+struct JStage {
+    double* ne;
+    float* te;
+    float* nd;
+};
+
 template <int DIM, int PREC, class TS, int GRP>
 __host__ __device__ constexpr size_t transport_smem(int nb)
 {
     using G = TileGeom<DIM, TS>;
-    return (size_t)(GRP + 1) * G::FTOT * sizeof(double) +
-           (size_t)(nb + GRP) * G::STOT * sizeof(typename VelT<PREC>::T);
+    return (size_t)(GRP + (PREC == PREC_MIXED)) * G::FTOT * sizeof(double) +
+           (size_t)(nb + GRP) * G::STOT * sizeof(typename VelT<PREC>::T) +
+           (joule_staged<DIM, PREC>() ? (size_t)G::STOT * (sizeof(double) + 2 * sizeof(float)) : 0);
 }
 
 // Species per group for a kernel that must keep MINB CTAs resident per SM: the
@@ -161,6 +178,121 @@ __device__ __forceinline__ double joule_face(const TransportArgs& a, int D, cons
     const double cur = a.charge_e * (mu * ne * ef - dc * gn);
     return cur * ef;
 }
+
+// the arithmetic of joule_face_mixed from the face's Te and density-sum averages,
+// the two cells' ne, the face field and the density gradient
+__device__ __forceinline__ double joule_mixed_core(const TransportArgs& a, float etemp, float ndens, double nel,
+                                                   double ner, double ef, double gn)
+{
+    const int eidx = a.e_id;
+    const float Tg = (float)a.Tg;
+    float mu, dc;
+    if (a.const_ele_trans) {
+        const float rn = rcp_approx(ndens);
+        mu = (float)a.ele_mob * rn;
+        dc = (float)a.ele_diff * rn;
+    } else {
+        mu = mob_f32(eidx, etemp, ndens, Tg);
+        const int dk = c_mech.diff_kind[eidx], dr = c_mech.diff_ref[eidx];
+        const float mr = dr == eidx ? mu : mob_f32(dr, etemp, ndens, Tg);
+        if (dk == VD_DIFF_TE_ABSMOB) dc = (float)c_mech.diff_factor[eidx] * (etemp * (float)(1.0 / EV)) * fabsf(mr);
+        else if (dk == VD_DIFF_TG_MOB) dc = (float)c_mech.diff_factor[eidx] * (Tg * (float)(1.0 / EV)) * mr;
+        else dc = 0.0f;
+    }
+    const double drift = (double)(mu * (float)(0.5 * (nel + ner)) * (float)ef);
+    const double diffusion = (double)(dc * (float)gn);
+    return a.charge_e * (drift - diffusion) * ef;
+}
+
+// joule_face of the mixed path: the face averages, mobility, diffusion and the
+// two current products (mu ne E_f and D grad ne) in FP32 on the special-function
+// unit's reciprocal and square root, as for the drift fluxes; their difference,
+// the charge and the product with E_f in FP64.
+__device__ __forceinline__ double joule_face_mixed(const TransportArgs& a, int D, const int* g)
+{
+    const int ns = a.ns, eidx = a.e_id;
+    int l[3] = {g[0], g[1], g[2]};
+    l[D] -= 1;
+    const int64_t ol = a.sb.off(l[0], l[1], l[2]);
+    const int64_t orr = a.sb.off(g[0], g[1], g[2]);
+    const double* p = a.sb.p;
+    const int64_t cs = a.sb.ns;
+    const float etemp = 0.5f * ((float)p[ol + VD_ETEMP(ns) * cs] + (float)p[orr + VD_ETEMP(ns) * cs]);
+    const double nel = p[ol + eidx * cs], ner = p[orr + eidx * cs];
+    const double ef = a.cs_technique ? 0.5 * (p[ol + (VD_EFX(ns) + D) * cs] + p[orr + (VD_EFX(ns) + D) * cs])
+                                     : a.ef[D](g[0], g[1], g[2]);
+    const double gn = a.gradne_from_state ? (ner - nel) * a.idx[D] : a.gne[D](g[0], g[1], g[2]);
+    const float ndens = 0.5f * ((float)a.Nv.p[a.Nv.off(l[0], l[1], l[2])] + (float)a.Nv.p[a.Nv.off(g[0], g[1], g[2])]);
+    return joule_mixed_core(a, etemp, ndens, nel, ner, ef, gn);
+}
+
+// Joule term of every valid cell of tile `tile` (x fastest over the box's
+// JouleTile tiles, joule_tile_count): half the sum of joule_face over the cell's
+// 2 DIM faces, a domain face replaced by the next face inward
+// (Source/ElecEnergySource.cpp:84-94), halved and floored at 0 when floor_jh
+// (:153-162); stored in the EJH component of the output, the reference's
+// diagnostic (:168), where the transport update of the cell reads it.  The mixed
+// path evaluates the faces with joule_face_mixed, the FP64 path with joule_face.
+// Each face of the tile is evaluated once, by the thread of the cell above it
+// (the last cells of the tile also take the face above them); a domain face that
+// the substitution never reads is skipped.  Every thread of the CTA must call it; sJ
+// holds DIM * joule_face_box<DIM>() doubles, and its reads are finished when the
+// function returns only after a barrier (callers that reuse it synchronise).
+template <int DIM, int PREC>
+__device__ __forceinline__ void joule_tile(const TransportArgs& a, int tile, double* sJ)
+{
+    using JT = JouleTile<DIM>;
+    constexpr int T[3] = {JT::X, JT::Y, JT::Z};
+    constexpr int FB0 = JT::X + 1, FB1 = JT::Y + (DIM > 1), FBOX = joule_face_box<DIM>();
+    const int tid = threadIdx.x;
+    const int nt0 = (a.hi[0] - a.lo[0] + JT::X) / JT::X, nt1 = (a.hi[1] - a.lo[1] + JT::Y) / JT::Y;
+    const int tix = tile % nt0, tr = tile / nt0;
+    const int tiy = tr % nt1, tiz = tr / nt1;
+    const int c[3] = {tid % JT::X, (tid / JT::X) % JT::Y, tid / (JT::X * JT::Y)};
+    const int org[3] = {a.lo[0] + tix * JT::X, a.lo[1] + tiy * JT::Y, a.lo[2] + tiz * JT::Z};
+    const int g[3] = {org[0] + c[0], org[1] + c[1], org[2] + c[2]};
+    const bool own = g[0] <= a.hi[0] && g[1] <= a.hi[1] && g[2] <= a.hi[2];
+    if (own) {
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            const bool last = c[d] == T[d] - 1 || g[d] == a.hi[d];
+#pragma unroll
+            for (int f = 0; f < 2; f++) {
+                if (f == 1 && !last) break;
+                const int fe = g[d] + f;
+                // a domain face is read only when the domain is one cell wide
+                const bool skip = (fe == a.domlo[d] || fe == a.domhi[d] + 1) && a.domhi[d] > a.domlo[d];
+                int gf[3] = {g[0], g[1], g[2]};
+                gf[d] = fe;
+                int l[3] = {c[0], c[1], c[2]};
+                l[d] += f;
+                double jf = 0.0;
+                if (!skip) jf = PREC == PREC_FP64 ? joule_face(a, d, gf) : joule_face_mixed(a, d, gf);
+                sJ[d * FBOX + l[0] + FB0 * (l[1] + FB1 * l[2])] = jf;
+            }
+        }
+    }
+    __syncthreads();
+    if (own) {
+        double jheat = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+#pragma unroll
+            for (int f = 0; f < 2; f++) {
+                int fe = g[d] + f;
+                if (fe == a.domlo[d]) fe += 1;
+                if (fe == a.domhi[d] + 1) fe -= 1;
+                int l[3] = {c[0], c[1], c[2]};
+                l[d] += fe - g[d];
+                jheat += sJ[d * FBOX + l[0] + FB0 * (l[1] + FB1 * l[2])];
+            }
+        }
+        jheat *= 0.5;
+        if (a.floor_jh && jheat < 0.0) jheat = 0.0;
+        a.pn(g[0], g[1], g[2], VD_EJH(a.ns)) = jheat;
+    }
+}
+
 template <int DIM, int PREC, class TS, int GRP>
 constexpr size_t transport_smem_max() { return transport_smem<DIM, PREC, TS, GRP>(3); }
 
@@ -189,34 +321,42 @@ __device__ __forceinline__ bool staged_cell(const TransportArgs& a, int cc, cons
 // velocity bases of staged position cc of direction D: sB[k*STOT + cc] for slot k
 template <int DIM, int PREC, int D, class TS>
 __device__ __forceinline__ void stage_basis(const TransportArgs& a, int cc, const int* org,
-                                            typename VelT<PREC>::T* sB)
+                                            typename VelT<PREC>::T* sB, JStage js, bool jst)
 {
     using G = TileGeom<DIM, TS>;
     using VT = typename VelT<PREC>::T;
     int g[3];
     const bool ok = staged_cell<DIM, D, TS>(a, cc, org, g);
     VT b[3] = {VT(0), VT(0), VT(0)};
+    double ne = 0.0, Te = 0.0, N = 0.0;
     if (ok) {
         const int ns = a.ns;
         const int64_t cs = a.sb.ns;
         const double* p = a.sb.p + a.sb.off(g[0], g[1], g[2]);
         const double E = p[(VD_EFX(ns) + D) * cs];
-        const double N = a.Nv(g[0], g[1], g[2]);
+        N = a.Nv(g[0], g[1], g[2]);
+        Te = p[VD_ETEMP(ns) * cs];
+        if (joule_staged<DIM, PREC>() && jst) ne = p[a.e_id * cs];
         for (int k = 0; k < a.nb; k++) {
             const int kind = a.bkind[k];
             if constexpr (PREC == PREC_FP64) {
-                if (kind == 0) b[k] = E / (sqrt(p[VD_ETEMP(ns) * cs]) * N);
+                if (kind == 0) b[k] = E / (sqrt(Te) * N);
                 else if (kind == 1) b[k] = E / N;
                 else b[k] = E;
             } else {
                 const float Ef = (float)E, rN = rcp_approx((float)N);
-                if (kind == 0) b[k] = Ef * rsqrtf((float)p[VD_ETEMP(ns) * cs]) * rN;
+                if (kind == 0) b[k] = Ef * rsqrtf((float)Te) * rN;
                 else if (kind == 1) b[k] = Ef * rN;
                 else b[k] = Ef;
             }
         }
     }
     for (int k = 0; k < a.nb; k++) sB[k * G::STOT + cc] = b[k];
+    if (joule_staged<DIM, PREC>() && jst) {
+        js.ne[cc] = ne;
+        js.te[cc] = (float)Te;
+        js.nd[cc] = (float)N;
+    }
 }
 
 // density of species s at staged position cc of direction D
@@ -307,9 +447,15 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     const int tiz = tb / a.ntile[1];
     const int org[3] = {a.lo[0] + tix * G::T[0], a.lo[1] + tiy * G::T[1], a.lo[2] + tiz * G::T[2]};
     double* sF = reinterpret_cast<double*>(smem);
-    double* sJ = sF + GRP * G::FTOT;
-    VT* sB = reinterpret_cast<VT*>(sJ + G::FTOT);
+    double* sJ = sF + GRP * G::FTOT;  // mixed path only
+    double* sNe = sJ + (PREC == PREC_MIXED ? G::FTOT : 0);
+    VT* sB = reinterpret_cast<VT*>(sNe + (joule_staged<DIM, PREC>() ? G::STOT : 0));
     VT* sU = sB + a.nb * G::STOT;
+    JStage js{sNe, nullptr, nullptr};
+    if constexpr (joule_staged<DIM, PREC>()) {
+        js.te = reinterpret_cast<float*>(sU + GRP * G::STOT);
+        js.nd = js.te + G::STOT;
+    }
 
     // own cell
     const int cx = tid % G::T[0], cy = (tid / G::T[0]) % G::T[1], cz = tid / (G::T[0] * G::T[1]);
@@ -320,13 +466,13 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     const int64_t own_o = own ? a.sb.off(gi, gj, gk) : 0;
     double ne_new = 0.0, een_new = 0.0;
     const int nfl = a.nfl;
-    // Joule faces of the tile are computed once (phase 0) when a barrier follows
-    const bool jfaces = a.elecenergy && nfl > 0;
+    // the mixed path's Joule faces, evaluated here (a barrier follows them)
+    const bool jin = joule_in_tile(a, PREC);
 
-    // Joule term of the own cell: half the sum of its faces, each domain face
-    // replaced as the reference does (Source/ElecEnergySource.cpp:95-99)
+    // Joule term of the own cell from the tile's faces: half the sum of its faces,
+    // each domain face replaced as the reference does
+    // (Source/ElecEnergySource.cpp:84-94,153-162)
     auto joule_own = [&]() -> double {
-        if (!jfaces) return joule_cell<true>(a, DIM, gi, gj, gk);
         const int gc[3] = {gi, gj, gk}, lc[3] = {cx, cy, cz};
         double jheat = 0.0;
 #pragma unroll
@@ -351,12 +497,15 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     // one species' own-cell result
     auto finish = [&](int s, double acc) {
         if (s == ns) {
-            const double jh = joule_own();
-            acc += jh;
-            if (a.write_diag) {
+            if (jin) {
+                const double jh = joule_own();
+                acc += jh;
                 a.pn(gi, gj, gk, VD_EJH(ns)) = jh;
-                a.pn(gi, gj, gk, VD_EIH(ns)) = a.rxn(gi, gj, gk, ns);
+            } else {
+                // the Joule term the joule_tile pass left in EJH
+                acc += a.pn(gi, gj, gk, VD_EJH(ns));
             }
+            if (a.write_diag) a.pn(gi, gj, gk, VD_EIH(ns)) = a.rxn(gi, gj, gk, ns);
         }
         double nn = a.sb.p[own_o + s * cs] + a.dt * acc;
         if (a.bound_specden && s != ns) {
@@ -373,27 +522,63 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     if (nfl > 0) {
         // (0) velocity bases of every staged position
         for (int c = tid; c < G::STOT; c += NTH) {
-            if (c < G::SOFF1) stage_basis<DIM, PREC, 0, TS>(a, c, org, sB);
-            else if (DIM > 1 && c < G::SOFF2)
-                stage_basis<DIM, PREC, (DIM > 1 ? 1 : 0), TS>(a, c - G::SOFF1, org, sB + G::SOFF1);
-            else if (DIM > 2)
-                stage_basis<DIM, PREC, (DIM > 2 ? 2 : 0), TS>(a, c - G::SOFF2, org, sB + G::SOFF2);
+            if (c < G::SOFF1) {
+                stage_basis<DIM, PREC, 0, TS>(a, c, org, sB, js, jin);
+            } else if (DIM > 1 && c < G::SOFF2) {
+                const JStage j1{js.ne + G::SOFF1, js.te + G::SOFF1, js.nd + G::SOFF1};
+                stage_basis<DIM, PREC, (DIM > 1 ? 1 : 0), TS>(a, c - G::SOFF1, org, sB + G::SOFF1, j1, jin);
+            } else if (DIM > 2) {
+                const JStage j2{js.ne + G::SOFF2, js.te + G::SOFF2, js.nd + G::SOFF2};
+                stage_basis<DIM, PREC, (DIM > 2 ? 2 : 0), TS>(a, c - G::SOFF2, org, sB + G::SOFF2, j2, jin);
+            }
         }
     }
-    if (jfaces) {
-        // (0') the Joule term of every face of the tile, once
-        for (int f = tid; f < G::FTOT; f += NTH) {
-            int d = 0, ff = f;
-            if (DIM > 1 && f >= G::FOFF1) {
-                d = (DIM > 2 && f >= G::FOFF2) ? 2 : 1;
-                ff = f - (d == 1 ? G::FOFF1 : G::FOFF2);
+    if constexpr (PREC == PREC_MIXED) {
+        if (jin) {
+            // (0') the Joule term of every face of the tile, once (from the staged
+            // inputs of the face's two cells when they are staged; the basis loop
+            // above wrote them, so a barrier comes first)
+            if constexpr (joule_staged<DIM, PREC>()) __syncthreads();
+            for (int f = tid; f < G::FTOT; f += NTH) {
+                int d = 0, ff = f;
+                if (DIM > 1 && f >= G::FOFF1) {
+                    d = (DIM > 2 && f >= G::FOFF2) ? 2 : 1;
+                    ff = f - (d == 1 ? G::FOFF1 : G::FOFF2);
+                }
+                const int F0 = G::T[0] + (d == 0), F1 = G::T[1] + (d == 1);
+                int g[3] = {org[0] + ff % F0, org[1] + (ff / F0) % F1, org[2] + ff / (F0 * F1)};
+                bool ok = g[d] <= a.hi[d] + 1;
+                for (int e = 0; e < DIM; e++)
+                    if (e != d) ok = ok && g[e] <= a.hi[e];
+                double jf = 0.0;
+                if constexpr (joule_staged<DIM, PREC>()) {
+                    if (ok) {
+                        // staged index of the face's rel cell (f_d - 3 + q) is f_d + q
+                        // along d: the cells below and above are q = 2 and 3
+                        const int S0 = G::T[0] + (d == 0 ? 6 : 0), S1 = G::T[1] + (d == 1 ? 6 : 0);
+                        const int STR = d == 0 ? 1 : (d == 1 ? S0 : S0 * S1);
+                        const int soff = d == 0 ? 0 : (d == 1 ? G::SOFF1 : G::SOFF2);
+                        const int l0 = ff % F0, l1 = (ff / F0) % F1, l2 = ff / (F0 * F1);
+                        const int pl = soff + l0 + S0 * (l1 + S1 * l2) + 2 * STR, pr = pl + STR;
+                        const double nel = js.ne[pl], ner = js.ne[pr];
+                        double ef;
+                        if (a.cs_technique) {
+                            int gl[3] = {g[0], g[1], g[2]};
+                            gl[d] -= 1;
+                            const int64_t cs = a.sb.ns, ce = (VD_EFX(ns) + d) * cs;
+                            ef = 0.5 * (a.sb.p[a.sb.off(gl[0], gl[1], gl[2]) + ce] + a.sb.p[a.sb.off(g[0], g[1], g[2]) + ce]);
+                        } else {
+                            ef = a.ef[d](g[0], g[1], g[2]);
+                        }
+                        const double gn = a.gradne_from_state ? (ner - nel) * a.idx[d] : a.gne[d](g[0], g[1], g[2]);
+                        jf = joule_mixed_core(a, 0.5f * (js.te[pl] + js.te[pr]), 0.5f * (js.nd[pl] + js.nd[pr]), nel,
+                                              ner, ef, gn);
+                    }
+                } else {
+                    if (ok) jf = joule_face_mixed(a, d, g);
+                }
+                sJ[f] = jf;
             }
-            const int F0 = G::T[0] + (d == 0), F1 = G::T[1] + (d == 1);
-            int g[3] = {org[0] + ff % F0, org[1] + (ff / F0) % F1, org[2] + ff / (F0 * F1)};
-            bool ok = g[d] <= a.hi[d] + 1;
-            for (int e = 0; e < DIM; e++)
-                if (e != d) ok = ok && g[e] <= a.hi[e];
-            sJ[f] = ok ? joule_face(a, d, g) : 0.0;
         }
     }
     for (int g0 = 0; g0 < nfl; g0 += GRP) {
