@@ -189,13 +189,24 @@ def test_graph_and_direct_launches_agree(mech):
     assert sa["graph_builds"] >= 1 and sb["graph_builds"] == 0
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 6])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 6, 7])
 def test_tile_variants_agree(mech, variant):
     cases = make_cases(mech, [(37, 29), (90,)], seed=11)
     a, _ = run_batch(cases, abi.PREC_FP64, 3, variant=0)
     b, _ = run_batch(cases, abi.PREC_FP64, 3, variant=variant)
     for c, x, y in zip(cases, a, b):
         assert max_elem_rel(valid_trim(c, x), valid_trim(c, y)) <= 1e-13
+
+
+@pytest.mark.parametrize("variant", [3, 5, 7])
+def test_mixed_tile_variants_agree(mech, variant):
+    """Tile shape, residency and species grouping change which thread computes a
+    face, not its arithmetic: the mixed path gives the same bits for every variant."""
+    cases = make_cases(mech, [(37, 29), (90,)], seed=12)
+    a, _ = run_batch(cases, abi.PREC_MIXED, 3, variant=0)
+    b, _ = run_batch(cases, abi.PREC_MIXED, 3, variant=variant)
+    for c, x, y in zip(cases, a, b):
+        assert np.array_equal(valid_trim(c, x), valid_trim(c, y))
 
 
 def test_budget_admission_and_reuse(mech):

@@ -19,17 +19,17 @@ cudaError_t upload_mech_batch(const VdMechDev* h, cudaStream_t st)
     return cudaMemcpyToSymbolAsync(c_mech, h, sizeof(VdMechDev), 0, cudaMemcpyHostToDevice, st);
 }
 
-template <class TS_, int MINB_>
+template <class TS_, int MINB_, int GMAX_ = 8>
 struct BatchVariant {
     using TS = TS_;
     static constexpr int MINB = MINB_;
+    static constexpr int GMAX = GMAX_;  // species group cap (group_fit)
 };
 
 using T1a = TileShape<256, 1, 1, 256>;
 using T1b = TileShape<128, 1, 1, 128>;
 using T2a = TileShape<32, 8, 1, 256>;
 using T2b = TileShape<16, 16, 1, 256>;
-using T2c = TileShape<64, 4, 1, 256>;
 using T3a = TileShape<8, 8, 8, 512>;
 using T3b = TileShape<16, 8, 4, 512>;
 
@@ -39,8 +39,8 @@ template <> struct BatchVariants<1> {
                          BatchVariant<T1b, 4>>;
 };
 template <> struct BatchVariants<2> {
-    using L = std::tuple<BatchVariant<T2a, 2>, BatchVariant<T2b, 2>, BatchVariant<T2c, 2>, BatchVariant<T2a, 3>,
-                         BatchVariant<T2b, 3>, BatchVariant<T2a, 4>, BatchVariant<T2b, 4>>;
+    using L = std::tuple<BatchVariant<T2a, 2>, BatchVariant<T2b, 2>, BatchVariant<T2a, 3>, BatchVariant<T2b, 3>,
+                         BatchVariant<T2a, 4>, BatchVariant<T2b, 4>, BatchVariant<T2a, 4, 4>, BatchVariant<T2b, 4, 4>>;
 };
 template <> struct BatchVariants<3> {
     using L = std::tuple<BatchVariant<T3a, 2>, BatchVariant<T3b, 2>>;
@@ -90,9 +90,9 @@ static cudaError_t launch_trb(const TransportArgs* boxes, const int2* items, int
 {
     using TS = typename BV::TS;
     constexpr int MINB = BV::MINB;
-    constexpr int GRP = group_fit<DIM, PREC, TS, MINB>();
+    constexpr int GRP = group_fit<DIM, PREC, TS, MINB, BV::GMAX>();
     constexpr size_t smem = transport_smem_max<DIM, PREC, TS, GRP>();  // boxes differ in basis count
-    auto fn = k_transport_batch<DIM, PREC, TS, MINB>;
+    auto fn = k_transport_batch<DIM, PREC, TS, MINB, BV::GMAX>;
     static int grid_of[32] = {0};  // persistent grid (SMs x resident CTAs), per device
     int dev = 0;
     cudaGetDevice(&dev);

@@ -156,10 +156,18 @@ std::string gen_prep_kernel(const VdMechDev& m, int prec)
     o << "  const int gx = a.ghi[0] - a.glo[0] + 1, gy = a.ghi[1] - a.glo[1] + 1;\n"
          "  const i64 cs = a.sb.ns, rs = a.rxn.ns;\n"
          "  {\n"
-         "    int k = (int)(idx / ((i64)gx * gy));\n"
-         "    i64 r = idx - (i64)k * gx * gy;\n"
-         "    int j = (int)(r / gx);\n"
-         "    int i = (int)(r - (i64)j * gx);\n"
+         "    int i, j, k;\n"
+         "    const i64 gxy = (i64)gx * gy;\n"
+         "    if (idx < 0xffffffffLL && gxy < 0xffffffffLL) {  // 32-bit division, the usual case\n"
+         "      const unsigned u = (unsigned)idx, pl = (unsigned)gxy;\n"
+         "      const unsigned kk = u / pl, rr = u - kk * pl, jj = rr / (unsigned)gx;\n"
+         "      k = (int)kk; j = (int)jj; i = (int)(rr - jj * (unsigned)gx);\n"
+         "    } else {\n"
+         "      k = (int)(idx / gxy);\n"
+         "      const i64 r = idx - (i64)k * gxy;\n"
+         "      j = (int)(r / gx);\n"
+         "      i = (int)(r - (i64)j * gx);\n"
+         "    }\n"
          "    i += a.glo[0]; j += a.glo[1]; k += a.glo[2];\n"
          "    const double* p = a.sb.p + a.sb.off(i, j, k);\n";
     for (int s = 0; s < ns; s++) o << "    const double n" << s << " = p[" << s << " * cs];\n";

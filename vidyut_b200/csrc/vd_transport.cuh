@@ -104,14 +104,10 @@ struct TileGeom {
 template <int PREC> struct VelT { using T = double; };
 template <> struct VelT<PREC_MIXED> { using T = float; };
 
-// dynamic shared memory of one tile with nb velocity bases and species groups of
-// GRP: the group's face fluxes (FP64) and, in the mixed path, the Joule term of
-// every face; then the bases and the group's staged densities (FP32 in the mixed
-// path)
 // The mixed path of 1-D and 2-D tiles also stages the Joule inputs of every staged
 // position: ne (FP64: its face differences are the density gradient), Te and the
-// density sum (FP32).  3-D tiles read them from global memory (the staged lines
-// of three directions would not fit).
+// density sum (FP32), in the space of the staged densities (they are read before
+// the first group is staged).  3-D tiles read them from global memory.
 template <int DIM, int PREC> constexpr bool joule_staged() { return PREC == PREC_MIXED && DIM < 3; }
 struct JStage {
     double* ne;
@@ -119,26 +115,47 @@ struct JStage {
     float* nd;
 };
 
+__host__ __device__ constexpr size_t smem_align(size_t x) { return (x + 15) & ~(size_t)15; }
+
+// Dynamic shared memory of one tile with nb velocity bases and species groups of
+// GRP, in this order: the Joule term of every face (FP64, mixed path); the group's
+// face fluxes; the bases; the group's staged densities (or the staged Joule
+// inputs).  Fluxes, bases and densities are FP32 in the mixed path: a mixed flux
+// is an FP32 value times a power of two, so it is stored exactly.
+template <int DIM, int PREC, class TS>
+struct TileSmem {
+    using G = TileGeom<DIM, TS>;
+    using VT = typename VelT<PREC>::T;
+    static constexpr size_t joule() { return PREC == PREC_MIXED ? smem_align((size_t)G::FTOT * sizeof(double)) : 0; }
+    static constexpr size_t flux(int grp) { return smem_align((size_t)grp * G::FTOT * sizeof(VT)); }
+    static constexpr size_t basis(int nb) { return smem_align((size_t)nb * G::STOT * sizeof(VT)); }
+    static constexpr size_t dens(int grp)
+    {
+        const size_t d = (size_t)grp * G::STOT * sizeof(VT);
+        const size_t j = joule_staged<DIM, PREC>() ? (size_t)G::STOT * (sizeof(double) + 2 * sizeof(float)) : 0;
+        return d > j ? d : j;
+    }
+};
+
 template <int DIM, int PREC, class TS, int GRP>
 __host__ __device__ constexpr size_t transport_smem(int nb)
 {
-    using G = TileGeom<DIM, TS>;
-    return (size_t)(GRP + (PREC == PREC_MIXED)) * G::FTOT * sizeof(double) +
-           (size_t)(nb + GRP) * G::STOT * sizeof(typename VelT<PREC>::T) +
-           (joule_staged<DIM, PREC>() ? (size_t)G::STOT * (sizeof(double) + 2 * sizeof(float)) : 0);
+    using S = TileSmem<DIM, PREC, TS>;
+    return S::joule() + S::flux(GRP) + S::basis(nb) + S::dens(GRP);
 }
 
 // Species per group for a kernel that must keep MINB CTAs resident per SM: the
-// largest of 8, 4, 2, 1 whose tile (with up to three velocity bases, the batched
-// kernel's copy of its record and the driver's reserve) fits MINB times into the
-// SM's 228 KB of shared memory.  Larger groups mean fewer barriers and more loads
-// in flight; smaller ones leave room for more resident CTAs.
-template <int DIM, int PREC, class TS, int MINB>
+// largest of 8, 4, 2, 1 (at most GMAX) whose tile (with up to three velocity
+// bases, the batched kernel's copy of its record and the driver's reserve) fits
+// MINB times into the SM's 228 KB of shared memory.  Larger groups mean fewer
+// barriers and more loads in flight; smaller ones leave room for more resident
+// CTAs and for the L1 cache, which shares the same 256 KB per SM.
+template <int DIM, int PREC, class TS, int MINB, int GMAX = 8>
 constexpr int group_fit()
 {
     constexpr size_t per_sm = 228 * 1024, extra = 3 * 1024;
-    if ((transport_smem<DIM, PREC, TS, 8>(3) + extra) * MINB <= per_sm) return 8;
-    if ((transport_smem<DIM, PREC, TS, 4>(3) + extra) * MINB <= per_sm) return 4;
+    if (GMAX >= 8 && (transport_smem<DIM, PREC, TS, 8>(3) + extra) * MINB <= per_sm) return 8;
+    if (GMAX >= 4 && (transport_smem<DIM, PREC, TS, 4>(3) + extra) * MINB <= per_sm) return 4;
     if ((transport_smem<DIM, PREC, TS, 2>(3) + extra) * MINB <= per_sm) return 2;
     return 1;
 }
@@ -446,16 +463,16 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     const int tiy = tb % a.ntile[1];
     const int tiz = tb / a.ntile[1];
     const int org[3] = {a.lo[0] + tix * G::T[0], a.lo[1] + tiy * G::T[1], a.lo[2] + tiz * G::T[2]};
-    double* sF = reinterpret_cast<double*>(smem);
-    double* sJ = sF + GRP * G::FTOT;  // mixed path only
-    double* sNe = sJ + (PREC == PREC_MIXED ? G::FTOT : 0);
-    VT* sB = reinterpret_cast<VT*>(sNe + (joule_staged<DIM, PREC>() ? G::STOT : 0));
-    VT* sU = sB + a.nb * G::STOT;
-    JStage js{sNe, nullptr, nullptr};
-    if constexpr (joule_staged<DIM, PREC>()) {
-        js.te = reinterpret_cast<float*>(sU + GRP * G::STOT);
-        js.nd = js.te + G::STOT;
-    }
+    using SM = TileSmem<DIM, PREC, TS>;
+    double* sJ = reinterpret_cast<double*>(smem);  // mixed path only
+    VT* sF = reinterpret_cast<VT*>(smem + SM::joule());
+    VT* sB = reinterpret_cast<VT*>(smem + SM::joule() + SM::flux(GRP));
+    unsigned char* const dens = smem + SM::joule() + SM::flux(GRP) + SM::basis(a.nb);
+    VT* sU = reinterpret_cast<VT*>(dens);
+    // the staged Joule inputs share the densities' space: read in phase (0'),
+    // before a barrier that precedes the first group's staging
+    const JStage js{reinterpret_cast<double*>(dens), reinterpret_cast<float*>(dens + G::STOT * sizeof(double)),
+                    reinterpret_cast<float*>(dens + G::STOT * (sizeof(double) + sizeof(float)))};
 
     // own cell
     const int cx = tid % G::T[0], cy = (tid / G::T[0]) % G::T[1], cz = tid / (G::T[0] * G::T[1]);
@@ -579,6 +596,8 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
                 }
                 sJ[f] = jf;
             }
+            // the first group's staging overwrites the staged Joule inputs
+            if constexpr (joule_staged<DIM, PREC>()) __syncthreads();
         }
     }
     for (int g0 = 0; g0 < nfl; g0 += GRP) {
@@ -598,8 +617,8 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
         for (int q = tid; q < gn * G::FTOT; q += NTH) {
             const int j = q / G::FTOT, f = q - j * G::FTOT;
             const int sl = a.fl_slot[g0 + j];
-            sF[q] = face_any<DIM, PREC, TS>(a, f, a.fl_cls[g0 + j], org, sU + j * G::STOT,
-                                            sl >= 0 ? sB + sl * G::STOT : nullptr, a.fl_K[g0 + j]);
+            sF[q] = (VT)face_any<DIM, PREC, TS>(a, f, a.fl_cls[g0 + j], org, sU + j * G::STOT,
+                                                sl >= 0 ? sB + sl * G::STOT : nullptr, a.fl_K[g0 + j]);
         }
         __syncthreads();
         // (3) divergence + sources of the own cell: dsdt = (Fx_lo - Fx_hi)/dx + rxn,
@@ -607,22 +626,22 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
         if (own) {
 #pragma unroll 1
             for (int j = 0; j < gn; j++) {
-                const double* Fj = sF + j * G::FTOT;
+                const VT* Fj = sF + j * G::FTOT;
                 double acc;
                 {
                     constexpr int F0 = G::template FE<0>(0), F1 = G::template FE<0>(1);
                     const int lo_f = cx + F0 * (cy + F1 * cz);
-                    acc = (Fj[lo_f] - Fj[lo_f + 1]) * a.idx[0] + a.rxn(gi, gj, gk, a.fl_sp[g0 + j]);
+                    acc = ((double)Fj[lo_f] - (double)Fj[lo_f + 1]) * a.idx[0] + a.rxn(gi, gj, gk, a.fl_sp[g0 + j]);
                 }
                 if constexpr (DIM > 1) {
                     constexpr int F0 = G::template FE<1>(0), F1 = G::template FE<1>(1);
                     const int lo_f = G::FOFF1 + cx + F0 * (cy + F1 * cz);
-                    acc += (Fj[lo_f] - Fj[lo_f + F0]) * a.idx[1];
+                    acc += ((double)Fj[lo_f] - (double)Fj[lo_f + F0]) * a.idx[1];
                 }
                 if constexpr (DIM > 2) {
                     constexpr int F0 = G::template FE<2>(0), F1 = G::template FE<2>(1);
                     const int lo_f = G::FOFF2 + cx + F0 * (cy + F1 * cz);
-                    acc += (Fj[lo_f] - Fj[lo_f + F0 * F1]) * a.idx[2];
+                    acc += ((double)Fj[lo_f] - (double)Fj[lo_f + F0 * F1]) * a.idx[2];
                 }
                 finish(a.fl_sp[g0 + j], acc);
             }
@@ -672,7 +691,7 @@ __global__ void __launch_bounds__(default_nth<DIM>(), MINB) k_transport(const __
 // with a grid stride.  Boxes are described by TransportArgs records in global
 // memory; the item's record is first copied to shared memory, so that the tile
 // body's many reads of it are shared-memory loads rather than global ones.
-template <int DIM, int PREC, class TS, int MINB>
+template <int DIM, int PREC, class TS, int MINB, int GMAX>
 __global__ void __launch_bounds__(TS::NTH, MINB)
     k_transport_batch(const TransportArgs* __restrict__ boxes, const int2* __restrict__ items, int nitems,
                       const BatchCtl ctl)
@@ -694,7 +713,7 @@ __global__ void __launch_bounds__(TS::NTH, MINB)
             cur = rec;
             __syncthreads();
         }
-        transport_tile_update<DIM, PREC, TS, group_fit<DIM, PREC, TS, MINB>()>(sA, w.y, smem_raw);
+        transport_tile_update<DIM, PREC, TS, group_fit<DIM, PREC, TS, MINB, GMAX>()>(sA, w.y, smem_raw);
         __syncthreads();  // the next item's staging (or record) must not overwrite a slow thread's reads
     }
 }
