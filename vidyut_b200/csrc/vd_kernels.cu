@@ -597,6 +597,10 @@ void finish_species_lists(TransportArgs& a, const VdMechDev& m)
         a.fl_cls[a.nfl] = a.tr_cls[it];
         a.fl_slot[a.nfl] = (int8_t)slot;
         a.fl_K[a.nfl] = K;
+        a.fl_Kf[a.nfl] = (float)K;
+        int zm = 0;
+        for (int d = 0; d < 3; d++) zm |= (a.zlo[a.tr_cls[it]][d] ? 1 : 0) << d | (a.zhi[a.tr_cls[it]][d] ? 1 : 0) << (3 + d);
+        a.fl_zm[a.nfl] = (int8_t)zm;
         a.nfl++;
     }
 }

@@ -41,6 +41,10 @@ struct TransportArgs {
     int8_t nf_sp[VD_MAX_SPECIES + 1];
     int8_t bkind[4];
     double fl_K[VD_MAX_SPECIES + 1];
+    float fl_Kf[VD_MAX_SPECIES + 1];  // fl_K rounded to FP32 (the mixed path's constant)
+    // zero-flux faces of a fluxed species: bit d set when its class has IHNEUBC at
+    // the low domain face of direction d (zlo), bit 3 + d at the high one (zhi)
+    int8_t fl_zm[VD_MAX_SPECIES + 1];
 };
 
 // The mixed path evaluates the Joule faces inside the transport tile when the tile

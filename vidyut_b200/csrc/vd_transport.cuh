@@ -118,15 +118,16 @@ struct JStage {
 __host__ __device__ constexpr size_t smem_align(size_t x) { return (x + 15) & ~(size_t)15; }
 
 // Dynamic shared memory of one tile with nb velocity bases and species groups of
-// GRP, in this order: the Joule term of every face (FP64, mixed path); the group's
-// face fluxes; the bases; the group's staged densities (or the staged Joule
-// inputs).  Fluxes, bases and densities are FP32 in the mixed path: a mixed flux
+// GRP, in this order: the Joule term of every face (FP64, mixed path); the face
+// info words (face_info); the group's face fluxes; the bases; the group's staged
+// densities (or the staged Joule inputs).  Fluxes, bases and densities are FP32 in the mixed path: a mixed flux
 // is an FP32 value times a power of two, so it is stored exactly.
 template <int DIM, int PREC, class TS>
 struct TileSmem {
     using G = TileGeom<DIM, TS>;
     using VT = typename VelT<PREC>::T;
     static constexpr size_t joule() { return PREC == PREC_MIXED ? smem_align((size_t)G::FTOT * sizeof(double)) : 0; }
+    static constexpr size_t finfo() { return smem_align((size_t)G::FTOT * sizeof(int)); }
     static constexpr size_t flux(int grp) { return smem_align((size_t)grp * G::FTOT * sizeof(VT)); }
     static constexpr size_t basis(int nb) { return smem_align((size_t)nb * G::STOT * sizeof(VT)); }
     static constexpr size_t dens(int grp)
@@ -141,7 +142,7 @@ template <int DIM, int PREC, class TS, int GRP>
 __host__ __device__ constexpr size_t transport_smem(int nb)
 {
     using S = TileSmem<DIM, PREC, TS>;
-    return S::joule() + S::flux(GRP) + S::basis(nb) + S::dens(GRP);
+    return S::joule() + S::finfo() + S::flux(GRP) + S::basis(nb) + S::dens(GRP);
 }
 
 // Species per group for a kernel that must keep MINB CTAs resident per SM: the
@@ -398,17 +399,18 @@ __device__ __forceinline__ void face_local(int ff, int* l)
     l[2] = ff / (F0 * F1);
 }
 
-// flux of face f of the tile (the faces of all directions in one index range) of
-// one species: sU / sB are the species' staged densities and its velocity basis
-// over all line sets (sB null: the user velocity of the face's direction).  One
-// copy of the flux arithmetic serves every direction.
-template <int DIM, int PREC, class TS>
-__device__ __forceinline__ double face_any(const TransportArgs& a, int f, int cls, const int* org,
-                                           const typename VelT<PREC>::T* sU, const typename VelT<PREC>::T* sB,
-                                           double K)
+// Face info word of face f of the tile (the faces of all directions in one index
+// range), built once per tile: bits 0-15 the staged index of the face's first
+// stencil cell in its direction's line set (staged index of rel cell f_d - 3 + q
+// is f_d + q along d), bits 16-17 the direction, then whether the face is one the
+// box updates and whether it is the low or high domain face of its direction.
+// face_tab reads it for every species.
+constexpr int kFaceOk = 1 << 18, kFaceDomLo = 1 << 19, kFaceDomHi = 1 << 20;
+template <int DIM, class TS>
+__device__ __forceinline__ int face_info(const TransportArgs& a, int f, const int* org)
 {
     using G = TileGeom<DIM, TS>;
-    using VT = typename VelT<PREC>::T;
+    static_assert(G::STOT < (1 << 16), "staged index fits 16 bits");
     int D = 0, l[3];
     if (DIM > 2 && f >= G::FOFF2) {
         D = 2;
@@ -420,17 +422,32 @@ __device__ __forceinline__ double face_any(const TransportArgs& a, int f, int cl
         face_local<DIM, 0, TS>(f, l);
     }
     const int S0 = G::T[0] + (D == 0 ? 6 : 0), S1 = G::T[1] + (D == 1 ? 6 : 0);
-    const int STR = D == 0 ? 1 : (D == 1 ? S0 : S0 * S1);
     const int soff = D == 0 ? 0 : (D == 1 ? G::SOFF1 : G::SOFF2);
     const int g[3] = {org[0] + l[0], org[1] + l[1], org[2] + l[2]};
     bool ok = g[D] <= a.hi[D] + 1;
 #pragma unroll
     for (int e = 0; e < DIM; e++)
         if (e != D) ok = ok && (g[e] <= a.hi[e]);
-    if (!ok) return 0.0;
-    // staged index of rel cell (f_d - 3 + q) is f_d + q along d
-    const int base = soff + l[0] + S0 * (l[1] + S1 * l[2]);
-    const VT k = (VT)(sB ? K : a.uvel[D]);
+    return (soff + l[0] + S0 * (l[1] + S1 * l[2])) | (D << 16) | (ok ? kFaceOk : 0) |
+           (g[D] == a.domlo[D] ? kFaceDomLo : 0) | (g[D] == a.domhi[D] + 1 ? kFaceDomHi : 0);
+}
+
+// Flux of one species through the tile face with info word `info`: sU / sB the
+// species' staged densities and velocity basis over all line sets (sB null: the
+// user velocity of the face's direction), k its velocity constant, zm its
+// zero-flux mask (TransportArgs::fl_zm).  One copy of the flux arithmetic serves
+// every direction.
+template <int DIM, int PREC, class TS>
+__device__ __forceinline__ double face_tab(const TransportArgs& a, int info, int zm,
+                                           const typename VelT<PREC>::T* sU, const typename VelT<PREC>::T* sB,
+                                           typename VelT<PREC>::T k)
+{
+    using VT = typename VelT<PREC>::T;
+    if (!(info & kFaceOk)) return 0.0;
+    const int D = (info >> 16) & 3, base = info & 0xffff;
+    constexpr int T0 = TS::X, T01 = TS::X * TS::Y;
+    const int STR = D == 0 ? 1 : (D == 1 ? T0 : T01);
+    if (!sB) k = (VT)a.uvel[D];
     VT u[6];
     VT v[6];
 #pragma unroll
@@ -441,8 +458,7 @@ __device__ __forceinline__ double face_any(const TransportArgs& a, int f, int cl
     double F;
     if constexpr (PREC == PREC_FP64) F = face_flux_fp64(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
     else F = face_flux_mixed32(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
-    if (g[D] == a.domlo[D] && a.zlo[cls][D]) F = 0.0;
-    if (g[D] == a.domhi[D] + 1 && a.zhi[cls][D]) F = 0.0;
+    if (((info & kFaceDomLo) && ((zm >> D) & 1)) || ((info & kFaceDomHi) && ((zm >> (3 + D)) & 1))) F = 0.0;
     return F;
 }
 
@@ -465,9 +481,10 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     const int org[3] = {a.lo[0] + tix * G::T[0], a.lo[1] + tiy * G::T[1], a.lo[2] + tiz * G::T[2]};
     using SM = TileSmem<DIM, PREC, TS>;
     double* sJ = reinterpret_cast<double*>(smem);  // mixed path only
-    VT* sF = reinterpret_cast<VT*>(smem + SM::joule());
-    VT* sB = reinterpret_cast<VT*>(smem + SM::joule() + SM::flux(GRP));
-    unsigned char* const dens = smem + SM::joule() + SM::flux(GRP) + SM::basis(a.nb);
+    int* sFI = reinterpret_cast<int*>(smem + SM::joule());
+    VT* sF = reinterpret_cast<VT*>(smem + SM::joule() + SM::finfo());
+    VT* sB = reinterpret_cast<VT*>(smem + SM::joule() + SM::finfo() + SM::flux(GRP));
+    unsigned char* const dens = smem + SM::joule() + SM::finfo() + SM::flux(GRP) + SM::basis(a.nb);
     VT* sU = reinterpret_cast<VT*>(dens);
     // the staged Joule inputs share the densities' space: read in phase (0'),
     // before a barrier that precedes the first group's staging
@@ -481,6 +498,12 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     const int ns = a.ns;
     const int64_t cs = a.sb.ns;
     const int64_t own_o = own ? a.sb.off(gi, gj, gk) : 0;
+    // The own cell's state and reaction source are read-only in this kernel (the
+    // update goes to a.pn): read through the non-coherent path, so that these
+    // loads may be issued ahead of the cell's stores.
+    const int64_t own_r = own ? a.rxn.off(gi, gj, gk) : 0;
+    auto state = [&](int s) -> double { return __ldg(a.sb.p + own_o + s * cs); };
+    auto rate = [&](int s) -> double { return __ldg(a.rxn.p + own_r + s * a.rxn.ns); };
     double ne_new = 0.0, een_new = 0.0;
     const int nfl = a.nfl;
     // the mixed path's Joule faces, evaluated here (a barrier follows them)
@@ -522,9 +545,9 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
                 // the Joule term the joule_tile pass left in EJH
                 acc += a.pn(gi, gj, gk, VD_EJH(ns));
             }
-            if (a.write_diag) a.pn(gi, gj, gk, VD_EIH(ns)) = a.rxn(gi, gj, gk, ns);
+            if (a.write_diag) a.pn(gi, gj, gk, VD_EIH(ns)) = rate(ns);
         }
-        double nn = a.sb.p[own_o + s * cs] + a.dt * acc;
+        double nn = state(s) + a.dt * acc;
         if (a.bound_specden && s != ns) {
             // solution clipping of the species solve (Source/ScalarSolve.cpp:597-622)
             const double lo = (s == a.e_id) ? a.min_elec : a.min_spec;
@@ -537,7 +560,8 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     };
 
     if (nfl > 0) {
-        // (0) velocity bases of every staged position
+        // (0) face info words and the velocity bases of every staged position
+        for (int f = tid; f < G::FTOT; f += NTH) sFI[f] = face_info<DIM, TS>(a, f, org);
         for (int c = tid; c < G::STOT; c += NTH) {
             if (c < G::SOFF1) {
                 stage_basis<DIM, PREC, 0, TS>(a, c, org, sB, js, jin);
@@ -617,8 +641,11 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
         for (int q = tid; q < gn * G::FTOT; q += NTH) {
             const int j = q / G::FTOT, f = q - j * G::FTOT;
             const int sl = a.fl_slot[g0 + j];
-            sF[q] = (VT)face_any<DIM, PREC, TS>(a, f, a.fl_cls[g0 + j], org, sU + j * G::STOT,
-                                                sl >= 0 ? sB + sl * G::STOT : nullptr, a.fl_K[g0 + j]);
+            VT k;
+            if constexpr (PREC == PREC_FP64) k = a.fl_K[g0 + j];
+            else k = a.fl_Kf[g0 + j];
+            sF[q] = (VT)face_tab<DIM, PREC, TS>(a, sFI[f], a.fl_zm[g0 + j], sU + j * G::STOT,
+                                                sl >= 0 ? sB + sl * G::STOT : nullptr, k);
         }
         __syncthreads();
         // (3) divergence + sources of the own cell: dsdt = (Fx_lo - Fx_hi)/dx + rxn,
@@ -631,7 +658,7 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
                 {
                     constexpr int F0 = G::template FE<0>(0), F1 = G::template FE<0>(1);
                     const int lo_f = cx + F0 * (cy + F1 * cz);
-                    acc = ((double)Fj[lo_f] - (double)Fj[lo_f + 1]) * a.idx[0] + a.rxn(gi, gj, gk, a.fl_sp[g0 + j]);
+                    acc = ((double)Fj[lo_f] - (double)Fj[lo_f + 1]) * a.idx[0] + rate(a.fl_sp[g0 + j]);
                 }
                 if constexpr (DIM > 1) {
                     constexpr int F0 = G::template FE<1>(0), F1 = G::template FE<1>(1);
@@ -653,12 +680,12 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     if (own) {
         for (int j = 0; j < a.nnf; j++) {
             const int s = a.nf_sp[j];
-            finish(s, a.rxn(gi, gj, gk, s));
+            finish(s, rate(s));
         }
         for (int ib = 0; ib < a.nbg; ib++) {
             const int s = a.bg_sp[ib];
-            double v = a.sb.p[own_o + s * cs];
-            double r = a.rxn(gi, gj, gk, s);
+            double v = state(s);
+            double r = rate(s);
             if (a.do_bg) {
                 v += r * a.dt;
                 if (v < a.min_spec && a.bound_specden) v = a.min_spec;
@@ -668,7 +695,7 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
         }
         if (a.update_te && a.elecenergy) {
             // Source/ScalarSolve.cpp:659-666
-            double te = (2.0 / 3.0) / K_B * een_new / a.sb.p[own_o + a.e_id * cs];
+            double te = (2.0 / 3.0) / K_B * een_new / state(a.e_id);
             if (te < a.min_te) {
                 te = a.min_te;
                 a.pn(gi, gj, gk, VD_EEN(ns)) = 1.5 * K_B * ne_new * te;
