@@ -119,8 +119,9 @@ __host__ __device__ constexpr size_t smem_align(size_t x) { return (x + 15) & ~(
 
 // Dynamic shared memory of one tile with nb velocity bases and species groups of
 // GRP, in this order: the Joule term of every face (FP64, mixed path); the face
-// info words (face_info); the group's face fluxes; the bases; the group's staged
-// densities (or the staged Joule inputs).  Fluxes, bases and densities are FP32 in the mixed path: a mixed flux
+// info words (face_info); the state offsets of the staged positions; the group's
+// face fluxes; the bases; the group's staged densities (or the staged Joule
+// inputs).  Fluxes, bases and densities are FP32 in the mixed path: a mixed flux
 // is an FP32 value times a power of two, so it is stored exactly.
 template <int DIM, int PREC, class TS>
 struct TileSmem {
@@ -128,6 +129,7 @@ struct TileSmem {
     using VT = typename VelT<PREC>::T;
     static constexpr size_t joule() { return PREC == PREC_MIXED ? smem_align((size_t)G::FTOT * sizeof(double)) : 0; }
     static constexpr size_t finfo() { return smem_align((size_t)G::FTOT * sizeof(int)); }
+    static constexpr size_t soffs() { return smem_align((size_t)G::STOT * sizeof(int)); }
     static constexpr size_t flux(int grp) { return smem_align((size_t)grp * G::FTOT * sizeof(VT)); }
     static constexpr size_t basis(int nb) { return smem_align((size_t)nb * G::STOT * sizeof(VT)); }
     static constexpr size_t dens(int grp)
@@ -142,7 +144,7 @@ template <int DIM, int PREC, class TS, int GRP>
 __host__ __device__ constexpr size_t transport_smem(int nb)
 {
     using S = TileSmem<DIM, PREC, TS>;
-    return S::joule() + S::finfo() + S::flux(GRP) + S::basis(nb) + S::dens(GRP);
+    return S::joule() + S::finfo() + S::soffs() + S::flux(GRP) + S::basis(nb) + S::dens(GRP);
 }
 
 // Species per group for a kernel that must keep MINB CTAs resident per SM: the
@@ -336,10 +338,12 @@ __device__ __forceinline__ bool staged_cell(const TransportArgs& a, int cc, cons
     return ok;
 }
 
-// velocity bases of staged position cc of direction D: sB[k*STOT + cc] for slot k
+// velocity bases of staged position cc of direction D: sB[k*STOT + cc] for slot k;
+// so[cc]: the position's cell offset in the state (-1: stages as zero), read by
+// every species group's staging
 template <int DIM, int PREC, int D, class TS>
 __device__ __forceinline__ void stage_basis(const TransportArgs& a, int cc, const int* org,
-                                            typename VelT<PREC>::T* sB, JStage js, bool jst)
+                                            typename VelT<PREC>::T* sB, JStage js, bool jst, int* so)
 {
     using G = TileGeom<DIM, TS>;
     using VT = typename VelT<PREC>::T;
@@ -347,6 +351,7 @@ __device__ __forceinline__ void stage_basis(const TransportArgs& a, int cc, cons
     const bool ok = staged_cell<DIM, D, TS>(a, cc, org, g);
     VT b[3] = {VT(0), VT(0), VT(0)};
     double ne = 0.0, Te = 0.0, N = 0.0;
+    so[cc] = ok ? (int)a.sb.off(g[0], g[1], g[2]) : -1;
     if (ok) {
         const int ns = a.ns;
         const int64_t cs = a.sb.ns;
@@ -482,9 +487,13 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     using SM = TileSmem<DIM, PREC, TS>;
     double* sJ = reinterpret_cast<double*>(smem);  // mixed path only
     int* sFI = reinterpret_cast<int*>(smem + SM::joule());
-    VT* sF = reinterpret_cast<VT*>(smem + SM::joule() + SM::finfo());
-    VT* sB = reinterpret_cast<VT*>(smem + SM::joule() + SM::finfo() + SM::flux(GRP));
-    unsigned char* const dens = smem + SM::joule() + SM::finfo() + SM::flux(GRP) + SM::basis(a.nb);
+    int* sSO = reinterpret_cast<int*>(smem + SM::joule() + SM::finfo());
+    const size_t o_f = SM::joule() + SM::finfo() + SM::soffs();
+    VT* sF = reinterpret_cast<VT*>(smem + o_f);
+    VT* sB = reinterpret_cast<VT*>(smem + o_f + SM::flux(GRP));
+    unsigned char* const dens = smem + o_f + SM::flux(GRP) + SM::basis(a.nb);
+    // staged positions by table when every cell offset of the state fits 32 bits
+    const bool stab = a.sb.ns <= 0x7fffffffLL;
     VT* sU = reinterpret_cast<VT*>(dens);
     // the staged Joule inputs share the densities' space: read in phase (0'),
     // before a barrier that precedes the first group's staging
@@ -564,22 +573,25 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
         for (int f = tid; f < G::FTOT; f += NTH) sFI[f] = face_info<DIM, TS>(a, f, org);
         for (int c = tid; c < G::STOT; c += NTH) {
             if (c < G::SOFF1) {
-                stage_basis<DIM, PREC, 0, TS>(a, c, org, sB, js, jin);
+                stage_basis<DIM, PREC, 0, TS>(a, c, org, sB, js, jin, sSO);
             } else if (DIM > 1 && c < G::SOFF2) {
                 const JStage j1{js.ne + G::SOFF1, js.te + G::SOFF1, js.nd + G::SOFF1};
-                stage_basis<DIM, PREC, (DIM > 1 ? 1 : 0), TS>(a, c - G::SOFF1, org, sB + G::SOFF1, j1, jin);
+                stage_basis<DIM, PREC, (DIM > 1 ? 1 : 0), TS>(a, c - G::SOFF1, org, sB + G::SOFF1, j1, jin,
+                                                              sSO + G::SOFF1);
             } else if (DIM > 2) {
                 const JStage j2{js.ne + G::SOFF2, js.te + G::SOFF2, js.nd + G::SOFF2};
-                stage_basis<DIM, PREC, (DIM > 2 ? 2 : 0), TS>(a, c - G::SOFF2, org, sB + G::SOFF2, j2, jin);
+                stage_basis<DIM, PREC, (DIM > 2 ? 2 : 0), TS>(a, c - G::SOFF2, org, sB + G::SOFF2, j2, jin,
+                                                              sSO + G::SOFF2);
             }
         }
+        // the offset table and the staged Joule inputs are read by other threads
+        if (stab || (joule_staged<DIM, PREC>() && jin)) __syncthreads();
     }
     if constexpr (PREC == PREC_MIXED) {
         if (jin) {
             // (0') the Joule term of every face of the tile, once (from the staged
-            // inputs of the face's two cells when they are staged; the basis loop
-            // above wrote them, so a barrier comes first)
-            if constexpr (joule_staged<DIM, PREC>()) __syncthreads();
+            // inputs of the face's two cells when they are staged, which the basis
+            // loop above wrote before its barrier)
             for (int f = tid; f < G::FTOT; f += NTH) {
                 int d = 0, ff = f;
                 if (DIM > 1 && f >= G::FOFF1) {
@@ -631,9 +643,16 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
             const int j = q / G::STOT, c = q - j * G::STOT;
             const int s = a.fl_sp[g0 + j];
             VT u;
-            if (c < G::SOFF1) u = stage_density<DIM, PREC, 0, TS>(a, c, s, org);
-            else if (DIM > 1 && c < G::SOFF2) u = stage_density<DIM, PREC, (DIM > 1 ? 1 : 0), TS>(a, c - G::SOFF1, s, org);
-            else u = stage_density<DIM, PREC, (DIM > 2 ? 2 : 0), TS>(a, c - G::SOFF2, s, org);
+            if (stab) {
+                const int o = sSO[c];
+                u = o >= 0 ? (VT)__ldg(a.sb.p + o + (int64_t)s * cs) : VT(0);
+            } else if (c < G::SOFF1) {
+                u = stage_density<DIM, PREC, 0, TS>(a, c, s, org);
+            } else if (DIM > 1 && c < G::SOFF2) {
+                u = stage_density<DIM, PREC, (DIM > 1 ? 1 : 0), TS>(a, c - G::SOFF1, s, org);
+            } else {
+                u = stage_density<DIM, PREC, (DIM > 2 ? 2 : 0), TS>(a, c - G::SOFF2, s, org);
+            }
             sU[q] = u;
         }
         __syncthreads();
