@@ -132,19 +132,23 @@ __device__ __forceinline__ double weno_fp64(double a, double b, double c, double
 //   WENO-Z   alpha_k ~ gamma_k (1 + (tau/q_k)^2)              if tau <= m
 //            alpha_k ~ gamma_k ((m/tau)^2 + (m/q_k)^2)        otherwise
 // (each a positive multiple of the reference's alpha_k); WENO-M keeps its map.
+// The smoothness indicators are kept as 4 beta_k (13/3 and 1 for the reference's
+// 13/12 and 1/4) and eps4 is 4 eps: every weight is a ratio of these, and scaling
+// by a power of two changes no rounding, so the result is the same and each
+// indicator costs one multiply less.
 __device__ __forceinline__ float weno_f32(float a, float b, float c, float d, float e, int scheme,
-                                          float eps)
+                                          float eps4)
 {
     float p1 = fmaf(1.0f / 3.0f, a, fmaf(-7.0f / 6.0f, b, (11.0f / 6.0f) * c));
     float p2 = fmaf(-1.0f / 6.0f, b, fmaf(5.0f / 6.0f, c, (1.0f / 3.0f) * d));
     float p3 = fmaf(1.0f / 3.0f, c, fmaf(5.0f / 6.0f, d, (-1.0f / 6.0f) * e));
     float t1 = fmaf(-2.0f, b, a) + c, t2 = fmaf(-4.0f, b, a) + 3.0f * c;
-    float b1 = fmaf(13.0f / 12.0f, t1 * t1, 0.25f * (t2 * t2));
+    float b1 = fmaf(13.0f / 3.0f, t1 * t1, t2 * t2);
     float t3 = fmaf(-2.0f, c, b) + d, t4 = b - d;
-    float b2 = fmaf(13.0f / 12.0f, t3 * t3, 0.25f * (t4 * t4));
+    float b2 = fmaf(13.0f / 3.0f, t3 * t3, t4 * t4);
     float t5 = fmaf(-2.0f, d, c) + e, t6 = fmaf(3.0f, c, fmaf(-4.0f, d, e));
-    float b3 = fmaf(13.0f / 12.0f, t5 * t5, 0.25f * (t6 * t6));
-    const float q1 = b1 + eps, q2 = b2 + eps, q3 = b3 + eps;
+    float b3 = fmaf(13.0f / 3.0f, t5 * t5, t6 * t6);
+    const float q1 = b1 + eps4, q2 = b2 + eps4, q3 = b3 + eps4;
     const float m = fminf(q1, fminf(q2, q3));
     const float r1 = rcp_approx(q1), r2 = rcp_approx(q2), r3 = rcp_approx(q3);
     float a1, a2, a3;
@@ -236,7 +240,7 @@ __device__ __forceinline__ double face_flux_mixed(const double* u, const float* 
     }
     // eps = 1e-20 in the unscaled units of u (and of f for |v| ~ 1)
     float s2 = (float)(s * s);
-    float eps = fmaxf(1e-20f * s2, 1e-30f);
+    float eps = 4.0f * fmaxf(1e-20f * s2, 1e-30f);  // weno_f32 takes 4 eps
     float lam = fabsf(0.5f * (v[2] + v[3]));
     float fp = weno_f32(fs[0], fs[1], fs[2], fs[3], fs[4], scheme, eps);
     float fm = weno_f32(fs[5], fs[4], fs[3], fs[2], fs[1], scheme, eps);
@@ -275,7 +279,7 @@ __device__ __forceinline__ double face_flux_mixed32(const float* u, const float*
     int b2 = 127 - 2 * e;
     b2 = b2 < 0 ? 0 : (b2 > 255 ? 255 : b2);
     const float s2 = __int_as_float(b2 << 23);        // 2^-2e, 0 or inf at the ends
-    const float eps = fminf(fmaxf(1e-20f * s2, 1e-30f), 1e30f);
+    const float eps = 4.0f * fminf(fmaxf(1e-20f * s2, 1e-30f), 1e30f);  // weno_f32 takes 4 eps
     float us[6], fs[6];
 #pragma unroll
     for (int q = 0; q < 6; q++) {
