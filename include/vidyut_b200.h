@@ -22,7 +22,8 @@
  *   vd_explicit_update_all     one explicit step of the whole path: rxnsrc, every transported
  *                              species' flux + dsdt (Source/ScalarSolve.cpp:57-111), the Joule
  *                              term, the background-species update (Source/Evolve.cpp:267-287)
- *                              and the accumulation n += dt*dsdt, fused into two launches.
+ *                              and the accumulation n += dt*dsdt, fused into two launches
+ *                              (three in FP64, where the Joule term has a pass of its own).
  *   vd_batch_*                 no single reference counterpart: the per-box MFIter loops of the
  *                              functions above run over many independent boxes in one
  *                              persistent launch (the reference iterates boxes with MFIter).
