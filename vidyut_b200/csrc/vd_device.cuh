@@ -255,9 +255,11 @@ __device__ __forceinline__ double face_flux_mixed(const double* u, const float* 
 // exponent bits of max|u| (so max|u*s| is in [1/2, 1)); eps = 1e-20 is carried
 // into the scaled units as 1e-20 s^2, clamped to [1e-30, 1e30] (for tiny fields
 // eps dominates the smoothness indicators and the weights become the ideal ones,
-// as in FP64).  The flux is unscaled exactly in FP64.
-__device__ __forceinline__ double face_flux_mixed32(const float* u, const float* v, int hyp_order, int scheme,
-                                                    double dxmin, double dt)
+// as in FP64).  The flux is unscaled by the exact power of two; the result is
+// returned in FP32, which holds it exactly while it is a normal FP32 value (the
+// FP64 route serves the one scale, 2^-127, that FP32 cannot hold).
+__device__ __forceinline__ float face_flux_mixed32(const float* u, const float* v, int hyp_order, int scheme,
+                                                   double dxmin, double dt)
 {
     if (hyp_order != 5) {
         double ud[6], vd[6];
@@ -266,7 +268,7 @@ __device__ __forceinline__ double face_flux_mixed32(const float* u, const float*
             ud[q] = (double)u[q];
             vd[q] = (double)v[q];
         }
-        return face_flux_fp64(ud, vd, hyp_order, scheme, dxmin, dt);
+        return (float)face_flux_fp64(ud, vd, hyp_order, scheme, dxmin, dt);
     }
     const float m = fmaxf(fmaxf(fmaxf(fabsf(u[0]), fabsf(u[1])), fmaxf(fabsf(u[2]), fabsf(u[3]))),
                           fmaxf(fabsf(u[4]), fabsf(u[5])));
@@ -292,8 +294,8 @@ __device__ __forceinline__ double face_flux_mixed32(const float* u, const float*
     const float up = weno_f32(us[0], us[1], us[2], us[3], us[4], scheme, eps);
     const float um = weno_f32(us[5], us[4], us[3], us[2], us[1], scheme, eps);
     const float F = 0.5f * (fmaf(lam, up, fp) + fmaf(-lam, um, fm));
-    const double inv_s = __longlong_as_double((long long)(1150 - bs) << 52);  // 2^(127-bs): exact
-    return (double)F * inv_s;
+    if (bs < 254) return F * __int_as_float((254 - bs) << 23);  // 2^(127-bs)
+    return (float)((double)F * __longlong_as_double((long long)(1150 - bs) << 52));
 }
 
 // 2^x for an FP64 exponent x as an FP32 value: x = i + f with i = rint(x) (exact in

@@ -443,12 +443,12 @@ __device__ __forceinline__ int face_info(const TransportArgs& a, int f, const in
 // zero-flux mask (TransportArgs::fl_zm).  One copy of the flux arithmetic serves
 // every direction.
 template <int DIM, int PREC, class TS>
-__device__ __forceinline__ double face_tab(const TransportArgs& a, int info, int zm,
+__device__ __forceinline__ typename VelT<PREC>::T face_tab(const TransportArgs& a, int info, int zm,
                                            const typename VelT<PREC>::T* sU, const typename VelT<PREC>::T* sB,
                                            typename VelT<PREC>::T k)
 {
     using VT = typename VelT<PREC>::T;
-    if (!(info & kFaceOk)) return 0.0;
+    if (!(info & kFaceOk)) return VT(0);
     const int D = (info >> 16) & 3, base = info & 0xffff;
     constexpr int T0 = TS::X, T01 = TS::X * TS::Y;
     const int STR = D == 0 ? 1 : (D == 1 ? T0 : T01);
@@ -460,10 +460,10 @@ __device__ __forceinline__ double face_tab(const TransportArgs& a, int info, int
         u[q] = sU[base + q * STR];
         v[q] = sB ? k * sB[base + q * STR] : k;
     }
-    double F;
+    VT F;
     if constexpr (PREC == PREC_FP64) F = face_flux_fp64(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
     else F = face_flux_mixed32(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
-    if (((info & kFaceDomLo) && ((zm >> D) & 1)) || ((info & kFaceDomHi) && ((zm >> (3 + D)) & 1))) F = 0.0;
+    if (((info & kFaceDomLo) && ((zm >> D) & 1)) || ((info & kFaceDomHi) && ((zm >> (3 + D)) & 1))) F = VT(0);
     return F;
 }
 
@@ -663,8 +663,8 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
             VT k;
             if constexpr (PREC == PREC_FP64) k = a.fl_K[g0 + j];
             else k = a.fl_Kf[g0 + j];
-            sF[q] = (VT)face_tab<DIM, PREC, TS>(a, sFI[f], a.fl_zm[g0 + j], sU + j * G::STOT,
-                                                sl >= 0 ? sB + sl * G::STOT : nullptr, k);
+            sF[q] = face_tab<DIM, PREC, TS>(a, sFI[f], a.fl_zm[g0 + j], sU + j * G::STOT,
+                                            sl >= 0 ? sB + sl * G::STOT : nullptr, k);
         }
         __syncthreads();
         // (3) divergence + sources of the own cell: dsdt = (Fx_lo - Fx_hi)/dx + rxn,
@@ -735,32 +735,65 @@ __global__ void __launch_bounds__(default_nth<DIM>(), MINB) k_transport(const __
 
 // batched persistent kernel: each CTA walks the work list of (box, tile) items
 // with a grid stride.  Boxes are described by TransportArgs records in global
-// memory; the item's record is first copied to shared memory, so that the tile
-// body's many reads of it are shared-memory loads rather than global ones.
+// memory; an item's record is copied to shared memory, so that the tile body's
+// many reads of it are shared-memory loads rather than global ones.  Two record
+// buffers: while a tile is updated, the next item's record (when it is another
+// box's) is fetched into the other buffer with asynchronous copies.
 template <int DIM, int PREC, class TS, int MINB, int GMAX>
 __global__ void __launch_bounds__(TS::NTH, MINB)
     k_transport_batch(const TransportArgs* __restrict__ boxes, const int2* __restrict__ items, int nitems,
                       const BatchCtl ctl)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ long long sA_raw[sizeof(TransportArgs) / 8];
+    constexpr int NW = (int)(sizeof(TransportArgs) / 8);
     static_assert(sizeof(TransportArgs) % 8 == 0, "record copied in 8-byte words");
-    const TransportArgs& sA = *reinterpret_cast<const TransportArgs*>(sA_raw);
-    int cur = -1;  // record held in sA
-    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-        const int2 w = items[it];
+    __shared__ __align__(16) long long sA_raw[2][NW];
+    // record index of item it, or -1 when its box takes no step now (the same for
+    // every thread of the CTA)
+    auto record_of = [&](int it, int2& w) -> int {
+        w = items[it];
         const int2 cc = ctl.ctrl[w.x];
-        if (ctl.t >= cc.x) continue;  // uniform over the CTA
-        const int rec = ((ctl.t + cc.y) & 1) * ctl.nbox + w.x;
-        if (rec != cur) {
-            const long long* src = reinterpret_cast<const long long*>(boxes + rec);
-            long long* dst = sA_raw;
-            for (int q = threadIdx.x; q < (int)(sizeof(TransportArgs) / 8); q += TS::NTH) dst[q] = src[q];
-            cur = rec;
-            __syncthreads();
+        return ctl.t >= cc.x ? -1 : ((ctl.t + cc.y) & 1) * ctl.nbox + w.x;
+    };
+    auto fetch = [&](int buf, int rec) {
+        const long long* src = reinterpret_cast<const long long*>(boxes + rec);
+        for (int q = threadIdx.x; q < NW; q += TS::NTH) {
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(&sA_raw[buf][q]);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src + q) : "memory");
         }
-        transport_tile_update<DIM, PREC, TS, group_fit<DIM, PREC, TS, MINB, GMAX>()>(sA, w.y, smem_raw);
-        __syncthreads();  // the next item's staging (or record) must not overwrite a slow thread's reads
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    int2 w;
+    int it = blockIdx.x, rec = -1;
+    while (it < nitems && (rec = record_of(it, w)) < 0) it += gridDim.x;
+    if (it >= nitems) return;
+    int held0 = rec, held1 = -1, b = 0;  // record in each buffer; buffer of the current item
+    fetch(0, rec);
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();
+    for (;;) {
+        // the next item of this CTA; its record goes to the other buffer now (that
+        // buffer was last read by the previous tile, before its barrier)
+        int itn = it + gridDim.x;
+        {
+            int2 wn;
+            int recn = -1;
+            while (itn < nitems && (recn = record_of(itn, wn)) < 0) itn += gridDim.x;
+            const int hb = b ? held1 : held0, ho = b ? held0 : held1;
+            if (itn < nitems && recn != hb && recn != ho) {
+                fetch(b ^ 1, recn);
+                if (b) held0 = recn;
+                else held1 = recn;
+            }
+        }
+        transport_tile_update<DIM, PREC, TS, group_fit<DIM, PREC, TS, MINB, GMAX>()>(
+            *reinterpret_cast<const TransportArgs*>(sA_raw[b]), w.y, smem_raw);
+        if (itn >= nitems) break;
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        __syncthreads();  // the record is complete; the next staging may overwrite this tile's shared memory
+        it = itn;
+        rec = record_of(it, w);
+        if (rec != (b ? held1 : held0)) b ^= 1;
     }
 }
 
