@@ -336,6 +336,38 @@ int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_array4 efield_e
                      const vd_params* prm, const vd_poisson_params* pp,
                      int32_t* vcycles_done, double* rel_residual, void* stream);
 
+/* Implicit diffusion solve of one species on one box that is the whole domain
+ * (replaces Vidyut::implicit_solve_scalar, Source/ScalarSolve.cpp:289-680, whose
+ * MLABecLaplacian/MLMG solve is replaced by this library's multigrid on the same
+ * discrete problem): (1/dt) n - div(D grad n) = n_old/dt + dsdt for species
+ * dp->spec (NS: the electron energy).  D from specDiff of `state` (the current
+ * state, covering the box grown by one) at cells, harmonic means on faces.  Domain
+ * faces by prm->bc_lo/bc_hi of the species' class, valued by species_bc
+ * (Source/PlasmaChem.H:75-184): VD_BC_DIRC holds that value at the face,
+ * VD_BC_IHNEU takes it as the derivative along the direction, VD_BC_HNEU and
+ * VD_BC_ROBIN (species_bc's default robin coefficients) zero gradient; a periodic
+ * direction is refused (VD_ERR_ARG).  n_old from state_old, the explicit source
+ * from component dp->dsdt_comp of dsdt.  The initial guess is the current state;
+ * FP64 V(2,2) cycles until max|residual| <= tol_rel * max|rhs| (tol_rel > 0, one
+ * host synchronisation per cycle) or max_vcycles (tol_rel == 0: exactly that many,
+ * no synchronisation).  Writes component spec of phi_new on the valid cells,
+ * floored when prm->bound_specden (not the energy); for the electrons, when
+ * gradne_fc is not NULL, the face gradients dn/dx_d on the face boxes
+ * (getGradSolution); for the electron energy also ETEMP = (2/3) eps / (kB n_e)
+ * with n_e from `state`, floored at min_electron_temp (then EEN = 1.5 kB n_e Te
+ * with n_e from phi_new).  Scratch from the stream-ordered allocator. */
+typedef struct {
+    int32_t spec;          /* 0..NS-1 a species, NS the electron energy             */
+    int32_t dsdt_comp;     /* component of dsdt holding this species' explicit source */
+    int32_t max_vcycles;
+    int32_t pad0;
+    double  tol_rel;
+} vd_diffusion_params;
+int vd_implicit_species_solve(const vd_box* bx, vd_array4 state, vd_array4 state_old, vd_array4 dsdt,
+                              vd_array4 phi_new, const vd_array4 gradne_fc[3], const vd_params* prm,
+                              const vd_diffusion_params* dp, int32_t* vcycles_done, double* rel_residual,
+                              void* stream);
+
 /* ---- batched cases (no single reference counterpart: the reference loops over
  * boxes with MFIter and calls the per-box functions above for each) -----------
  * A batch owns a device arena of hbm_budget_bytes and keeps every resident case's

@@ -271,3 +271,14 @@ PROTOTYPES.update({
 PROTOTYPES.update({
     "vd_time_scales": (C.c_int, [BOXP, A4, PRMP, DP, C.c_void_p]),
 })
+
+
+class VdDiffusionParams(C.Structure):
+    _fields_ = [("spec", C.c_int32), ("dsdt_comp", C.c_int32), ("max_vcycles", C.c_int32), ("pad0", C.c_int32),
+                ("tol_rel", C.c_double)]
+
+
+PROTOTYPES.update({
+    "vd_implicit_species_solve": (C.c_int, [BOXP, A4, A4, A4, A4, A4P, PRMP, C.POINTER(VdDiffusionParams), I32P,
+                                            DP, C.c_void_p]),
+})

@@ -408,6 +408,32 @@ def poisson_solve(dc: DeviceCase, prm: abi.VdParams, pp: abi.VdPoissonParams, st
     return nv.value, rr.value
 
 
+def implicit_species_solve(dc: DeviceCase, spec: int, state_old: torch.Tensor, dsdt: torch.Tensor,
+                           phi_new: torch.Tensor, prm: abi.VdParams, *, dsdt_comp: int | None = None,
+                           gradne: list | None = None, tol_rel: float = 1e-12, max_vcycles: int = 50,
+                           stream=None):
+    """Implicit diffusion solve of species `spec` (NS: the electron energy) of dc
+    (Vidyut::implicit_solve_scalar): state_old laid out like dc.state, dsdt and
+    phi_new over the valid cells (phi_new with NVAR components).  gradne: three
+    face tensors that receive the electron face gradients.  Returns (V-cycles done,
+    relative residual or -1 when not checked)."""
+    dp = abi.VdDiffusionParams()
+    dp.spec = spec
+    dp.dsdt_comp = spec if dsdt_comp is None else dsdt_comp
+    dp.max_vcycles = max_vcycles
+    dp.tol_rel = tol_rel
+    nv = C.c_int32()
+    rr = C.c_double()
+    g = None
+    if gradne is not None:
+        g = (abi.VdArray4 * 3)(*[t_a4(gradne[d], (0, 0, 0)) for d in range(3)])
+    rc = abi.lib().vd_implicit_species_solve(C.byref(dc.box()), dc.sb(), t_a4(state_old, dc.case.state_begin()),
+                                             t_a4(dsdt, (0, 0, 0)), t_a4(phi_new, (0, 0, 0)), g, C.byref(prm),
+                                             C.byref(dp), C.byref(nv), C.byref(rr), _stream(stream))
+    abi.check(rc, "vd_implicit_species_solve")
+    return nv.value, rr.value
+
+
 def time_scales(dc: DeviceCase, prm: abi.VdParams, stream=None):
     """(dt_edrift, dt_ediff, dt_diel_relax) of the case's current state
     (Vidyut::find_time_scales)."""

@@ -985,6 +985,13 @@ int set_error(int code, const char* msg) { return fail(code, "%s", msg); }
 
 int ensure_mech(cudaStream_t st) { return ensure_mech_on_device(st); }
 
+double species_mw(int s)
+{
+    std::lock_guard<std::mutex> lk(g_mech_mu);
+    if (!g_mech || s < 0 || s >= g_mech->nspecies) return 0.0;
+    return g_mech->mw[s];
+}
+
 int mech_info(MechInfo* out)
 {
     std::lock_guard<std::mutex> lk(g_mech_mu);

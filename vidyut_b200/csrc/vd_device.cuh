@@ -19,7 +19,8 @@ namespace vd {
 // The loaded mechanism.  Every translation unit that includes this header has its
 // own copy (internal linkage; the library is compiled without relocatable device
 // code) and uploads it through its own upload function (upload_mech in
-// vd_kernels.cu, upload_mech_batch in vd_batch_kernels.cu).
+// vd_kernels.cu, which also calls upload_mech_batch in vd_batch_kernels.cu and
+// upload_mech_diffusion in vd_diffusion.cu).
 static __constant__ VdMechDev c_mech;
 
 // Approximate reciprocal on the special-function unit (rcp.approx.ftz.f32,

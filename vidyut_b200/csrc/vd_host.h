@@ -19,6 +19,8 @@ struct MechInfo {
     int charge[VD_MAX_SPECIES];
 };
 int mech_info(MechInfo* out);
+// Molecular weight [g/mol] of species s of the loaded mechanism (0 when none).
+double species_mw(int s);
 // Validation of a box + parameter block as vd_explicit_update_all does it.
 int check_update_params(const vd_box* bx, const vd_params* p, const MechInfo& m);
 // Fills the per-box transport record (everything but the array views and ntile).

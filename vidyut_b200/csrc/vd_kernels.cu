@@ -118,6 +118,8 @@ int upload_mech(const VdMechDev* h, cudaStream_t st)
     if (e != cudaSuccess) return (int)e;
     e = upload_mech_batch(h, st);  // the batched transport kernels' copy
     if (e != cudaSuccess) return (int)e;
+    e = upload_mech_diffusion(h, st);  // the implicit species solve's copy
+    if (e != cudaSuccess) return (int)e;
     e = cudaStreamSynchronize(st);
     return (int)e;
 }

@@ -83,7 +83,8 @@ struct GhostArgs {
 };
 
 int upload_mech(const VdMechDev* h, cudaStream_t st);
-cudaError_t upload_mech_batch(const VdMechDev* h, cudaStream_t st);  // vd_batch_kernels.cu
+cudaError_t upload_mech_batch(const VdMechDev* h, cudaStream_t st);      // vd_batch_kernels.cu
+cudaError_t upload_mech_diffusion(const VdMechDev* h, cudaStream_t st);  // vd_diffusion.cu
 
 // Step control of a batched launch.  ctrl[c] = {steps case c takes in this call,
 // index (0/1) of the buffer holding its current state}.  At step t a work item of
