@@ -24,6 +24,9 @@
  *                              term, the background-species update (Source/Evolve.cpp:267-287)
  *                              and the accumulation n += dt*dsdt, fused into two launches
  *                              (three in FP64, where the Joule term has a pass of its own).
+ *   vd_implicit_species_solve  Vidyut::implicit_solve_scalar (Source/ScalarSolve.cpp:289-680):
+ *                              the implicit diffusion solve of one species, on this library's
+ *                              multigrid in place of AMReX's MLMG.
  *   vd_batch_*                 no single reference counterpart: the per-box MFIter loops of the
  *                              functions above run over many independent boxes in one
  *                              persistent launch (the reference iterates boxes with MFIter).
