@@ -70,6 +70,13 @@ def test_calls_before_mech_init_fail_cleanly(lib):
     z = abi.null_array4()
     rc = lib.vd_reaction_source(C.byref(b), z, z, 300.0, 0.0, 0.0, None)
     assert rc in (abi.ERR_MECH, abi.ERR_CUDA, abi.ERR_ARG)
+    # the implicit species solve checks its argument blocks before anything else
+    prm = abi.VdParams()
+    rc = lib.vd_implicit_species_solve(C.byref(b), z, z, z, z, None, C.byref(prm), None, None, None, None)
+    assert rc == abi.ERR_ARG and b"null" in lib.vd_last_error()
+    dp = abi.VdDiffusionParams()
+    rc = lib.vd_implicit_species_solve(C.byref(b), z, z, z, z, None, C.byref(prm), C.byref(dp), None, None, None)
+    assert rc in (abi.ERR_MECH, abi.ERR_CUDA, abi.ERR_ARG, abi.ERR_DIM)
 
 
 @pytest.mark.parametrize("mech", [mm.argon(10, 20261204), mm.synthetic(8, 40, 20261224),
