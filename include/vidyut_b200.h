@@ -27,6 +27,8 @@
  *   vd_implicit_species_solve  Vidyut::implicit_solve_scalar (Source/ScalarSolve.cpp:289-680):
  *                              the implicit diffusion solve of one species, on this library's
  *                              multigrid in place of AMReX's MLMG.
+ *   vd_write_plotfile          Vidyut::WritePlotFile (Source/Plot.cpp:29-39): the plotfile layout
+ *                              that amrex::WriteMultiLevelPlotfile writes, for one level.
  *   vd_batch_*                 no single reference counterpart: the per-box MFIter loops of the
  *                              functions above run over many independent boxes in one
  *                              persistent launch (the reference iterates boxes with MFIter).
@@ -370,6 +372,19 @@ int vd_implicit_species_solve(const vd_box* bx, vd_array4 state, vd_array4 state
                               vd_array4 phi_new, const vd_array4 gradne_fc[3], const vd_params* prm,
                               const vd_diffusion_params* dp, int32_t* vcycles_done, double* rel_residual,
                               void* stream);
+
+/* Plotfile of one box that is the whole domain (replaces Vidyut::WritePlotFile,
+ * Source/Plot.cpp:29-39, which calls amrex::WriteMultiLevelPlotfile): writes the
+ * single-level plotfile layout -- dir/Header, dir/Level_0/Cell_H and
+ * dir/Level_0/Cell_D_00000 -- from HOST memory: data holds ncomp components of the
+ * box's cells, component slowest, x fastest; names the ncomp variable names (the
+ * reference uses the species names then Electron_energy, Electron_Temp, Potential,
+ * Efieldx..z, Electron_Jheat, Electron_inelasticHeat, Electron_elasticHeat,
+ * ReducedEF, Source/Vidyut.cpp:32-52); the domain starts at prob_lo with cells of
+ * dx.  Synchronous file output; creates dir and dir/Level_0 when missing.        */
+int vd_write_plotfile(const char* dir, const vd_box* bx, const double* data, int ncomp,
+                      const char* const* names, const double prob_lo[3], const double dx[3], double time,
+                      int step);
 
 /* ---- batched cases (no single reference counterpart: the reference loops over
  * boxes with MFIter and calls the per-box functions above for each) -----------

@@ -273,6 +273,12 @@ PROTOTYPES.update({
 })
 
 
+PROTOTYPES.update({
+    "vd_write_plotfile": (C.c_int, [C.c_char_p, BOXP, DP, C.c_int, C.POINTER(C.c_char_p), DP, DP, C.c_double,
+                                    C.c_int]),
+})
+
+
 class VdDiffusionParams(C.Structure):
     _fields_ = [("spec", C.c_int32), ("dsdt_comp", C.c_int32), ("max_vcycles", C.c_int32), ("pad0", C.c_int32),
                 ("tol_rel", C.c_double)]

@@ -434,6 +434,39 @@ def implicit_species_solve(dc: DeviceCase, spec: int, state_old: torch.Tensor, d
     return nv.value, rr.value
 
 
+# Source/Vidyut.cpp:32-42: the names of the state components after the species
+PLASMA_VAR_NAMES = ("Electron_energy", "Electron_Temp", "Potential", "Efieldx", "Efieldy", "Efieldz",
+                    "Electron_Jheat", "Electron_inelasticHeat", "Electron_elasticHeat", "ReducedEF")
+
+
+def plot_var_names(mech: Mechanism) -> list:
+    """The reference's plotfile variable names (allvarnames, Source/Vidyut.cpp:44-52)."""
+    return list(mech.species) + list(PLASMA_VAR_NAMES)
+
+
+def write_plotfile(path, case: BoxCase, valid_state, *, time: float = 0.0, step: int = 0,
+                   prob_lo=(0.0, 0.0, 0.0), names=None) -> None:
+    """Writes a plotfile of the case's valid cells: valid_state is a host (numpy) or
+    device (torch) array (NVAR, nz, ny, nx), e.g. the phi_new of an update."""
+    if isinstance(valid_state, torch.Tensor):
+        valid_state = valid_state.detach().cpu().numpy()
+    a = np.ascontiguousarray(valid_state, dtype=np.float64)
+    names = list(names) if names is not None else plot_var_names(case.mech)
+    if len(names) != a.shape[0]:
+        raise ValueError(f"{len(names)} names for {a.shape[0]} components")
+    cn = (C.c_char_p * len(names))(*[n.encode() for n in names])
+    lo = (C.c_double * 3)(*prob_lo)
+    dx = (C.c_double * 3)(*case.dx)
+    rc = abi.lib().vd_write_plotfile(str(path).encode(), C.byref(case_box(case)),
+                                     a.ctypes.data_as(C.POINTER(C.c_double)), a.shape[0], cn, lo, dx, float(time),
+                                     int(step))
+    abi.check(rc, "vd_write_plotfile")
+
+
+def case_box(case: BoxCase) -> abi.VdBox:
+    return abi.make_box(case.lo, case.hi, case.dim)
+
+
 def time_scales(dc: DeviceCase, prm: abi.VdParams, stream=None):
     """(dt_edrift, dt_ediff, dt_diel_relax) of the case's current state
     (Vidyut::find_time_scales)."""

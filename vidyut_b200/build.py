@@ -19,7 +19,7 @@ LIB = PKG / "libvidyut_b200.so"
 BUILD = PKG / "_build"
 
 SOURCES = ["vd_kernels.cu", "vd_batch_kernels.cu", "vd_abi.cu", "vd_spec.cpp", "vd_batch.cu", "vd_server.cu",
-           "vd_poisson.cu", "vd_diffusion.cu"]
+           "vd_poisson.cu", "vd_diffusion.cu", "vd_plotfile.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC,-O3", "-Xptxas", "-O3"]
