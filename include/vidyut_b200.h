@@ -29,6 +29,8 @@
  *                              multigrid in place of AMReX's MLMG.
  *   vd_write_plotfile          Vidyut::WritePlotFile (Source/Plot.cpp:29-39): the plotfile layout
  *                              that amrex::WriteMultiLevelPlotfile writes, for one level.
+ *   vd_write_checkpoint,       Vidyut::WriteCheckpointFile / ReadCheckpointFile
+ *   vd_read_checkpoint         (Source/Plot.cpp:41-178), for one level.
  *   vd_batch_*                 no single reference counterpart: the per-box MFIter loops of the
  *                              functions above run over many independent boxes in one
  *                              persistent launch (the reference iterates boxes with MFIter).
@@ -385,6 +387,19 @@ int vd_implicit_species_solve(const vd_box* bx, vd_array4 state, vd_array4 state
 int vd_write_plotfile(const char* dir, const vd_box* bx, const double* data, int ncomp,
                       const char* const* names, const double prob_lo[3], const double dx[3], double time,
                       int step);
+
+/* Checkpoint of one box (replaces Vidyut::WriteCheckpointFile and
+ * ReadCheckpointFile, Source/Plot.cpp:41-178, on one level): dir/Header with the
+ * title line "Checkpoint file for Vidyut", the finest level (0), the step, dt and
+ * time lines and the box array; the state (host memory, ncomp components, component
+ * slowest, x fastest) as the multi-fab dir/Level_0/phi in the plotfile's layout.
+ * vd_read_checkpoint fills bx, ncomp, istep, dt and time; with data == NULL it only
+ * reports them (a size query), otherwise it reads the values into data, which
+ * must hold capacity >= cells * ncomp doubles.  Synchronous file I/O.            */
+int vd_write_checkpoint(const char* dir, const vd_box* bx, const double* data, int ncomp, int istep, double dt,
+                        double time);
+int vd_read_checkpoint(const char* dir, vd_box* bx, double* data, int64_t capacity, int* ncomp, int* istep,
+                       double* dt, double* time);
 
 /* ---- batched cases (no single reference counterpart: the reference loops over
  * boxes with MFIter and calls the per-box functions above for each) -----------

@@ -87,3 +87,35 @@ def test_plotfile_refusals(tmp_path):
     from vidyut_b200 import _abi as abi
     with pytest.raises(abi.VidyutError):
         api.write_plotfile(tmp_path / "p", case, valid, names=["x"] * (valid.shape[0] - 1) + [""])
+
+
+@pytest.mark.parametrize("dim,n", [(1, (30,)), (2, (12, 9)), (3, (6, 5, 4))])
+def test_checkpoint_round_trip(tmp_path, dim, n):
+    """Vidyut::WriteCheckpointFile's Header (title, finest level, istep / dt / t_new
+    lines, box array) and the state read back bit for bit."""
+    m = mm.argon(10, 20261204)
+    case = inputs.build_case(m, dim, n, (1e-5,) * dim, 43, density="loguniform")
+    g = case.gvec
+    valid = np.ascontiguousarray(case.state[:, g[2]:g[2] + case.n[2], g[1]:g[1] + case.n[1],
+                                            g[0]:g[0] + case.n[0]])
+    path = tmp_path / "chk00042"
+    api.write_checkpoint(path, case, valid, istep=42, dt=1.25e-12, time=5.25e-11)
+    lines = (path / "Header").read_text().split("\n")
+    assert lines[0] == "Checkpoint file for Vidyut" and lines[1] == "0"
+    assert int(lines[2]) == 42 and float(lines[3]) == 1.25e-12 and float(lines[4]) == 5.25e-11
+    assert lines[5] == "(1 0" and lines[7] == ")"
+    st, lo, hi, d, istep, dt, time = api.read_checkpoint(path)
+    assert (d, istep, dt, time) == (dim, 42, 1.25e-12, 5.25e-11)
+    assert lo == (0, 0, 0) and hi == tuple(v - 1 for v in case.n)
+    assert st.shape == valid.shape and np.array_equal(st, valid)
+    assert (path / "Level_0" / "phi_H").exists()
+
+
+def test_checkpoint_refusals(tmp_path):
+    from vidyut_b200 import _abi as abi
+    (tmp_path / "bad").mkdir()
+    (tmp_path / "bad" / "Header").write_text("something else\n")
+    with pytest.raises(abi.VidyutError):
+        api.read_checkpoint(tmp_path / "bad")
+    with pytest.raises(abi.VidyutError):
+        api.read_checkpoint(tmp_path / "missing")

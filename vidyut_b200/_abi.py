@@ -276,6 +276,9 @@ PROTOTYPES.update({
 PROTOTYPES.update({
     "vd_write_plotfile": (C.c_int, [C.c_char_p, BOXP, DP, C.c_int, C.POINTER(C.c_char_p), DP, DP, C.c_double,
                                     C.c_int]),
+    "vd_write_checkpoint": (C.c_int, [C.c_char_p, BOXP, DP, C.c_int, C.c_int, C.c_double, C.c_double]),
+    "vd_read_checkpoint": (C.c_int, [C.c_char_p, BOXP, DP, C.c_int64, C.POINTER(C.c_int), C.POINTER(C.c_int), DP,
+                                     DP]),
 })
 
 

@@ -463,6 +463,35 @@ def write_plotfile(path, case: BoxCase, valid_state, *, time: float = 0.0, step:
     abi.check(rc, "vd_write_plotfile")
 
 
+def write_checkpoint(path, case: BoxCase, valid_state, *, istep: int = 0, dt: float = 0.0,
+                     time: float = 0.0) -> None:
+    """Checkpoint of the case's valid cells (Vidyut::WriteCheckpointFile)."""
+    if isinstance(valid_state, torch.Tensor):
+        valid_state = valid_state.detach().cpu().numpy()
+    a = np.ascontiguousarray(valid_state, dtype=np.float64)
+    rc = abi.lib().vd_write_checkpoint(str(path).encode(), C.byref(case_box(case)),
+                                       a.ctypes.data_as(C.POINTER(C.c_double)), a.shape[0], int(istep), float(dt),
+                                       float(time))
+    abi.check(rc, "vd_write_checkpoint")
+
+
+def read_checkpoint(path):
+    """(state (ncomp, nz, ny, nx), box lo, box hi, dim, istep, dt, time) of a
+    checkpoint (Vidyut::ReadCheckpointFile)."""
+    L = abi.lib()
+    bx = abi.VdBox()
+    nc, st = C.c_int(), C.c_int()
+    dt, tm = C.c_double(), C.c_double()
+    abi.check(L.vd_read_checkpoint(str(path).encode(), C.byref(bx), None, 0, C.byref(nc), C.byref(st), C.byref(dt),
+                                   C.byref(tm)), "vd_read_checkpoint")
+    n = [bx.hi[d] - bx.lo[d] + 1 for d in range(3)]
+    out = np.empty((nc.value, n[2], n[1], n[0]), dtype=np.float64)
+    abi.check(L.vd_read_checkpoint(str(path).encode(), C.byref(bx), out.ctypes.data_as(C.POINTER(C.c_double)),
+                                   out.size, C.byref(nc), C.byref(st), C.byref(dt), C.byref(tm)),
+              "vd_read_checkpoint")
+    return out, tuple(bx.lo), tuple(bx.hi), bx.dim, st.value, dt.value, tm.value
+
+
 def case_box(case: BoxCase) -> abi.VdBox:
     return abi.make_box(case.lo, case.hi, case.dim)
 

@@ -1,4 +1,5 @@
-// vd_plotfile.cpp -- plotfile output of one box (vd_write_plotfile in vidyut_b200.h).
+// vd_plotfile.cpp -- plotfile and checkpoint files of one box (vd_write_plotfile,
+// vd_write_checkpoint, vd_read_checkpoint in vidyut_b200.h).
 //
 // The reference writes its state with amrex::WriteMultiLevelPlotfile
 // (Vidyut::WritePlotFile, Source/Plot.cpp:29-39) under the names of
@@ -14,6 +15,11 @@
 //   <dir>/Level_0/Cell_D_00000 the FAB: a one-line descriptor of the number format
 //                              (IEEE double, little-endian) and the box, then the
 //                              values, component by component, x fastest.
+// Checkpoints follow Vidyut::WriteCheckpointFile / ReadCheckpointFile
+// (Source/Plot.cpp:41-178): a text Header ("Checkpoint file for Vidyut", the
+// finest level, then lines of istep, dt and t_new per level, then the box array)
+// and the state as a multi-fab Level_0/phi (phi_H, phi_D_00000) in the same
+// layout as the plotfile's.
 #include <sys/stat.h>
 #include <sys/types.h>
 
@@ -75,6 +81,62 @@ bool little_endian()
     return c == 1;
 }
 
+const char* kFabFormat = "FAB ((8, (64 11 52 0 1 12 0 1023)),(8, ";
+
+// Level directory lev holding one FAB of the box: <lev>/<prefix>_D_00000 and the
+// multi-fab header <lev>/<prefix>_H with the per-component extrema.
+int write_multifab(const std::string& lev, const char* prefix, const vd_box* bx, int dim, const double* data,
+                   int ncomp, int64_t ncell)
+{
+    const std::string dname = std::string(prefix) + "_D_00000";
+    {
+        std::ofstream d(lev + "/" + dname, std::ios::out | std::ios::trunc | std::ios::binary);
+        if (!d) return perr(VD_ERR_ARG, "cannot write %s/%s", lev.c_str(), dname.c_str());
+        d << kFabFormat << (little_endian() ? "(8 7 6 5 4 3 2 1)" : "(1 2 3 4 5 6 7 8)") << "))" << box_text(bx, dim)
+          << ' ' << ncomp << '\n';
+        d.write(reinterpret_cast<const char*>(data), (std::streamsize)(sizeof(double) * ncell * ncomp));
+        if (!d) return perr(VD_ERR_ARG, "writing %s/%s failed", lev.c_str(), dname.c_str());
+    }
+    std::ofstream h(lev + "/" + prefix + "_H", std::ios::out | std::ios::trunc);
+    if (!h) return perr(VD_ERR_ARG, "cannot write %s/%s_H", lev.c_str(), prefix);
+    h << std::setprecision(17);
+    h << 1 << '\n' << 1 << '\n' << ncomp << '\n' << 0 << '\n';
+    h << "(1 0\n" << box_text(bx, dim) << "\n)\n";
+    h << 1 << '\n' << "FabOnDisk: " << dname << " 0\n\n";
+    std::vector<double> mn(ncomp), mx(ncomp);
+    for (int c = 0; c < ncomp; c++) {
+        const double* p = data + (int64_t)c * ncell;
+        double a = p[0], b = p[0];
+        for (int64_t q = 1; q < ncell; q++) {
+            a = std::fmin(a, p[q]);
+            b = std::fmax(b, p[q]);
+        }
+        mn[c] = a;
+        mx[c] = b;
+    }
+    h << 1 << ',' << ncomp << '\n';
+    for (int c = 0; c < ncomp; c++) h << mn[c] << ',';
+    h << "\n\n" << 1 << ',' << ncomp << '\n';
+    for (int c = 0; c < ncomp; c++) h << mx[c] << ',';
+    h << '\n';
+    if (!h) return perr(VD_ERR_ARG, "writing %s/%s_H failed", lev.c_str(), prefix);
+    return VD_OK;
+}
+
+// box extent checks shared by the writers; n[] and ncell out
+int check_box(const vd_box* bx, int n[3], int64_t* ncell)
+{
+    const int dim = bx->dim;
+    if (dim < 1 || dim > 3) return perr(VD_ERR_DIM, "dimension %d", dim);
+    *ncell = 1;
+    for (int d = 0; d < 3; d++) {
+        n[d] = bx->hi[d] - bx->lo[d] + 1;
+        if (n[d] < 1 || (d >= dim && n[d] != 1)) return perr(VD_ERR_ARG, "box extent %d along %d", n[d], d);
+        *ncell *= n[d];
+    }
+    return VD_OK;
+}
+
 }  // namespace
 
 extern "C" int vd_write_plotfile(const char* dir, const vd_box* bx, const double* data, int ncomp,
@@ -83,15 +145,11 @@ extern "C" int vd_write_plotfile(const char* dir, const vd_box* bx, const double
 {
     if (!dir || !bx || !data || !names || !prob_lo || !dx) return perr(VD_ERR_ARG, "null argument");
     const int dim = bx->dim;
-    if (dim < 1 || dim > 3) return perr(VD_ERR_DIM, "dimension %d", dim);
     if (ncomp < 1) return perr(VD_ERR_ARG, "ncomp %d", ncomp);
     int64_t ncell = 1;
     int n[3];
-    for (int d = 0; d < 3; d++) {
-        n[d] = bx->hi[d] - bx->lo[d] + 1;
-        if (n[d] < 1 || (d >= dim && n[d] != 1)) return perr(VD_ERR_ARG, "box extent %d along %d", n[d], d);
-        ncell *= n[d];
-    }
+    int rc = check_box(bx, n, &ncell);
+    if (rc) return rc;
     for (int c = 0; c < ncomp; c++)
         if (!names[c] || !names[c][0] || strchr(names[c], '\n'))
             return perr(VD_ERR_ARG, "variable name %d is empty or spans lines", c);
@@ -122,44 +180,104 @@ extern "C" int vd_write_plotfile(const char* dir, const vd_box* bx, const double
         h << "Level_0/Cell\n";
         if (!h) return perr(VD_ERR_ARG, "writing %s/Header failed", dir);
     }
-    // the FAB
-    std::string fab_head;
+    return write_multifab(lev, "Cell", bx, dim, data, ncomp, ncell);
+}
+
+extern "C" int vd_write_checkpoint(const char* dir, const vd_box* bx, const double* data, int ncomp, int istep,
+                                   double dt, double time)
+{
+    if (!dir || !bx || !data) return perr(VD_ERR_ARG, "null argument");
+    if (ncomp < 1) return perr(VD_ERR_ARG, "ncomp %d", ncomp);
+    int n[3];
+    int64_t ncell = 1;
+    int rc = check_box(bx, n, &ncell);
+    if (rc) return rc;
+    const std::string root(dir), lev = root + "/Level_0";
+    if (!make_dir(root) || !make_dir(lev)) return perr(VD_ERR_ARG, "cannot create %s: %s", lev.c_str(), strerror(errno));
     {
-        std::ostringstream f;
-        f << "FAB ((8, (64 11 52 0 1 12 0 1023)),(8, " << (little_endian() ? "(8 7 6 5 4 3 2 1)" : "(1 2 3 4 5 6 7 8)")
-          << "))" << box_text(bx, dim) << ' ' << ncomp << '\n';
-        fab_head = f.str();
-        std::ofstream d(lev + "/Cell_D_00000", std::ios::out | std::ios::trunc | std::ios::binary);
-        if (!d) return perr(VD_ERR_ARG, "cannot write %s/Cell_D_00000", lev.c_str());
-        d << fab_head;
-        d.write(reinterpret_cast<const char*>(data), (std::streamsize)(sizeof(double) * ncell * ncomp));
-        if (!d) return perr(VD_ERR_ARG, "writing %s/Cell_D_00000 failed", lev.c_str());
-    }
-    // Cell_H: the multi-fab header with the per-component extrema
-    {
-        std::ofstream h(lev + "/Cell_H", std::ios::out | std::ios::trunc);
-        if (!h) return perr(VD_ERR_ARG, "cannot write %s/Cell_H", lev.c_str());
+        std::ofstream h(root + "/Header", std::ios::out | std::ios::trunc);
+        if (!h) return perr(VD_ERR_ARG, "cannot write %s/Header", dir);
         h << std::setprecision(17);
-        h << 1 << '\n' << 1 << '\n' << ncomp << '\n' << 0 << '\n';
-        h << "(1 0\n" << box_text(bx, dim) << "\n)\n";
-        h << 1 << '\n' << "FabOnDisk: Cell_D_00000 0\n\n";
-        std::vector<double> mn(ncomp), mx(ncomp);
-        for (int c = 0; c < ncomp; c++) {
-            const double* p = data + (int64_t)c * ncell;
-            double a = p[0], b = p[0];
-            for (int64_t q = 1; q < ncell; q++) {
-                a = std::fmin(a, p[q]);
-                b = std::fmax(b, p[q]);
-            }
-            mn[c] = a;
-            mx[c] = b;
-        }
-        h << 1 << ',' << ncomp << '\n';
-        for (int c = 0; c < ncomp; c++) h << mn[c] << ',';
-        h << "\n\n" << 1 << ',' << ncomp << '\n';
-        for (int c = 0; c < ncomp; c++) h << mx[c] << ',';
-        h << '\n';
-        if (!h) return perr(VD_ERR_ARG, "writing %s/Cell_H failed", lev.c_str());
+        h << "Checkpoint file for Vidyut\n" << 0 << '\n';
+        h << istep << " \n" << dt << " \n" << time << " \n";
+        h << "(1 0\n" << box_text(bx, bx->dim) << "\n)\n";
+        if (!h) return perr(VD_ERR_ARG, "writing %s/Header failed", dir);
     }
+    return write_multifab(lev, "phi", bx, bx->dim, data, ncomp, ncell);
+}
+
+namespace {
+
+// "((a,b,c) (d,e,f) (0,0,0))" -> lo, hi; the dimension from the comma count
+bool parse_box(const std::string& t, vd_box* bx)
+{
+    int v[6] = {0, 0, 0, 0, 0, 0};
+    const size_t a = t.find("(("), b = t.find(") (", a == std::string::npos ? 0 : a);
+    if (a == std::string::npos || b == std::string::npos) return false;
+    const std::string lo = t.substr(a + 2, b - a - 2);
+    const size_t c = t.find(')', b + 3);
+    if (c == std::string::npos) return false;
+    const std::string hi = t.substr(b + 3, c - b - 3);
+    int dim = 1;
+    for (char ch : lo) dim += ch == ',';
+    if (dim < 1 || dim > 3) return false;
+    std::string l = lo, h = hi;
+    for (char& ch : l) ch = ch == ',' ? ' ' : ch;
+    for (char& ch : h) ch = ch == ',' ? ' ' : ch;
+    std::istringstream il(l), ih(h);
+    for (int d = 0; d < dim; d++)
+        if (!(il >> v[d]) || !(ih >> v[3 + d])) return false;
+    memset(bx, 0, sizeof(*bx));
+    bx->dim = dim;
+    for (int d = 0; d < 3; d++) {
+        bx->lo[d] = d < dim ? v[d] : 0;
+        bx->hi[d] = d < dim ? v[3 + d] : 0;
+    }
+    return true;
+}
+
+}  // namespace
+
+extern "C" int vd_read_checkpoint(const char* dir, vd_box* bx, double* data, int64_t capacity, int* ncomp,
+                                  int* istep, double* dt, double* time)
+{
+    if (!dir || !bx || !ncomp || !istep || !dt || !time) return perr(VD_ERR_ARG, "null argument");
+    const std::string root(dir);
+    std::ifstream h(root + "/Header");
+    if (!h) return perr(VD_ERR_ARG, "cannot read %s/Header", dir);
+    std::string title, line;
+    std::getline(h, title);
+    if (title != "Checkpoint file for Vidyut") return perr(VD_ERR_ARG, "%s/Header is not a Vidyut checkpoint", dir);
+    int finest = -1;
+    h >> finest;
+    std::getline(h, line);
+    if (finest != 0) return perr(VD_ERR_ARG, "checkpoint has %d refinement levels; one is supported", finest);
+    std::getline(h, line);
+    *istep = std::stoi(line);
+    std::getline(h, line);
+    *dt = std::stod(line);
+    std::getline(h, line);
+    *time = std::stod(line);
+    std::getline(h, line);  // "(1 0"
+    if (line.rfind("(1 ", 0) != 0) return perr(VD_ERR_ARG, "checkpoint box array must hold one box");
+    std::getline(h, line);
+    if (!parse_box(line, bx)) return perr(VD_ERR_ARG, "unreadable box in %s/Header", dir);
+    int n[3];
+    int64_t ncell = 1;
+    int rc = check_box(bx, n, &ncell);
+    if (rc) return rc;
+    std::ifstream d(root + "/Level_0/phi_D_00000", std::ios::binary);
+    if (!d) return perr(VD_ERR_ARG, "cannot read %s/Level_0/phi_D_00000", dir);
+    std::string head;
+    std::getline(d, head);
+    const std::string want = std::string(kFabFormat) + (little_endian() ? "(8 7 6 5 4 3 2 1)" : "(1 2 3 4 5 6 7 8)") + "))";
+    if (head.rfind(want, 0) != 0) return perr(VD_ERR_ARG, "FAB data not in this machine's IEEE double format");
+    const int nc = std::atoi(head.substr(head.rfind(' ') + 1).c_str());
+    if (nc < 1) return perr(VD_ERR_ARG, "FAB component count unreadable");
+    *ncomp = nc;
+    if (!data) return VD_OK;  // size query
+    if (capacity < ncell * nc) return perr(VD_ERR_ARG, "buffer of %lld doubles for %lld values", (long long)capacity, (long long)(ncell * nc));
+    d.read(reinterpret_cast<char*>(data), (std::streamsize)(sizeof(double) * ncell * nc));
+    if (!d) return perr(VD_ERR_ARG, "%s/Level_0/phi_D_00000 is truncated", dir);
     return VD_OK;
 }
