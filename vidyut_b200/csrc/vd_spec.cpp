@@ -114,9 +114,10 @@ std::string gen_prep_kernel(const VdMechDev& m, int prec)
     std::ostringstream o;
     // minimum resident blocks per SM (caps registers at 65536 / (128 * min)); 0 leaves
     // the choice to the compiler.  VD_SPEC_MINBLOCKS overrides it for tuning.
-    // Default: about 4 registers per species plus 48, measured best on B200 for the
-    // 24-species mechanism (3 blocks of 128 threads per SM).
-    int minb = 65536 / (128 * (4 * ns + 48));
+    // Default: about 4 registers per species plus 48 (FP64) or plus 32 (mixed: the
+    // rates are FP32), measured best on B200 for the 8- and 24-species mechanisms
+    // (FP64: 6 and 3 blocks of 128 threads per SM; mixed: 8 and 4).
+    int minb = 65536 / (128 * (4 * ns + (prec == PREC_MIXED ? 32 : 48)));
     minb = minb < 1 ? 1 : (minb > 8 ? 8 : minb);
     if (const char* e = getenv("VD_SPEC_MINBLOCKS")) minb = atoi(e);
     const std::string sfx = prec == PREC_MIXED ? "mixed" : "fp64";
