@@ -2,6 +2,8 @@
 through amrex::WriteMultiLevelPlotfile, Source/Plot.cpp:29-39) read back with an
 independent parser of that layout: header fields, the multi-fab header, the FAB
 descriptor and every value bit for bit.  No GPU needed."""
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -119,3 +121,34 @@ def test_checkpoint_refusals(tmp_path):
         api.read_checkpoint(tmp_path / "bad")
     with pytest.raises(abi.VidyutError):
         api.read_checkpoint(tmp_path / "missing")
+
+
+def test_restart_from_checkpoint_continues_the_run(tmp_path):
+    """Two steps, a checkpoint, a restart from it and two more steps give the same
+    state as four steps in one go (the C oracle steps the case; the restart refills
+    the ghosts of species, EEN and ETEMP as the stepping does after each step)."""
+    import oracle
+    from vidyut_b200 import _abi as abi
+    from vidyut_b200.inputs import MULTISTEP_PARAMS, fill_ghosts
+    m = mm.synthetic(8, 40, 20261224)
+    case = inputs.build_case(m, 2, (20, 14), (1e-5, 1e-5), 44, density="loguniform_smooth",
+                             dens_range=(1e10, 1e18), te_range_ev=(0.3, 10.0), params=dict(MULTISTEP_PARAMS))
+    prm = case.vd_params()
+    port = oracle.Port(m)
+    g = case.gvec
+    valid = (slice(None), slice(g[2], g[2] + case.n[2]), slice(g[1], g[1] + case.n[1]),
+             slice(g[0], g[0] + case.n[0]))
+    four = oracle.run_steps(port, case, prm, 4)
+    two = oracle.run_steps(port, case, prm, 2)
+    api.write_checkpoint(tmp_path / "chk00002", case, two[valid], istep=2, dt=prm.dt, time=2 * prm.dt)
+    st, _, _, _, istep, dt, time = api.read_checkpoint(tmp_path / "chk00002")
+    assert (istep, dt, time) == (2, prm.dt, 2 * prm.dt)
+    restored = case.state.copy()
+    restored[valid] = st
+    comps = list(range(m.ns)) + [abi.EEN(m.ns), abi.ETEMP(m.ns)]
+    sub = np.ascontiguousarray(restored[comps])
+    fill_ghosts(sub, case.dim, case.ghost, case.periodic)
+    restored[comps] = sub
+    assert np.array_equal(restored, two)
+    again = oracle.run_steps(port, dataclasses.replace(case, state=restored), prm, 2)
+    assert np.array_equal(again, four)

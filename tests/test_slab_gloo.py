@@ -1,4 +1,4 @@
-"""One box split into slabs over two ranks (vidyut_b200/slab.py), on the CPU with
+"""One box split into slabs over two or three ranks (vidyut_b200/slab.py), on the CPU with
 the gloo backend: after the halo exchange each rank's slab holds exactly the
 cells of the single box, the explicit update of each slab (the C oracle, with the
 global domain passed in its parameters) equals the single-box update of those
@@ -99,6 +99,12 @@ def test_split_extent():
 @pytest.mark.parametrize("dim,periodic", [(2, False), (2, True), (3, False)])
 def test_two_rank_slabs_match_single_box(dim, periodic):
     mp.spawn(_worker, args=(2, _free_port(), dim, periodic), nprocs=2, join=True)
+
+
+@pytest.mark.parametrize("periodic", [False, True])
+def test_three_rank_slabs_match_single_box(periodic):
+    """A middle rank exchanges with both neighbours; uneven slabs (17 = 6 + 6 + 5)."""
+    mp.spawn(_worker, args=(3, _free_port(), 2, periodic), nprocs=3, join=True)
 
 
 def test_single_rank_periodic_wrap():
