@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define VD_ABI_VERSION 1
+#define VD_ABI_VERSION 2
 
 /* ---- limits of the runtime mechanism table ---------------------------------- */
 #define VD_MAX_SPECIES   64
@@ -64,7 +64,7 @@ extern "C" {
 #define VD_ERR_CUDA      -6   /* a CUDA runtime call failed (vd_last_error has the text)    */
 #define VD_ERR_TIMEOUT   -7   /* a bounded wait ran out (vd_server_wait)                    */
 #define VD_ERR_NOMEM     -8   /* device scratch could not be obtained                       */
-#define VD_ERR_NONFINITE -9   /* input scan found NaN/Inf                                   */
+#define VD_ERR_NONFINITE -9   /* NaN/Inf in an input or result (vd_params.check_finite)     */
 #define VD_ERR_BUDGET   -10   /* serving: case does not fit the HBM budget                  */
 #define VD_ERR_STATE    -11   /* call out of order (e.g. batch not built)                   */
 
@@ -198,6 +198,14 @@ typedef struct vd_params {
     uint64_t bg_mask;            /* bit s: species s is a background species       */
     int32_t update_te;           /* 1: Te = (2/3) eps/(kB ne_old), floored         */
     int32_t gradne_from_state;   /* 1: gradne_fc = face difference of ne (state)   */
+    int32_t check_finite;        /* 1: vd_explicit_update_all[_noalloc] waits for its
+                                    kernels and returns VD_ERR_NONFINITE when a NaN or
+                                    infinity was met: in the E field, Te or density sum
+                                    of a cell the stencil reads, or in an updated value
+                                    (so also in a density, the energy, a face field or a
+                                    rate feeding one).  The outputs are then written but
+                                    not meaningful.  0: no check, no synchronisation.  */
+    int32_t pad1;
 } vd_params;
 
 /* ---- library ------------------------------------------------------------- */
@@ -275,17 +283,19 @@ int vd_explicit_update_all(const vd_box* bx, vd_array4 sborder,
  * AMReX application normally hands most of the GPU to its own memory arena at
  * start-up, and some callers forbid any allocation inside their time-step loop.
  * Same arguments, work and results as vd_explicit_update_all, but the per-call
- * scratch (per-cell density sums on the stencil-grown box, plus the reaction
- * source when rxn.p is NULL) comes from one fixed array compiled into the library:
- * VD_NOALLOC_SCRATCH_BYTES on every GPU that loads the library, held until the
- * process exits.  A box whose scratch would not fit is rejected with
- * VD_ERR_NOMEM before anything is launched (pass rxn to need less scratch).
- * The first call on a device does that device's set-up (it looks up the array's
- * device address and, if needed, uploads the mechanism table, which synchronises
- * the stream); make that first call before any stream capture.  All calls share
- * the one array: calls that overlap on the GPU (different streams, or another
- * host thread) race on it, so order them on one stream.  Nothing in the array
- * needs clearing between calls: each call writes every scratch value it reads. */
+ * scratch (a status word, the per-cell density sums on the stencil-grown box, plus
+ * the reaction source when rxn.p is NULL) comes from one fixed array compiled into
+ * the library: VD_NOALLOC_SCRATCH_BYTES on every GPU the library is set up on,
+ * held until the process exits.  The array is reserved on a device, and its
+ * device address looked up, when vd_mech_init runs with that device current (or
+ * at the first call of any entry point on another device); make that happen
+ * before the host's arena takes the GPU, and before any stream capture.  After
+ * it, this entry point allocates nothing.  A box whose scratch would not fit is
+ * rejected with VD_ERR_NOMEM before anything is launched (pass rxn to need less
+ * scratch).  All calls share the one array: calls that overlap on the GPU
+ * (different streams, or another host thread) race on it, so order them on one
+ * stream.  Each call clears the status word it uses and writes every other
+ * scratch value before reading it.                                               */
 #define VD_NOALLOC_SCRATCH_BYTES (64u << 20)
 int vd_explicit_update_all_noalloc(const vd_box* bx, vd_array4 sborder,
                                    const vd_array4 efield_ec[3], const vd_array4 gradne_fc[3],
@@ -449,6 +459,11 @@ int      vd_batch_add_case(vd_batch* b, const vd_box* bx, const double* state,
 int      vd_batch_remove_case(vd_batch* b, int32_t case_id);
 int      vd_batch_step(vd_batch* b, int nsteps, void* stream);
 int      vd_batch_case_info(vd_batch* b, int32_t case_id, int64_t* steps_done, int64_t* steps_left);
+/* *nonfinite = 1 when a step of the case met a NaN or infinity (in the E field,
+ * Te or density sum of a cell its stencil reads, or in an updated value); the
+ * case then takes no further steps (vd_batch_load_case clears it).  Waits for the
+ * batch's queued work.  The reference aborts the run in that situation. */
+int      vd_batch_case_status(vd_batch* b, int32_t case_id, int32_t* nonfinite);
 int      vd_batch_read_case(vd_batch* b, int32_t case_id, double* state, void* stream);
 /* replaces a resident case's state (same layout as add; both copies are written)
  * and restarts its step count with nsteps; the arena region and the captured
@@ -477,7 +492,9 @@ int      vd_batch_get_stats(vd_batch* b, vd_batch_stats* out);
  * and retires finished cases to host memory.  vd_server_wait blocks until the
  * request is done (timeout_s < 0: no limit; VD_ERR_TIMEOUT otherwise), copies its
  * final state (the ghost-grown layout) to state_out when not NULL, gives its
- * latency (submission to result in host memory) and forgets the request.
+ * latency (submission to result in host memory) and forgets the request; a
+ * request that failed returns its status, VD_ERR_NONFINITE when one of its steps
+ * met a NaN or infinity (vd_batch_case_status).
  * A request larger than the whole budget is rejected at submission with
  * VD_ERR_BUDGET.  The server uses the device current at creation and the
  * mechanism loaded then.                                                         */

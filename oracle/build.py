@@ -7,8 +7,10 @@
                                  unmodified against oracle/refshim, one library
                                  per (case, dimension) as the reference builds
                                  one executable per case.  Needs the reference
-                                 tree; skipped (not an error) when it is absent,
-                                 in which case previously built libraries are used.
+                                 tree ($VIDYUT_REFERENCE, or a checkout named
+                                 "reference" beside this repository); skipped (not
+                                 an error) when it is absent, in which case
+                                 previously built libraries are used.
 
     python oracle/build.py            # oracle + every reference case
 """
@@ -24,7 +26,9 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 BUILD = HERE / "_build"
 REF_OUT = HERE / "_ref"
-REF_TREE = Path(os.environ.get("VIDYUT_REFERENCE", "/root/reference"))
+# The reference tree: $VIDYUT_REFERENCE, else a checkout named "reference" beside
+# this repository's directory.
+REF_TREE = Path(os.environ["VIDYUT_REFERENCE"]) if os.environ.get("VIDYUT_REFERENCE") else ROOT.parent / "reference"
 
 ORACLE_LIB = BUILD / "libvdoracle.so"
 

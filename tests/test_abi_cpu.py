@@ -36,7 +36,7 @@ def test_exports_every_declared_symbol(lib):
 
 def test_struct_layouts(lib):
     abi.check_layout(lib)
-    assert lib.vd_abi_version() == 1
+    assert lib.vd_abi_version() == 2
     # vd_array4 has amrex::Array4<Real>'s layout: pointer, 3 strides, begin/end Dim3, ncomp
     assert C.sizeof(abi.VdArray4) == 64
 

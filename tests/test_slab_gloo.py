@@ -115,3 +115,12 @@ def test_single_rank_periodic_wrap():
     local.narrow(2, local.shape[2] - case.ghost, case.ghost).fill_(float("nan"))
     sl.exchange(local)
     assert np.array_equal(local.numpy(), case.state)
+
+
+def test_thin_slab_is_refused_on_one_rank_too():
+    """A slab with fewer valid planes than ghost planes cannot fill its ghosts from
+    its own cells: the periodic one-rank wrap refuses it like the exchange does."""
+    s = Slab(n_global=(4, 2, 1), dim=2, ghost=3, rank=0, world=1, periodic=True)
+    state = torch.zeros((1, 1, 2 + 6, 4 + 6), dtype=torch.float64)
+    with pytest.raises(ValueError, match="thinner"):
+        s.exchange(state)

@@ -6,10 +6,19 @@ allow no allocation inside the time-step loop) call
 vd_explicit_update_all_noalloc, whose scratch is a fixed array inside the
 library.  Its results must equal those of vd_explicit_update_all within the
 FP64 parity tolerance of the other GPU tests (1e-12), on consecutive calls that
-reuse the same array, and a box whose scratch does not fit must be refused.
+reuse the same array, and a box whose scratch does not fit must be refused.  The
+array is reserved when the device is set up (vd_mech_init); after that the entry
+point must not take any device memory, which a fresh process checks with the
+device's free-memory count.
 This file is collected last so that a run stopping at the first failure has run
 everything else first; it also passes on its own in a fresh process.
 """
+import json
+import os
+import subprocess
+import sys
+from pathlib import Path
+
 import numpy as np
 import pytest
 import torch
@@ -91,3 +100,45 @@ def test_noalloc_refuses_boxes_beyond_the_fixed_scratch():
     assert e.value.status == abi.ERR_NOMEM
     assert "scratch" in str(e.value)
     assert abi.NOALLOC_SCRATCH_BYTES == 64 << 20
+
+
+_NO_ALLOC_PROBE = r"""
+import json, torch
+from vidyut_b200 import api, inputs as vin
+torch.cuda.set_device(0)
+big = vin.config_argon2d(n=(96, 80))
+small = vin.config_argon2d(n=(12, 10))
+torch.zeros(1, device="cuda")
+torch.cuda.synchronize()
+free0 = torch.cuda.mem_get_info()[0]
+api.mech_init(big.mech)                 # device set-up: the fixed array is reserved here
+torch.cuda.synchronize()
+free1 = torch.cuda.mem_get_info()[0]
+dcs, dcb = api.upload(small), api.upload(big)
+outs, outb = dcs.new_outputs(), dcb.new_outputs()
+prms = [big.vd_params(precision=p, check_finite=c) for p in (0, 1) for c in (0, 1)]
+api.explicit_update_all_noalloc(dcs, small.vd_params(), outs[0])   # first launch of each kernel
+torch.cuda.synchronize()
+free2 = torch.cuda.mem_get_info()[0]
+for prm in prms:
+    for keep in (False, True):
+        api.explicit_update_all_noalloc(dcb, prm, outb[0], outb[1], outb[2] if keep else None)
+torch.cuda.synchronize()
+free3 = torch.cuda.mem_get_info()[0]
+print(json.dumps({"reserved_at_setup": free0 - free1, "taken_by_calls": free2 - free3}))
+"""
+
+
+def test_noalloc_calls_take_no_device_memory():
+    """In a fresh process: after set-up and one first call (which loads the
+    kernels' code), eight allocation-free calls on a larger box, both
+    precisions, with and without the non-finite check and the caller's rxn,
+    leave the device's free memory exactly as it was."""
+    root = Path(__file__).resolve().parents[1]
+    env = dict(os.environ, CUDA_MODULE_LOADING="LAZY", PYTHONPATH=str(root))
+    r = subprocess.run([sys.executable, "-c", _NO_ALLOC_PROBE], cwd=root, env=env, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = json.loads(r.stdout.strip().splitlines()[-1])
+    assert got["taken_by_calls"] == 0, got
+    assert got["reserved_at_setup"] >= abi.NOALLOC_SCRATCH_BYTES, got

@@ -86,7 +86,7 @@ class VdParams(C.Structure):
                 ("bound_specden", C.c_int32), ("ele_mob", C.c_double), ("ele_diff", C.c_double),
                 ("min_species_density", C.c_double), ("min_electron_density", C.c_double),
                 ("min_electron_temp", C.c_double), ("bg_mask", C.c_uint64), ("update_te", C.c_int32),
-                ("gradne_from_state", C.c_int32)]
+                ("gradne_from_state", C.c_int32), ("check_finite", C.c_int32), ("pad1", C.c_int32)]
 
 
 STRUCTS = [VdArray4, VdBox, VdReaction, VdMech, VdParams]
@@ -231,6 +231,7 @@ PROTOTYPES.update({
     "vd_batch_remove_case": (C.c_int, [C.c_void_p, C.c_int32]),
     "vd_batch_step": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "vd_batch_case_info": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "vd_batch_case_status": (C.c_int, [C.c_void_p, C.c_int32, I32P]),
     "vd_batch_read_case": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "vd_batch_load_case": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p]),
     "vd_batch_tune": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, DP]),

@@ -254,6 +254,13 @@ class Batch:
     def step(self, nsteps: int, stream=None) -> None:
         abi.check(abi.lib().vd_batch_step(self._h, int(nsteps), _stream(stream)), "vd_batch_step")
 
+    def nonfinite(self, cid: int) -> bool:
+        """True when a step of case cid met a NaN or infinity (it then takes no
+        further steps); waits for the batch's queued work."""
+        f = C.c_int32()
+        abi.check(abi.lib().vd_batch_case_status(self._h, int(cid), C.byref(f)), "vd_batch_case_status")
+        return bool(f.value)
+
     def info(self, cid: int):
         done, left = C.c_int64(), C.c_int64()
         abi.check(abi.lib().vd_batch_case_info(self._h, int(cid), C.byref(done), C.byref(left)),

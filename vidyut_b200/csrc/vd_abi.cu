@@ -16,6 +16,7 @@
 #include <string>
 #include <vector>
 #include "../../include/vidyut_b200.h"
+#include "vd_host.h"
 #include "vd_kernels.cuh"
 
 using namespace vd;
@@ -46,7 +47,57 @@ int cuda_fail(cudaError_t e, const char* what)
     return fail(VD_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
-// Loads the mechanism table onto the current device if it is not there yet.
+// ---------------------------------------------------------------------------
+// Per-device resources set up once per device, at vd_mech_init or the first call
+// on that device: the mechanism table, the library's own stream-ordered memory
+// pool for per-call scratch, and the allocation-free update's fixed array.
+//
+// The scratch pool is the library's, not the device's default pool, so a host's
+// own cudaMallocAsync frees keep the release behaviour the host chose; this pool
+// keeps what it has taken between calls (no release at synchronisation) so that a
+// time-step loop does not map and unmap memory at every step.
+constexpr int kMaxDev = 64;
+cudaMemPool_t g_pool[kMaxDev] = {};
+
+// The allocation-free update's scratch (vd_explicit_update_all_noalloc).  In host
+// code the name below is only a host-side stand-in; the array's device address is
+// looked up once per device, with that device current, and passed to the kernels.
+// The lookup makes the runtime load this file's module, which is when the array
+// is reserved on the device.
+constexpr size_t kNoallocDoubles = VD_NOALLOC_SCRATCH_BYTES / sizeof(double);
+static __device__ __align__(256) double g_noalloc_scratch[kNoallocDoubles];
+double* g_noalloc_ptr[kMaxDev] = {nullptr};
+
+int setup_device(int dev)
+{
+    if (!g_pool[dev]) {
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool;
+        cudaError_t e = cudaMemPoolCreate(&pool, &props);
+        if (e != cudaSuccess) return cuda_fail(e, "creating the scratch memory pool");
+        uint64_t keep = UINT64_MAX;
+        e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) {
+            cudaMemPoolDestroy(pool);
+            return cuda_fail(e, "configuring the scratch memory pool");
+        }
+        g_pool[dev] = pool;
+    }
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(allocation-free scratch)");
+        g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    return VD_OK;
+}
+
+// Loads the mechanism table onto the current device if it is not there yet, and
+// sets the device up (setup_device).
 int ensure_mech_on_device(cudaStream_t st)
 {
     std::lock_guard<std::mutex> lk(g_mech_mu);
@@ -54,19 +105,26 @@ int ensure_mech_on_device(cudaStream_t st)
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if (dev < 0 || dev >= kMaxDev) return fail(VD_ERR_ARG, "device ordinal %d not supported", dev);
     for (int d : g_loaded_dev)
         if (d == dev) return VD_OK;
-    int rc = upload_mech(g_mech_dev, st);
+    int rc = setup_device(dev);
+    if (rc) return rc;
+    rc = upload_mech(g_mech_dev, st);
     if (rc != 0) return cuda_fail((cudaError_t)rc, "uploading mechanism table");
-    // keep freed scratch in this process's default pool between calls instead of
-    // handing it back to the driver at every synchronisation
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-        uint64_t keep = UINT64_MAX;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    }
     g_loaded_dev.push_back(dev);
     return VD_OK;
+}
+
+// Scratch of one call from the library's pool on the current device (set up by
+// ensure_mech_on_device), stream-ordered on st; released with cudaFreeAsync.
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDev || !g_pool[dev]) return cudaErrorNotReady;
+    return cudaMallocFromPoolAsync(p, bytes, g_pool[dev], st);
 }
 
 int nspecies()
@@ -151,13 +209,6 @@ void finish_lists(TransportArgs& a)
 {
     std::lock_guard<std::mutex> lk(g_mech_mu);
     finish_species_lists(a, *g_mech_dev);
-}
-
-int species_class(const vd_mech* m, int s)
-{
-    if (s == m->nspecies) return VD_CLASS_ENERGY;
-    if (s == m->e_id) return VD_CLASS_ELECTRON;
-    return m->charge[s] != 0 ? VD_CLASS_ION : VD_CLASS_NEUTRAL;
 }
 
 }  // namespace
@@ -448,13 +499,31 @@ static int check_params(const vd_box* bx, const vd_params* p)
     if (!p) return fail(VD_ERR_ARG, "null params");
     if (p->dim != bx->dim) return fail(VD_ERR_DIM, "params.dim %d != box.dim %d", p->dim, bx->dim);
     for (int d = 0; d < bx->dim; d++)
-        if (!(p->dx[d] > 0.0)) return fail(VD_ERR_ARG, "dx[%d] must be > 0", d);
+        if (!(p->dx[d] > 0.0) || !std::isfinite(p->dx[d])) return fail(VD_ERR_ARG, "dx[%d] must be finite and > 0", d);
     if (p->precision != VD_PREC_FP64 && p->precision != VD_PREC_MIXED)
         return fail(VD_ERR_ARG, "unknown precision %d", p->precision);
+    // the chemistry takes log(Tg) and 1/Tg, the ion mobility sqrt(Tg)
+    if (!(p->Tg > 0.0) || !std::isfinite(p->Tg)) return fail(VD_ERR_ARG, "Tg must be finite and > 0 (got %g)", p->Tg);
+    if (!(p->dt >= 0.0) || !std::isfinite(p->dt)) return fail(VD_ERR_ARG, "dt must be finite and >= 0 (got %g)", p->dt);
     return check_scheme(p->hyp_order, p->weno_scheme);
 }
 
-static void fill_cfg(TransportArgs& a, const vd_box* bx, const vd_params* p, const vd_mech* m)
+// The loaded mechanism as the update's host code needs it.
+static vd_host::MechInfo mech_snapshot()
+{
+    vd_host::MechInfo mi;
+    memset(&mi, 0, sizeof(mi));
+    std::lock_guard<std::mutex> lk(g_mech_mu);
+    mi.ns = g_mech->nspecies;
+    mi.e_id = g_mech->e_id;
+    mi.generation = g_mech_gen;
+    for (int s = 0; s <= g_mech->nspecies; s++) mi.mob_kind[s] = g_mech->mob_kind[s];
+    for (int s = 0; s < g_mech->nspecies; s++) mi.charge[s] = g_mech->charge[s];
+    return mi;
+}
+
+// Scalars of a transport record from the box and the parameters.
+static void fill_cfg(TransportArgs& a, const vd_box* bx, const vd_params* p, int ns, int e_id, int e_charge)
 {
     memset(&a, 0, sizeof(a));
     for (int d = 0; d < 3; d++) {
@@ -471,8 +540,8 @@ static void fill_cfg(TransportArgs& a, const vd_box* bx, const vd_params* p, con
     a.dt = p->dt;
     a.Tg = p->Tg;
     fill_class_flags(p, a.zlo, a.zhi);
-    a.ns = m->nspecies;
-    a.e_id = m->e_id;
+    a.ns = ns;
+    a.e_id = e_id;
     a.hyp_order = p->hyp_order;
     a.weno = p->weno_scheme;
     a.udv = p->user_defined_vel;
@@ -490,9 +559,72 @@ static void fill_cfg(TransportArgs& a, const vd_box* bx, const vd_params* p, con
     a.ele_mob = p->ele_mob;
     a.ele_diff = p->ele_diff;
     a.min_te = p->min_electron_temp;
-    a.charge_e = (double)m->charge[m->e_id] * ECHARGE;
+    a.charge_e = (double)e_charge * ECHARGE;
     a.ghost = stencil_halo(p->hyp_order);
     a.write_diag = 1;
+}
+
+// The species of a transport record: transported species (and the electron
+// energy when it is solved) in species order with their BC class and whether they
+// have a drift flux, background species apart (Source/Evolve.cpp:208-288); then
+// the derived fluxed / unfluxed lists and velocity bases (finish_species_lists).
+static void fill_species(TransportArgs& a, const vd_params* p, const vd_host::MechInfo& m)
+{
+    const int ns = m.ns;
+    a.ntr = 0;
+    a.nbg = 0;
+    for (int s = 0; s <= ns; s++) {
+        const bool energy = (s == ns);
+        if (energy && !p->elecenergy_solve) continue;
+        if (!energy && ((p->bg_mask >> s) & 1ull)) {
+            a.bg_sp[a.nbg++] = (int8_t)s;
+            continue;
+        }
+        a.tr_sp[a.ntr] = (int8_t)s;
+        const int cls = energy ? VD_CLASS_ENERGY
+                               : (s == m.e_id ? VD_CLASS_ELECTRON : (m.charge[s] != 0 ? VD_CLASS_ION : VD_CLASS_NEUTRAL));
+        a.tr_cls[a.ntr] = (int8_t)cls;
+        const bool has_vel = p->user_defined_vel ? (s == p->vel_species) : (m.mob_kind[s] != VD_MOB_ZERO);
+        a.tr_flux[a.ntr] = (p->do_transport && has_vel) ? 1 : 0;
+        a.ntr++;
+    }
+    finish_lists(a);
+}
+
+// Validation beyond check_params that every update of a box makes.
+static int check_update_species(const vd_params* p, const vd_host::MechInfo& m)
+{
+    if (p->bg_mask >> m.ns) return fail(VD_ERR_ARG, "bg_mask names species >= %d", m.ns);
+    if (p->bg_mask & (1ull << m.e_id)) return fail(VD_ERR_ARG, "electrons cannot be a background species");
+    if (p->user_defined_vel && (p->vel_species < 0 || p->vel_species > m.ns))
+        return fail(VD_ERR_ARG, "vel_species invalid");
+    return VD_OK;
+}
+
+// Views of the face arrays the Joule term reads (efield_ec unless cs_technique,
+// gradne_fc unless gradne_from_state), each checked to cover the face box of its
+// direction.
+static int face_views(const vd_box* bx, const vd_params* prm, const vd_array4 efield_ec[3],
+                      const vd_array4 gradne_fc[3], A4 ef[3], A4 gne[3])
+{
+    std::string why;
+    for (int d = 0; d < bx->dim; d++) {
+        int fhi[3] = {bx->hi[0], bx->hi[1], bx->hi[2]};
+        fhi[d] += 1;
+        if (!prm->cs_technique) {
+            if (!efield_ec) return fail(VD_ERR_ARG, "efield_ec is null");
+            if (!covers(efield_ec[d], bx->lo, fhi, 1, &why))
+                return fail(VD_ERR_ARG, "efield_ec[%d]: %s", d, why.c_str());
+            ef[d] = A4(efield_ec[d]);
+        }
+        if (!prm->gradne_from_state) {
+            if (!gradne_fc) return fail(VD_ERR_ARG, "gradne_fc is null");
+            if (!covers(gradne_fc[d], bx->lo, fhi, 1, &why))
+                return fail(VD_ERR_ARG, "gradne_fc[%d]: %s", d, why.c_str());
+            gne[d] = A4(gradne_fc[d]);
+        }
+    }
+    return VD_OK;
 }
 
 int vd_elecenergy_source(const vd_box* bx, vd_array4 sborder, vd_array4 rxn, const vd_array4 efield_ec[3],
@@ -504,14 +636,9 @@ int vd_elecenergy_source(const vd_box* bx, vd_array4 sborder, vd_array4 rxn, con
     if (rc) return rc;
     if (!valid_box(bx) || !prm) return fail(VD_ERR_ARG, "invalid box or params");
     if (prm->dim != bx->dim) return fail(VD_ERR_DIM, "params.dim != box.dim");
-    vd_mech mcopy;
-    {
-        std::lock_guard<std::mutex> lk(g_mech_mu);
-        mcopy.nspecies = g_mech->nspecies;
-        mcopy.e_id = g_mech->e_id;
-        memcpy(mcopy.charge, g_mech->charge, sizeof(mcopy.charge));
-    }
-    const int ns = mcopy.nspecies;
+    if (!(prm->Tg > 0.0) || !std::isfinite(prm->Tg)) return fail(VD_ERR_ARG, "Tg must be finite and > 0");
+    const vd_host::MechInfo m = mech_snapshot();
+    const int ns = m.ns;
     std::string why;
     int glo[3] = {bx->lo[0], bx->lo[1], bx->lo[2]}, ghi[3] = {bx->hi[0], bx->hi[1], bx->hi[2]};
     for (int d = 0; d < bx->dim; d++) {
@@ -523,27 +650,152 @@ int vd_elecenergy_source(const vd_box* bx, vd_array4 sborder, vd_array4 rxn, con
     if (!covers(dsdt, bx->lo, bx->hi, 1, &why)) return fail(VD_ERR_ARG, "dsdt: %s", why.c_str());
     if (!covers(phi_new, bx->lo, bx->hi, VD_NVAR(ns), &why)) return fail(VD_ERR_ARG, "phi_new: %s", why.c_str());
     A4 ef[3], gne[3];
-    for (int d = 0; d < 3; d++) {
-        if (d < bx->dim) {
-            int fhi[3] = {bx->hi[0], bx->hi[1], bx->hi[2]};
-            fhi[d] += 1;
-            if (!prm->cs_technique) {
-                if (!efield_ec || !covers(efield_ec[d], bx->lo, fhi, 1, &why))
-                    return fail(VD_ERR_ARG, "efield_ec[%d]: %s", d, why.c_str());
-                ef[d] = A4(efield_ec[d]);
-            }
-            if (!prm->gradne_from_state) {
-                if (!gradne_fc || !covers(gradne_fc[d], bx->lo, fhi, 1, &why))
-                    return fail(VD_ERR_ARG, "gradne_fc[%d]: %s", d, why.c_str());
-                gne[d] = A4(gradne_fc[d]);
-            }
-        }
-    }
+    if ((rc = face_views(bx, prm, efield_ec, gradne_fc, ef, gne))) return rc;
     TransportArgs cfg;
-    fill_cfg(cfg, bx, prm, &mcopy);
+    fill_cfg(cfg, bx, prm, ns, m.e_id, m.charge[m.e_id]);
     cudaError_t e = launch_joule(box_idx(bx->lo, bx->hi), bx->dim, A4(sborder), A4(rxn), ef, gne, A4(dsdt),
                                  A4(phi_new), cfg, st);
     if (e != cudaSuccess) return cuda_fail(e, "k_joule launch");
+    return VD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// One fused explicit update of a box (vd_explicit_update_all and its
+// allocation-free form share all of it but the origin of the scratch).
+//
+// Scratch layout: the status word of the non-finite check (kStatusBytes, so the
+// rest stays 256-byte aligned), the density sums N over the stencil-grown box,
+// then the reaction source (NS+1 components over the valid box) when the caller
+// passes no rxn array.
+constexpr size_t kStatusBytes = 256;
+
+struct UpdatePlan {
+    TransportArgs a;
+    PrepArgs pa;
+    int glo[3], ghi[3];
+    int64_t gn, vn;   // cells of the grown box and of the valid box
+    bool own_rxn;     // the reaction source lives in scratch
+    bool check;       // prm->check_finite
+    int dim, prec;
+    size_t scratch_bytes() const
+    {
+        return kStatusBytes + (size_t)gn * sizeof(double) + (own_rxn ? (size_t)vn * (a.ns + 1) * sizeof(double) : 0);
+    }
+};
+
+// Validates the arguments and fills everything of the plan but the scratch
+// pointers.  Launches nothing.
+static int plan_update(const vd_box* bx, vd_array4 sborder, const vd_array4 efield_ec[3],
+                       const vd_array4 gradne_fc[3], vd_array4 phi_new, vd_array4 dsdt, vd_array4 rxn,
+                       const vd_params* prm, UpdatePlan* P)
+{
+    int rc;
+    if ((rc = check_params(bx, prm))) return rc;
+    const vd_host::MechInfo m = mech_snapshot();
+    if ((rc = check_update_species(prm, m))) return rc;
+    const int ns = m.ns, dim = bx->dim;
+    const int H = stencil_halo(prm->hyp_order);
+    std::string why;
+    for (int d = 0; d < 3; d++) {
+        P->glo[d] = bx->lo[d];
+        P->ghi[d] = bx->hi[d];
+    }
+    for (int d = 0; d < dim; d++) {
+        P->glo[d] -= H;
+        P->ghi[d] += H;
+    }
+    // the stencil only reaches along one axis at a time; corners are never read,
+    // but the per-cell density sums cover the whole grown box, so require it.
+    if (!covers(sborder, P->glo, P->ghi, VD_NVAR(ns), &why)) return fail(VD_ERR_GHOST, "sborder: %s", why.c_str());
+    if (!covers(phi_new, bx->lo, bx->hi, VD_NVAR(ns), &why)) return fail(VD_ERR_ARG, "phi_new: %s", why.c_str());
+    if (dsdt.p && !covers(dsdt, bx->lo, bx->hi, ns + 1, &why)) return fail(VD_ERR_ARG, "dsdt: %s", why.c_str());
+    if (rxn.p && !covers(rxn, bx->lo, bx->hi, ns + 1, &why)) return fail(VD_ERR_ARG, "rxn: %s", why.c_str());
+    A4 ef[3], gne[3];
+    if (prm->elecenergy_solve && (rc = face_views(bx, prm, efield_ec, gradne_fc, ef, gne))) return rc;
+
+    TransportArgs& a = P->a;
+    fill_cfg(a, bx, prm, ns, m.e_id, m.charge[m.e_id]);
+    fill_species(a, prm, m);
+    int tile[3];
+    transport_tile(dim, tile);
+    for (int d = 0; d < 3; d++) {
+        const int n = bx->hi[d] - bx->lo[d] + 1;
+        a.ntile[d] = (n + tile[d] - 1) / tile[d];
+    }
+    a.sb = A4(sborder);
+    a.pn = A4(phi_new);
+    a.dsdt = dsdt.p ? A4(dsdt) : A4();
+    a.rxn = rxn.p ? A4(rxn) : A4();
+    for (int d = 0; d < 3; d++) {
+        a.ef[d] = ef[d];
+        a.gne[d] = gne[d];
+    }
+    PrepArgs& pa = P->pa;
+    memset(&pa, 0, sizeof(pa));
+    pa.sb = a.sb;
+    for (int d = 0; d < 3; d++) {
+        pa.glo[d] = P->glo[d];
+        pa.ghi[d] = P->ghi[d];
+        pa.lo[d] = bx->lo[d];
+        pa.hi[d] = bx->hi[d];
+    }
+    pa.Tg = prm->Tg;
+    pa.do_reactions = prm->do_reactions;
+    pa.write_n = 1;
+    P->gn = (int64_t)(P->ghi[0] - P->glo[0] + 1) * (P->ghi[1] - P->glo[1] + 1) * (P->ghi[2] - P->glo[2] + 1);
+    P->vn = (int64_t)(bx->hi[0] - bx->lo[0] + 1) * (bx->hi[1] - bx->lo[1] + 1) * (bx->hi[2] - bx->lo[2] + 1);
+    P->own_rxn = rxn.p == nullptr;
+    P->check = prm->check_finite != 0;
+    P->dim = dim;
+    P->prec = prm->precision;
+    return VD_OK;
+}
+
+// Points the plan at its scratch and launches the update on st (prep, the FP64
+// path's Joule pass, transport).  With the non-finite check it clears the status
+// word first and afterwards reads it back, synchronising st.
+static int launch_update(UpdatePlan& P, char* scratch, cudaStream_t st)
+{
+    unsigned int* status = reinterpret_cast<unsigned int*>(scratch);
+    double* Np = reinterpret_cast<double*>(scratch + kStatusBytes);
+    A4 Nv;
+    Nv.p = Np;
+    Nv.bx = P.glo[0];
+    Nv.by = P.glo[1];
+    Nv.bz = P.glo[2];
+    Nv.js = P.ghi[0] - P.glo[0] + 1;
+    Nv.ks = Nv.js * (P.ghi[1] - P.glo[1] + 1);
+    Nv.ns = Nv.ks * (P.ghi[2] - P.glo[2] + 1);
+    Nv.ncomp = 1;
+    TransportArgs& a = P.a;
+    if (P.own_rxn) {
+        A4 R;
+        R.p = Np + P.gn;
+        R.bx = a.lo[0];
+        R.by = a.lo[1];
+        R.bz = a.lo[2];
+        R.js = a.hi[0] - a.lo[0] + 1;
+        R.ks = R.js * (a.hi[1] - a.lo[1] + 1);
+        R.ns = R.ks * (a.hi[2] - a.lo[2] + 1);
+        R.ncomp = a.ns + 1;
+        a.rxn = R;
+    }
+    a.Nv = Nv;
+    a.status = P.check ? status : nullptr;
+    P.pa.rxn = a.rxn;
+    P.pa.Nv = Nv;
+    cudaError_t e = P.check ? cudaMemsetAsync(status, 0, sizeof(unsigned int), st) : cudaSuccess;
+    if (e == cudaSuccess) e = launch_prep(P.pa, P.prec, a.ns, st);
+    if (e == cudaSuccess && a.elecenergy && !joule_in_tile(a, P.prec)) e = launch_joule_pre(a, P.dim, P.prec, st);
+    if (e == cudaSuccess) e = launch_transport(a, P.dim, P.prec, st);
+    if (e != cudaSuccess) return cuda_fail(e, "fused update launch");
+    if (P.check) {
+        unsigned int h = 0;
+        e = cudaMemcpyAsync(&h, status, sizeof(h), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, "reading the non-finite status");
+        if (h) return fail(VD_ERR_NONFINITE, "NaN or infinity in the inputs or results of the update");
+    }
     return VD_OK;
 }
 
@@ -554,132 +806,15 @@ int vd_explicit_update_all(const vd_box* bx, vd_array4 sborder, const vd_array4 
     cudaStream_t st = (cudaStream_t)stream;
     int rc = ensure_mech_on_device(st);
     if (rc) return rc;
-    if ((rc = check_params(bx, prm))) return rc;
-    vd_mech* m;
-    {
-        std::lock_guard<std::mutex> lk(g_mech_mu);
-        m = g_mech;
-    }
-    const int ns = m->nspecies, dim = bx->dim;
-    const int H = stencil_halo(prm->hyp_order);
-    std::string why;
-    int glo[3] = {bx->lo[0], bx->lo[1], bx->lo[2]}, ghi[3] = {bx->hi[0], bx->hi[1], bx->hi[2]};
-    for (int d = 0; d < dim; d++) {
-        glo[d] -= H;
-        ghi[d] += H;
-    }
-    // the stencil only reaches along one axis at a time; corners are never read,
-    // but the per-cell density sums cover the whole grown box, so require it.
-    if (!covers(sborder, glo, ghi, VD_NVAR(ns), &why)) return fail(VD_ERR_GHOST, "sborder: %s", why.c_str());
-    if (!covers(phi_new, bx->lo, bx->hi, VD_NVAR(ns), &why)) return fail(VD_ERR_ARG, "phi_new: %s", why.c_str());
-    if (dsdt.p && !covers(dsdt, bx->lo, bx->hi, ns + 1, &why)) return fail(VD_ERR_ARG, "dsdt: %s", why.c_str());
-    if (rxn.p && !covers(rxn, bx->lo, bx->hi, ns + 1, &why)) return fail(VD_ERR_ARG, "rxn: %s", why.c_str());
-    if (prm->bg_mask >> ns) return fail(VD_ERR_ARG, "bg_mask names species >= %d", ns);
-    if (prm->bg_mask & (1ull << m->e_id)) return fail(VD_ERR_ARG, "electrons cannot be a background species");
-    if (prm->user_defined_vel && (prm->vel_species < 0 || prm->vel_species > ns))
-        return fail(VD_ERR_ARG, "vel_species invalid");
-    A4 ef[3], gne[3];
-    if (prm->elecenergy_solve) {
-        for (int d = 0; d < dim; d++) {
-            int fhi[3] = {bx->hi[0], bx->hi[1], bx->hi[2]};
-            fhi[d] += 1;
-            if (!prm->cs_technique) {
-                if (!efield_ec || !covers(efield_ec[d], bx->lo, fhi, 1, &why))
-                    return fail(VD_ERR_ARG, "efield_ec[%d]: %s", d, why.c_str());
-                ef[d] = A4(efield_ec[d]);
-            }
-            if (!prm->gradne_from_state) {
-                if (!gradne_fc || !covers(gradne_fc[d], bx->lo, fhi, 1, &why))
-                    return fail(VD_ERR_ARG, "gradne_fc[%d]: %s", d, why.c_str());
-                gne[d] = A4(gradne_fc[d]);
-            }
-        }
-    }
-
-    TransportArgs a;
-    fill_cfg(a, bx, prm, m);
-    int tile[3];
-    transport_tile(dim, tile);
-    for (int d = 0; d < 3; d++) {
-        int n = bx->hi[d] - bx->lo[d] + 1;
-        a.ntile[d] = (n + tile[d] - 1) / tile[d];
-    }
-    a.sb = A4(sborder);
-    a.pn = A4(phi_new);
-    a.dsdt = dsdt.p ? A4(dsdt) : A4();
-    for (int d = 0; d < 3; d++) {
-        a.ef[d] = ef[d];
-        a.gne[d] = gne[d];
-    }
-    a.ntr = 0;
-    a.nbg = 0;
-    for (int s = 0; s <= ns; s++) {
-        bool energy = (s == ns);
-        if (energy && !prm->elecenergy_solve) continue;
-        if (!energy && ((prm->bg_mask >> s) & 1ull)) {
-            a.bg_sp[a.nbg++] = (int8_t)s;
-            continue;
-        }
-        a.tr_sp[a.ntr] = (int8_t)s;
-        a.tr_cls[a.ntr] = (int8_t)species_class(m, s);
-        bool has_vel = prm->user_defined_vel ? (s == prm->vel_species) : (m->mob_kind[s] != VD_MOB_ZERO);
-        a.tr_flux[a.ntr] = (prm->do_transport && has_vel) ? 1 : 0;
-        a.ntr++;
-    }
-    finish_lists(a);
-
-    // scratch: N on the grown box, rxn on the valid box when the caller does not keep it
-    const int64_t gn = (int64_t)(ghi[0] - glo[0] + 1) * (ghi[1] - glo[1] + 1) * (ghi[2] - glo[2] + 1);
-    const int64_t vn = (int64_t)(bx->hi[0] - bx->lo[0] + 1) * (bx->hi[1] - bx->lo[1] + 1) * (bx->hi[2] - bx->lo[2] + 1);
-    size_t bytes = (size_t)gn * sizeof(double) + (rxn.p ? 0 : (size_t)vn * (ns + 1) * sizeof(double));
+    UpdatePlan P;
+    if ((rc = plan_update(bx, sborder, efield_ec, gradne_fc, phi_new, dsdt, rxn, prm, &P))) return rc;
+    const size_t bytes = P.scratch_bytes();
     void* scratch = nullptr;
-    cudaError_t e = cudaMallocAsync(&scratch, bytes, st);
+    cudaError_t e = scratch_alloc(&scratch, bytes, st);
     if (e != cudaSuccess) return fail(VD_ERR_NOMEM, "scratch of %zu bytes: %s", bytes, cudaGetErrorString(e));
-    double* Np = (double*)scratch;
-    A4 Nv;
-    Nv.p = Np;
-    Nv.bx = glo[0];
-    Nv.by = glo[1];
-    Nv.bz = glo[2];
-    Nv.js = ghi[0] - glo[0] + 1;
-    Nv.ks = Nv.js * (ghi[1] - glo[1] + 1);
-    Nv.ns = Nv.ks * (ghi[2] - glo[2] + 1);
-    Nv.ncomp = 1;
-    A4 R;
-    if (rxn.p) {
-        R = A4(rxn);
-    } else {
-        R.p = Np + gn;
-        R.bx = bx->lo[0];
-        R.by = bx->lo[1];
-        R.bz = bx->lo[2];
-        R.js = bx->hi[0] - bx->lo[0] + 1;
-        R.ks = R.js * (bx->hi[1] - bx->lo[1] + 1);
-        R.ns = R.ks * (bx->hi[2] - bx->lo[2] + 1);
-        R.ncomp = ns + 1;
-    }
-    a.Nv = Nv;
-    a.rxn = R;
-
-    PrepArgs pa;
-    pa.sb = a.sb;
-    pa.rxn = R;
-    pa.Nv = Nv;
-    for (int d = 0; d < 3; d++) {
-        pa.glo[d] = glo[d];
-        pa.ghi[d] = ghi[d];
-        pa.lo[d] = bx->lo[d];
-        pa.hi[d] = bx->hi[d];
-    }
-    pa.Tg = prm->Tg;
-    pa.do_reactions = prm->do_reactions;
-    pa.write_n = 1;
-    e = launch_prep(pa, prm->precision, ns, st);
-    if (e == cudaSuccess && a.elecenergy && !joule_in_tile(a, prm->precision))
-        e = launch_joule_pre(a, dim, prm->precision, st);
-    if (e == cudaSuccess) e = launch_transport(a, dim, prm->precision, st);
+    rc = launch_update(P, static_cast<char*>(scratch), st);
     cudaError_t e2 = cudaFreeAsync(scratch, st);
-    if (e != cudaSuccess) return cuda_fail(e, "fused update launch");
+    if (rc) return rc;
     if (e2 != cudaSuccess) return cuda_fail(e2, "scratch release");
     return VD_OK;
 }
@@ -707,18 +842,14 @@ int vd_time_scales(const vd_box* bx, vd_array4 state, const vd_params* prm, doub
     if (rc) return rc;
     if (!out) return fail(VD_ERR_ARG, "null output");
     if ((rc = check_params(bx, prm))) return rc;
-    vd_mech* m;
-    {
-        std::lock_guard<std::mutex> lk(g_mech_mu);
-        m = g_mech;
-    }
-    const int ns = m->nspecies;
+    const vd_host::MechInfo m = mech_snapshot();
+    const int ns = m.ns;
     std::string why;
     if (!covers(state, bx->lo, bx->hi, VD_NVAR(ns), &why)) return fail(VD_ERR_ARG, "state: %s", why.c_str());
     TransportArgs a;
-    fill_cfg(a, bx, prm, m);
+    fill_cfg(a, bx, prm, ns, m.e_id, m.charge[m.e_id]);
     unsigned long long* d = nullptr;
-    cudaError_t e = cudaMallocAsync(&d, 3 * sizeof(unsigned long long), st);
+    cudaError_t e = scratch_alloc(reinterpret_cast<void**>(&d), 3 * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return fail(VD_ERR_NOMEM, "3 words of scratch: %s", cudaGetErrorString(e));
     unsigned long long h[3] = {0, 0, 0};
     e = cudaMemsetAsync(d, 0, sizeof(h), st);
@@ -807,39 +938,9 @@ int vd_box_checksums(const vd_box* bx, vd_array4 rxn, vd_array4 phi_new, double*
 // Some hosts cannot let this library allocate device memory while they step: an
 // AMReX application usually gives most of the GPU to its own arena when it
 // starts, and some callers allow no allocation inside the time-step loop at all.
-// For them the scratch of the fused update lives in this fixed array instead of
-// coming from the stream-ordered allocator.  Every GPU that loads the library
-// holds the array until the process exits.  In host code the name below is only a
-// host-side stand-in, so its device address is looked up once per device (with
-// that device current) and passed to the kernels.
-namespace {
-
-constexpr size_t kNoallocDoubles = VD_NOALLOC_SCRATCH_BYTES / sizeof(double);
-static __device__ __align__(256) double g_noalloc_scratch[kNoallocDoubles];
-
-std::mutex g_noalloc_mu;
-double* g_noalloc_ptr[64] = {nullptr};  // device address of the array, per device
-
-// Once per device: find the array's device address.
-int noalloc_scratch_for_current_device(double** out)
-{
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-    if (dev < 0 || dev >= 64) return fail(VD_ERR_ARG, "device ordinal %d not supported", dev);
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
-        g_noalloc_ptr[dev] = static_cast<double*>(p);
-    }
-    *out = g_noalloc_ptr[dev];
-    return VD_OK;
-}
-
-}  // namespace
-
+// For them the scratch of the fused update lives in the fixed array
+// g_noalloc_scratch (top of this file), reserved and located per device by
+// setup_device, instead of coming from the scratch pool.
 extern "C" int vd_explicit_update_all_noalloc(const vd_box* bx, vd_array4 sborder, const vd_array4 efield_ec[3],
                                               const vd_array4 gradne_fc[3], vd_array4 phi_new, vd_array4 dsdt,
                                               vd_array4 rxn, const vd_params* prm, void* stream)
@@ -847,137 +948,25 @@ extern "C" int vd_explicit_update_all_noalloc(const vd_box* bx, vd_array4 sborde
     cudaStream_t st = (cudaStream_t)stream;
     int rc = ensure_mech_on_device(st);
     if (rc) return rc;
-    double* scratch = nullptr;
-    if ((rc = noalloc_scratch_for_current_device(&scratch))) return rc;
-    if ((rc = check_params(bx, prm))) return rc;
-    vd_mech* m;
-    {
-        std::lock_guard<std::mutex> lk(g_mech_mu);
-        m = g_mech;
-    }
-    const int ns = m->nspecies, dim = bx->dim;
-    const int H = stencil_halo(prm->hyp_order);
-    std::string why;
-    int glo[3] = {bx->lo[0], bx->lo[1], bx->lo[2]}, ghi[3] = {bx->hi[0], bx->hi[1], bx->hi[2]};
-    for (int d = 0; d < dim; d++) {
-        glo[d] -= H;
-        ghi[d] += H;
-    }
-    if (!covers(sborder, glo, ghi, VD_NVAR(ns), &why)) return fail(VD_ERR_GHOST, "sborder: %s", why.c_str());
-    if (!covers(phi_new, bx->lo, bx->hi, VD_NVAR(ns), &why)) return fail(VD_ERR_ARG, "phi_new: %s", why.c_str());
-    if (dsdt.p && !covers(dsdt, bx->lo, bx->hi, ns + 1, &why)) return fail(VD_ERR_ARG, "dsdt: %s", why.c_str());
-    if (rxn.p && !covers(rxn, bx->lo, bx->hi, ns + 1, &why)) return fail(VD_ERR_ARG, "rxn: %s", why.c_str());
-    if (prm->bg_mask >> ns) return fail(VD_ERR_ARG, "bg_mask names species >= %d", ns);
-    if (prm->bg_mask & (1ull << m->e_id)) return fail(VD_ERR_ARG, "electrons cannot be a background species");
-    if (prm->user_defined_vel && (prm->vel_species < 0 || prm->vel_species > ns))
-        return fail(VD_ERR_ARG, "vel_species invalid");
-    A4 ef[3], gne[3];
-    if (prm->elecenergy_solve) {
-        for (int d = 0; d < dim; d++) {
-            int fhi[3] = {bx->hi[0], bx->hi[1], bx->hi[2]};
-            fhi[d] += 1;
-            if (!prm->cs_technique) {
-                if (!efield_ec || !covers(efield_ec[d], bx->lo, fhi, 1, &why))
-                    return fail(VD_ERR_ARG, "efield_ec[%d]: %s", d, why.c_str());
-                ef[d] = A4(efield_ec[d]);
-            }
-            if (!prm->gradne_from_state) {
-                if (!gradne_fc || !covers(gradne_fc[d], bx->lo, fhi, 1, &why))
-                    return fail(VD_ERR_ARG, "gradne_fc[%d]: %s", d, why.c_str());
-                gne[d] = A4(gradne_fc[d]);
-            }
-        }
-    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    char* scratch = reinterpret_cast<char*>(g_noalloc_ptr[dev]);  // set by ensure_mech_on_device
+    if (!scratch) return fail(VD_ERR_STATE, "allocation-free scratch not set up on device %d", dev);
+    UpdatePlan P;
+    if ((rc = plan_update(bx, sborder, efield_ec, gradne_fc, phi_new, dsdt, rxn, prm, &P))) return rc;
     // scratch need, checked against the fixed array before anything is launched
-    const int64_t gn = (int64_t)(ghi[0] - glo[0] + 1) * (ghi[1] - glo[1] + 1) * (ghi[2] - glo[2] + 1);
-    const int64_t vn =
-        (int64_t)(bx->hi[0] - bx->lo[0] + 1) * (bx->hi[1] - bx->lo[1] + 1) * (bx->hi[2] - bx->lo[2] + 1);
-    const int64_t need = gn + (rxn.p ? 0 : vn * (ns + 1));
-    if (need > (int64_t)kNoallocDoubles)
+    const size_t need = P.scratch_bytes();
+    if (need > (size_t)VD_NOALLOC_SCRATCH_BYTES)
         return fail(VD_ERR_NOMEM,
-                    "box needs %lld bytes of scratch; the allocation-free update has %zu bytes "
-                    "(pass a rxn array to need %lld bytes, or use vd_explicit_update_all)",
-                    (long long)(need * 8), (size_t)VD_NOALLOC_SCRATCH_BYTES, (long long)(gn * 8));
-
-    TransportArgs a;
-    fill_cfg(a, bx, prm, m);
-    int tile[3];
-    transport_tile(dim, tile);
-    for (int d = 0; d < 3; d++) {
-        int n = bx->hi[d] - bx->lo[d] + 1;
-        a.ntile[d] = (n + tile[d] - 1) / tile[d];
-    }
-    a.sb = A4(sborder);
-    a.pn = A4(phi_new);
-    a.dsdt = dsdt.p ? A4(dsdt) : A4();
-    for (int d = 0; d < 3; d++) {
-        a.ef[d] = ef[d];
-        a.gne[d] = gne[d];
-    }
-    a.ntr = 0;
-    a.nbg = 0;
-    for (int s = 0; s <= ns; s++) {
-        bool energy = (s == ns);
-        if (energy && !prm->elecenergy_solve) continue;
-        if (!energy && ((prm->bg_mask >> s) & 1ull)) {
-            a.bg_sp[a.nbg++] = (int8_t)s;
-            continue;
-        }
-        a.tr_sp[a.ntr] = (int8_t)s;
-        a.tr_cls[a.ntr] = (int8_t)species_class(m, s);
-        bool has_vel = prm->user_defined_vel ? (s == prm->vel_species) : (m->mob_kind[s] != VD_MOB_ZERO);
-        a.tr_flux[a.ntr] = (prm->do_transport && has_vel) ? 1 : 0;
-        a.ntr++;
-    }
-    finish_lists(a);
-    A4 Nv;
-    Nv.p = scratch;
-    Nv.bx = glo[0];
-    Nv.by = glo[1];
-    Nv.bz = glo[2];
-    Nv.js = ghi[0] - glo[0] + 1;
-    Nv.ks = Nv.js * (ghi[1] - glo[1] + 1);
-    Nv.ns = Nv.ks * (ghi[2] - glo[2] + 1);
-    Nv.ncomp = 1;
-    A4 R;
-    if (rxn.p) {
-        R = A4(rxn);
-    } else {
-        R.p = scratch + gn;
-        R.bx = bx->lo[0];
-        R.by = bx->lo[1];
-        R.bz = bx->lo[2];
-        R.js = bx->hi[0] - bx->lo[0] + 1;
-        R.ks = R.js * (bx->hi[1] - bx->lo[1] + 1);
-        R.ns = R.ks * (bx->hi[2] - bx->lo[2] + 1);
-        R.ncomp = ns + 1;
-    }
-    a.Nv = Nv;
-    a.rxn = R;
-    PrepArgs pa;
-    pa.sb = a.sb;
-    pa.rxn = R;
-    pa.Nv = Nv;
-    for (int d = 0; d < 3; d++) {
-        pa.glo[d] = glo[d];
-        pa.ghi[d] = ghi[d];
-        pa.lo[d] = bx->lo[d];
-        pa.hi[d] = bx->hi[d];
-    }
-    pa.Tg = prm->Tg;
-    pa.do_reactions = prm->do_reactions;
-    pa.write_n = 1;
-    cudaError_t e = launch_prep(pa, prm->precision, ns, st);
-    if (e == cudaSuccess && a.elecenergy && !joule_in_tile(a, prm->precision))
-        e = launch_joule_pre(a, dim, prm->precision, st);
-    if (e == cudaSuccess) e = launch_transport(a, dim, prm->precision, st);
-    if (e != cudaSuccess) return cuda_fail(e, "allocation-free update launch");
-    return VD_OK;
+                    "box needs %zu bytes of scratch; the allocation-free update has %zu bytes "
+                    "(pass a rxn array to need %zu bytes, or use vd_explicit_update_all)",
+                    need, (size_t)VD_NOALLOC_SCRATCH_BYTES, kStatusBytes + (size_t)P.gn * sizeof(double));
+    return launch_update(P, scratch, st);
 }
 
 // ===========================================================================
 // Host services for the batch layer (vd_host.h).
-#include "vd_host.h"
 
 namespace vd_host {
 
@@ -994,13 +983,11 @@ double species_mw(int s)
 
 int mech_info(MechInfo* out)
 {
-    std::lock_guard<std::mutex> lk(g_mech_mu);
-    if (!g_mech) return fail(VD_ERR_MECH, "no mechanism loaded: call vd_mech_init first");
-    out->ns = g_mech->nspecies;
-    out->e_id = g_mech->e_id;
-    out->generation = g_mech_gen;
-    for (int s = 0; s <= g_mech->nspecies; s++) out->mob_kind[s] = g_mech->mob_kind[s];
-    for (int s = 0; s < g_mech->nspecies; s++) out->charge[s] = g_mech->charge[s];
+    {
+        std::lock_guard<std::mutex> lk(g_mech_mu);
+        if (!g_mech) return fail(VD_ERR_MECH, "no mechanism loaded: call vd_mech_init first");
+    }
+    *out = mech_snapshot();
     return VD_OK;
 }
 
@@ -1008,43 +995,16 @@ int check_update_params(const vd_box* bx, const vd_params* p, const MechInfo& m)
 {
     int rc = check_params(bx, p);
     if (rc) return rc;
-    if (p->bg_mask >> m.ns) return fail(VD_ERR_ARG, "bg_mask names species >= %d", m.ns);
-    if (p->bg_mask & (1ull << m.e_id)) return fail(VD_ERR_ARG, "electrons cannot be a background species");
-    if (p->user_defined_vel && (p->vel_species < 0 || p->vel_species > m.ns))
-        return fail(VD_ERR_ARG, "vel_species invalid");
-    if (!(p->dt >= 0.0) || !std::isfinite(p->dt)) return fail(VD_ERR_ARG, "dt must be finite and >= 0");
-    return VD_OK;
+    return check_update_species(p, m);
 }
 
 void fill_transport_args(TransportArgs& a, const vd_box* bx, const vd_params* p, const MechInfo& m)
 {
-    vd_mech* mm = new vd_mech;  // fill_cfg reads nspecies, e_id and the electron charge
-    memset(mm, 0, sizeof(vd_mech));
-    mm->nspecies = m.ns;
-    mm->e_id = m.e_id;
-    for (int s = 0; s < m.ns; s++) mm->charge[s] = m.charge[s];
-    fill_cfg(a, bx, p, mm);
-    delete mm;
-    const int ns = m.ns;
-    a.ntr = 0;
-    a.nbg = 0;
-    for (int s = 0; s <= ns; s++) {
-        bool energy = (s == ns);
-        if (energy && !p->elecenergy_solve) continue;
-        if (!energy && ((p->bg_mask >> s) & 1ull)) {
-            a.bg_sp[a.nbg++] = (int8_t)s;
-            continue;
-        }
-        a.tr_sp[a.ntr] = (int8_t)s;
-        int cls = energy ? VD_CLASS_ENERGY
-                         : (s == m.e_id ? VD_CLASS_ELECTRON : (m.charge[s] != 0 ? VD_CLASS_ION : VD_CLASS_NEUTRAL));
-        a.tr_cls[a.ntr] = (int8_t)cls;
-        bool has_vel = p->user_defined_vel ? (s == p->vel_species) : (m.mob_kind[s] != VD_MOB_ZERO);
-        a.tr_flux[a.ntr] = (p->do_transport && has_vel) ? 1 : 0;
-        a.ntr++;
-    }
-    finish_lists(a);
+    fill_cfg(a, bx, p, m.ns, m.e_id, m.charge[m.e_id]);
+    fill_species(a, p, m);
 }
+
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st) { return ::scratch_alloc(p, bytes, st); }
 
 int stencil_halo(int hyp_order) { return ::stencil_halo(hyp_order); }
 

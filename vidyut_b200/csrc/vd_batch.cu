@@ -158,6 +158,8 @@ struct Case {
     int cur;              // state copy (0/1) holding the current state
     int64_t steps_done;
     int64_t steps_left;   // < 0: no limit
+    int sslot;            // its word in vd_batch::d_status
+    bool failed;          // a NaN or infinity was met: takes no more steps
 };
 
 }  // namespace
@@ -180,6 +182,11 @@ struct vd_batch {
     PrepArgs* d_pr = nullptr;
     GhostArgs* d_gh = nullptr;
     int2* d_ctrl = nullptr;
+    // Non-finite status word per case (max_cases words; a case keeps its word
+    // while resident): the transport tiles set bit 0 when they meet a NaN or
+    // infinity (TransportArgs::status).
+    unsigned int* d_status = nullptr;
+    std::vector<int> free_sslot;
     int2* d_items = nullptr;
     size_t items_cap = 0;
     int n_prep = 0, n_ghost = 0, n_tr[4] = {0, 0, 0, 0}, n_jl[4] = {0, 0, 0, 0};
@@ -315,6 +322,7 @@ int rebuild(vd_batch* b)
             t = a;
             t.sb = sb;
             t.pn = pn;
+            t.status = b->d_status + k.sslot;
             PrepArgs& q = pr[(size_t)par * b->max_cases + c];
             q = p;
             q.sb = sb;
@@ -551,6 +559,9 @@ int vd_batch_create(vd_batch** out, int precision, uint64_t hbm_budget_bytes, in
     if (e == cudaSuccess) e = cudaMalloc(&b->d_pr, 2 * mc * sizeof(PrepArgs));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_gh, 2 * mc * sizeof(GhostArgs));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_ctrl, mc * sizeof(int2));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_status, mc * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemset(b->d_status, 0, mc * sizeof(unsigned int));
+    for (int q = max_cases - 1; q >= 0; q--) b->free_sslot.push_back(q);
     for (int s = 0; s < 2 && e == cudaSuccess; s++) {
         e = cudaMallocHost(&b->h_ctrl[s], mc * sizeof(int2));
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ctrl_done[s], cudaEventDisableTiming);
@@ -583,6 +594,7 @@ int vd_batch_destroy(vd_batch* b)
     cudaFree(b->d_pr);
     cudaFree(b->d_gh);
     cudaFree(b->d_ctrl);
+    cudaFree(b->d_status);
     cudaFree(b->d_items);
     for (int s = 0; s < 2; s++) {
         if (b->h_ctrl[s]) cudaFreeHost(b->h_ctrl[s]);
@@ -638,11 +650,14 @@ int vd_batch_add_case(vd_batch* b, const vd_box* bx, const double* state, const 
         if (L.has_ef) e = cudaMemcpyAsync(base + L.ef[d], efield_ec[d], fb, cudaMemcpyDefault, st);
         if (e == cudaSuccess && L.has_gne) e = cudaMemcpyAsync(base + L.gne[d], gradne_fc[d], fb, cudaMemcpyDefault, st);
     }
+    const int sslot = b->free_sslot.back();
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_status + sslot, 0, sizeof(unsigned int), st);
     if (e == cudaSuccess) e = cudaEventRecord(b->last_done, st);
     if (e != cudaSuccess) {
         b->arena.release(off, L.bytes);
         return cuda_err(e, "uploading the case");
     }
+    b->free_sslot.pop_back();
     b->pending = true;
     Case k;
     k.id = b->next_id++;
@@ -654,6 +669,8 @@ int vd_batch_add_case(vd_batch* b, const vd_box* bx, const double* state, const 
     k.cur = 0;
     k.steps_done = 0;
     k.steps_left = nsteps;
+    k.sslot = sslot;
+    k.failed = false;
     b->cases.push_back(k);
     b->dirty = true;
     *case_id = k.id;
@@ -668,6 +685,7 @@ int vd_batch_remove_case(vd_batch* b, int32_t case_id)
     int rc = settle(b);
     if (rc) return rc;
     b->arena.release(b->cases[c].off, b->cases[c].L.bytes);
+    b->free_sslot.push_back(b->cases[c].sslot);
     b->cases.erase(b->cases.begin() + c);
     b->dirty = true;
     return VD_OK;
@@ -685,6 +703,7 @@ int vd_batch_step(vd_batch* b, int nsteps, void* stream)
     int maxs = 0;
     for (int c = 0; c < nb; c++) {
         int64_t s = b->cases[c].steps_left < 0 ? nsteps : std::min<int64_t>(nsteps, b->cases[c].steps_left);
+        if (b->cases[c].failed) s = 0;
         steps[c] = (int)s;
         maxs = std::max(maxs, steps[c]);
     }
@@ -729,6 +748,22 @@ int vd_batch_case_info(vd_batch* b, int32_t case_id, int64_t* steps_done, int64_
     return VD_OK;
 }
 
+int vd_batch_case_status(vd_batch* b, int32_t case_id, int32_t* nonfinite)
+{
+    if (!b || !nonfinite) return err(VD_ERR_ARG, "null argument");
+    int rc = check_device(b);
+    if (rc) return rc;
+    int c = slot_of(b, case_id);
+    if (c < 0) return err(VD_ERR_ARG, "no case %d in the batch", case_id);
+    if ((rc = settle(b))) return rc;
+    unsigned int h = 0;
+    cudaError_t e = cudaMemcpy(&h, b->d_status + b->cases[c].sslot, sizeof(h), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_err(e, "reading the case status");
+    if (h) b->cases[c].failed = true;
+    *nonfinite = (h || b->cases[c].failed) ? 1 : 0;
+    return VD_OK;
+}
+
 int vd_batch_read_case(vd_batch* b, int32_t case_id, double* state, void* stream)
 {
     if (!b || !state) return err(VD_ERR_ARG, "null argument");
@@ -764,11 +799,13 @@ int vd_batch_load_case(vd_batch* b, int32_t case_id, const double* state, int64_
     char* oth = b->arena_base + k.off + k.L.st[k.cur ^ 1];
     if (e == cudaSuccess) e = cudaMemcpyAsync(cur, state, sbytes, cudaMemcpyDefault, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(oth, cur, sbytes, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_status + k.sslot, 0, sizeof(unsigned int), st);
     if (e == cudaSuccess) e = cudaEventRecord(b->last_done, st);
     if (e != cudaSuccess) return cuda_err(e, "loading the case");
     b->pending = true;
     k.steps_done = 0;
     k.steps_left = nsteps;
+    k.failed = false;
     return VD_OK;
 }
 
@@ -891,3 +928,23 @@ int vd_batch_get_stats(vd_batch* b, vd_batch_stats* out)
 }
 
 }  // extern "C"
+
+// ===========================================================================
+namespace vd_host {
+
+int batch_failed_cases(vd_batch* b, std::vector<int>* ids)
+{
+    ids->clear();
+    int rc = settle(b);
+    if (rc) return rc;
+    std::vector<unsigned int> h((size_t)b->max_cases);
+    cudaError_t e = cudaMemcpy(h.data(), b->d_status, h.size() * sizeof(unsigned int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_err(e, "reading the case statuses");
+    for (Case& k : b->cases) {
+        if (h[k.sslot]) k.failed = true;
+        if (k.failed) ids->push_back(k.id);
+    }
+    return VD_OK;
+}
+
+}  // namespace vd_host

@@ -652,7 +652,7 @@ extern "C" int vd_implicit_species_solve(const vd_box* bx, vd_array4 state, vd_a
         total += 2 * (size_t)plane[d];
     }
     double* buf = nullptr;
-    cudaError_t e = cudaMallocAsync(&buf, (total + 1) * sizeof(double) + 64, st);
+    cudaError_t e = vd_host::scratch_alloc(reinterpret_cast<void**>(&buf), (total + 1) * sizeof(double) + 64, st);
     if (e != cudaSuccess) return derr(VD_ERR_NOMEM, "solver scratch of %zu bytes: %s", total * 8, cudaGetErrorString(e));
     double* p = buf;
     for (auto& L : lv) {

@@ -1,6 +1,7 @@
 // vd_host.h -- host-side services of vd_abi.cu used by the batch layer (vd_batch.cu).
 #pragma once
 #include <cstdint>
+#include <vector>
 #include "../../include/vidyut_b200.h"
 #include "vd_kernels.cuh"
 
@@ -26,5 +27,11 @@ int check_update_params(const vd_box* bx, const vd_params* p, const MechInfo& m)
 // Fills the per-box transport record (everything but the array views and ntile).
 void fill_transport_args(vd::TransportArgs& a, const vd_box* bx, const vd_params* p, const MechInfo& m);
 int stencil_halo(int hyp_order);
+// Per-call scratch from the library's stream-ordered pool on the current device
+// (set up by ensure_mech); release it with cudaFreeAsync on the same stream.
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st);
+// Ids of the resident cases of a batch that met a NaN or infinity (vd_batch.cu);
+// waits for the batch's queued work.  Those cases take no further steps.
+int batch_failed_cases(vd_batch* b, std::vector<int>* ids);
 
 }  // namespace vd_host

@@ -45,6 +45,10 @@ struct TransportArgs {
     // zero-flux faces of a fluxed species: bit d set when its class has IHNEUBC at
     // the low domain face of direction d (zlo), bit 3 + d at the high one (zhi)
     int8_t fl_zm[VD_MAX_SPECIES + 1];
+    // Non-finite check (null: off).  The tile sets bit 0 of *status when a staged
+    // cell's E, Te or density sum, or an updated value of an own cell, is NaN or
+    // infinite; a NaN or infinity anywhere in a cell's inputs reaches one of them.
+    unsigned int* status;
 };
 
 // The mixed path evaluates the Joule faces inside the transport tile when the tile

@@ -383,9 +383,10 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
                                 void* stream)
 {
     cudaStream_t st = (cudaStream_t)stream;
-    vd_host::MechInfo m;
-    int rc = vd_host::mech_info(&m);
+    int rc = vd_host::ensure_mech(st);  // sets the device up (scratch pool)
     if (rc) return rc;
+    vd_host::MechInfo m;
+    if ((rc = vd_host::mech_info(&m))) return rc;
     if (!bx || !prm || !pp) return err(VD_ERR_ARG, "null argument");
     if ((rc = vd_host::check_update_params(bx, prm, m))) return rc;
     const int dim = bx->dim, ns = m.ns;
@@ -462,7 +463,7 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
     size_t total = 0;
     for (auto& L : lv) total += 3 * (size_t)L.cells();
     double* buf = nullptr;
-    cudaError_t e = cudaMallocAsync(&buf, (total + 1) * sizeof(double) + 64, st);
+    cudaError_t e = vd_host::scratch_alloc(reinterpret_cast<void**>(&buf), (total + 1) * sizeof(double) + 64, st);
     if (e != cudaSuccess) return err(VD_ERR_NOMEM, "multigrid scratch of %zu bytes: %s", total * 8, cudaGetErrorString(e));
     {
         double* p = buf;

@@ -183,9 +183,26 @@ void worker_main(vd_server* s)
             s->quanta++;
             s->graph_builds = bs.graph_builds;
         }
+        // cases that met a NaN or infinity fail (the reference aborts the run there)
+        std::vector<int> bad;
+        if ((rc = vd_host::batch_failed_cases(s->batch, &bad)) != VD_OK) {
+            fail_all(s, rc);
+            break;
+        }
         // retire
         std::vector<std::shared_ptr<Request>> keep;
         for (auto& r : s->resident) {
+            if (std::find(bad.begin(), bad.end(), r->case_id) != bad.end()) {
+                vd_batch_remove_case(s->batch, r->case_id);
+                std::lock_guard<std::mutex> lk(s->mu);
+                r->t_done = Clock::now();
+                r->status = VD_ERR_NONFINITE;
+                s->failed++;
+                for (int p = 0; p < 2; p++)
+                    for (int d = 0; d < 3; d++) std::vector<double>().swap(r->face[p][d]);
+                s->cv_done.notify_all();
+                continue;
+            }
             int64_t done = 0, left = 0;
             vd_batch_case_info(s->batch, r->case_id, &done, &left);
             if (left != 0) {

@@ -49,13 +49,7 @@ __device__ __forceinline__ double joule_cell(const TransportArgs& a, int dim, in
             const double* p = a.sb.p;
             const int64_t cs = a.sb.ns;
             double etemp = 0.5 * (p[ol + VD_ETEMP(ns) * cs] + p[orr + VD_ETEMP(ns) * cs]);
-            double Esum = 0.0, evf_d = 0.0;
-            for (int d = 0; d < dim; d++) {
-                double e = 0.5 * (p[ol + (VD_EFX(ns) + d) * cs] + p[orr + (VD_EFX(ns) + d) * cs]);
-                Esum += e * e;
-                if (d == idim) evf_d = e;
-            }
-            (void)Esum;
+            const double evf_d = 0.5 * (p[ol + (VD_EFX(ns) + idim) * cs] + p[orr + (VD_EFX(ns) + idim) * cs]);
             double nel = p[ol + eidx * cs], ner = p[orr + eidx * cs];
             double ne = 0.5 * (nel + ner);
             double ef = a.cs_technique ? evf_d : a.ef[idim](face[0], face[1], face[2]);
@@ -359,6 +353,7 @@ __device__ __forceinline__ void stage_basis(const TransportArgs& a, int cc, cons
         const double E = p[(VD_EFX(ns) + D) * cs];
         N = a.Nv(g[0], g[1], g[2]);
         Te = p[VD_ETEMP(ns) * cs];
+        if (a.status && !(isfinite(E) && isfinite(Te) && isfinite(N))) atomicOr(a.status, 1u);
         if (joule_staged<DIM, PREC>() && jst) ne = p[a.e_id * cs];
         for (int k = 0; k < a.nb; k++) {
             const int kind = a.bkind[k];
@@ -562,6 +557,7 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
             const double lo = (s == a.e_id) ? a.min_elec : a.min_spec;
             if (nn < lo) nn = lo;
         }
+        if (a.status && !isfinite(nn)) atomicOr(a.status, 1u);
         a.pn(gi, gj, gk, s) = nn;
         if (a.dsdt.p) a.dsdt(gi, gj, gk, s) = acc;
         if (s == a.e_id) ne_new = nn;
@@ -709,6 +705,7 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
                 v += r * a.dt;
                 if (v < a.min_spec && a.bound_specden) v = a.min_spec;
             }
+            if (a.status && !isfinite(v)) atomicOr(a.status, 1u);
             a.pn(gi, gj, gk, s) = v;
             if (a.dsdt.p) a.dsdt(gi, gj, gk, s) = r;
         }

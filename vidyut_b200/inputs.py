@@ -71,7 +71,7 @@ def make_params(dim, dx, n, dt=1e-12, Tg=300.0, Pg=101325.0, hyp_order=5, weno_s
                 cs_technique=0, bound_specden=0, ele_mob=0.0, ele_diff=0.0, min_species_density=1e10,
                 min_electron_density=1e10, min_electron_temp=300.0, update_te=0, gradne_from_state=0,
                 user_defined_vel=0, user_vel=(0.0, 0.0, 0.0), vel_species=0, time=0.0,
-                bc_lo=None, bc_hi=None) -> abi.VdParams:
+                bc_lo=None, bc_hi=None, check_finite=0) -> abi.VdParams:
     p = abi.VdParams()
     p.dim = dim
     p.hyp_order = hyp_order
@@ -104,6 +104,7 @@ def make_params(dim, dx, n, dt=1e-12, Tg=300.0, Pg=101325.0, hyp_order=5, weno_s
     p.bg_mask = bg_mask
     p.update_te = update_te
     p.gradne_from_state = gradne_from_state
+    p.check_finite = check_finite
     return p
 
 

@@ -93,19 +93,17 @@ class Slab:
         if self.world == 1 and not self.periodic:
             return
         g = self.ghost
+        ax = 3 - self.axis                     # tensor axis of the split direction
+        n = state.shape[ax] - 2 * g            # valid planes of this slab
+        if n < g:
+            raise ValueError(f"slab of {n} planes is thinner than the {g} ghost planes")
         if self.world == 1:
             # one rank, periodic: the wrap is local
-            ax = 3 - self.axis
-            n = state.shape[ax] - 2 * g
             lo_src = state.narrow(ax, n, g).clone()
             hi_src = state.narrow(ax, g, g).clone()
             state.narrow(ax, 0, g).copy_(lo_src)
             state.narrow(ax, n + g, g).copy_(hi_src)
             return
-        ax = 3 - self.axis                     # tensor axis of the split direction
-        n = state.shape[ax] - 2 * g            # valid planes of this slab
-        if n < g:
-            raise ValueError(f"slab of {n} planes is thinner than the {g} ghost planes")
         below, above = self.neighbours()
         send_lo = state.narrow(ax, g, g).contiguous()          # first valid planes, to the rank below
         send_hi = state.narrow(ax, n, g).contiguous()          # last valid planes, to the rank above
