@@ -8,15 +8,19 @@ n += dt*(-div F + S) per "step".  The state (134^3 x 34 comps, 654 MB) and the s
 face fields are larger than the 126 MB L2, so every step streams them from HBM.
 
 One JSON line on rank 0:
-  value        cell-updates/s of the mixed-precision fused update (inputs resident)
-  e2e          the same through the C ABI with the step's inputs copied from pinned
-               host memory and its updated densities copied back, inside the timing
-  fp64         the plain-FP64 fused update on the same inputs, and the per-species
-               error of the mixed result against it
+  value        cell-updates/s of the plain FP64 fused update (inputs resident), the
+               same arithmetic as the reference's CPU code
+  e2e          the same through the C ABI with each step's inputs copied from
+               pinned host memory and its updated densities copied back, inside the
+               timing (double-buffered copy streams)
   roofline     dominant kernel: algorithmic bytes / average launch time vs the
-               measured HBM copy bandwidth
-  cpu_baseline the reference's own hot-path code (oracle/_ref, all host cores) on a
-               bounded slab of the same workload
+               measured HBM copy bandwidth; roofline_compute: its issue and pipe
+               fractions from the committed ncu summaries
+  cpu_baseline the reference's own hot-path code (oracle/_ref) on all host cores
+               and on one core, on a bounded slab of the same workload
+  summary      compact figures of every path (mixed, batched, serving, large)
+  mixed        the mixed-precision path on the same inputs, with its error against
+               FP64 per species at the end of the line
 Multi-GPU: one process per GPU, each updating its own box (independent boxes, as
 AMReX distributes boxes over ranks; no data-path collective); value sums the
 cells of all ranks over the slowest rank's time.
@@ -83,6 +87,14 @@ def make_case(workload: str, rank: int = 0):
     if workload == "precision3d":
         return vin.config_precision3d(seed=seed) if rank else vin.config_precision3d()
     return vin.config_argon2d(seed=seed) if rank else vin.config_argon2d()
+
+
+def box_config(case, workload: str, world: int) -> dict:
+    """The config object of a one-box workload line (both arms print the same)."""
+    return {"workload": WORKLOADS[workload], "cells_per_gpu": case.ncell, "species": case.mech.ns,
+            "reactions": len(case.mech.reactions), "dim": case.dim, "hyp_order": 5, "weno_scheme": 3,
+            "precision": "fp64", "l2": "inputs larger than L2 (state + faces stream from HBM every step)",
+            "parallelism": f"{world} independent boxes (one per GPU)"}
 
 
 def ref_case_name(case) -> str:
@@ -206,8 +218,7 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": WORKLOADS[args.workload], "cells": case.ncell, "species": case.mech.ns,
-                       "reactions": len(case.mech.reactions)},
+            "config": box_config(case, args.workload, args.gpus),
             "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": kind,
                              "sample": sample},
             "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -323,6 +334,133 @@ def read_profile_traffic(kernel: str, workload: str):
     return None
 
 
+def read_profile_metrics(kernel: str, workload: str) -> dict | None:
+    """Pipe and issue fractions of one kernel from the committed ncu summary
+    (profiles/<kernel>_<workload>.md, lines ``metric_<name>: value``), if any."""
+    p = ROOT / "profiles" / f"{kernel}_{workload}.md"
+    if not p.exists():
+        return None
+    out = {}
+    for line in p.read_text().splitlines():
+        line = line.strip()
+        if line.startswith("metric_") and ":" in line:
+            k, v = line.split(":", 1)
+            try:
+                out[k[len("metric_"):].strip()] = float(v.split()[0])
+            except (ValueError, IndexError):
+                continue
+    if not out:
+        return None
+    out["source"] = f"profiles/{p.name}"
+    return out
+
+
+def hbm_peak():
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    hbm = peaks.get("hbm_gbs")
+    return (hbm, "measured") if hbm else (6650.0, "fallback")
+
+
+def e2e_pipelined(case, prm, nsteps: int, world: int, barrier, max_over_ranks) -> dict:
+    """cell-updates/s through vd_explicit_update_all with host buffers: every step
+    copies its inputs from pinned host memory (the components the update reads:
+    species, EEN and Te, the D cell field components, the 2D face arrays) and its
+    result (the NS+1 updated densities and energy) back to pinned host memory.
+    Double-buffered on three streams, so that step k+1's upload and step k-1's
+    download overlap step k's update; the timed region runs from the first upload
+    to the last download."""
+    import torch
+
+    from vidyut_b200 import _abi as abi
+    from vidyut_b200 import api
+
+    ns, dim = case.mech.ns, case.dim
+    efx = abi.EFX(ns)
+    h_state = torch.from_numpy(case.state).pin_memory()
+    h_ef = [torch.from_numpy(a).pin_memory() for a in case.efield[:dim]]
+    h_gn = [torch.from_numpy(a).pin_memory() for a in case.gradne[:dim]]
+    dcs = [api.upload(case), api.upload(case)]
+    phis = [dcs[0].new_outputs()[0], dcs[1].new_outputs()[0]]
+    h_out = [torch.empty((ns + 1,) + tuple(phis[0].shape[1:]), dtype=torch.float64).pin_memory() for _ in range(2)]
+    need_ef = prm.elecenergy_solve and not prm.cs_technique
+    need_gn = prm.elecenergy_solve and not prm.gradne_from_state
+    h2d = 8 * (h_state[:ns + 2].numel() + h_state[efx:efx + dim].numel()
+               + (sum(a.numel() for a in h_ef) if need_ef else 0) + (sum(a.numel() for a in h_gn) if need_gn else 0))
+    d2h = 8 * h_out[0].numel()
+    comp = torch.cuda.current_stream()
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    ev = {k: [torch.cuda.Event(), torch.cuda.Event()] for k in ("h2d", "comp", "d2h")}
+    for k in ev:
+        for e in ev[k]:
+            e.record(comp)
+
+    def step(k):
+        b = k & 1
+        dc = dcs[b]
+        s_in.wait_event(ev["comp"][b])          # step k-2 has finished reading buffer b
+        with torch.cuda.stream(s_in):
+            dc.state[:ns + 2].copy_(h_state[:ns + 2], non_blocking=True)
+            dc.state[efx:efx + dim].copy_(h_state[efx:efx + dim], non_blocking=True)
+            for d in range(dim):
+                if need_ef:
+                    dc.efield[d].copy_(h_ef[d], non_blocking=True)
+                if need_gn:
+                    dc.gradne[d].copy_(h_gn[d], non_blocking=True)
+        ev["h2d"][b].record(s_in)
+        comp.wait_event(ev["h2d"][b])
+        comp.wait_event(ev["d2h"][b])           # step k-2's result has left phis[b]
+        api.explicit_update_all(dc, prm, phis[b], stream=comp)
+        ev["comp"][b].record(comp)
+        s_out.wait_event(ev["comp"][b])
+        with torch.cuda.stream(s_out):
+            h_out[b].copy_(phis[b][:ns + 1], non_blocking=True)
+        ev["d2h"][b].record(s_out)
+
+    for k in range(3):
+        step(k)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s_in)
+    for k in range(nsteps):
+        step(k)
+    e1.record(s_out)
+    torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1)) / nsteps
+    del dcs, phis
+    return {"value": world * case.ncell / (ms * 1e-3), "unit": "cell-updates/s", "ms_per_step": ms,
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "path": "vd_explicit_update_all; per step the inputs it reads from pinned host memory and its "
+                    "updated densities back, double-buffered on copy streams, inside the timing"}
+
+
+def cpu_baselines(case, seconds: float) -> dict:
+    """The reference build on all host cores, and on one core, each on a bounded
+    slab of the same workload."""
+    threads = os.cpu_count() or 1
+    lib, kind, run, nplanes, cpp = cpu_reference_rate(case, seconds)
+    t = run(nplanes)
+    cpu = {"value": nplanes * cpp / t, "unit": "cell-updates/s", "cores": threads, "kind": kind,
+           "sample": f"{nplanes} of {case.n[case.dim - 1]} planes ({nplanes * cpp} cells), one step, {t:.1f} s"}
+    import ctypes
+    try:
+        gomp = ctypes.CDLL("libgomp.so.1")
+        gomp.omp_set_num_threads(1)
+        _, _, run1, np1, cpp1 = cpu_reference_rate(case, seconds / 2, warm=False)
+        t1 = run1(np1)
+        gomp.omp_set_num_threads(threads)
+        cpu["one_core"] = {"value": np1 * cpp1 / t1, "unit": "cell-updates/s", "cores": 1, "kind": kind,
+                           "sample": f"{np1} planes ({np1 * cpp1} cells), one step, {t1:.1f} s"}
+    except OSError:
+        cpu["one_core"] = None
+    return cpu
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -377,6 +515,15 @@ def run_ours(args):
         ms = e0.elapsed_time(e1)
         return max_over_ranks(ms) / steps, L.vd_launch_count() - n0
 
+    def kernel_profile(prm, steps):
+        L.vd_profile_enable(1)
+        for _ in range(steps):
+            api.explicit_update_all(dc, prm, phi_new)
+        torch.cuda.synchronize()
+        prof = abi.profile_read()
+        L.vd_profile_enable(0)
+        return prof
+
     if args.only_update:
         prm = prm_mixed if args.precision == "mixed" else prm_fp64
         ms, launches = timed(prm, args.steps, args.warmup)
@@ -387,29 +534,18 @@ def run_ours(args):
             dist.destroy_process_group()
         return 0
 
+    # headline: the plain FP64 path (the reference's own arithmetic)
     clock = ClockSampler(local)
     clock.start()
-    ms_mixed, launches = timed(prm_mixed, args.steps, args.warmup)
+    ms_fp64, launches = timed(prm_fp64, args.steps, args.warmup)
     clocks = clock.stop()
     cells = case.ncell
-    value = world * cells / (ms_mixed * 1e-3)
+    value = world * cells / (ms_fp64 * 1e-3)
+    prof64 = kernel_profile(prm_fp64, args.steps)
 
-    # per-kernel device time of the same steps (CUDA events on the launch stream)
-    L.vd_profile_enable(1)
-    for _ in range(args.steps):
-        api.explicit_update_all(dc, prm_mixed, phi_new)
-    torch.cuda.synchronize()
-    prof = abi.profile_read()
-    L.vd_profile_enable(0)
-
-    # plain FP64 path on the same inputs
-    fp64_steps = max(2, args.steps // 2)
-    ms_fp64, _ = timed(prm_fp64, fp64_steps, 1)
-    L.vd_profile_enable(1)
-    api.explicit_update_all(dc, prm_fp64, phi_new)
-    torch.cuda.synchronize()
-    prof64 = abi.profile_read()
-    L.vd_profile_enable(0)
+    # the mixed-precision path on the same inputs
+    ms_mixed, launches_mixed = timed(prm_mixed, args.steps, args.warmup)
+    prof_mixed = kernel_profile(prm_mixed, args.steps)
 
     # per-species error of the mixed result against the FP64 result (which matches
     # the CPU oracle to 1e-12, tests/test_gpu_parity.py)
@@ -427,137 +563,125 @@ def run_ours(args):
     err_scaled = srel.max(dim=1).values.cpu().numpy()
     err_l2 = ((diff ** 2).reshape(ns + 1, -1).sum(1).sqrt() /
               (ref64 ** 2).reshape(ns + 1, -1).sum(1).sqrt()).cpu().numpy()
-    del dsdt64
+    del dsdt64, ref64, diff, rel, srel
 
-    # end to end through the C ABI: pinned host inputs -> device -> update -> host
-    e2e = None
+    # end to end through the C ABI with host buffers, both precisions
+    e2e = e2e_mixed = None
     if not args.no_e2e:
-        h_state = torch.from_numpy(case.state).pin_memory()
-        h_ef = [torch.from_numpy(a).pin_memory() for a in case.efield]
-        h_gn = [torch.from_numpy(a).pin_memory() for a in case.gradne]
-        h_out = torch.empty((ns + 1,) + tuple(phi_new.shape[1:]), dtype=torch.float64).pin_memory()
-        h2d = h_state.numel() * 8 + sum(a.numel() * 8 for a in h_ef[:case.dim] + h_gn[:case.dim])
-        d2h = h_out.numel() * 8
-
-        def e2e_step():
-            dc.state.copy_(h_state, non_blocking=True)
-            for d in range(case.dim):
-                dc.efield[d].copy_(h_ef[d], non_blocking=True)
-                dc.gradne[d].copy_(h_gn[d], non_blocking=True)
-            api.explicit_update_all(dc, prm_mixed, phi_new)
-            h_out.copy_(phi_new[:ns + 1], non_blocking=True)
-
-        e2e_steps = max(3, args.steps // 2)
-        for _ in range(2):
-            e2e_step()
-        torch.cuda.synchronize()
-        barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(e2e_steps):
-            e2e_step()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-        ms_e2e = max_over_ranks(e0.elapsed_time(e1)) / e2e_steps
-        e2e = {"value": world * cells / (ms_e2e * 1e-3), "unit": "cell-updates/s", "ms_per_step": ms_e2e,
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "path": "vd_explicit_update_all with pinned-host copies in the timed region"}
+        dc = phi_new = None
+        torch.cuda.empty_cache()
+        n_e2e = max(4, args.steps // 2)
+        e2e = e2e_pipelined(case, prm_fp64, n_e2e, world, barrier, max_over_ranks)
+        e2e_mixed = e2e_pipelined(case, prm_mixed, n_e2e, world, barrier, max_over_ranks)
+        torch.cuda.empty_cache()
 
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
         return 0
 
-    # roofline of the dominant kernel
-    peaks = {}
-    pk = ROOT / "MEASURED_PEAKS.json"
-    if pk.exists():
-        peaks = json.loads(pk.read_text())
-    hbm = peaks.get("hbm_gbs")
-    peak_src = "measured" if hbm else "fallback"
-    hbm = hbm or 6650.0
-    dom = max(prof.items(), key=lambda kv: kv[1][1])
-    kname, (kcount, kms) = dom
+    # roofline of the dominant kernel of each path
+    hbm, peak_src = hbm_peak()
     alg = algorithmic_bytes_per_cell(case)
-    per_launch_ms = kms / kcount
-    bytes_per_launch = alg.get(kname, alg["step"]) * cells
-    achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
-    traffic = read_profile_traffic(kname, args.workload)
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": traffic, "kernel": kname, "peak_source": peak_src,
-                "kernel_ms": per_launch_ms,
-                "kernel_share": kms / sum(v[1] for v in prof.values()),
-                "step_achieved_gbs": alg["step"] * cells / (ms_mixed * 1e-3) / 1e9}
 
-    batched = None
-    if not args.no_batched and world == 1 and args.workload == "precision3d":
-        dc = phi_new = None  # free the 3-D case's device memory
-        torch.cuda.empty_cache()
-        r = measure_batched(args.steps, args.warmup, e2e=not args.no_e2e)
-        api.mech_init(case.mech)
-        batched = {k: r[k] for k in ("value", "ms_per_solve", "solves_per_s", "cases", "cells", "steps_per_solve",
-                                     "speedup_vs_plain_fp64", "plain_fp64", "batched_fp64",
-                                     "mixed_vs_fp64_max_rel", "roofline", "tile_2d", "gpu_launches", "e2e",
-                                     "kernels_ms_per_launch") if k in r}
-        batched["unit"] = "cell-updates/s"
-        batched["workload"] = WORKLOADS["batched"]
+    def roof(prof, ms_step, workload_tag):
+        kname, (kcount, kms) = max(prof.items(), key=lambda kv: kv[1][1])
+        per_launch_ms = kms / kcount
+        achieved = alg.get(kname, alg["step"]) * cells / (per_launch_ms * 1e-3) / 1e9
+        return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": read_profile_traffic(kname, workload_tag), "kernel": kname, "peak_source": peak_src,
+                "kernel_ms": per_launch_ms, "kernel_share": kms / sum(v[1] for v in prof.values()),
+                "alg_bytes_per_cell": alg.get(kname, alg["step"]),
+                "step_achieved_gbs": alg["step"] * cells / (ms_step * 1e-3) / 1e9}
 
-    serving = None
-    if not args.no_serving and world == 1 and args.workload == "precision3d":
+    roofline = roof(prof64, ms_fp64, f"{args.workload}_fp64")
+    roofline_mixed = roof(prof_mixed, ms_mixed, args.workload)
+    roofline_compute = {}
+    for k, tag in (("k_transport", f"{args.workload}_fp64"), ("k_prep_spec", f"{args.workload}_fp64"),
+                   ("k_transport", args.workload), ("k_prep_spec", args.workload)):
+        m = read_profile_metrics(k, tag)
+        if m:
+            roofline_compute[f"{k}_{'fp64' if tag.endswith('fp64') else 'mixed'}"] = m
+
+    batched = serving = large = None
+    if world == 1 and args.workload == "precision3d":
         dc = phi_new = None
         torch.cuda.empty_cache()
-        serving = measure_serving(args.requests, args.budget_gb)
-        serving.pop("clocks", None)
-        serving["workload"] = WORKLOADS["serving"]
-        api.mech_init(case.mech)
-
-    large = None
-    if not args.no_large and world == 1 and args.workload == "precision3d":
-        dc = phi_new = None
-        torch.cuda.empty_cache()
-        large = measure_large(100, 3, n=args.large_n)
-        large.pop("clocks", None)
-        large["workload"] = WORKLOADS["large"].replace("384^3", f"{args.large_n}^3")
-        torch.cuda.empty_cache()
-        api.mech_init(case.mech)
+        if not args.no_batched:
+            r = measure_batched(args.steps, args.warmup, e2e=not args.no_e2e)
+            api.mech_init(case.mech)
+            batched = {k: r[k] for k in ("speedup_vs_plain_fp64", "value", "ms_per_solve", "solves_per_s", "cases",
+                                         "cells", "steps_per_solve", "plain_fp64", "batched_fp64",
+                                         "mixed_vs_fp64_max_rel", "roofline", "tile_2d", "gpu_launches", "e2e",
+                                         "kernels_ms_per_launch") if k in r}
+            batched["unit"] = "cell-updates/s"
+            batched["workload"] = WORKLOADS["batched"]
+            torch.cuda.empty_cache()
+        if not args.no_serving:
+            serving = measure_serving(args.requests, args.budget_gb)
+            serving.pop("clocks", None)
+            serving["workload"] = WORKLOADS["serving"]
+            api.mech_init(case.mech)
+            torch.cuda.empty_cache()
+        if not args.no_large:
+            large = measure_large(100, 3, n=args.large_n)
+            large.pop("clocks", None)
+            large["workload"] = WORKLOADS["large"].replace("384^3", f"{args.large_n}^3")
+            torch.cuda.empty_cache()
+            api.mech_init(case.mech)
 
     cpu = None
     if not args.no_cpu_baseline and world == 1:
-        threads = os.cpu_count() or 1
-        lib, kind, run, nplanes, cpp = cpu_reference_rate(case, args.cpu_seconds)
-        t = run(nplanes)
-        cpu = {"value": nplanes * cpp / t, "unit": "cell-updates/s", "cores": threads, "kind": kind,
-               "sample": f"{nplanes} of {case.n[case.dim - 1]} planes ({nplanes * cpp} cells), one step, "
-                         f"{t:.1f} s"}
+        cpu = cpu_baselines(case, args.cpu_seconds)
+
+    # compact figures first (a reader of a truncated line keeps them), long arrays last
+    summary = {
+        "fp64_ms_per_step": ms_fp64, "mixed_ms_per_step": ms_mixed, "mixed_speedup_vs_fp64": ms_fp64 / ms_mixed,
+        "mixed_max_rel_vs_fp64": float(np.max(err_max)),
+        "e2e_fp64_ms_per_step": e2e["ms_per_step"] if e2e else None,
+        "e2e_mixed_ms_per_step": e2e_mixed["ms_per_step"] if e2e_mixed else None,
+        "cpu_cores_value": cpu["value"] if cpu else None,
+        "cpu_one_core_value": (cpu.get("one_core") or {}).get("value") if cpu else None,
+    }
+    if batched:
+        summary.update({"batched_mixed_speedup_vs_plain_fp64": batched.get("speedup_vs_plain_fp64"),
+                        "batched_ms_per_solve": batched.get("ms_per_solve"),
+                        "batched_max_rel_vs_fp64": batched.get("mixed_vs_fp64_max_rel", {}).get("max")})
+    if serving:
+        summary.update({"serving_solves_per_s": serving.get("solves_per_s"), "serving_p50_ms": serving.get("p50_ms"),
+                        "serving_p99_ms": serving.get("p99_ms"),
+                        "serving_speedup_vs_plain_fp64": serving.get("speedup_solves_vs_plain_fp64")})
+    if large:
+        summary.update({"large_ms_per_step": large.get("ms_per_step"),
+                        "large_max_rel_vs_fp64": (large.get("mixed_vs_fp64_max_rel") or {}).get("max")})
 
     line = {
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 (mixed: FP32 WENO, rates, fluxes; FP64 accumulate)",
-        "data": "synthetic",
-        "config": {"workload": WORKLOADS[args.workload], "cells_per_gpu": cells, "species": ns,
-                   "reactions": len(case.mech.reactions), "dim": case.dim, "hyp_order": 5, "weno_scheme": 3,
-                   "precision": "mixed", "l2": "inputs larger than L2 (state + faces stream from HBM every step)",
-                   "parallelism": f"{world} independent boxes (one per GPU)"},
-        "roofline": roofline,
-        "cpu_baseline": cpu,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_fp64, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": box_config(case, args.workload, world),
         "e2e": e2e,
+        "roofline": roofline,
+        "roofline_compute": roofline_compute or None,
+        "cpu_baseline": cpu,
         "gpu_launches": int(launches),
         "clocks": clocks,
-        "fp64": {"value": world * cells / (ms_fp64 * 1e-3), "ms_per_step": ms_fp64,
-                 "mixed_speedup": ms_fp64 / ms_mixed,
-                 "kernels_ms": {k: v[1] / v[0] for k, v in prof64.items()}},
-        "kernels_ms": {k: v[1] / v[0] for k, v in prof.items()},
-        "mixed_vs_fp64_error": {"against": "FP64 GPU result (matches the CPU oracle to 1e-12)",
-                                "max_rel_per_species": [float(x) for x in err_max],
-                                "l2_rel_per_species": [float(x) for x in err_l2],
-                                "max_rel_to_step_scale_per_species": [float(x) for x in err_scaled],
-                                "max_rel": float(np.max(err_max)),
-                                "max_rel_to_step_scale": float(np.max(err_scaled))},
+        "summary": summary,
+        "mixed": {"value": world * cells / (ms_mixed * 1e-3), "ms_per_step": ms_mixed,
+                  "speedup_vs_fp64": ms_fp64 / ms_mixed, "e2e": e2e_mixed, "roofline": roofline_mixed,
+                  "gpu_launches": int(launches_mixed),
+                  "dtype": "f32/f64 (FP32 WENO, rates, flux arithmetic; FP64 accumulate)",
+                  "max_rel_vs_fp64": float(np.max(err_max)),
+                  "max_rel_to_step_scale": float(np.max(err_scaled))},
+        "kernels_ms_fp64": {k: v[1] / v[0] for k, v in prof64.items()},
+        "kernels_ms_mixed": {k: v[1] / v[0] for k, v in prof_mixed.items()},
         "batched": batched,
         "serving": serving,
         "large": large,
+        "mixed_vs_fp64_error": {"against": "FP64 GPU result (matches the CPU oracle to 1e-12)",
+                                "max_rel_per_species": [float(x) for x in err_max],
+                                "l2_rel_per_species": [float(x) for x in err_l2],
+                                "max_rel_to_step_scale_per_species": [float(x) for x in err_scaled]},
     }
     print(json.dumps(line), flush=True)
     return 0

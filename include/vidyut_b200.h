@@ -211,7 +211,9 @@ typedef struct vd_params {
 /* ---- library ------------------------------------------------------------- */
 int         vd_abi_version(void);
 /* sizeof of the ABI structs, for binding checks: which = 0 vd_array4, 1 vd_box,
- * 2 vd_reaction, 3 vd_mech, 4 vd_params (no reference counterpart).           */
+ * 2 vd_reaction, 3 vd_mech, 4 vd_params, 5 vd_poisson_params,
+ * 6 vd_diffusion_params, 7 vd_batch_stats, 8 vd_server_stats (no reference
+ * counterpart).                                                                  */
 size_t      vd_sizeof(int which);
 const char* vd_last_error(void);           /* text of the last failure on this thread */
 const char* vd_status_string(int status);
@@ -340,14 +342,18 @@ int vd_fill_ghosts(const vd_box* bx, vd_array4 state, int ghost, const int32_t* 
  * EFX..EFZ (centred differences, one-sided at domain faces), REF (|E|/N in Td) in
  * the valid cells and refills their ghosts, and efield_ec[d] = -dphi/dx_d on the
  * face boxes (Dirichlet faces: to the face value over half a cell; unless
- * prm->cs_technique).  Scratch (3 doubles per cell over the hierarchy) comes from
- * the stream-ordered allocator. */
+ * prm->cs_technique).  user_rhs (p == NULL: none) is added to the right-hand side
+ * cell by cell (one component covering the box, in the units of del^2 phi): the
+ * reference's user_sources::add_user_potential_sources
+ * (Source/PotentialSolve.cpp:220-222).  Scratch (3 doubles per cell over the
+ * hierarchy) comes from the library's stream-ordered pool. */
 typedef struct {
     int32_t bc_lo[3], bc_hi[3];
     double  value_lo[3], value_hi[3];
     int32_t max_vcycles;
     int32_t pad0;
     double  tol_rel;
+    vd_array4 user_rhs;
 } vd_poisson_params;
 int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_array4 efield_ec[3],
                      const vd_params* prm, const vd_poisson_params* pp,
@@ -379,6 +385,14 @@ typedef struct {
     int32_t max_vcycles;
     int32_t pad0;
     double  tol_rel;
+    /* 1: the domain faces take the given Robin coefficients instead of species_bc:
+     * a n + b dn/dnu = f on the face, nu the outward normal ([side][direction],
+     * side 0 low, 1 high); the reference's case files set them through
+     * user_transport::species_bc (e.g. test/verification/MMS/UserFunctions.H:60-104),
+     * whose robin_a/b/f arrays MLMG reads.  a = 1, b = 0 holds the value f.       */
+    int32_t user_robin;
+    int32_t pad1;
+    double  robin_a[2][3], robin_b[2][3], robin_f[2][3];
 } vd_diffusion_params;
 int vd_implicit_species_solve(const vd_box* bx, vd_array4 state, vd_array4 state_old, vd_array4 dsdt,
                               vd_array4 phi_new, const vd_array4 gradne_fc[3], const vd_params* prm,

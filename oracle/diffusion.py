@@ -108,10 +108,14 @@ def boundary_value(case, spec, d, sgn, face_cell, Tg, port, mw):
     return -flx / D
 
 
-def solve(case, spec, state_old, dsdt, prm, port):
+def solve(case, spec, state_old, dsdt, prm, port, robin=None):
     """Solution on the valid cells (nz, ny, nx), plus the electron face gradients
     (list per direction, (nz, ny, nx) with +1 along d) when spec is the electrons,
-    and the Te that the energy solve writes (or None)."""
+    and the Te that the energy solve writes (or None).  robin: the case's own
+    species_bc coefficients ((a_lo, b_lo, f_lo), (a_hi, b_hi, f_hi)), one value
+    per direction each: a n + b dn/dnu = f on the face (nu the outward normal),
+    with the face value (n_c + n_g)/2 and dn/dnu = (n_g - n_c)/dx between the cell
+    and its ghost, as MLMG's Robin faces; None: species_bc's values."""
     from vidyut_b200 import _abi as abi
     mech, dim, n, dx, g = case.mech, case.dim, case.n, case.dx, case.gvec
     ns = mech.ns
@@ -157,6 +161,14 @@ def solve(case, spec, state_old, dsdt, prm, port):
                 face = list(cell)
                 if sgn > 0:
                     face[d] += 1
+                if robin is not None:
+                    ra, rb, rf = (robin[0] if sgn < 0 else robin[1])
+                    den = 0.5 * ra[d] + rb[d] / dx[d]
+                    # -b (n_g - n_c)/dx^2 with n_g - n_c = (f - a n_c)/den
+                    diag[r] += b * w * ra[d] / den
+                    rhs[r] += b * w * rf[d] / den
+                    bfaces[(d, sgn, tuple(face))] = ("robin", (ra[d], rf[d], den), b)
+                    continue
                 val = boundary_value(case, spec, d, sgn, tuple(face), Tg, port, mw)
                 bfaces[(d, sgn, tuple(face))] = (bc, val, b)
                 if bc == BC_DIRC:
@@ -199,6 +211,9 @@ def solve(case, spec, state_old, dsdt, prm, port):
                             G[c] = (ni - val) / (0.5 * dx[d]) if sgn < 0 else (val - ni) / (0.5 * dx[d])
                         elif bc == BC_IHNEU:
                             G[c] = val
+                        elif bc == "robin":
+                            ra, rf, den = val
+                            G[c] = sgn * (rf - ra * ni) / den / dx[d]
             grads.append(G)
     te = None
     if spec == ns:

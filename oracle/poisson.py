@@ -26,9 +26,10 @@ def _lin(n, i, j, k):
     return i + n[0] * (j + n[1] * k)
 
 
-def solve(case, dirichlet_lo, dirichlet_hi, v_lo, v_hi):
+def solve(case, dirichlet_lo, dirichlet_hi, v_lo, v_hi, user_rhs=None):
     """phi (nz, ny, nx) of the valid cells.  dirichlet_lo/hi[d]: bool per direction,
-    v_lo/hi[d]: the face values."""
+    v_lo/hi[d]: the face values; user_rhs (nz, ny, nx) is added to the right-hand
+    side (the case's add_user_potential_sources, Source/PotentialSolve.cpp:220)."""
     dim, n, dx = case.dim, case.n, case.dx
     ns = case.mech.ns
     g = case.gvec
@@ -38,6 +39,8 @@ def solve(case, dirichlet_lo, dirichlet_hi, v_lo, v_hi):
         if case.mech.charge[s] != 0:
             rho += case.mech.charge[s] * valid[s]
     rhs = (rho * (-ECHARGE / EPS0)).reshape(-1).copy()
+    if user_rhs is not None:
+        rhs += np.asarray(user_rhs, dtype=float).reshape(-1)
     N = n[0] * n[1] * n[2]
     rows, cols, vals = [], [], []
     diag = np.zeros(N)

@@ -164,7 +164,8 @@ def lib() -> C.CDLL:
 
 def check_layout(L=None) -> None:
     L = L or lib()
-    for i, S in enumerate(STRUCTS):
+    structs = STRUCTS + [VdPoissonParams, VdDiffusionParams, VdBatchStats, VdServerStats]
+    for i, S in enumerate(structs):
         n = L.vd_sizeof(i)
         if n != C.sizeof(S):
             raise RuntimeError(f"ABI layout mismatch for {S.__name__}: C {n} vs ctypes {C.sizeof(S)}")
@@ -262,7 +263,7 @@ PROTOTYPES.update({
 class VdPoissonParams(C.Structure):
     _fields_ = [("bc_lo", C.c_int32 * 3), ("bc_hi", C.c_int32 * 3), ("value_lo", C.c_double * 3),
                 ("value_hi", C.c_double * 3), ("max_vcycles", C.c_int32), ("pad0", C.c_int32),
-                ("tol_rel", C.c_double)]
+                ("tol_rel", C.c_double), ("user_rhs", VdArray4)]
 
 
 PROTOTYPES.update({
@@ -285,7 +286,9 @@ PROTOTYPES.update({
 
 class VdDiffusionParams(C.Structure):
     _fields_ = [("spec", C.c_int32), ("dsdt_comp", C.c_int32), ("max_vcycles", C.c_int32), ("pad0", C.c_int32),
-                ("tol_rel", C.c_double)]
+                ("tol_rel", C.c_double), ("user_robin", C.c_int32), ("pad1", C.c_int32),
+                ("robin_a", (C.c_double * 3) * 2), ("robin_b", (C.c_double * 3) * 2),
+                ("robin_f", (C.c_double * 3) * 2)]
 
 
 PROTOTYPES.update({

@@ -401,6 +401,13 @@ def poisson_params(dim: int, v_lo: float, v_hi: float = 0.0, max_vcycles: int = 
     return pp
 
 
+def set_poisson_user_rhs(pp: abi.VdPoissonParams, rhs: torch.Tensor | None) -> None:
+    """Add rhs (one component over the valid cells, (1, nz, ny, nx)) to the
+    potential's right-hand side (the case's add_user_potential_sources); None
+    removes it.  pp keeps a pointer: rhs must stay alive while pp is used."""
+    pp.user_rhs = t_a4(rhs, (0, 0, 0)) if rhs is not None else abi.null_array4()
+
+
 def poisson_solve(dc: DeviceCase, prm: abi.VdParams, pp: abi.VdPoissonParams, state: torch.Tensor | None = None,
                   stream=None):
     """Potential and fields of dc (or of `state`, laid out like dc.state): writes
@@ -418,17 +425,25 @@ def poisson_solve(dc: DeviceCase, prm: abi.VdParams, pp: abi.VdPoissonParams, st
 def implicit_species_solve(dc: DeviceCase, spec: int, state_old: torch.Tensor, dsdt: torch.Tensor,
                            phi_new: torch.Tensor, prm: abi.VdParams, *, dsdt_comp: int | None = None,
                            gradne: list | None = None, tol_rel: float = 1e-12, max_vcycles: int = 50,
-                           stream=None):
+                           robin=None, stream=None):
     """Implicit diffusion solve of species `spec` (NS: the electron energy) of dc
     (Vidyut::implicit_solve_scalar): state_old laid out like dc.state, dsdt and
     phi_new over the valid cells (phi_new with NVAR components).  gradne: three
-    face tensors that receive the electron face gradients.  Returns (V-cycles done,
-    relative residual or -1 when not checked)."""
+    face tensors that receive the electron face gradients.  robin: the case's own
+    species_bc coefficients, ((a_lo, b_lo, f_lo), (a_hi, b_hi, f_hi)) with one
+    value per direction each (a n + b dn/dnu = f, nu outward), else species_bc's
+    defaults.  Returns (V-cycles done, relative residual or -1 when not checked)."""
     dp = abi.VdDiffusionParams()
     dp.spec = spec
     dp.dsdt_comp = spec if dsdt_comp is None else dsdt_comp
     dp.max_vcycles = max_vcycles
     dp.tol_rel = tol_rel
+    if robin is not None:
+        dp.user_robin = 1
+        for side in range(2):
+            a, b, f = robin[side]
+            for d in range(3):
+                dp.robin_a[side][d], dp.robin_b[side][d], dp.robin_f[side][d] = a[d], b[d], f[d]
     nv = C.c_int32()
     rr = C.c_double()
     g = None

@@ -226,6 +226,10 @@ size_t vd_sizeof(int which)
     case 2: return sizeof(vd_reaction);
     case 3: return sizeof(vd_mech);
     case 4: return sizeof(vd_params);
+    case 5: return sizeof(vd_poisson_params);
+    case 6: return sizeof(vd_diffusion_params);
+    case 7: return sizeof(vd_batch_stats);
+    case 8: return sizeof(vd_server_stats);
     default: return 0;
     }
 }

@@ -213,44 +213,6 @@ __device__ __forceinline__ double face_flux_fp64(const double* u, const double* 
     return 0.5 * (fp + lam * up) + 0.5 * (fm - lam * um);
 }
 
-// Exact power-of-two scale 2^-e with 2^(e-1) <= m < 2^e (m > 0 finite), else 1.
-__device__ __forceinline__ double pow2_inv_scale(double m)
-{
-    if (!(m > 0.0) || !isfinite(m)) return 1.0;
-    int e = ((int)((__double_as_longlong(m) >> 52) & 0x7ff)) - 1022;  // m in [2^(e-1), 2^e)
-    return __longlong_as_double((long long)(1023 - e) << 52);
-}
-
-__device__ __forceinline__ double face_flux_mixed(const double* u, const float* v, int hyp_order,
-                                                  int scheme, double dxmin, double dt)
-{
-    if (hyp_order != 5) {
-        double vd[6];
-#pragma unroll
-        for (int q = 0; q < 6; q++) vd[q] = (double)v[q];
-        return face_flux_fp64(u, vd, hyp_order, scheme, dxmin, dt);
-    }
-    double m = fmax(fmax(fmax(fabs(u[0]), fabs(u[1])), fmax(fabs(u[2]), fabs(u[3]))),
-                    fmax(fabs(u[4]), fabs(u[5])));
-    double s = pow2_inv_scale(m);
-    float us[6], fs[6];
-#pragma unroll
-    for (int q = 0; q < 6; q++) {
-        us[q] = (float)(u[q] * s);
-        fs[q] = us[q] * v[q];
-    }
-    // eps = 1e-20 in the unscaled units of u (and of f for |v| ~ 1)
-    float s2 = (float)(s * s);
-    float eps = 4.0f * fmaxf(1e-20f * s2, 1e-30f);  // weno_f32 takes 4 eps
-    float lam = fabsf(0.5f * (v[2] + v[3]));
-    float fp = weno_f32(fs[0], fs[1], fs[2], fs[3], fs[4], scheme, eps);
-    float fm = weno_f32(fs[5], fs[4], fs[3], fs[2], fs[1], scheme, eps);
-    float up = weno_f32(us[0], us[1], us[2], us[3], us[4], scheme, eps);
-    float um = weno_f32(us[5], us[4], us[3], us[2], us[1], scheme, eps);
-    float F = 0.5f * (fmaf(lam, up, fp) + fmaf(-lam, um, fm));
-    return (double)F * (1.0 / s);  // s is a power of two: exact
-}
-
 // Mixed-precision face flux from densities already staged in FP32 (|n| < 3e38).
 // The six values are scaled by an exact power of two s = 2^-e chosen from the
 // exponent bits of max|u| (so max|u*s| is in [1/2, 1)); eps = 1e-20 is carried
@@ -297,6 +259,130 @@ __device__ __forceinline__ float face_flux_mixed32(const float* u, const float* 
     const float F = 0.5f * (fmaf(lam, up, fp) + fmaf(-lam, um, fm));
     if (bs < 254) return F * __int_as_float((254 - bs) << 23);  // 2^(127-bs)
     return (float)((double)F * __longlong_as_double((long long)(1150 - bs) << 52));
+}
+
+// ---------------------------------------------------------------------------
+// WENO-5 around one cell centre.  For the values a..e of cells c-2..c+2 the
+// reference reconstructs the right face of c as weno(a,b,c,d,e) (the
+// left-biased value of that face) and the left face of c as weno(e,d,c,b,a) (the
+// right-biased value of that face).  Both use the same three smoothness
+// indicators -- the left-face ones are the right-face ones in reverse order
+// (b1' = b3, b2' = b2, b3' = b1) -- and the same tau = |b1 - b3|, so everything up
+// to the nonlinear weights is computed once per centre as Y_1..Y_3, with
+//   WENO-Z   alpha_k = gamma_k Y_k,  Y_k = 1 + (tau/(beta_k + eps))^2
+//   WENO-JS  alpha_k = gamma_k Y_k,  Y_k = 1/(beta_k + eps)^2  (M: then the map)
+// at the right face and alpha'_k = gamma_k Y_(4-k) at the left face
+// (Source/compute_explicit_flux.H:38-109).  The candidate polynomials are linear
+// in the values; the caller evaluates them once per face and window and shares
+// them between the reconstructions that use them (weno_combine_*).
+struct WenoY64 {
+    double y1, y2, y3;
+};
+__device__ __forceinline__ WenoY64 weno_center_fp64(double a, double b, double c, double d, double e, int scheme)
+{
+    const double eps = 1e-20;
+    const double t1 = a - 2.0 * b + c, t2 = a - 4.0 * b + 3.0 * c;
+    const double b1 = (13.0 / 12.0) * (t1 * t1) + 0.25 * (t2 * t2);
+    const double t3 = b - 2.0 * c + d, t4 = b - d;
+    const double b2 = (13.0 / 12.0) * (t3 * t3) + 0.25 * (t4 * t4);
+    const double t5 = c - 2.0 * d + e, t6 = 3.0 * c - 4.0 * d + e;
+    const double b3 = (13.0 / 12.0) * (t5 * t5) + 0.25 * (t6 * t6);
+    const double r1 = 1.0 / (b1 + eps), r2 = 1.0 / (b2 + eps), r3 = 1.0 / (b3 + eps);
+    WenoY64 y;
+    if (scheme == 3) {
+        const double tau = fabs(b1 - b3);
+        const double s1 = tau * r1, s2 = tau * r2, s3 = tau * r3;
+        y.y1 = 1.0 + s1 * s1;
+        y.y2 = 1.0 + s2 * s2;
+        y.y3 = 1.0 + s3 * s3;
+    } else {
+        y.y1 = r1 * r1;
+        y.y2 = r2 * r2;
+        y.y3 = r3 * r3;
+    }
+    return y;
+}
+// sum_k alpha_k p_k / sum_k alpha_k with alpha = gamma (0.1, 0.6, 0.3) times (y1, y2, y3)
+__device__ __forceinline__ double weno_combine_fp64(double y1, double y2, double y3, double p1, double p2, double p3,
+                                                    int scheme)
+{
+    double a1 = 0.1 * y1, a2 = 0.6 * y2, a3 = 0.3 * y3;
+    if (scheme == 2) {
+        const double is = 1.0 / (a1 + a2 + a3);
+        a1 = gk_map(a1 * is, 0.1);
+        a2 = gk_map(a2 * is, 0.6);
+        a3 = gk_map(a3 * is, 0.3);
+    }
+    const double is = 1.0 / (a1 + a2 + a3);
+    return (a1 * is) * p1 + (a2 * is) * p2 + (a3 * is) * p3;
+}
+// the candidate polynomials: the value at x2 + 1/2 of the parabola through a window
+// (x0, x1, x2) (p1 of the reference), at x1 + 1/2 (p2) and at x0 + 1/2 (p3)
+template <class R> __device__ __forceinline__ R wpoly_end(R x0, R x1, R x2)
+{
+    return (R(1) / R(3)) * x0 - (R(7) / R(6)) * x1 + (R(11) / R(6)) * x2;
+}
+template <class R> __device__ __forceinline__ R wpoly_mid(R x0, R x1, R x2)
+{
+    return -(R(1) / R(6)) * x0 + (R(5) / R(6)) * x1 + (R(1) / R(3)) * x2;
+}
+template <class R> __device__ __forceinline__ R wpoly_near(R x0, R x1, R x2)
+{
+    return (R(1) / R(3)) * x0 + (R(5) / R(6)) * x1 - (R(1) / R(6)) * x2;
+}
+
+// FP32 form from values scaled by an exact power of two s (max |value| of the run
+// of cells in [1/2, 1)); eps4 = 4 eps s^2 (the indicators are kept as 4 beta_k:
+// 13/3 and 1 for 13/12 and 1/4, an exact power-of-two scaling), which may be zero
+// when it underflows: q_k = beta_k + eps is held at the smallest normal FP32 value
+// so that a stencil of equal values (beta = 0) gets the reference's limit.  The Y_k
+// are rescaled by a common factor so that nothing overflows whatever the spread of
+// the indicators (a positive multiple of the reference's; weno_f32 explains it).
+struct WenoY32 {
+    float y1, y2, y3;
+};
+__device__ __forceinline__ WenoY32 weno_center_f32(float a, float b, float c, float d, float e, int scheme, float eps4)
+{
+    const float t1 = fmaf(-2.0f, b, a) + c, t2 = fmaf(-4.0f, b, a) + 3.0f * c;
+    const float b1 = fmaf(13.0f / 3.0f, t1 * t1, t2 * t2);
+    const float t3 = fmaf(-2.0f, c, b) + d, t4 = b - d;
+    const float b2 = fmaf(13.0f / 3.0f, t3 * t3, t4 * t4);
+    const float t5 = fmaf(-2.0f, d, c) + e, t6 = fmaf(3.0f, c, fmaf(-4.0f, d, e));
+    const float b3 = fmaf(13.0f / 3.0f, t5 * t5, t6 * t6);
+    const float tiny = 1.17549435e-38f;
+    const float q1 = fmaxf(b1 + eps4, tiny), q2 = fmaxf(b2 + eps4, tiny), q3 = fmaxf(b3 + eps4, tiny);
+    const float m = fminf(q1, fminf(q2, q3));
+    const float r1 = rcp_approx(q1), r2 = rcp_approx(q2), r3 = rcp_approx(q3);
+    WenoY32 y;
+    if (scheme == 3) {
+        const float tau = fabsf(b1 - b3);
+        const bool big = tau > m;
+        const float cr = big ? m * rcp_approx(tau) : 1.0f;
+        const float t = big ? m : tau;
+        const float B1 = t * r1, B2 = t * r2, B3 = t * r3;
+        const float c2 = cr * cr;
+        y.y1 = fmaf(B1, B1, c2);
+        y.y2 = fmaf(B2, B2, c2);
+        y.y3 = fmaf(B3, B3, c2);
+    } else {
+        const float B1 = m * r1, B2 = m * r2, B3 = m * r3;
+        y.y1 = B1 * B1;
+        y.y2 = B2 * B2;
+        y.y3 = B3 * B3;
+    }
+    return y;
+}
+__device__ __forceinline__ float weno_combine_f32(float y1, float y2, float y3, float p1, float p2, float p3,
+                                                  int scheme)
+{
+    float a1 = 0.1f * y1, a2 = 0.6f * y2, a3 = 0.3f * y3;
+    if (scheme == 2) {
+        const float is = rcp_approx(a1 + a2 + a3);
+        a1 = gk_map(a1 * is, 0.1f);
+        a2 = gk_map(a2 * is, 0.6f);
+        a3 = gk_map(a3 * is, 0.3f);
+    }
+    return fmaf(a1, p1, fmaf(a2, p2, a3 * p3)) * rcp_approx(a1 + a2 + a3);
 }
 
 // 2^x for an FP64 exponent x as an FP32 value: x = i + f with i = rint(x) (exact in

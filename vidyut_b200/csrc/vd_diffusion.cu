@@ -60,7 +60,19 @@ struct DBc {
     int type_lo[3], type_hi[3];
     const double* val_lo[3];
     const double* val_hi[3];
+    // faces of type kBcUserRobin: a n + b dn/dnu = f (nu the outward normal), per
+    // [side][direction]; f is zero on the correction levels
+    double ra[2][3], rb[2][3], rf[2][3];
 };
+// the caller's Robin coefficients (vd_diffusion_params.user_robin) on a face
+constexpr int kBcUserRobin = 100;
+
+// A face with a n_f + b (n_g - n_c)/h = f, n_f = (n_c + n_g)/2, between the cell
+// value n_c and its ghost n_g: n_g - n_c = (f - a n_c) / (a/2 + b/h).
+__device__ __forceinline__ double robin_den(const DBc& bc, int side, int d, double idx)
+{
+    return 0.5 * bc.ra[side][d] + bc.rb[side][d] * idx;
+}
 
 __device__ __forceinline__ int64_t dlin(const DLevel& L, int i, int j, int k)
 {
@@ -106,6 +118,11 @@ __device__ __forceinline__ void dstencil(const DLevel& L, const DBc& bc, int dim
             if (bc.val_lo[d]) off -= 2.0 * blo * w * bc.val_lo[d][plin(L, d, c)];
         } else if (bc.type_lo[d] == VD_BC_IHNEU && bc.val_lo[d]) {
             off += blo * bc.val_lo[d][plin(L, d, c)] * L.idx[d];
+        } else if (bc.type_lo[d] == kBcUserRobin) {
+            // -b (n_g - n_c)/dx^2 with n_g - n_c = (f - a n_c)/den
+            const double den = robin_den(bc, 0, d, L.idx[d]);
+            diag += blo * w * bc.ra[0][d] / den;
+            off -= blo * w * bc.rf[0][d] / den;
         }
         if (c[d] < L.n[d] - 1) {
             off -= bhi * w * phi[dlin(L, p[0], p[1], p[2])];
@@ -115,6 +132,10 @@ __device__ __forceinline__ void dstencil(const DLevel& L, const DBc& bc, int dim
             if (bc.val_hi[d]) off -= 2.0 * bhi * w * bc.val_hi[d][plin(L, d, c)];
         } else if (bc.type_hi[d] == VD_BC_IHNEU && bc.val_hi[d]) {
             off -= bhi * bc.val_hi[d][plin(L, d, c)] * L.idx[d];
+        } else if (bc.type_hi[d] == kBcUserRobin) {
+            const double den = robin_den(bc, 1, d, L.idx[d]);
+            diag += bhi * w * bc.ra[1][d] / den;
+            off -= bhi * w * bc.rf[1][d] / den;
         }
     }
 }
@@ -211,7 +232,8 @@ __global__ void __launch_bounds__(128) k_dif_coarsen_b(DLevel F, DLevel C)
 }
 
 // fine phi += linear interpolation of the coarse correction; outside a domain face
-// the correction's mirror value: -c for a Dirichlet face, c otherwise
+// the correction's mirror value: -c for a Dirichlet face, the homogeneous ghost
+// relation for a Robin face, c otherwise
 template <int DIM>
 __global__ void __launch_bounds__(128) k_dif_prolong(DLevel F, DLevel C, DBc bc)
 {
@@ -243,9 +265,13 @@ __global__ void __launch_bounds__(128) k_dif_prolong(DLevel F, DLevel C, DBc bc)
                         if (q[d] < 0) {
                             q[d] = 0;
                             if (bc.type_lo[d] == VD_BC_DIRC) sign = -sign;
+                            if (bc.type_lo[d] == kBcUserRobin)
+                                sign *= 1.0 - bc.ra[0][d] / robin_den(bc, 0, d, C.idx[d]);
                         } else if (q[d] >= C.n[d]) {
                             q[d] = C.n[d] - 1;
                             if (bc.type_hi[d] == VD_BC_DIRC) sign = -sign;
+                            if (bc.type_hi[d] == kBcUserRobin)
+                                sign *= 1.0 - bc.ra[1][d] / robin_den(bc, 1, d, C.idx[d]);
                         }
                     }
                 }
@@ -428,9 +454,13 @@ __global__ void __launch_bounds__(128) k_dif_grad(DLevel L, DBc bc, A4 out, int 
     } else if (f[D] == 0) {
         if (bc.type_lo[D] == VD_BC_DIRC) g = (L.phi[c] - bc.val_lo[D][plin(L, D, f)]) / (0.5 * h);
         else if (bc.type_lo[D] == VD_BC_IHNEU) g = bc.val_lo[D][plin(L, D, f)];
+        else if (bc.type_lo[D] == kBcUserRobin)  // outward derivative (n_g - n_c)/h, outward = -x
+            g = -(bc.rf[0][D] - bc.ra[0][D] * L.phi[c]) / robin_den(bc, 0, D, L.idx[D]) / h;
     } else {
         if (bc.type_hi[D] == VD_BC_DIRC) g = (bc.val_hi[D][plin(L, D, f)] - L.phi[c - s1]) / (0.5 * h);
         else if (bc.type_hi[D] == VD_BC_IHNEU) g = bc.val_hi[D][plin(L, D, f)];
+        else if (bc.type_hi[D] == kBcUserRobin)
+            g = (bc.rf[1][D] - bc.ra[1][D] * L.phi[c - s1]) / robin_den(bc, 1, D, L.idx[D]) / h;
     }
     out.p[out.off(lo0 + i, lo1 + j, lo2 + k)] = g;
 }
@@ -585,6 +615,19 @@ extern "C" int vd_implicit_species_solve(const vd_box* bx, vd_array4 state, vd_a
         if (bc.type_lo[d] < VD_BC_PER || bc.type_lo[d] > VD_BC_ROBIN || bc.type_hi[d] < VD_BC_PER ||
             bc.type_hi[d] > VD_BC_ROBIN)
             return derr(VD_ERR_ARG, "unknown boundary code in direction %d", d);
+        if (dp->user_robin) {
+            // the caller's species_bc coefficients replace the default face values
+            for (int side = 0; side < 2; side++) {
+                const double ra = dp->robin_a[side][d], rb = dp->robin_b[side][d], rf = dp->robin_f[side][d];
+                if (!std::isfinite(ra) || !std::isfinite(rb) || !std::isfinite(rf) ||
+                    !(std::fabs(0.5 * ra + rb / prm->dx[d]) > 0.0))
+                    return derr(VD_ERR_ARG, "Robin coefficients of direction %d side %d invalid", d, side);
+                bc.ra[side][d] = ra;
+                bc.rb[side][d] = rb;
+                bc.rf[side][d] = rf;
+            }
+            bc.type_lo[d] = bc.type_hi[d] = kBcUserRobin;
+        }
     }
     int glo[3], ghi[3];
     for (int d = 0; d < 3; d++) {
@@ -681,7 +724,10 @@ extern "C" int vd_implicit_species_solve(const vd_box* bx, vd_array4 state, vd_a
     }
     unsigned long long* d_max = reinterpret_cast<unsigned long long*>(p);
     DBc bc0 = bc;  // homogeneous faces for the correction levels
-    for (int d = 0; d < 3; d++) bc0.val_lo[d] = bc0.val_hi[d] = nullptr;
+    for (int d = 0; d < 3; d++) {
+        bc0.val_lo[d] = bc0.val_hi[d] = nullptr;
+        bc0.rf[0][d] = bc0.rf[1][d] = 0.0;
+    }
 
     DifArgs a;
     memset(&a, 0, sizeof(a));
@@ -717,7 +763,11 @@ extern "C" int vd_implicit_species_solve(const vd_box* bx, vd_array4 state, vd_a
         }
         return VD_OK;
     };
-    ops.setup(a, lv[0], Dg, bv_lo, bv_hi, st);
+    {
+        // species_bc face values are needed only when the caller gives no coefficients
+        double* const none[3] = {nullptr, nullptr, nullptr};
+        ops.setup(a, lv[0], Dg, dp->user_robin ? none : bv_lo, dp->user_robin ? none : bv_hi, st);
+    }
     for (size_t l = 1; l < lv.size(); l++) ops.coarsen_b(lv[l - 1], lv[l], st);
     if ((rc = fail_launch("solver set-up"))) return rc;
 

@@ -263,6 +263,7 @@ __global__ void k_maxabs(const double* x, int64_t n, unsigned long long* out)
 
 struct PoisArgs {
     A4 st;
+    A4 urhs;  // user source added to the right-hand side (p null: none)
     int lo[3], hi[3];
     int ns, dim;
     int8_t charge[VD_MAX_SPECIES];
@@ -281,6 +282,7 @@ __global__ void k_pois_rhs(PoisArgs a, Level L)
         for (int s = 0; s < a.ns; s++)
             if (a.charge[s] != 0) r += (double)a.charge[s] * a.st.p[o + (int64_t)s * a.st.ns];
         L.rhs[c] = r * (-ECHARGE / EPS0);
+        if (a.urhs.p) L.rhs[c] += a.urhs(a.lo[0] + i, a.lo[1] + j, a.lo[2] + k);
         L.phi[c] = a.st.p[o + (int64_t)VD_POT(a.ns) * a.st.ns];
     }
 }
@@ -426,6 +428,13 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
                 if (efield_ec[d].begin[e] > bx->lo[e] || efield_ec[d].end[e] <= fhi[e])
                     return err(VD_ERR_ARG, "efield_ec[%d] does not cover the face box", d);
         }
+    if (pp->user_rhs.p) {
+        const vd_array4& u = pp->user_rhs;
+        if (u.ncomp < 1 || ((uintptr_t)u.p) % 8) return err(VD_ERR_ARG, "user_rhs: bad component count or alignment");
+        for (int d = 0; d < 3; d++)
+            if (u.begin[d] > bx->lo[d] || u.end[d] <= bx->hi[d])
+                return err(VD_ERR_ARG, "user_rhs does not cover the box in direction %d", d);
+    }
     BcInfo bc;
     memset(&bc, 0, sizeof(bc));
     for (int d = 0; d < dim; d++) {
@@ -484,6 +493,7 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
     PoisArgs pa;
     memset(&pa, 0, sizeof(pa));
     pa.st = A4(state);
+    if (pp->user_rhs.p) pa.urhs = A4(pp->user_rhs);
     for (int d = 0; d < 3; d++) {
         pa.lo[d] = bx->lo[d];
         pa.hi[d] = bx->hi[d];

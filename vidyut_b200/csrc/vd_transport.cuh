@@ -95,6 +95,19 @@ struct TileGeom {
     static constexpr int FOFF1 = NF<0>(), FOFF2 = NF<0>() + NF<1>(), FTOT = NF<0>() + NF<1>() + NF<2>();
 };
 
+template <int DIM, class TS, int RUN>
+struct RunGeom {
+    using G = TileGeom<DIM, TS>;
+    static constexpr int NR(int D) { return D < DIM ? (G::T[D] + RUN) / RUN : 0; }  // runs per line
+    static constexpr int NL(int D)                                                   // lines
+    {
+        return D < DIM ? (G::T[0] * G::T[1] * G::T[2]) / G::T[D] : 0;
+    }
+    static constexpr int R0 = NL(0) * NR(0), R1 = NL(1) * NR(1), R2 = NL(2) * NR(2);
+    static constexpr int ROFF1 = R0, ROFF2 = R0 + R1, NRUN = R0 + R1 + R2;
+    static_assert(RUN >= 1 && RUN <= 60, "run length fits the info fields");
+};
+
 template <int PREC> struct VelT { using T = double; };
 template <> struct VelT<PREC_MIXED> { using T = float; };
 
@@ -111,9 +124,12 @@ struct JStage {
 
 __host__ __device__ constexpr size_t smem_align(size_t x) { return (x + 15) & ~(size_t)15; }
 
+// Faces per run of the face phase (run_faces) for a tile shape.
+template <int DIM, class TS> constexpr int run_len() { return 3; }
+
 // Dynamic shared memory of one tile with nb velocity bases and species groups of
-// GRP, in this order: the Joule term of every face (FP64, mixed path); the face
-// info words (face_info); the state offsets of the staged positions; the group's
+// GRP, in this order: the Joule term of every face (FP64, mixed path); the run
+// info words (run_info); the state offsets of the staged positions; the group's
 // face fluxes; the bases; the group's staged densities (or the staged Joule
 // inputs).  Fluxes, bases and densities are FP32 in the mixed path: a mixed flux
 // is an FP32 value times a power of two, so it is stored exactly.
@@ -122,7 +138,10 @@ struct TileSmem {
     using G = TileGeom<DIM, TS>;
     using VT = typename VelT<PREC>::T;
     static constexpr size_t joule() { return PREC == PREC_MIXED ? smem_align((size_t)G::FTOT * sizeof(double)) : 0; }
-    static constexpr size_t finfo() { return smem_align((size_t)G::FTOT * sizeof(int)); }
+    static constexpr size_t finfo()
+    {
+        return smem_align((size_t)RunGeom<DIM, TS, run_len<DIM, TS>()>::NRUN * sizeof(int2));
+    }
     static constexpr size_t soffs() { return smem_align((size_t)G::STOT * sizeof(int)); }
     static constexpr size_t flux(int grp) { return smem_align((size_t)grp * G::FTOT * sizeof(VT)); }
     static constexpr size_t basis(int nb) { return smem_align((size_t)nb * G::STOT * sizeof(VT)); }
@@ -388,78 +407,186 @@ __device__ __forceinline__ typename VelT<PREC>::T stage_density(const TransportA
     return (VT)a.sb.p[a.sb.off(g[0], g[1], g[2]) + (int64_t)s * a.sb.ns];
 }
 
-// local coordinates of face ff of direction D's face set
-template <int DIM, int D, class TS>
-__device__ __forceinline__ void face_local(int ff, int* l)
+// ---------------------------------------------------------------------------
+// Runs of faces.  The faces of the tile along a line of direction D (T_D + 1 of
+// them) are taken in runs of up to RUN consecutive faces; one thread computes a
+// run: it loads the run's RUN + 5 stencil cells once, evaluates the WENO
+// smoothness indicators and nonlinear weights once per cell centre
+// (weno_center_*) and the candidate polynomials once per face, so that adjacent
+// faces and the two reconstructions of a centre share them.
+// Run info of run r (RunGeom numbering: direction, then line, then the segment
+// along the line), built once per tile.
+//   x: bits 0-15 staged index of the first stencil cell of the run's first face
+//      (the staged index of rel cell f_d - 3 + q is f_d + q along d), bits 16-17
+//      the direction, bits 18-23 the number of faces nf, bits 24-29 one plus the
+//      position in the run of the high domain face (0: none);
+//   y: bits 0-15 tile face index of the first face (faces of direction D from
+//      FOFF_D, x fastest), bits
+//      16-21 the number of leading faces the box updates (the others lie beyond
+//      the box), bits 22-27 one plus the position of the low domain face.
+template <int DIM, class TS, int RUN>
+__device__ __forceinline__ int2 run_info(const TransportArgs& a, int r, const int* org)
 {
     using G = TileGeom<DIM, TS>;
-    constexpr int F0 = G::template FE<D>(0), F1 = G::template FE<D>(1);
-    l[0] = ff % F0;
-    l[1] = (ff / F0) % F1;
-    l[2] = ff / (F0 * F1);
-}
-
-// Face info word of face f of the tile (the faces of all directions in one index
-// range), built once per tile: bits 0-15 the staged index of the face's first
-// stencil cell in its direction's line set (staged index of rel cell f_d - 3 + q
-// is f_d + q along d), bits 16-17 the direction, then whether the face is one the
-// box updates and whether it is the low or high domain face of its direction.
-// face_tab reads it for every species.
-constexpr int kFaceOk = 1 << 18, kFaceDomLo = 1 << 19, kFaceDomHi = 1 << 20;
-template <int DIM, class TS>
-__device__ __forceinline__ int face_info(const TransportArgs& a, int f, const int* org)
-{
-    using G = TileGeom<DIM, TS>;
-    static_assert(G::STOT < (1 << 16), "staged index fits 16 bits");
-    int D = 0, l[3];
-    if (DIM > 2 && f >= G::FOFF2) {
+    using RG = RunGeom<DIM, TS, RUN>;
+    static_assert(G::FTOT < (1 << 16), "face index fits 16 bits");
+    int D = 0;
+    if (DIM > 2 && r >= RG::ROFF2) {
         D = 2;
-        face_local<DIM, (DIM > 2 ? 2 : 0), TS>(f - G::FOFF2, l);
-    } else if (DIM > 1 && f >= G::FOFF1) {
+        r -= RG::ROFF2;
+    } else if (DIM > 1 && r >= RG::ROFF1) {
         D = 1;
-        face_local<DIM, (DIM > 1 ? 1 : 0), TS>(f - G::FOFF1, l);
-    } else {
-        face_local<DIM, 0, TS>(f, l);
+        r -= RG::ROFF1;
     }
-    const int S0 = G::T[0] + (D == 0 ? 6 : 0), S1 = G::T[1] + (D == 1 ? 6 : 0);
+    const int nr = D == 0 ? RG::NR(0) : (D == 1 ? RG::NR(1) : RG::NR(2));
+    const int line = r / nr, seg = r - line * nr;
+    const int TD = D == 0 ? TS::X : (D == 1 ? TS::Y : TS::Z);
+    const int f0 = seg * RUN;
+    const int nf = min(RUN, TD + 1 - f0);
+    int l[3];  // local coordinates of the run's first face
+    if (D == 0) {
+        l[0] = f0;
+        l[1] = line % TS::Y;
+        l[2] = line / TS::Y;
+    } else if (D == 1) {
+        l[0] = line % TS::X;
+        l[1] = f0;
+        l[2] = line / TS::X;
+    } else {
+        l[0] = line % TS::X;
+        l[1] = line / TS::X;
+        l[2] = f0;
+    }
+    const int S0 = TS::X + (D == 0 ? 6 : 0), S1 = TS::Y + (D == 1 ? 6 : 0);
     const int soff = D == 0 ? 0 : (D == 1 ? G::SOFF1 : G::SOFF2);
-    const int g[3] = {org[0] + l[0], org[1] + l[1], org[2] + l[2]};
-    bool ok = g[D] <= a.hi[D] + 1;
+    const int F0 = TS::X + (D == 0), F1 = TS::Y + (D == 1);
+    const int foff = D == 0 ? 0 : (D == 1 ? G::FOFF1 : G::FOFF2);
+    bool line_ok = true;
 #pragma unroll
     for (int e = 0; e < DIM; e++)
-        if (e != D) ok = ok && (g[e] <= a.hi[e]);
-    return (soff + l[0] + S0 * (l[1] + S1 * l[2])) | (D << 16) | (ok ? kFaceOk : 0) |
-           (g[D] == a.domlo[D] ? kFaceDomLo : 0) | (g[D] == a.domhi[D] + 1 ? kFaceDomHi : 0);
+        if (e != D) line_ok = line_ok && (org[e] + l[e] <= a.hi[e]);
+    const int g0 = org[D] + f0;  // global index of the first face
+    const int nok = line_ok ? max(0, min(nf, a.hi[D] + 2 - g0)) : 0;
+    const int ilo = a.domlo[D] - g0, ihi = a.domhi[D] + 1 - g0;
+    int2 w;
+    w.x = (soff + l[0] + S0 * (l[1] + S1 * l[2])) | (D << 16) | (nf << 18) |
+          ((ihi >= 0 && ihi < nf) ? (ihi + 1) << 24 : 0);
+    w.y = (foff + l[0] + F0 * (l[1] + F1 * l[2])) | (nok << 16) | ((ilo >= 0 && ilo < nf) ? (ilo + 1) << 22 : 0);
+    return w;
 }
 
-// Flux of one species through the tile face with info word `info`: sU / sB the
-// species' staged densities and velocity basis over all line sets (sB null: the
-// user velocity of the face's direction), k its velocity constant, zm its
-// zero-flux mask (TransportArgs::fl_zm).  One copy of the flux arithmetic serves
-// every direction.
-template <int DIM, int PREC, class TS>
-__device__ __forceinline__ typename VelT<PREC>::T face_tab(const TransportArgs& a, int info, int zm,
-                                           const typename VelT<PREC>::T* sU, const typename VelT<PREC>::T* sB,
-                                           typename VelT<PREC>::T k)
+// The faces of one run for one species: sU / sB the species' staged densities and
+// velocity basis over all line sets (sB null: the user velocity of the run's
+// direction), k its velocity constant, zm its zero-flux mask
+// (TransportArgs::fl_zm); writes the nf face fluxes to sF (tile face numbering),
+// zero where the box updates no face or IHNEUBC holds
+// (Source/compute_explicit_flux.H:200-326).
+template <int DIM, int PREC, class TS, int RUN>
+__device__ __forceinline__ void run_faces(const TransportArgs& a, int2 ri, int zm,
+                                          const typename VelT<PREC>::T* __restrict__ sU,
+                                          const typename VelT<PREC>::T* __restrict__ sB,
+                                          typename VelT<PREC>::T k, typename VelT<PREC>::T* sF)
 {
     using VT = typename VelT<PREC>::T;
-    if (!(info & kFaceOk)) return VT(0);
-    const int D = (info >> 16) & 3, base = info & 0xffff;
-    constexpr int T0 = TS::X, T01 = TS::X * TS::Y;
-    const int STR = D == 0 ? 1 : (D == 1 ? T0 : T01);
+    constexpr int NC = RUN + 5;
+    const int base = ri.x & 0xffff, D = (ri.x >> 16) & 3, nf = (ri.x >> 18) & 63;
+    const int ihi = ((ri.x >> 24) & 63) - 1;
+    const int fbase = ri.y & 0xffff, nok = (ri.y >> 16) & 63, ilo = ((ri.y >> 22) & 63) - 1;
+    const int STR = D == 0 ? 1 : (D == 1 ? TS::X : TS::X * TS::Y);  // staged and face stride along D
+    const bool zlo = (zm >> D) & 1, zhi = (zm >> (3 + D)) & 1;
     if (!sB) k = (VT)a.uvel[D];
-    VT u[6];
-    VT v[6];
+    auto store = [&](int i, VT F) {
+        if (i >= nok || (i == ilo && zlo) || (i == ihi && zhi)) F = VT(0);
+        sF[fbase + i * STR] = F;
+    };
+    if (a.hyp_order != 5) {
+        // upwind / WAF: FP64 arithmetic on the face's own stencil (both paths)
+        for (int i = 0; i < nf; i++) {
+            double ud[6], vd[6];
 #pragma unroll
-    for (int q = 0; q < 6; q++) {
-        u[q] = sU[base + q * STR];
-        v[q] = sB ? k * sB[base + q * STR] : k;
+            for (int q = 0; q < 6; q++) {
+                ud[q] = (double)sU[base + (i + q) * STR];
+                vd[q] = (double)(sB ? k * sB[base + (i + q) * STR] : k);
+            }
+            store(i, (VT)face_flux_fp64(ud, vd, a.hyp_order, a.weno, a.dxmin, a.dt));
+        }
+        return;
     }
-    VT F;
-    if constexpr (PREC == PREC_FP64) F = face_flux_fp64(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
-    else F = face_flux_mixed32(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
-    if (((info & kFaceDomLo) && ((zm >> D) & 1)) || ((info & kFaceDomHi) && ((zm >> (3 + D)) & 1))) F = VT(0);
-    return F;
+    // the run's cells: densities u and drift fluxes f = u v; lam[i] = |v| at face i
+    VT u[NC], f[NC], lam[RUN];
+    {
+        VT vp = VT(0);
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            const bool in = i < nf + 5;
+            const VT ui = in ? sU[base + i * STR] : VT(0);
+            const VT vi = in ? (sB ? k * sB[base + i * STR] : k) : VT(0);
+            u[i] = ui;
+            f[i] = ui * vi;
+            if (i >= 3 && i - 3 < RUN) lam[i - 3] = VT(0.5) * (vp + vi);
+            vp = vi;
+        }
+    }
+    const int scheme = a.weno;
+    if constexpr (PREC == PREC_FP64) {
+        // face i lies between centres i+2 (left) and i+3 (right)
+        WenoY64 yu = weno_center_fp64(u[0], u[1], u[2], u[3], u[4], scheme);
+        WenoY64 yf = weno_center_fp64(f[0], f[1], f[2], f[3], f[4], scheme);
+#pragma unroll
+        for (int i = 0; i < RUN; i++) {
+            if (i >= nf) break;
+            const WenoY64 zu = weno_center_fp64(u[i + 1], u[i + 2], u[i + 3], u[i + 4], u[i + 5], scheme);
+            const double pu2 = wpoly_mid(u[i + 1], u[i + 2], u[i + 3]), pu3 = wpoly_near(u[i + 2], u[i + 3], u[i + 4]);
+            const double up = weno_combine_fp64(yu.y1, yu.y2, yu.y3, wpoly_end(u[i], u[i + 1], u[i + 2]), pu2, pu3, scheme);
+            const double um = weno_combine_fp64(zu.y3, zu.y2, zu.y1, wpoly_end(u[i + 5], u[i + 4], u[i + 3]), pu3, pu2, scheme);
+            const WenoY64 zf = weno_center_fp64(f[i + 1], f[i + 2], f[i + 3], f[i + 4], f[i + 5], scheme);
+            const double pf2 = wpoly_mid(f[i + 1], f[i + 2], f[i + 3]), pf3 = wpoly_near(f[i + 2], f[i + 3], f[i + 4]);
+            const double fp = weno_combine_fp64(yf.y1, yf.y2, yf.y3, wpoly_end(f[i], f[i + 1], f[i + 2]), pf2, pf3, scheme);
+            const double fm = weno_combine_fp64(zf.y3, zf.y2, zf.y1, wpoly_end(f[i + 5], f[i + 4], f[i + 3]), pf3, pf2, scheme);
+            const double l = fabs(lam[i]);
+            store(i, 0.5 * (fp + l * up) + 0.5 * (fm - l * um));
+            yu = zu;
+            yf = zf;
+        }
+    } else {
+        // one exact power-of-two scale for the run: s = 2^-e with max |u| in
+        // [2^(e-1), 2^e) (1 for zero, denormal or non-finite maxima); the
+        // reconstructions work on u s and f s and each face flux is unscaled by
+        // 1/s, which is exact
+        float mx = 0.0f;
+#pragma unroll
+        for (int i = 0; i < NC; i++) mx = fmaxf(mx, fabsf(u[i]));
+        const int eb = (__float_as_int(mx) >> 23) & 0xff;
+        int e = (eb > 0 && eb < 255) ? eb - 126 : 0;
+        e = max(-125, min(e, 126));
+        const float s = __int_as_float((127 - e) << 23), inv_s = __int_as_float((127 + e) << 23);
+        const int b2 = 127 - 2 * e;
+        const float s2 = b2 > 0 ? __int_as_float(min(b2, 254) << 23) : 0.0f;  // s^2, 0 when it underflows
+        const float eps4 = 4e-20f * s2;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            u[i] *= s;
+            f[i] *= s;
+        }
+        WenoY32 yu = weno_center_f32(u[0], u[1], u[2], u[3], u[4], scheme, eps4);
+        WenoY32 yf = weno_center_f32(f[0], f[1], f[2], f[3], f[4], scheme, eps4);
+#pragma unroll
+        for (int i = 0; i < RUN; i++) {
+            if (i >= nf) break;
+            const WenoY32 zu = weno_center_f32(u[i + 1], u[i + 2], u[i + 3], u[i + 4], u[i + 5], scheme, eps4);
+            const float pu2 = wpoly_mid(u[i + 1], u[i + 2], u[i + 3]), pu3 = wpoly_near(u[i + 2], u[i + 3], u[i + 4]);
+            const float up = weno_combine_f32(yu.y1, yu.y2, yu.y3, wpoly_end(u[i], u[i + 1], u[i + 2]), pu2, pu3, scheme);
+            const float um = weno_combine_f32(zu.y3, zu.y2, zu.y1, wpoly_end(u[i + 5], u[i + 4], u[i + 3]), pu3, pu2, scheme);
+            const WenoY32 zf = weno_center_f32(f[i + 1], f[i + 2], f[i + 3], f[i + 4], f[i + 5], scheme, eps4);
+            const float pf2 = wpoly_mid(f[i + 1], f[i + 2], f[i + 3]), pf3 = wpoly_near(f[i + 2], f[i + 3], f[i + 4]);
+            const float fp = weno_combine_f32(yf.y1, yf.y2, yf.y3, wpoly_end(f[i], f[i + 1], f[i + 2]), pf2, pf3, scheme);
+            const float fm = weno_combine_f32(zf.y3, zf.y2, zf.y1, wpoly_end(f[i + 5], f[i + 4], f[i + 3]), pf3, pf2, scheme);
+            const float l = fabsf(lam[i]);
+            store(i, 0.5f * (fmaf(l, up, fp) + fmaf(-l, um, fm)) * inv_s);
+            yu = zu;
+            yf = zf;
+        }
+    }
 }
 
 // Update tile `tile` (index over a.ntile) of the box described by a.  Every thread
@@ -480,8 +607,10 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     const int tiz = tb / a.ntile[1];
     const int org[3] = {a.lo[0] + tix * G::T[0], a.lo[1] + tiy * G::T[1], a.lo[2] + tiz * G::T[2]};
     using SM = TileSmem<DIM, PREC, TS>;
+    constexpr int RUN = run_len<DIM, TS>();
+    using RG = RunGeom<DIM, TS, RUN>;
     double* sJ = reinterpret_cast<double*>(smem);  // mixed path only
-    int* sFI = reinterpret_cast<int*>(smem + SM::joule());
+    int2* sRI = reinterpret_cast<int2*>(smem + SM::joule());
     int* sSO = reinterpret_cast<int*>(smem + SM::joule() + SM::finfo());
     const size_t o_f = SM::joule() + SM::finfo() + SM::soffs();
     VT* sF = reinterpret_cast<VT*>(smem + o_f);
@@ -565,8 +694,8 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     };
 
     if (nfl > 0) {
-        // (0) face info words and the velocity bases of every staged position
-        for (int f = tid; f < G::FTOT; f += NTH) sFI[f] = face_info<DIM, TS>(a, f, org);
+        // (0) run info words and the velocity bases of every staged position
+        for (int r = tid; r < RG::NRUN; r += NTH) sRI[r] = run_info<DIM, TS, RUN>(a, r, org);
         for (int c = tid; c < G::STOT; c += NTH) {
             if (c < G::SOFF1) {
                 stage_basis<DIM, PREC, 0, TS>(a, c, org, sB, js, jin, sSO);
@@ -652,15 +781,15 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
             sU[q] = u;
         }
         __syncthreads();
-        // (2) every face flux of the group
-        for (int q = tid; q < gn * G::FTOT; q += NTH) {
-            const int j = q / G::FTOT, f = q - j * G::FTOT;
+        // (2) every face flux of the group, by runs of faces along the lines
+        for (int q = tid; q < gn * RG::NRUN; q += NTH) {
+            const int j = q / RG::NRUN, r = q - j * RG::NRUN;
             const int sl = a.fl_slot[g0 + j];
             VT k;
             if constexpr (PREC == PREC_FP64) k = a.fl_K[g0 + j];
             else k = a.fl_Kf[g0 + j];
-            sF[q] = face_tab<DIM, PREC, TS>(a, sFI[f], a.fl_zm[g0 + j], sU + j * G::STOT,
-                                            sl >= 0 ? sB + sl * G::STOT : nullptr, k);
+            run_faces<DIM, PREC, TS, RUN>(a, sRI[r], a.fl_zm[g0 + j], sU + j * G::STOT,
+                                          sl >= 0 ? sB + sl * G::STOT : nullptr, k, sF + j * G::FTOT);
         }
         __syncthreads();
         // (3) divergence + sources of the own cell: dsdt = (Fx_lo - Fx_hi)/dx + rxn,
