@@ -143,6 +143,7 @@ typedef struct vd_box {
 #define VD_DIFF_ZERO       0
 #define VD_DIFF_TE_ABSMOB  1   /* D = (factor * Te/eV) * |mu[ref]|  */
 #define VD_DIFF_TG_MOB     2   /* D = (factor * Tg/eV) *  mu[ref]   */
+#define VD_DIFF_CONST      3   /* D = factor (e.g. test/models/ionelec_DC_1d/Chemistry.H:190-209) */
 
 typedef struct vd_reaction {
     int32_t kind;                       /* VD_RATE_*                                   */

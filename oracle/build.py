@@ -55,6 +55,7 @@ def _ref_cases():
     cases = [
         ("ar_dc_1d", t / "models" / "Ar_DC_1d", (2,), [], None),
         ("axisym_ar", t / "models" / "Axisymmetric_streamer_Ar", (2,), [], None),
+        ("ionelec", t / "models" / "ionelec_DC_1d", (1, 2), [], None),
         ("advect", t / "verification" / "Advect", (2, 3), ["-DVD_PROBPARM_HAS_VEL"], None),
     ]
     gen = [

@@ -54,6 +54,8 @@ def _diff_expr(m: Mechanism, s: int) -> str:
     if k == abi.DIFF_TG_MOB:
         return (f"{{ amrex::Real mb = specMob({m.diff_ref[s]},Te,ndens,emag,T); amrex::Real Tg_in_ev = T/eV;"
                 f" dcoeff = {_r(m.diff_factor[s])}*Tg_in_ev*mb; }}")
+    if k == abi.DIFF_CONST:
+        return f"{{ dcoeff = {_r(m.diff_factor[s])}; }}"
     return "{ dcoeff = 0.0; }"
 
 

@@ -82,6 +82,9 @@ double orc_specdiff(const vd_mech *m, int specid, double Te, double ndens, doubl
         double mob = orc_specmob(m, m->diff_ref[specid], Te, ndens, emag, T);
         double Tg_in_ev = T / eV;
         dcoeff = m->diff_factor[specid] * Tg_in_ev * mob;
+    } else if (kind == VD_DIFF_CONST) {
+        /* a constant coefficient (test/models/ionelec_DC_1d/Chemistry.H:190-209) */
+        dcoeff = m->diff_factor[specid];
     }
     return dcoeff;
 }

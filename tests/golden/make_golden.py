@@ -33,59 +33,14 @@ from vidyut_b200 import mechanism as mm  # noqa: E402
 from vidyut_b200.inputs import build_case, BASE_SEED  # noqa: E402
 import oracle  # noqa: E402
 from oracle.build import REF_TREE, build_ref  # noqa: E402
+from oracle.headers import parse_case_header  # noqa: E402
 
 FLUX_VARIANTS = [(1, 3), (2, 3), (5, 1), (5, 2), (5, 3)]
 
 
 def parse_argon_header(path: Path) -> mm.Mechanism:
-    """Mechanism table of a generated argon case header (the Ar_DC_1d form)."""
-    txt = path.read_text()
-    species = {}
-    for name, idx in re.findall(r"#define\s+(\w+)_ID\s+(\d+)", txt):
-        if name not in ("NUM",):
-            species[int(idx)] = name
-    ns = int(re.search(r"#define\s+NUM_SPECIES\s+(\d+)", txt).group(1))
-    names = [species[i] for i in range(ns)]
-    charge = [0] * ns
-    for i, z in re.findall(r"kcharge\[(\d+)\]\s*=\s*(-?\d+)", txt):
-        charge[int(i)] = int(z)
-    mwb = re.search(r"get_mw\(amrex::Real \*mw_new\)\s*\{(.*?)\}", txt, re.S).group(1)
-    mw = [0.0] * ns
-    for i, v in re.findall(r"mw_new\[(\d+)\]\s*=\s*([0-9.eE+-]+)", mwb):
-        mw[int(i)] = float(v)
-    e_cs = float(re.search(r"E_cs\s*=\s*([0-9.eE+-]+)", txt).group(1))
-    ion_cs = float(re.search(r"Arp_cs\s*=\s*([0-9.eE+-]+)", txt).group(1))
-    ion_amu = float(re.search(r"nu_Arp=std::sqrt\(8\.0\*K_B\*T/PI/\(([0-9.]+)\*M_AMU\)\)", txt).group(1))
-    el_amu = float(re.search(r"\(2\.0\*ME/\(([0-9.]+)\*M_AMU\)\)", txt).group(1))
-    e_id = names.index("E")
-    ion = names.index("ARp")
-    body = re.search(r"productionRate\(amrex::Real\* wdot.*?\n\}\n", txt, re.S).group(0)
-    blocks = re.findall(r"\{\s*//\s*reaction\s+\d+:\s*([^\n]*)\n(.*?)\n\s*\}", body, re.S)
-    rx = []
-    for label, blk in blocks:
-        b1 = " ".join(blk.split())
-        mk = re.search(r"k_f = ([0-9.eE+-]+)\*std::pow\(Te,([0-9.eE+-]+)\)\*std::exp\((-?[0-9.eE+-]+)/Te\)", b1)
-        if mk:
-            A, b, C = float(mk.group(1)), float(mk.group(2)), -float(mk.group(3))
-            kind = abi.RATE_ARRHENIUS_TE
-        else:
-            A = float(re.search(r"k_f = ([0-9.eE+-]+)\s*;", b1).group(1))
-            b = C = 0.0
-            kind = abi.RATE_CONST
-        reac = [int(s) for s in re.findall(r"sc\[(\d+)\]", re.search(r"qf = k_f \* \((.*?)\);", b1).group(1))]
-        terms = []
-        for s, op, coef in re.findall(r"wdot\[(\d+)\] ([+-])= (?:([0-9.]+) \* )?qdot;", b1):
-            c = float(coef) if coef else 1.0
-            terms.append((int(s), c if op == "+" else -c))
-        mt = re.search(r"int rxntype = (\d+);", b1)
-        rxntype = int(mt.group(1)) if mt else abi.RXN_NONE
-        me = re.search(r"eexci = (-?[0-9.eE+-]+);", b1)
-        ml = re.search(r"int elidx = (\d+);", b1)
-        rx.append(mm.Reaction(reac, [], A, b, C, kind, rxntype, float(me.group(1)) if me else 0.0,
-                              int(ml.group(1)) if ml else 0, terms=terms, label=label.strip()))
-    tr = mm._ar_like_transport(ns, e_id, {ion: (ion_cs, ion_amu * mm.M_AMU)}, ion, e_cs=e_cs)
-    return mm.Mechanism(name="ar_dc_1d", species=names, charge=charge, mw=mw, e_id=e_id, reactions=rx,
-                        elastic_loss=1, elastic_mass=el_amu * mm.M_AMU, bg_species=[names.index("AR")], **tr)
+    """Mechanism table of the Ar_DC_1d case header."""
+    return parse_case_header(path, "ar_dc_1d", ["AR"])
 
 
 def advect_mechanism() -> mm.Mechanism:
@@ -129,6 +84,25 @@ def main():
     upd = ref.update_all(case, case.vd_params())
     out.update({f"upd_{k}": v for k, v in upd.items()})
     _save("ar_dc_1d_2d", case, mech, out, {"ref": "ar_dc_1d", "header": "test/models/Ar_DC_1d/Chemistry.H"})
+
+    # 1b. the reference's other model headers: Axisymmetric_streamer_Ar (the argon
+    # form) and ionelec_DC_1d (constant mobilities and diffusion coefficients)
+    models = [("axisym_ar", "Axisymmetric_streamer_Ar", ["AR"], [2]), ("ionelec", "ionelec_DC_1d", ["HE"], [1, 2])]
+    for name, sub, bg, dims in models:
+        hdr = REF_TREE / "test" / "models" / sub / "Chemistry.H"
+        m = parse_case_header(hdr, name, bg)
+        for dim in dims:
+            n = (12, 10) if dim == 2 else (48,)
+            case = build_case(m, dim, n, (1e-5,) * dim, BASE_SEED + 110 + dim, density="blob",
+                              te_range_ev=(0.5, 5.0))
+            ref = oracle.RefLib(name, dim)
+            out = {"rxn": ref.reaction_source(case)}
+            out.update(flux_outputs(ref, case, range(m.ns + 1)))
+            upd = ref.update_all(case, case.vd_params())
+            out.update({f"upd_{k}": v for k, v in upd.items()})
+            # ionelec_DC_1d writes k = A exp(-C/Te) N_A: the table holds A N_A (rounding apart)
+            _save(f"{name}_{dim}d", case, m, out, {"ref": name, "header": f"test/models/{sub}/Chemistry.H",
+                                                   "exact": name != "ionelec"})
 
     # 2. the Advect verification case: constant user velocity (udv=1) for AR
     am = advect_mechanism()

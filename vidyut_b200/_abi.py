@@ -26,7 +26,7 @@ CLASS_ELECTRON, CLASS_ENERGY, CLASS_ION, CLASS_NEUTRAL = 0, 1, 2, 3
 RATE_ARRHENIUS_TE, RATE_CONST, RATE_ARRHENIUS_TG = 0, 1, 2
 RXN_NONE, RXN_EXCITATION, RXN_IONIZATION, RXN_RECOMB, RXN_ELASTIC = 0, 1, 2, 3, 5
 MOB_ZERO, MOB_ELECTRON, MOB_ION_TG, MOB_SCALED, MOB_CONST_N, MOB_CONST = 0, 1, 2, 3, 4, 5
-DIFF_ZERO, DIFF_TE_ABSMOB, DIFF_TG_MOB = 0, 1, 2
+DIFF_ZERO, DIFF_TE_ABSMOB, DIFF_TG_MOB, DIFF_CONST = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 NOALLOC_SCRATCH_BYTES = 64 << 20
 

@@ -277,8 +277,8 @@ static int build_mech_table(const vd_mech* m, VdMechDev** out)
         if (k == VD_MOB_ION_TG && !(m->mob_p1[s] > 0.0))
             return fail(VD_ERR_MECH, "species %d: particle mass must be > 0", s);
         int dk = m->diff_kind[s];
-        if (dk < 0 || dk > 2) return fail(VD_ERR_MECH, "species %d: unknown diffusion kind %d", s, dk);
-        if (dk != VD_DIFF_ZERO && (m->diff_ref[s] < 0 || m->diff_ref[s] > ns))
+        if (dk < 0 || dk > 3) return fail(VD_ERR_MECH, "species %d: unknown diffusion kind %d", s, dk);
+        if ((dk == VD_DIFF_TE_ABSMOB || dk == VD_DIFF_TG_MOB) && (m->diff_ref[s] < 0 || m->diff_ref[s] > ns))
             return fail(VD_ERR_MECH, "species %d: diffusion reference invalid", s);
     }
     if (m->elastic_loss && !(m->elastic_mass > 0.0)) return fail(VD_ERR_MECH, "elastic_mass must be > 0");

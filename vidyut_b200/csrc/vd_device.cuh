@@ -76,6 +76,7 @@ __device__ __forceinline__ double diff_fp64(int s, double Te, double N, double T
         return c_mech.diff_factor[s] * (Te / EV) * fabs(mob_fp64(c_mech.diff_ref[s], Te, N, Tg));
     case VD_DIFF_TG_MOB:
         return c_mech.diff_factor[s] * (Tg / EV) * mob_fp64(c_mech.diff_ref[s], Te, N, Tg);
+    case VD_DIFF_CONST: return c_mech.diff_factor[s];
     default: return 0.0;
     }
 }

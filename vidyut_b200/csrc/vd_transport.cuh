@@ -230,6 +230,7 @@ __device__ __forceinline__ double joule_mixed_core(const TransportArgs& a, float
         const float mr = dr == eidx ? mu : mob_f32(dr, etemp, ndens, Tg);
         if (dk == VD_DIFF_TE_ABSMOB) dc = (float)c_mech.diff_factor[eidx] * (etemp * (float)(1.0 / EV)) * fabsf(mr);
         else if (dk == VD_DIFF_TG_MOB) dc = (float)c_mech.diff_factor[eidx] * (Tg * (float)(1.0 / EV)) * mr;
+        else if (dk == VD_DIFF_CONST) dc = (float)c_mech.diff_factor[eidx];
         else dc = 0.0f;
     }
     const double drift = (double)(mu * (float)(0.5 * (nel + ner)) * (float)ef);
