@@ -50,7 +50,8 @@ extern "C" {
 
 /* ---- limits of the runtime mechanism table ---------------------------------- */
 #define VD_MAX_SPECIES   64
-#define VD_MAX_REACTIONS 512
+#define VD_MAX_REACTIONS 448
+#define VD_MAX_FITS      48   /* reactions with Janev / F-fit rates              */
 #define VD_MAX_REACTANTS 3
 #define VD_MAX_TERMS     6
 
@@ -124,12 +125,19 @@ typedef struct vd_box {
 #define VD_RATE_ARRHENIUS_TE 0   /* k = A * Te^b * exp(-C/Te)                      */
 #define VD_RATE_CONST        1   /* k = A                                           */
 #define VD_RATE_ARRHENIUS_TG 2   /* k = A * Tg^b * exp(-C/Tg)                       */
+/* electron-impact fits in Te_eV = Te/11595 (test/Reactor/CO2_H2_Ar_mechanism_reduced/
+ * Chemistry.H:940-1030), coefficients in vd_mech.fits[fit], k in m^3/mol/s:       */
+#define VD_RATE_JANEV        3   /* k = jA exp(sum_{j=0..8} jc_j ln(Te_eV)^j) NA    */
+#define VD_RATE_FFIT         4   /* k = fA exp(sum_{j=0..3} fc_j Te_eV^-(j+1)) NA    */
+#define VD_RATE_JANEV_FFIT   5   /* Janev below Te_eV = switch_ev, F-fit from there  */
 
 /* electron-energy exchange types (comp_ener_exch, rxntype) */
 #define VD_RXN_NONE       0
 #define VD_RXN_EXCITATION 1
 #define VD_RXN_IONIZATION 2
 #define VD_RXN_RECOMB     3
+#define VD_RXN_ATTACH     4   /* -mean electron energy * q, the CO2 reactor header's     */
+#define VD_RXN_DETACH     7   /* +mean electron energy * q  comp_ener_exch (:872-881)    */
 #define VD_RXN_ELASTIC    5
 
 /* mobility models (specMob): mob_kind[s] for s in [0, NS]; s = NS is the energy  */
@@ -156,7 +164,16 @@ typedef struct vd_reaction {
     double  term_coef[VD_MAX_TERMS];
     double  A, b, C;                    /* C in kelvin, A in (m^3/mol)^(nreac-1)/s     */
     double  eexci;                      /* threshold energy [eV]                       */
+    int32_t fit;                        /* index into vd_mech.fits (fit rate kinds)    */
+    int32_t pad0;
 } vd_reaction;
+
+/* coefficients of a Janev / F-fit rate (NA = 6.02214085774e23 as in the headers) */
+typedef struct vd_rate_fit {
+    double jA, jc[9];                   /* Janev: A [cm^3/s] and the 9 coefficients    */
+    double fA, fc[4];                   /* F-fit: A and the 4 coefficients             */
+    double switch_ev;                   /* VD_RATE_JANEV_FFIT: the Te [eV] switch      */
+} vd_rate_fit;
 
 typedef struct vd_mech {
     int32_t nspecies, nreactions;
@@ -174,6 +191,8 @@ typedef struct vd_mech {
     int32_t pad0;
     double  elastic_mass;                           /* heavy-partner mass [kg]        */
     vd_reaction rxn[VD_MAX_REACTIONS];
+    int32_t nfits, pad1;
+    vd_rate_fit fits[VD_MAX_FITS];
 } vd_mech;
 
 /* ---- run parameters (Vidyut::ReadParameters keys, Source/Vidyut.cpp:258-392) -- */

@@ -64,6 +64,10 @@ def _ref_cases():
         (mm.synthetic(8, 40, BASE_SEED + 21), (1, 2, 3)),    # batched / serving mechanism
         (mm.synthetic(12, 60, BASE_SEED + 31), (3,)),        # large-case mechanism
     ]
+    co2 = t / "Reactor" / "CO2_H2_Ar_mechanism_reduced" / "Chemistry.H"
+    if co2.exists():  # its Janev / F-fit reactions, in that header's code form
+        from headers import fit_submechanism
+        gen.append((fit_submechanism(co2, "co2fits"), (2,)))
     for m, dims in gen:
         cases.append((m.name, REF_OUT / "gen" / m.name, dims, [], m))
     return cases

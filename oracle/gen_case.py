@@ -65,7 +65,7 @@ def chemistry_h(m: Mechanism) -> str:
     w = L.append
     w("/* generated for a runtime mechanism in the reference's Chemistry.H form (test infrastructure) */")
     w("#ifndef MECHANISM_H\n#define MECHANISM_H\n#include <AMReX_Gpu.H>\n#include <AMReX_REAL.H>")
-    w("#include <UnivConstants.H>\n#include <VarDefines.H>\n")
+    w("#include <UnivConstants.H>\n#include <VarDefines.H>\n#include <vector>\n")
     w(f"#define E_ID {m.e_id}")
     w(f"#define NUM_SPECIES {ns}\n#define NUM_REACTIONS {len(m.reactions)}\n")
     w("AMREX_GPU_HOST_DEVICE AMREX_FORCE_INLINE void get_mw(amrex::Real *mw_new) {")
@@ -100,6 +100,8 @@ def chemistry_h(m: Mechanism) -> str:
     w("  amrex::Real sefact = (tanh((Te - T) / 0.5) + 1.0) / 2.0 ;")
     w("  if(rxntype == 1 || rxntype == 2){ *enerExch -= (eexci*eV2J)*NA*(qf - qr) * sefact; }")
     w("  if(rxntype == 3){ *enerExch -= mee*NA*(qf - qr); }")
+    w("  if(rxntype == 4){ *enerExch -= mee*NA*(qf - qr); }")
+    w("  if(rxntype == 7){ *enerExch += mee*NA*(qf - qr); }")
     w("  if(rxntype == 5){ amrex::Real qq = sc[E_ID] * sc[elidx] * kf;"
       " *enerExch -= 3.0 * kB * (wt[E_ID] / wt[elidx]) * (Te - T) * qq * NA; }")
     w("}")
@@ -108,10 +110,42 @@ def chemistry_h(m: Mechanism) -> str:
       "amrex::Real * enerExch)\n{")
     w(f"  for (int i = 0; i < {ns}; ++i) wdot[i] = 0.0;")
     w("  amrex::Real ne = sc[E_ID] * 6.02214085774e23;\n  amrex::Real Ue = 1.5 * Te * ne * 1.380649e-23;")
+    if any(r.kind >= abi.RATE_JANEV for r in m.reactions):
+        # the fit-rate preamble of the CO2 reactor header
+        # (test/Reactor/CO2_H2_Ar_mechanism_reduced/Chemistry.H:943-955)
+        w("  double Janev_sum;\n  double TeeV = Te / 11595.0;\n  double logTe = log(TeeV);")
+        w("  double invTeeV = (Te == 0) ? 1.0:1.0 / (TeeV);")
+        w("  double Te_pow[] = {" + ", ".join(f"pow(logTe, {j})" for j in range(9)) + "};")
+        w("  double invTe_pow[] = {" + ", ".join(f"pow(invTeeV, {j})" for j in range(1, 5)) + "};")
+        w("  std::vector<double> Jfit_coefs = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};")
+        w("  std::vector<double> Ffit_coefs = {0.0, 0.0, 0.0, 0.0};")
+
+    def fit_block(f, janev, ind):
+        if janev:
+            w(f"{ind}Jfit_coefs = {{{', '.join(_r(c) for c in f['jc'])}}};")
+            w(f"{ind}double Jfit_A = {_r(f['jA'])};")
+            w(f"{ind}for(int j = 0; j<9; j++) Janev_sum += Jfit_coefs[j] * Te_pow[j];")
+            w(f"{ind}k_f = Jfit_A * exp(Janev_sum) * 6.02214085774e23;")
+        else:
+            w(f"{ind}Ffit_coefs = {{{', '.join(_r(c) for c in f['fc'])}}};")
+            w(f"{ind}double Ffit_A = {_r(f['fA'])};")
+            w(f"{ind}for(int j = 0; j<4; j++) Janev_sum += Ffit_coefs[j] * invTe_pow[j];")
+            w(f"{ind}k_f = Ffit_A * exp(Janev_sum) * 6.02214085774e23;")
+
     for i, r in enumerate(m.reactions):
         r.fill_terms()
         w(f"  {{\n    // reaction {i}: {r.label}")
-        if r.kind == abi.RATE_ARRHENIUS_TE:
+        if r.kind >= abi.RATE_JANEV:
+            w("    Janev_sum = 0.0;\n    amrex::Real k_f;")
+            if r.kind == abi.RATE_JANEV_FFIT:
+                w(f"    if(TeeV < {_r(r.fit['switch_ev'])}){{")
+                fit_block(r.fit, True, "        ")
+                w("    } else {")
+                fit_block(r.fit, False, "        ")
+                w("    }")
+            else:
+                fit_block(r.fit, r.kind == abi.RATE_JANEV, "    ")
+        elif r.kind == abi.RATE_ARRHENIUS_TE:
             w(f"    const amrex::Real k_f = {_r(r.A)}*std::pow(Te,{_r(r.b)})*std::exp(-{_r(r.C)}/Te);")
         elif r.kind == abi.RATE_ARRHENIUS_TG:
             w(f"    const amrex::Real k_f = {_r(r.A)}*std::pow(T,{_r(r.b)})*std::exp(-{_r(r.C)}/T);")

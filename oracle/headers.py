@@ -155,3 +155,56 @@ def parse_case_header(path: Path, name: str, bg: list) -> mm.Mechanism:
     return mm.Mechanism(name=name, species=names, charge=charge, mw=mw, e_id=e_id, reactions=rx,
                         elastic_loss=1, elastic_mass=el_amu * mm.M_AMU, bg_species=[names.index(b) for b in bg],
                         **tr)
+
+
+def fit_submechanism(path: Path, name: str) -> mm.Mechanism:
+    """The Janev / F-fit electron-impact reactions of the CO2 reactor header
+    (test/Reactor/CO2_H2_Ar_mechanism_reduced/Chemistry.H:940-1030 and the like) as a
+    mechanism of their own: the electrons and every species these reactions touch
+    (electrons first, then in header order), each reaction with its reactants,
+    wdot updates, rxntype, eexci and fit coefficients as the header writes them.
+    Transport: the argon form, the first ion as the reference ion (the
+    sub-mechanism's header is generated from this table, so any consistent
+    transport serves)."""
+    txt = Path(path).read_text()
+    names, charge, mw = header_species(txt)
+    blocks = []
+    for label, blk in reaction_blocks(production_rate_body(txt)):
+        if "Janev_sum = 0.0" not in blk or "qf = k_f" not in blk:
+            continue
+        b1 = " ".join(blk.split())
+        if "Corr" in b1 or "qr = 0.0" not in b1:
+            continue  # third-body or reversible forms stay out
+        fit = {"jA": 0.0, "jc": [0.0] * 9, "fA": 0.0, "fc": [0.0] * 4, "switch_ev": 0.0}
+        mj = re.search(r"Jfit_coefs = \{([^}]*)\}; double Jfit_A = ([0-9.eE+-]+);", b1)
+        mf = re.search(r"Ffit_coefs = \{([^}]*)\}; double Ffit_A = ([0-9.eE+-]+);", b1)
+        ms = re.search(r"if\(TeeV < ([0-9.eE+-]+)\)", b1)
+        if mj:
+            fit["jc"] = [float(v) for v in mj.group(1).split(",")]
+            fit["jA"] = float(mj.group(2))
+        if mf:
+            fit["fc"] = [float(v) for v in mf.group(1).split(",")]
+            fit["fA"] = float(mf.group(2))
+        if mj and mf:
+            kind = abi.RATE_JANEV_FFIT
+            fit["switch_ev"] = float(ms.group(1))
+        else:
+            kind = abi.RATE_JANEV if mj else abi.RATE_FFIT
+        reac, terms, rxntype, eexci, elidx = _reactants_terms(b1, names)
+        blocks.append((label, reac, terms, rxntype, eexci, elidx, kind, fit))
+    used = sorted({names.index("E")} | {s for b in blocks for s in b[1] + [t for t, _ in b[2]]})
+    e_old = names.index("E")
+    order = [e_old] + [s for s in used if s != e_old]
+    new = {s: i for i, s in enumerate(order)}
+    rx = []
+    for label, reac, terms, rxntype, eexci, elidx, kind, fit in blocks:
+        rx.append(mm.Reaction([new[s] for s in reac], [], 0.0, 0.0, 0.0, kind, rxntype, eexci,
+                              new.get(elidx, 0), terms=[(new[s], c) for s, c in terms], label=label, fit=fit))
+    sub_names = [names[s] for s in order]
+    sub_charge = [charge[s] for s in order]
+    ns = len(order)
+    ion = next(i for i, z in enumerate(sub_charge) if z > 0)
+    tr = mm._ar_like_transport(ns, 0, {ion: (120e-20, mw[order[ion]] * mm.M_AMU)}, ion)
+    return mm.Mechanism(name=name, species=[n.replace("+", "p") for n in sub_names], charge=sub_charge,
+                        mw=[mw[s] for s in order], e_id=0, reactions=rx, elastic_loss=0, elastic_mass=0.0,
+                        bg_species=[], **tr)

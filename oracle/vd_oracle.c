@@ -106,17 +106,49 @@ static void orc_comp_ener_exch(const vd_mech *m, double qf, double qr, const dou
     if (rxntype == 3) {
         *enerExch -= mee * NA * (qf - qr);
     }
+    /* attachment and detachment, as the CO2 reactor header's comp_ener_exch
+     * (test/Reactor/CO2_H2_Ar_mechanism_reduced/Chemistry.H:872-881)        */
+    if (rxntype == 4) {
+        *enerExch -= mee * NA * (qf - qr);
+    }
+    if (rxntype == 7) {
+        *enerExch += mee * NA * (qf - qr);
+    }
     if (rxntype == 5) {
         double qq = sc[m->e_id] * sc[elidx] * kf;
         *enerExch -= 3.0 * kB * (m->mw[m->e_id] / m->mw[elidx]) * (Te - T) * qq * NA;
     }
 }
 
+/* Janev / F-fit electron-impact rates as the CO2 reactor header evaluates them
+ * (test/Reactor/CO2_H2_Ar_mechanism_reduced/Chemistry.H:945-964,1013-1030):
+ * Te_eV = Te/11595, the powers of ln(Te_eV) and 1/Te_eV by pow(), the sum
+ * accumulated in order, k = A exp(sum) * 6.02214085774e23.                    */
+static double orc_fit_rate(const vd_mech *m, const vd_reaction *r, double Te)
+{
+    const vd_rate_fit *F = &m->fits[r->fit];
+    double TeeV = Te / 11595.0;
+    double logTe = log(TeeV);
+    double invTeeV = (Te == 0) ? 1.0 : 1.0 / (TeeV);
+    double Te_pow[9], invTe_pow[4];
+    for (int j = 0; j < 9; j++) Te_pow[j] = pow(logTe, j);
+    for (int j = 0; j < 4; j++) invTe_pow[j] = pow(invTeeV, j + 1);
+    double Janev_sum = 0.0;
+    int janev = r->kind == VD_RATE_JANEV || (r->kind == VD_RATE_JANEV_FFIT && TeeV < F->switch_ev);
+    if (janev) {
+        for (int j = 0; j < 9; j++) Janev_sum += F->jc[j] * Te_pow[j];
+        return F->jA * exp(Janev_sum) * 6.02214085774e23;
+    }
+    for (int j = 0; j < 4; j++) Janev_sum += F->fc[j] * invTe_pow[j];
+    return F->fA * exp(Janev_sum) * 6.02214085774e23;
+}
+
 /* k_f of one reaction (productionRate, e.g. Ar_DC_1d/Chemistry.H:392). */
-static double orc_rate(const vd_reaction *r, double T, double Te)
+static double orc_rate(const vd_mech *m, const vd_reaction *r, double T, double Te)
 {
     if (r->kind == VD_RATE_ARRHENIUS_TE) return r->A * pow(Te, r->b) * exp(-r->C / Te);
     if (r->kind == VD_RATE_ARRHENIUS_TG) return r->A * pow(T, r->b) * exp(-r->C / T);
+    if (r->kind >= VD_RATE_JANEV) return orc_fit_rate(m, r, Te);
     return r->A;
 }
 
@@ -132,7 +164,7 @@ void orc_production_rate(const vd_mech *m, double *wdot, const double *sc, doubl
     double Ue = 1.5 * Te * ne * 1.380649e-23;
     for (int ir = 0; ir < m->nreactions; ++ir) {
         const vd_reaction *r = &m->rxn[ir];
-        double k_f = orc_rate(r, T, Te);
+        double k_f = orc_rate(m, r, T, Te);
         double prod = sc[r->reac[0]];
         for (int t = 1; t < r->nreac; ++t) prod = prod * sc[r->reac[t]];
         double qf = k_f * prod;
@@ -622,7 +654,7 @@ static void orc_production_gross(const vd_mech *m, double *gw, const double *sc,
     double Ue = 1.5 * Te * ne * 1.380649e-23;
     for (int ir = 0; ir < m->nreactions; ++ir) {
         const vd_reaction *r = &m->rxn[ir];
-        double k_f = orc_rate(r, T, Te);
+        double k_f = orc_rate(m, r, T, Te);
         double prod = sc[r->reac[0]];
         for (int t = 1; t < r->nreac; ++t) prod = prod * sc[r->reac[t]];
         double q = k_f * prod;

@@ -33,7 +33,7 @@ from vidyut_b200 import mechanism as mm  # noqa: E402
 from vidyut_b200.inputs import build_case, BASE_SEED  # noqa: E402
 import oracle  # noqa: E402
 from oracle.build import REF_TREE, build_ref  # noqa: E402
-from oracle.headers import parse_case_header  # noqa: E402
+from oracle.headers import fit_submechanism, parse_case_header  # noqa: E402
 
 FLUX_VARIANTS = [(1, 3), (2, 3), (5, 1), (5, 2), (5, 3)]
 
@@ -114,6 +114,22 @@ def main():
             out[f"flux_s1_d{d}_h{h}_w{w}"] = ref.flux(case, d, 1, hyp_order=h, weno=w, udv=1, uvel=(1.0, 0.5, 0.0),
                                                       bclo=(0, 0, 0), bchi=(0, 0, 0))
     _save("advect_2d", case, am, out, {"ref": "advect", "uvel": [1.0, 0.5, 0.0], "vel_species": 1})
+
+    # 2b. the Janev / F-fit electron-impact reactions of the CO2 reactor header
+    # (test/Reactor/CO2_H2_Ar_mechanism_reduced/Chemistry.H:940-1030) in that header's
+    # code form; Te over 0.3-20 eV so that both branches of the piecewise fits run
+    fm = fit_submechanism(REF_TREE / "test" / "Reactor" / "CO2_H2_Ar_mechanism_reduced" / "Chemistry.H", "co2fits")
+    case = build_case(fm, 2, (11, 9), (1e-5, 1e-5), BASE_SEED + 120, density="loguniform", te_range_ev=(0.3, 20.0),
+                      dens_range=(1e10, 1e20))
+    ref = oracle.RefLib("co2fits", 2)
+    out = {"rxn": ref.reaction_source(case)}
+    upd = ref.update_all(case, case.vd_params())
+    out.update({f"upd_{k}": v for k, v in upd.items()})
+    # rate_tol: the fit sums cancel terms up to ~1e5 times larger than the result, so
+    # a difference of a few ulp in pow() or in the summation moves a rate by up to
+    # ~1e-9 relative (the reference's own result carries the same spread)
+    _save("co2fits_2d", case, fm, out, {"ref": "co2fits", "rate_tol": 2e-9,
+                                        "header": "test/Reactor/CO2_H2_Ar_mechanism_reduced/Chemistry.H"})
 
     # 3. generated-header mechanisms of the workloads, one small box each
     gens = [

@@ -79,8 +79,13 @@ def test_calls_before_mech_init_fail_cleanly(lib):
     assert rc in (abi.ERR_MECH, abi.ERR_CUDA, abi.ERR_ARG, abi.ERR_DIM)
 
 
+def _co2fits():
+    from tests._util import load_fixture
+    return load_fixture("co2fits_2d")[0].mech
+
+
 @pytest.mark.parametrize("mech", [mm.argon(10, 20261204), mm.synthetic(8, 40, 20261224),
-                                  mm.synthetic(24, 150, 20261214)], ids=lambda m: m.name)
+                                  mm.synthetic(24, 150, 20261214), _co2fits()], ids=lambda m: m.name)
 def test_specialised_chemistry_compiles_for_sm100a(lib, mech):
     """vd_mech_init compiles the mechanism-specialised chemistry with NVRTC; the same
     source must compile here (no GPU needed) without local-memory spills of note."""

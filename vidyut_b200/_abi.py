@@ -12,7 +12,8 @@ import os
 from pathlib import Path
 
 MAX_SPECIES = 64
-MAX_REACTIONS = 512
+MAX_REACTIONS = 448
+MAX_FITS = 48
 MAX_REACTANTS = 3
 MAX_TERMS = 6
 
@@ -24,7 +25,9 @@ BC_PER, BC_DIRC, BC_HNEU, BC_IHNEU, BC_ROBIN = 0, 1, 2, 3, 4
 CLASS_ELECTRON, CLASS_ENERGY, CLASS_ION, CLASS_NEUTRAL = 0, 1, 2, 3
 
 RATE_ARRHENIUS_TE, RATE_CONST, RATE_ARRHENIUS_TG = 0, 1, 2
+RATE_JANEV, RATE_FFIT, RATE_JANEV_FFIT = 3, 4, 5
 RXN_NONE, RXN_EXCITATION, RXN_IONIZATION, RXN_RECOMB, RXN_ELASTIC = 0, 1, 2, 3, 5
+RXN_ATTACH, RXN_DETACH = 4, 7
 MOB_ZERO, MOB_ELECTRON, MOB_ION_TG, MOB_SCALED, MOB_CONST_N, MOB_CONST = 0, 1, 2, 3, 4, 5
 DIFF_ZERO, DIFF_TE_ABSMOB, DIFF_TG_MOB, DIFF_CONST = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
@@ -59,7 +62,13 @@ class VdReaction(C.Structure):
     _fields_ = [("kind", C.c_int32), ("nreac", C.c_int32), ("reac", C.c_int32 * MAX_REACTANTS),
                 ("rxntype", C.c_int32), ("elidx", C.c_int32), ("nterms", C.c_int32),
                 ("term_sp", C.c_int32 * MAX_TERMS), ("term_coef", C.c_double * MAX_TERMS),
-                ("A", C.c_double), ("b", C.c_double), ("C", C.c_double), ("eexci", C.c_double)]
+                ("A", C.c_double), ("b", C.c_double), ("C", C.c_double), ("eexci", C.c_double),
+                ("fit", C.c_int32), ("pad0", C.c_int32)]
+
+
+class VdRateFit(C.Structure):
+    _fields_ = [("jA", C.c_double), ("jc", C.c_double * 9), ("fA", C.c_double), ("fc", C.c_double * 4),
+                ("switch_ev", C.c_double)]
 
 
 class VdMech(C.Structure):
@@ -70,7 +79,8 @@ class VdMech(C.Structure):
                 ("diff_kind", C.c_int32 * (MAX_SPECIES + 1)), ("diff_ref", C.c_int32 * (MAX_SPECIES + 1)),
                 ("diff_factor", C.c_double * (MAX_SPECIES + 1)),
                 ("elastic_loss", C.c_int32), ("pad0", C.c_int32), ("elastic_mass", C.c_double),
-                ("rxn", VdReaction * MAX_REACTIONS)]
+                ("rxn", VdReaction * MAX_REACTIONS), ("nfits", C.c_int32), ("pad1", C.c_int32),
+                ("fits", VdRateFit * MAX_FITS)]
 
 
 class VdParams(C.Structure):

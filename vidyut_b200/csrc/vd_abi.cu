@@ -282,9 +282,19 @@ static int build_mech_table(const vd_mech* m, VdMechDev** out)
             return fail(VD_ERR_MECH, "species %d: diffusion reference invalid", s);
     }
     if (m->elastic_loss && !(m->elastic_mass > 0.0)) return fail(VD_ERR_MECH, "elastic_mass must be > 0");
+    if (m->nfits < 0 || m->nfits > VD_MAX_FITS) return fail(VD_ERR_MECH, "nfits %d outside [0,%d]", m->nfits, VD_MAX_FITS);
+    for (int f = 0; f < m->nfits; f++) {
+        const vd_rate_fit& F = m->fits[f];
+        bool ok = std::isfinite(F.jA) && std::isfinite(F.fA) && F.jA >= 0.0 && F.fA >= 0.0 && std::isfinite(F.switch_ev);
+        for (int j = 0; j < 9; j++) ok = ok && std::isfinite(F.jc[j]);
+        for (int j = 0; j < 4; j++) ok = ok && std::isfinite(F.fc[j]);
+        if (!ok) return fail(VD_ERR_MECH, "fit %d: coefficients must be finite, A >= 0", f);
+    }
     for (int r = 0; r < nr; r++) {
         const vd_reaction& R = m->rxn[r];
-        if (R.kind < 0 || R.kind > 2) return fail(VD_ERR_MECH, "reaction %d: unknown rate kind %d", r, R.kind);
+        if (R.kind < 0 || R.kind > 5) return fail(VD_ERR_MECH, "reaction %d: unknown rate kind %d", r, R.kind);
+        if (R.kind >= VD_RATE_JANEV && (R.fit < 0 || R.fit >= m->nfits))
+            return fail(VD_ERR_MECH, "reaction %d: fit index %d outside [0,%d)", r, R.fit, m->nfits);
         if (R.nreac < 1 || R.nreac > VD_MAX_REACTANTS)
             return fail(VD_ERR_MECH, "reaction %d: %d reactants", r, R.nreac);
         for (int t = 0; t < R.nreac; t++)
@@ -292,7 +302,7 @@ static int build_mech_table(const vd_mech* m, VdMechDev** out)
         if (R.nterms < 0 || R.nterms > VD_MAX_TERMS) return fail(VD_ERR_MECH, "reaction %d: bad term count", r);
         for (int t = 0; t < R.nterms; t++)
             if (R.term_sp[t] < 0 || R.term_sp[t] >= ns) return fail(VD_ERR_MECH, "reaction %d: bad term", r);
-        if (R.rxntype != 0 && R.rxntype != 1 && R.rxntype != 2 && R.rxntype != 3 && R.rxntype != 5)
+        if (R.rxntype < 0 || R.rxntype > 7 || R.rxntype == 6)
             return fail(VD_ERR_MECH, "reaction %d: unknown rxntype %d", r, R.rxntype);
         if (R.rxntype == VD_RXN_ELASTIC && (R.elidx < 0 || R.elidx >= ns))
             return fail(VD_ERR_MECH, "reaction %d: bad elidx", r);
@@ -320,6 +330,18 @@ static int build_mech_table(const vd_mech* m, VdMechDev** out)
         else if (m->mob_kind[s] == VD_MOB_ION_TG)
             d->mob_c[s] = (ECHARGE / m->mob_p1[s]) / std::sqrt(8.0 * K_B / PI / m->mob_p1[s]);
     }
+    d->nfits = m->nfits;
+    for (int f = 0; f < m->nfits; f++) {
+        const vd_rate_fit& F = m->fits[f];
+        VdFitDev& G = d->fits[f];
+        G.jA = F.jA;
+        G.fA = F.fA;
+        for (int j = 0; j < 9; j++) G.jc[j] = F.jc[j];
+        for (int j = 0; j < 4; j++) G.fc[j] = F.fc[j];
+        G.switch_ev = F.switch_ev;
+        G.l2jA = F.jA > 0.0 ? std::log2(F.jA * NA_CE) : -INFINITY;
+        G.l2fA = F.fA > 0.0 ? std::log2(F.fA * NA_CE) : -INFINITY;
+    }
     for (int r = 0; r < nr; r++) {
         const vd_reaction& R = m->rxn[r];
         VdRxnDev& D = d->rxn[r];
@@ -336,6 +358,7 @@ static int build_mech_table(const vd_mech* m, VdMechDev** out)
         D.rxntype = (int8_t)R.rxntype;
         D.elidx = (int8_t)R.elidx;
         D.nterms = (int8_t)R.nterms;
+        D.fit = (int8_t)(R.kind >= VD_RATE_JANEV ? R.fit : 0);
         for (int t = 0; t < R.nreac; t++) D.reac[t] = (int8_t)R.reac[t];
         for (int t = 0; t < R.nterms; t++) {
             D.sp[t] = (int8_t)R.term_sp[t];

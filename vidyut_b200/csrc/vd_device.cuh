@@ -401,6 +401,53 @@ __device__ __forceinline__ float exp2_split(double x)
 }
 
 // ---------------------------------------------------------------------------
+// Janev / F-fit electron-impact rates (test/Reactor/CO2_H2_Ar_mechanism_reduced/
+// Chemistry.H:940-1030): with Te_eV = Te/11595, tep[j] = ln(Te_eV)^j (j = 0..8) and
+// itp[j] = Te_eV^-(j+1) (j = 0..3; 1 for Te = 0),
+//   Janev  k = jA exp(sum_j jc_j tep[j]) NA,   F-fit  k = fA exp(sum_j fc_j itp[j]) NA,
+// the sums accumulated in order.  FP64 takes the powers with pow() as the header
+// does; the mixed path by products and the exponential on the FP32 unit.
+template <int PREC>
+__device__ __forceinline__ void fit_powers(double Te, double* tep, double* itp, double& teev)
+{
+    teev = Te / TE_FIT_EV;
+    const double lte = log(teev);
+    const double ite = (Te == 0) ? 1.0 : 1.0 / teev;
+    if (PREC == PREC_FP64) {
+#pragma unroll
+        for (int j = 0; j < 9; j++) tep[j] = pow(lte, (double)j);
+#pragma unroll
+        for (int j = 0; j < 4; j++) itp[j] = pow(ite, (double)(j + 1));
+    } else {
+        tep[0] = 1.0;
+#pragma unroll
+        for (int j = 1; j < 9; j++) tep[j] = tep[j - 1] * lte;
+        itp[0] = ite;
+#pragma unroll
+        for (int j = 1; j < 4; j++) itp[j] = itp[j - 1] * ite;
+    }
+}
+template <int PREC>
+__device__ __forceinline__ double fit_rate(int kind, const VdFitDev& F, const double* tep, const double* itp,
+                                           double teev)
+{
+    const bool janev = kind == VD_RATE_JANEV || (kind == VD_RATE_JANEV_FFIT && teev < F.switch_ev);
+    // products and sums rounded separately as the header's loop (no contraction):
+    // the sums cancel terms up to ~1e5 times larger than the result
+    double sum = 0.0;
+    if (janev) {
+#pragma unroll
+        for (int j = 0; j < 9; j++) sum = __dadd_rn(sum, __dmul_rn(F.jc[j], tep[j]));
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++) sum = __dadd_rn(sum, __dmul_rn(F.fc[j], itp[j]));
+    }
+    if (PREC == PREC_FP64) return (janev ? F.jA : F.fA) * exp(sum) * NA_CE;
+    constexpr double LOG2E = 1.4426950408889634074;
+    return (double)exp2_split(fma(sum, LOG2E, janev ? F.l2jA : F.l2fA));
+}
+
+// ---------------------------------------------------------------------------
 // CKWC for one cell (Source/ScalarSolve.cpp:143-157 + the generated productionRate,
 // test/models/Ar_DC_1d/Chemistry.H:315-506).  The thread's species arrays live in
 // shared memory with a stride of the block size ([species][thread]): every thread
@@ -432,6 +479,10 @@ __device__ __forceinline__ double chem_cell(double* sc, double* wd, const int st
         lnTg = log2(Tg);
     }
     const double invTe = 1.0 / Te, invTg = 1.0 / Tg;
+    // the powers of ln(Te_eV) and 1/Te_eV the fit rates share
+    // (test/Reactor/CO2_H2_Ar_mechanism_reduced/Chemistry.H:945-952)
+    double tep[9], itp[4], teev = 0.0;
+    if (c_mech.nfits > 0) fit_powers<PREC>(Te, tep, itp, teev);
     double ee = 0.0;
     const int nr = c_mech.nr;
     for (int r = 0; r < nr; r++) {
@@ -439,6 +490,8 @@ __device__ __forceinline__ double chem_cell(double* sc, double* wd, const int st
         double k;
         if (R.kind == VD_RATE_CONST) {
             k = R.A;
+        } else if (R.kind >= VD_RATE_JANEV) {
+            k = fit_rate<PREC>(R.kind, c_mech.fits[R.fit], tep, itp, teev);
         } else {
             const bool te = (R.kind == VD_RATE_ARRHENIUS_TE);
             const double lT = te ? lnTe : lnTg;
@@ -458,8 +511,10 @@ __device__ __forceinline__ double chem_cell(double* sc, double* wd, const int st
         }
         if (R.rxntype == VD_RXN_EXCITATION || R.rxntype == VD_RXN_IONIZATION) {
             ee -= R.ex * q * sefact;
-        } else if (R.rxntype == VD_RXN_RECOMB) {
+        } else if (R.rxntype == VD_RXN_RECOMB || R.rxntype == VD_RXN_ATTACH) {
             ee -= mee_na * q;
+        } else if (R.rxntype == VD_RXN_DETACH) {
+            ee += mee_na * q;
         } else if (R.rxntype == VD_RXN_ELASTIC) {
             ee -= R.ex * dT * (sce * sc[R.elidx * st] * k) * NA_CE;
         }

@@ -191,11 +191,53 @@ std::string gen_prep_kernel(const VdMechDev& m, int prec)
     if (prec == PREC_FP64) o << "    const double lTe = log(Te), lTg = log(Tg);\n";
     else o << "    const double lTe = log2(Te), lTg = log2(Tg);\n";
     o << "    const double invTe = 1.0 / Te, invTg = 1.0 / Tg;\n    double ee = 0.0;\n";
+    if (m.nfits > 0) {
+        // the powers the Janev / F-fit rates share (fit_powers in vd_device.cuh)
+        o << "    const double teev = Te / " << hexd(TE_FIT_EV) << ", lte = log(teev);\n"
+          << "    const double ite = (Te == 0) ? 1.0 : 1.0 / teev;\n";
+        if (prec == PREC_FP64) {
+            for (int j = 0; j < 9; j++) o << "    const double tep" << j << " = pow(lte, " << j << ".0);\n";
+            for (int j = 0; j < 4; j++) o << "    const double itp" << j << " = pow(ite, " << (j + 1) << ".0);\n";
+        } else {
+            o << "    const double tep0 = 1.0;\n";
+            for (int j = 1; j < 9; j++) o << "    const double tep" << j << " = tep" << (j - 1) << " * lte;\n";
+            o << "    const double itp0 = ite;\n";
+            for (int j = 1; j < 4; j++) o << "    const double itp" << j << " = itp" << (j - 1) << " * ite;\n";
+        }
+    }
+    // a fit rate's sum, accumulated in order as the header does (fit_rate)
+    auto fit_sum = [&](const VdFitDev& F, bool janev) {
+        o << "        double sum = 0.0;\n";
+        if (janev)
+            for (int j = 0; j < 9; j++)
+                o << "        sum = __dadd_rn(sum, __dmul_rn(" << hexd(F.jc[j]) << ", tep" << j << "));\n";
+        else
+            for (int j = 0; j < 4; j++)
+                o << "        sum = __dadd_rn(sum, __dmul_rn(" << hexd(F.fc[j]) << ", itp" << j << "));\n";
+        if (prec == PREC_FP64)
+            o << "        k = " << hexd(janev ? F.jA : F.fA) << " * exp(sum) * NA_CE;\n";
+        else
+            o << "        k = (double)exp2_split(fma(sum, " << hexd(1.4426950408889634074) << ", "
+              << hexd(janev ? F.l2jA : F.l2fA) << "));\n";
+    };
     for (int r = 0; r < m.nr; r++) {
         const VdRxnDev& R = m.rxn[r];
         o << "    { // reaction " << r << "\n      double k;\n";
         if (R.kind == VD_RATE_CONST) {
             o << "      k = " << hexd(R.A) << ";\n";
+        } else if (R.kind >= VD_RATE_JANEV) {
+            const VdFitDev& F = m.fits[R.fit];
+            if (R.kind == VD_RATE_JANEV_FFIT) {
+                o << "      if (teev < " << hexd(F.switch_ev) << ") {\n";
+                fit_sum(F, true);
+                o << "      } else {\n";
+                fit_sum(F, false);
+                o << "      }\n";
+            } else {
+                o << "      {\n";
+                fit_sum(F, R.kind == VD_RATE_JANEV);
+                o << "      }\n";
+            }
         } else if (!(R.A > 0.0)) {
             o << "      k = 0.0;\n";
         } else {
@@ -217,8 +259,10 @@ std::string gen_prep_kernel(const VdMechDev& m, int prec)
             o << "      w" << (int)R.sp[t] << " = fma(" << hexd(R.coef[t]) << ", q, w" << (int)R.sp[t] << ");\n";
         if (R.rxntype == VD_RXN_EXCITATION || R.rxntype == VD_RXN_IONIZATION)
             o << "      ee -= " << hexd(R.ex) << " * q * sefact;\n";
-        else if (R.rxntype == VD_RXN_RECOMB)
+        else if (R.rxntype == VD_RXN_RECOMB || R.rxntype == VD_RXN_ATTACH)
             o << "      ee -= mee_na * q;\n";
+        else if (R.rxntype == VD_RXN_DETACH)
+            o << "      ee += mee_na * q;\n";
         else if (R.rxntype == VD_RXN_ELASTIC)
             o << "      ee -= " << hexd(R.ex) << " * dT * (sc" << eid << " * sc" << (int)R.elidx << " * k) * NA_CE;\n";
         o << "    }\n";
@@ -286,9 +330,10 @@ int spec_build(const VdMechDev& m)
         g_spec_err = "nvrtcCreateProgram failed";
         return 2;
     }
+    // 177: concentrations of species that are no reactant are declared but unused
     const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-default-device", "--fmad=true",
-                          "--extra-device-vectorization"};
-    nvrtcResult rc = nvrtcCompileProgram(prog, 5, opts);
+                          "--extra-device-vectorization", "--diag-suppress=177"};
+    nvrtcResult rc = nvrtcCompileProgram(prog, 6, opts);
     if (rc != NVRTC_SUCCESS) {
         size_t n = 0;
         nvrtcGetProgramLogSize(prog, &n);
@@ -348,8 +393,8 @@ int spec_compile_only(const VdMechDev& m, size_t* cubin_bytes)
         return 2;
     }
     const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-default-device", "--fmad=true",
-                          "--ptxas-options=-v"};
-    nvrtcResult rc = nvrtcCompileProgram(prog, 5, opts);
+                          "--ptxas-options=-v", "--diag-suppress=177"};
+    nvrtcResult rc = nvrtcCompileProgram(prog, 6, opts);
     size_t n = 0;
     nvrtcGetProgramLogSize(prog, &n);
     std::string log(n, '\0');

@@ -18,6 +18,7 @@ constexpr double EV = ECHARGE / K_B;          // kelvin per eV
 constexpr double NA_CE = 6.02214085774e23;    // Avogadro as written in comp_ener_exch
 constexpr double KB_CE = 1.380649e-23;
 constexpr double EV2J = 1.602176620800000e-19;
+constexpr double TE_FIT_EV = 11595.0;         // kelvin per eV of the Janev / F-fit headers
 
 enum { PREC_FP64 = 0, PREC_MIXED = 1 };
 
@@ -31,7 +32,14 @@ struct VdRxnDev {
     int8_t kind, nreac, rxntype, elidx, nterms;
     int8_t reac[VD_MAX_REACTANTS];
     int8_t sp[VD_MAX_TERMS];
-    int8_t pad[2];
+    int8_t fit;               // index into VdMechDev::fits for the fit rate kinds
+    int8_t pad;
+};
+
+// Janev / F-fit coefficients; l2jA = log2(jA NA), l2fA = log2(fA NA) for the
+// mixed-precision rate
+struct VdFitDev {
+    double jA, jc[9], fA, fc[4], switch_ev, l2jA, l2fA;
 };
 
 struct VdMechDev {
@@ -46,8 +54,10 @@ struct VdMechDev {
     int8_t mob_ref[VD_MAX_SPECIES + 1];
     int8_t diff_kind[VD_MAX_SPECIES + 1];
     int8_t diff_ref[VD_MAX_SPECIES + 1];
-    int8_t pad[7];
+    int8_t pad[3];
+    int32_t nfits;
     VdRxnDev rxn[VD_MAX_REACTIONS];
+    VdFitDev fits[VD_MAX_FITS];
 };
 static_assert(sizeof(VdMechDev) <= 64000, "mechanism table must fit in constant memory");
 

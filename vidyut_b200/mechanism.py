@@ -51,6 +51,9 @@ class Reaction:
     elidx: int = 0
     terms: list = field(default_factory=list)   # [(species, coef)] update order
     label: str = ""
+    # fit rate kinds (RATE_JANEV, RATE_FFIT, RATE_JANEV_FFIT): {"jA", "jc" (9), "fA",
+    # "fc" (4), "switch_ev"} as the CO2 reactor header writes them
+    fit: dict | None = None
 
     def fill_terms(self) -> "Reaction":
         """Default update order: species ascending; reactant loss then product gain."""
@@ -115,6 +118,7 @@ class Mechanism:
             m.diff_factor[s] = float(self.diff_factor[s])
         m.elastic_loss = int(self.elastic_loss)
         m.elastic_mass = float(self.elastic_mass)
+        nfits = 0
         for i, r in enumerate(self.reactions):
             r.fill_terms()
             if len(r.terms) > abi.MAX_TERMS or len(r.reactants) > abi.MAX_REACTANTS:
@@ -131,6 +135,19 @@ class Mechanism:
                 c.term_sp[t] = s
                 c.term_coef[t] = coef
             c.A, c.b, c.C, c.eexci = float(r.A), float(r.b), float(r.C), float(r.eexci)
+            if r.kind >= abi.RATE_JANEV:
+                if nfits >= abi.MAX_FITS:
+                    raise ValueError("too many fit rates")
+                f = m.fits[nfits]
+                f.jA, f.fA = float(r.fit.get("jA", 0.0)), float(r.fit.get("fA", 0.0))
+                for j, v in enumerate(r.fit.get("jc", [0.0] * 9)):
+                    f.jc[j] = float(v)
+                for j, v in enumerate(r.fit.get("fc", [0.0] * 4)):
+                    f.fc[j] = float(v)
+                f.switch_ev = float(r.fit.get("switch_ev", 0.0))
+                c.fit = nfits
+                nfits += 1
+        m.nfits = nfits
         return m
 
     def to_dict(self) -> dict:
