@@ -130,6 +130,10 @@ typedef struct vd_box {
 #define VD_RATE_JANEV        3   /* k = jA exp(sum_{j=0..8} jc_j ln(Te_eV)^j) NA    */
 #define VD_RATE_FFIT         4   /* k = fA exp(sum_{j=0..3} fc_j Te_eV^-(j+1)) NA    */
 #define VD_RATE_JANEV_FFIT   5   /* Janev below Te_eV = switch_ev, F-fit from there  */
+/* field-driven ionisation (test/verification/Streamer/Chemistry.H:266-280) with
+ * E = EN * N * 1e-21 (EN the cell's reduced field REF [Td], N the density sum) and
+ * c = fits[fit].jc: k = ((c0 + c1/E^3) exp(-c2/E) - c3) * c4 E^c5 * E  [1/s]     */
+#define VD_RATE_TOWNSEND     6
 
 /* electron-energy exchange types (comp_ener_exch, rxntype) */
 #define VD_RXN_NONE       0
@@ -147,11 +151,26 @@ typedef struct vd_box {
 #define VD_MOB_SCALED    3   /* mu = p0 * mu[ref]                                          */
 #define VD_MOB_CONST_N   4   /* mu = p0 / N                                                */
 #define VD_MOB_CONST     5   /* mu = p0                                                    */
+#define VD_MOB_POW_EMAG  6   /* mu = p0 * |E|^p1 (test/verification/Streamer/Chemistry.H:169) */
+/* the two models of test/verification/He_RF_1d/Chemistry.H:218-265, coefficients
+ * c = fits[mob_ref].jc (mob_ref is the fit index for these two kinds):          */
+#define VD_MOB_EN_POLY   7   /* mu = p0 * (1 + c0 x^2 + c1 x^4)^p1, x = |E|/N               */
+#define VD_MOB_EXP_MEANE 8   /* mu = p0 * exp(c0 + c1 ln m + c2/m + c3/m^2 + c4/m^3) / N,
+                                m = 1.5 Te/eV (the mean electron energy in eV)             */
 /* diffusion models (specDiff) */
 #define VD_DIFF_ZERO       0
 #define VD_DIFF_TE_ABSMOB  1   /* D = (factor * Te/eV) * |mu[ref]|  */
 #define VD_DIFF_TG_MOB     2   /* D = (factor * Tg/eV) *  mu[ref]   */
 #define VD_DIFF_CONST      3   /* D = factor (e.g. test/models/ionelec_DC_1d/Chemistry.H:190-209) */
+#define VD_DIFF_POW_EMAG   4   /* D = factor * |E|^diff_p1 (Streamer/Chemistry.H:189)            */
+/* pressure-scaled coefficients, P_r = 101325 / (N kB Tg) (He_RF_1d/Chemistry.H:267-299) */
+#define VD_DIFF_PRES       5   /* D = factor * P_r                                               */
+#define VD_DIFF_TE_PRES    6   /* D = factor * (Te / diff_p1) * P_r                              */
+#define VD_DIFF_SCALED     7   /* D = factor * D[ref]                                            */
+/* |E| in mobilities and diffusion coefficients: the magnitude of the cell-centred
+ * field of the state (EFX..EFZ) for the drift velocity and the diffusion solve;
+ * of the two cells' average over the active directions for the Joule term
+ * (Source/ElecEnergySource.cpp:103-119); EN * N * 1e-21 in the chemistry.       */
 
 typedef struct vd_reaction {
     int32_t kind;                       /* VD_RATE_*                                   */
@@ -181,12 +200,13 @@ typedef struct vd_mech {
     int32_t charge[VD_MAX_SPECIES];                 /* CKCHRG                         */
     double  mw[VD_MAX_SPECIES];                     /* g/mol (get_mw)                 */
     int32_t mob_kind[VD_MAX_SPECIES + 1];
-    int32_t mob_ref[VD_MAX_SPECIES + 1];
+    int32_t mob_ref[VD_MAX_SPECIES + 1];            /* SCALED: species; 7, 8: fit     */
     double  mob_p0[VD_MAX_SPECIES + 1];             /* cross section [m^2] / factor   */
-    double  mob_p1[VD_MAX_SPECIES + 1];             /* particle mass [kg]             */
+    double  mob_p1[VD_MAX_SPECIES + 1];             /* particle mass [kg] / exponent  */
     int32_t diff_kind[VD_MAX_SPECIES + 1];
     int32_t diff_ref[VD_MAX_SPECIES + 1];
     double  diff_factor[VD_MAX_SPECIES + 1];
+    double  diff_p1[VD_MAX_SPECIES + 1];            /* VD_DIFF_POW_EMAG exponent      */
     int32_t elastic_loss;                           /* trailing elastic-collision loss */
     int32_t pad0;
     double  elastic_mass;                           /* heavy-partner mass [kg]        */

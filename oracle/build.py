@@ -57,6 +57,8 @@ def _ref_cases():
         ("axisym_ar", t / "models" / "Axisymmetric_streamer_Ar", (2,), [], None),
         ("ionelec", t / "models" / "ionelec_DC_1d", (1, 2), [], None),
         ("advect", t / "verification" / "Advect", (2, 3), ["-DVD_PROBPARM_HAS_VEL"], None),
+        ("streamer", t / "verification" / "Streamer", (2,), [], None),
+        ("he_rf", t / "verification" / "He_RF_1d", (1,), [], None),
     ]
     gen = [
         (mm.argon(10, BASE_SEED + 1), (1, 2, 3)),            # argon 2-D workload mechanism

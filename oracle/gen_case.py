@@ -43,6 +43,8 @@ def _mob_expr(m: Mechanism, s: int) -> str:
         return f"{{ mob = {_r(m.mob_p0[s])}/ndens; }}"
     if k == abi.MOB_CONST:
         return f"{{ mob = {_r(m.mob_p0[s])}; }}"
+    if k != abi.MOB_ZERO:  # the |E| forms are pinned on the reference's own headers
+        raise ValueError(f"mobility kind {k} is not generated")
     return "{ mob = 0.0; }"
 
 
@@ -56,6 +58,8 @@ def _diff_expr(m: Mechanism, s: int) -> str:
                 f" dcoeff = {_r(m.diff_factor[s])}*Tg_in_ev*mb; }}")
     if k == abi.DIFF_CONST:
         return f"{{ dcoeff = {_r(m.diff_factor[s])}; }}"
+    if k != abi.DIFF_ZERO:
+        raise ValueError(f"diffusion kind {k} is not generated")
     return "{ dcoeff = 0.0; }"
 
 
@@ -135,6 +139,8 @@ def chemistry_h(m: Mechanism) -> str:
     for i, r in enumerate(m.reactions):
         r.fill_terms()
         w(f"  {{\n    // reaction {i}: {r.label}")
+        if r.kind == abi.RATE_TOWNSEND:
+            raise ValueError("the field-driven rate is pinned on the Streamer header, not generated")
         if r.kind >= abi.RATE_JANEV:
             w("    Janev_sum = 0.0;\n    amrex::Real k_f;")
             if r.kind == abi.RATE_JANEV_FFIT:

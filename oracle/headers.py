@@ -11,6 +11,11 @@ unmodified in oracle/_ref.  Forms read:
       mobilities and diffusion coefficients (Chemistry.H:167-209)
   test/Reactor/CO2_H2_Ar_mechanism_reduced         its Janev / F-fit electron-impact
       reactions (Chemistry.H:940-1030) as a sub-mechanism (fit_submechanism)
+  test/verification/Streamer                       the field-driven ionisation rate and
+      power laws in |E| for the electron mobility and diffusion (Chemistry.H:164-282)
+  test/verification/He_RF_1d                       E/N-polynomial ion mobility, mean-energy
+      fit electron mobility, pressure-scaled diffusion, elastic loss with
+      |E| = EN N 1e-21 (Chemistry.H:217-299,603-625)
 """
 from __future__ import annotations
 
@@ -102,8 +107,13 @@ def header_reactions(txt: str, names: list):
         b1 = " ".join(blk.split())
         mk = re.search(r"k_f = " + NUM + r"\*std::pow\(Te,(-?[0-9.eE+-]+)\)\*std::exp\((-?[0-9.eE+-]+)/Te\)", b1)
         mk2 = re.search(r"k_f = " + NUM + r"\*std::exp\((-?[0-9.eE+-]+)/Te\)\*" + NUM + r"\s*;", b1)
+        # A Te^b alone (He_RF_1d): A Te^b exp(-0/Te) is the same number
+        mk3 = re.search(r"k_f = " + NUM + r"\*std::pow\(Te,(-?[0-9.eE+-]+)\)\s*;", b1)
         if mk:
             A, b, C = float(mk.group(1)), float(mk.group(2)), -float(mk.group(3))
+            kind = abi.RATE_ARRHENIUS_TE
+        elif mk3:
+            A, b, C = float(mk3.group(1)), float(mk3.group(2)), 0.0
             kind = abi.RATE_ARRHENIUS_TE
         elif mk2:  # A exp(-C/Te) times Avogadro's number (ionelec_DC_1d)
             A, b, C = float(mk2.group(1)) * float(mk2.group(3)), 0.0, -float(mk2.group(2))
@@ -208,3 +218,92 @@ def fit_submechanism(path: Path, name: str) -> mm.Mechanism:
     return mm.Mechanism(name=name, species=[n.replace("+", "p") for n in sub_names], charge=sub_charge,
                         mw=[mw[s] for s in order], e_id=0, reactions=rx, elastic_loss=0, elastic_mass=0.0,
                         bg_species=[], **tr)
+
+
+def _num(pat: str, txt: str, group: int = 1) -> float:
+    return float(re.search(pat, txt, re.S).group(group))
+
+
+def _transport_table(ns: int) -> dict:
+    return dict(mob_kind=[abi.MOB_ZERO] * (ns + 1), mob_ref=[0] * (ns + 1), mob_p0=[0.0] * (ns + 1),
+                mob_p1=[0.0] * (ns + 1), diff_kind=[abi.DIFF_ZERO] * (ns + 1), diff_ref=[0] * (ns + 1),
+                diff_factor=[0.0] * (ns + 1), diff_p1=[0.0] * (ns + 1))
+
+
+def streamer_header(path: Path, name: str, bg: list) -> mm.Mechanism:
+    """Mechanism table of the Streamer verification header
+    (test/verification/Streamer/Chemistry.H): electron mobility p0 |E|^p1 and
+    diffusion f |E|^q, the energy's 5/3 of both, an immobile ion, and the one
+    field-driven ionisation reaction (alpha - eta) mu_e |E| of :260-281, first
+    order in the electrons, with wdot updates E +1, N2 -1, N2p +1."""
+    txt = Path(path).read_text()
+    names, charge, mw = header_species(txt)
+    ns = len(names)
+    e_id = names.index("E")
+    mob = re.search(r"specMob\(.*?\n\}", txt, re.S).group(0)
+    dif = re.search(r"specDiff\(.*?\n\}", txt, re.S).group(0)
+    tr = _transport_table(ns)
+    m = re.search(r"elecmob\s*=\s*(-?[0-9.eE+-]+)\*std::pow\(emag,(-?[0-9.eE+-]+)\)", mob)
+    tr["mob_kind"][e_id], tr["mob_p0"][e_id], tr["mob_p1"][e_id] = abi.MOB_POW_EMAG, float(m.group(1)), float(m.group(2))
+    m = re.search(r"elecdcoeff\s*=\s*(-?[0-9.eE+-]+)\s*\*\s*std::pow\(emag,(-?[0-9.eE+-]+)\)", dif)
+    tr["diff_kind"][e_id], tr["diff_factor"][e_id], tr["diff_p1"][e_id] = \
+        abi.DIFF_POW_EMAG, float(m.group(1)), float(m.group(2))
+    assert re.search(r"mob=\(5\.0/3\.0\)\*elecmob", mob) and re.search(r"dcoeff=\(5\.0/3\.0\)\*elecdcoeff", dif)
+    tr["mob_kind"][ns], tr["mob_ref"][ns], tr["mob_p0"][ns] = abi.MOB_SCALED, e_id, 5.0 / 3.0
+    tr["diff_kind"][ns], tr["diff_ref"][ns], tr["diff_factor"][ns] = abi.DIFF_SCALED, e_id, 5.0 / 3.0
+    body = " ".join(production_rate_body(txt).split())
+    c = [_num(r"alpha = \(" + NUM + r" \+", body), _num(r"\+ " + NUM + r"/std::pow\(efield_mag,3\.0\)", body),
+         _num(r"std::exp\(-" + NUM + r"/efield_mag\)", body), _num(r"eta = " + NUM + r";", body)]
+    m = re.search(r"mu_e = " + NUM + r" \* std::pow\(efield_mag,(-?[0-9.eE+-]+)\)", body)
+    c += [float(m.group(1)), float(m.group(2))]
+    terms = [(_species_index(sp, names), 1.0 if op == "+" else -1.0)
+             for sp, op in re.findall(r"wdot\[(\w+)\] ([+-])= k_f\*sc\[E_ID\];", body)]
+    rx = [mm.Reaction([e_id], [], 0.0, kind=abi.RATE_TOWNSEND, terms=terms, label="N2 + E => E + N2p + E",
+                      fit={"jc": c + [0.0] * 3})]
+    return mm.Mechanism(name=name, species=names, charge=charge, mw=mw, e_id=e_id, reactions=rx,
+                        elastic_loss=0, elastic_mass=0.0, bg_species=[names.index(b) for b in bg], **tr)
+
+
+def he_rf_header(path: Path, name: str, bg: list) -> mm.Mechanism:
+    """Mechanism table of the He_RF_1d verification header
+    (test/verification/He_RF_1d/Chemistry.H): the ions' mobility
+    p0 (1 + c0 (|E|/N)^2 + c1 (|E|/N)^4)^p, the electrons' exp(mean-energy fit)/N,
+    pressure-scaled diffusion (the electrons' also times Te / T0), the energy's
+    5/3 of the electrons' mobility and diffusion, Arrhenius / constant rates and
+    the elastic loss of CKWC (:603-625) with a 4 amu partner."""
+    txt = Path(path).read_text()
+    names, charge, mw = header_species(txt)
+    ns = len(names)
+    e_id = names.index("E")
+    mob = re.search(r"specMob\(.*?\n\}", txt, re.S).group(0)
+    dif = re.search(r"specDiff\(.*?\n\}", txt, re.S).group(0)
+    tr = _transport_table(ns)
+    mob_coef = {}
+    m = re.search(r"(\w+)mob=" + NUM + r"\*std::pow\(\(1\.0\+" + NUM + r"\*std::pow\(EbyN,2\.0\)\+" + NUM
+                  + r"\*std::pow\(EbyN,4\.0\)\),(-?[0-9.eE+-]+)\);", mob)
+    ion_var, p0, c0, c1, pw = m.group(1), float(m.group(2)), float(m.group(3)), float(m.group(4)), float(m.group(5))
+    same = {ion_var} | set(re.findall(r"(\w+)mob=" + ion_var + r"mob;", mob))
+    for sp, var in re.findall(r"if\(specid==(\w+)_ID\)\s*\{(?:\s*//[^\n]*)*\s*mob=(\w+);", mob):
+        if var in {v + "mob" for v in same}:
+            s = names.index(sp)
+            tr["mob_kind"][s], tr["mob_p0"][s], tr["mob_p1"][s] = abi.MOB_EN_POLY, p0, pw
+            mob_coef[str(s)] = [c0, c1]
+    m = re.search(r"elecmob = \((-?[0-9.]+)\)\*std::exp\(" + NUM + r" \+ " + NUM + r"\*std::log\(meanE\) \+ "
+                  + NUM + r"/meanE\s*-" + NUM + r"/std::pow\(meanE,2\.0\) \+ \(" + NUM
+                  + r"\)/std::pow\(meanE,3\.0\)\) / ndens;", mob)
+    tr["mob_kind"][e_id], tr["mob_p0"][e_id] = abi.MOB_EXP_MEANE, float(m.group(1))
+    mob_coef[str(e_id)] = [float(m.group(2)), float(m.group(3)), float(m.group(4)), -float(m.group(5)),
+                           float(m.group(6))]
+    tr["mob_kind"][ns], tr["mob_ref"][ns], tr["mob_p0"][ns] = abi.MOB_SCALED, e_id, 5.0 / 3.0
+    m = re.search(r"elecdcoeff=" + NUM + r"\*\(Te/" + NUM + r"\)\*Pres_ratio;", dif)
+    tr["diff_kind"][e_id], tr["diff_factor"][e_id], tr["diff_p1"][e_id] = \
+        abi.DIFF_TE_PRES, float(m.group(1)), float(m.group(2))
+    for sp, v in re.findall(r"if\(specid==(\w+)_ID\)\s*\{(?:\s*//[^\n]*)*\s*dcoeff=" + NUM + r"\*Pres_ratio;", dif):
+        s = names.index(sp)
+        tr["diff_kind"][s], tr["diff_factor"][s] = abi.DIFF_PRES, float(v)
+    tr["diff_kind"][ns], tr["diff_ref"][ns], tr["diff_factor"][ns] = abi.DIFF_SCALED, e_id, 5.0 / 3.0
+    rx = header_reactions(txt, names)
+    el_amu = float(re.search(r"\(2\.0\*ME/\(([0-9.]+)\*M_AMU\)\)", txt).group(1))
+    return mm.Mechanism(name=name, species=names, charge=charge, mw=mw, e_id=e_id, reactions=rx,
+                        elastic_loss=1, elastic_mass=el_amu * mm.M_AMU, bg_species=[names.index(b) for b in bg],
+                        mob_coef=mob_coef, **tr)

@@ -19,6 +19,7 @@
 #include "vd_amrex_shim.H"
 #include <ProbParm.H>
 #include <Chemistry.H>
+#include <VarDefines.H>  /* before UserFunctions.H, as Vidyut.H orders them */
 #include <UserFunctions.H>
 #include <compute_explicit_flux.H>
 #include "../../include/vidyut_b200.h"

@@ -32,6 +32,7 @@
 #define ECHARGE 1.60217662e-19
 #define eV (ECHARGE / K_B)
 #define ME 9.10938188e-31
+#define P_NTP 101325.0
 #define fivebythree (5.0 / 3.0)
 #define twothird (2.0 / 3.0)
 
@@ -44,10 +45,10 @@ static inline double *A4P(const vd_array4 *a, int i, int j, int k, int n)
 #define A4(a, i, j, k, n) (*A4P((a), (i), (j), (k), (n)))
 
 /* ------------------------------------------------------------------------- */
-/* specMob (test/models/Ar_DC_1d/Chemistry.H:177-202), table-driven.           */
+/* specMob (test/models/Ar_DC_1d/Chemistry.H:177-202), table-driven; the power
+ * law in |E| of test/verification/Streamer/Chemistry.H:165-183.                 */
 double orc_specmob(const vd_mech *m, int specid, double Te, double ndens, double emag, double T)
 {
-    (void)emag;
     int kind = m->mob_kind[specid];
     double mob = 0.0;
     if (kind == VD_MOB_ELECTRON) {
@@ -65,6 +66,19 @@ double orc_specmob(const vd_mech *m, int specid, double Te, double ndens, double
         mob = m->mob_p0[specid] / ndens;
     } else if (kind == VD_MOB_CONST) {
         mob = m->mob_p0[specid];
+    } else if (kind == VD_MOB_POW_EMAG) {
+        mob = m->mob_p0[specid] * pow(emag, m->mob_p1[specid]);
+    } else if (kind == VD_MOB_EN_POLY) {
+        /* test/verification/He_RF_1d/Chemistry.H:231-238 (the ions) */
+        const double *c = m->fits[m->mob_ref[specid]].jc;
+        double EbyN = emag / ndens;
+        mob = m->mob_p0[specid] * pow((1.0 + c[0] * pow(EbyN, 2.0) + c[1] * pow(EbyN, 4.0)), m->mob_p1[specid]);
+    } else if (kind == VD_MOB_EXP_MEANE) {
+        /* test/verification/He_RF_1d/Chemistry.H:232,242-243 (the electrons) */
+        const double *c = m->fits[m->mob_ref[specid]].jc;
+        double meanE = 1.5 * Te / eV;
+        mob = m->mob_p0[specid] * exp(c[0] + c[1] * log(meanE) + c[2] / meanE + c[3] / pow(meanE, 2.0) +
+                                      c[4] / pow(meanE, 3.0)) / ndens;
     }
     return mob;
 }
@@ -85,6 +99,20 @@ double orc_specdiff(const vd_mech *m, int specid, double Te, double ndens, doubl
     } else if (kind == VD_DIFF_CONST) {
         /* a constant coefficient (test/models/ionelec_DC_1d/Chemistry.H:190-209) */
         dcoeff = m->diff_factor[specid];
+    } else if (kind == VD_DIFF_POW_EMAG) {
+        /* test/verification/Streamer/Chemistry.H:185-204 */
+        dcoeff = m->diff_factor[specid] * pow(emag, m->diff_p1[specid]);
+    } else if (kind == VD_DIFF_PRES || kind == VD_DIFF_TE_PRES) {
+        /* test/verification/He_RF_1d/Chemistry.H:270-296 */
+        double Pg = ndens * K_B * T;
+        double Pres_ratio = (P_NTP / Pg);
+        if (kind == VD_DIFF_PRES)
+            dcoeff = m->diff_factor[specid] * Pres_ratio;
+        else
+            dcoeff = m->diff_factor[specid] * (Te / m->diff_p1[specid]) * Pres_ratio;
+    } else if (kind == VD_DIFF_SCALED) {
+        /* the energy's 5/3 of the electrons' coefficient (Streamer/Chemistry.H:199-202) */
+        dcoeff = m->diff_factor[specid] * orc_specdiff(m, m->diff_ref[specid], Te, ndens, emag, T);
     }
     return dcoeff;
 }
@@ -143,9 +171,22 @@ static double orc_fit_rate(const vd_mech *m, const vd_reaction *r, double Te)
     return F->fA * exp(Janev_sum) * 6.02214085774e23;
 }
 
-/* k_f of one reaction (productionRate, e.g. Ar_DC_1d/Chemistry.H:392). */
-static double orc_rate(const vd_mech *m, const vd_reaction *r, double T, double Te)
+/* Field-driven ionisation (test/verification/Streamer/Chemistry.H:266-280) at the
+ * field magnitude efm, coefficients c = fits[fit].jc in the header's order.   */
+static double orc_townsend_rate(const double *c, double efm)
 {
+    double alpha = (c[0] + c[1] / pow(efm, 3.0)) * exp(-c[2] / efm);
+    double eta = c[3];
+    double alpha_bar = alpha - eta;
+    double mu_e = c[4] * pow(efm, c[5]);
+    return alpha_bar * mu_e * efm;
+}
+
+/* k_f of one reaction (productionRate, e.g. Ar_DC_1d/Chemistry.H:392); efm is
+ * the field magnitude EN * N * 1e-21 of the field-driven kinds. */
+static double orc_rate(const vd_mech *m, const vd_reaction *r, double T, double Te, double efm)
+{
+    if (r->kind == VD_RATE_TOWNSEND) return orc_townsend_rate(m->fits[r->fit].jc, efm);
     if (r->kind == VD_RATE_ARRHENIUS_TE) return r->A * pow(Te, r->b) * exp(-r->C / Te);
     if (r->kind == VD_RATE_ARRHENIUS_TG) return r->A * pow(T, r->b) * exp(-r->C / T);
     if (r->kind >= VD_RATE_JANEV) return orc_fit_rate(m, r, Te);
@@ -157,14 +198,17 @@ static double orc_rate(const vd_mech *m, const vd_reaction *r, double T, double 
 void orc_production_rate(const vd_mech *m, double *wdot, const double *sc, double T, double Te,
                          double EN, double *enerExch)
 {
-    (void)EN;
     int ns = m->nspecies;
     for (int i = 0; i < ns; ++i) wdot[i] = 0.0;
+    /* E/N [Td] to |E| (test/verification/Streamer/Chemistry.H:256-264) */
+    double mixture = 0.0;
+    for (int i = 0; i < ns; ++i) mixture += sc[i];
+    double efm = EN * (mixture * 6.02214076e23) * 1e-21;
     double ne = sc[m->e_id] * 6.02214085774e23;
     double Ue = 1.5 * Te * ne * 1.380649e-23;
     for (int ir = 0; ir < m->nreactions; ++ir) {
         const vd_reaction *r = &m->rxn[ir];
-        double k_f = orc_rate(m, r, T, Te);
+        double k_f = orc_rate(m, r, T, Te, efm);
         double prod = sc[r->reac[0]];
         for (int t = 1; t < r->nreac; ++t) prod = prod * sc[r->reac[t]];
         double qf = k_f * prod;
@@ -176,10 +220,11 @@ void orc_production_rate(const vd_mech *m, double *wdot, const double *sc, doubl
                                Te);
     }
     if (m->elastic_loss) {
-        /* Ar_DC_1d/Chemistry.H:479-486 */
-        double emag = 0.0;
+        /* Ar_DC_1d/Chemistry.H:479-486; |E| = EN N 1e-21 as the He_RF_1d header
+         * passes it (its mobility reads it; the argon ones pass 0 and do not) */
         double ndens = 0.0;
         for (int sp = 0; sp < ns; sp++) ndens += sc[sp] * N_A;
+        double emag = EN * ndens * 1.0e-21;
         double mu = orc_specmob(m, m->e_id, Te, ndens, emag, T);
         double nu = -ECHARGE / ME / mu;
         double term = 3.0 / 2.0 * K_B * sc[m->e_id] * N_A * (Te - T) * nu *
@@ -645,16 +690,19 @@ void orc_fill_ghosts(const vd_box *bx, const vd_array4 *a, int ng, const int *pe
 /* gross magnitude of productionRate: gw[s] = sum |coef*qdot|, *ge = sum of the
  * absolute energy-exchange terms (same order and units as orc_production_rate). */
 static void orc_production_gross(const vd_mech *m, double *gw, const double *sc, double T, double Te,
-                                 double *ge)
+                                 double EN, double *ge)
 {
     int ns = m->nspecies;
     for (int i = 0; i < ns; ++i) gw[i] = 0.0;
     *ge = 0.0;
+    double mixture = 0.0;
+    for (int i = 0; i < ns; ++i) mixture += sc[i];
+    double efm = EN * (mixture * 6.02214076e23) * 1e-21;
     double ne = sc[m->e_id] * 6.02214085774e23;
     double Ue = 1.5 * Te * ne * 1.380649e-23;
     for (int ir = 0; ir < m->nreactions; ++ir) {
         const vd_reaction *r = &m->rxn[ir];
-        double k_f = orc_rate(m, r, T, Te);
+        double k_f = orc_rate(m, r, T, Te, efm);
         double prod = sc[r->reac[0]];
         for (int t = 1; t < r->nreac; ++t) prod = prod * sc[r->reac[t]];
         double q = k_f * prod;
@@ -668,7 +716,7 @@ static void orc_production_gross(const vd_mech *m, double *gw, const double *sc,
     if (m->elastic_loss) {
         double ndens = 0.0;
         for (int sp = 0; sp < ns; sp++) ndens += sc[sp] * N_A;
-        double mu = orc_specmob(m, m->e_id, Te, ndens, 0.0, T);
+        double mu = orc_specmob(m, m->e_id, Te, ndens, EN * ndens * 1.0e-21, T);
         double nu = -ECHARGE / ME / mu;
         *ge += fabs(3.0 / 2.0 * K_B * sc[m->e_id] * N_A * (Te - T) * nu * (2.0 * ME / m->elastic_mass));
     }
@@ -688,7 +736,8 @@ int orc_update_scale(const vd_mech *m, const vd_box *bx, const vd_array4 *sb, co
                 double sc[VD_MAX_SPECIES], gw[VD_MAX_SPECIES], ge = 0.0;
                 for (int sp = 0; sp < ns; sp++) sc[sp] = A4(sb, i, j, k, sp) * 1.0e-6 / N_A * 1.0e6;
                 if (p->do_reactions)
-                    orc_production_gross(m, gw, sc, p->Tg, A4(sb, i, j, k, VD_ETEMP(ns)), &ge);
+                    orc_production_gross(m, gw, sc, p->Tg, A4(sb, i, j, k, VD_ETEMP(ns)),
+                                         A4(sb, i, j, k, VD_REF(ns)), &ge);
                 else
                     for (int sp = 0; sp < ns; sp++) gw[sp] = 0.0;
                 for (int sp = 0; sp < ns; sp++) A4(scale, i, j, k, sp) = gw[sp] * 1.0e-6 * N_A * 1.0e6;
@@ -747,10 +796,15 @@ int orc_update_scale(const vd_mech *m, const vd_box *bx, const vd_array4 *sb, co
                                                       A4(sb, face[0], face[1], face[2], VD_EFX(ns) + idim))
                                              : A4(&ef[idim], face[0], face[1], face[2], 0);
                             double gn = A4(&gne[idim], face[0], face[1], face[2], 0);
+                            double esum = 0.0;
+                            for (int d = 0; d < dim; d++)
+                                esum += sq(0.5 * (A4(sb, l[0], l[1], l[2], VD_EFX(ns) + d) +
+                                                  A4(sb, face[0], face[1], face[2], VD_EFX(ns) + d)));
+                            double emag = sqrt(esum);
                             double mu = p->const_ele_trans ? p->ele_mob / ndens
-                                                           : orc_specmob(m, eidx, etemp, ndens, 0.0, p->Tg);
+                                                           : orc_specmob(m, eidx, etemp, ndens, emag, p->Tg);
                             double dc = p->const_ele_trans ? p->ele_diff / ndens
-                                                           : orc_specdiff(m, eidx, etemp, ndens, 0.0, p->Tg);
+                                                           : orc_specdiff(m, eidx, etemp, ndens, emag, p->Tg);
                             g += charge * (fabs(mu * ne * efc * efc) + fabs(dc * gn * efc));
                         }
                     A4(scale, i, j, k, ns) += 0.5 * g;

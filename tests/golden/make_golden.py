@@ -2,7 +2,7 @@
 
 Run here, where the reference tree and oracle/_ref/ exist:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [fixture ...]   # all, or only the named ones
 
 1. Parses the reference's test/models/Ar_DC_1d/Chemistry.H (species, charges,
    molecular weights, the specMob constants, every productionRate block) into a
@@ -33,7 +33,7 @@ from vidyut_b200 import mechanism as mm  # noqa: E402
 from vidyut_b200.inputs import build_case, BASE_SEED  # noqa: E402
 import oracle  # noqa: E402
 from oracle.build import REF_TREE, build_ref  # noqa: E402
-from oracle.headers import fit_submechanism, parse_case_header  # noqa: E402
+from oracle.headers import fit_submechanism, he_rf_header, parse_case_header, streamer_header  # noqa: E402
 
 FLUX_VARIANTS = [(1, 3), (2, 3), (5, 1), (5, 2), (5, 3)]
 
@@ -53,7 +53,12 @@ def advect_mechanism() -> mm.Mechanism:
                         bg_species=[])
 
 
+ONLY: set = set()   # fixture names to write (empty: all)
+
+
 def _save(name: str, case, mech: mm.Mechanism, out: dict, meta: dict):
+    if ONLY and name not in ONLY:
+        return
     arrays = {"state": case.state}
     for d in range(3):
         arrays[f"efield{d}"] = case.efield[d]
@@ -104,6 +109,24 @@ def main():
             _save(f"{name}_{dim}d", case, m, out, {"ref": name, "header": f"test/models/{sub}/Chemistry.H",
                                                    "exact": name != "ionelec"})
 
+    # 1c. the verification headers with field-dependent transport: Streamer (power
+    # laws in |E|, the field-driven ionisation rate, which reads the reduced field
+    # REF) and He_RF_1d (|E|/N and mean-energy mobility fits, pressure-scaled
+    # diffusion, the elastic loss at |E| = EN N 1e-21)
+    vmodels = [("streamer", "Streamer", streamer_header, ["N2"], 2, 1),
+               ("he_rf", "He_RF_1d", he_rf_header, ["HE"], 1, 1)]
+    for name, sub, parse, bg, dim, een in vmodels:
+        m = parse(REF_TREE / "test" / "verification" / sub / "Chemistry.H", name, bg)
+        n = (12, 10) if dim == 2 else (48,)
+        case = build_case(m, dim, n, (1e-5,) * dim, BASE_SEED + 130 + dim, density="blob", te_range_ev=(0.5, 5.0),
+                          params=dict(elecenergy_solve=een))
+        ref = oracle.RefLib(name, dim)
+        out = {"rxn": ref.reaction_source(case)}
+        out.update(flux_outputs(ref, case, range(m.ns + 1)))
+        upd = ref.update_all(case, case.vd_params())
+        out.update({f"upd_{k}": v for k, v in upd.items()})
+        _save(f"{name}_{dim}d", case, m, out, {"ref": name, "header": f"test/verification/{sub}/Chemistry.H"})
+
     # 2. the Advect verification case: constant user velocity (udv=1) for AR
     am = advect_mechanism()
     case = build_case(am, 2, (16, 6), (0.1, 0.1), BASE_SEED + 102, density="loguniform", dens_range=(1.0, 2.0))
@@ -151,4 +174,5 @@ def main():
 
 
 if __name__ == "__main__":
+    ONLY.update(sys.argv[1:])
     main()

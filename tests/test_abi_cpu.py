@@ -62,6 +62,21 @@ def test_mechanism_validation_rejects_bad_tables(lib):
     m = mm.argon(10, 1).to_c()
     m.rxn[0].A = -1.0
     assert lib.vd_mech_init(C.byref(m)) == abi.ERR_MECH
+    # field-dependent models: the coefficient fit must exist, kinds must be known,
+    # the temperature scale of the pressure-scaled diffusion nonzero
+    m = mm.argon(10, 1).to_c()
+    m.mob_kind[0], m.mob_ref[0] = abi.MOB_EXP_MEANE, 0
+    assert lib.vd_mech_init(C.byref(m)) == abi.ERR_MECH
+    assert b"fit index" in lib.vd_last_error()
+    m = mm.argon(10, 1).to_c()
+    m.diff_kind[0] = 8
+    assert lib.vd_mech_init(C.byref(m)) == abi.ERR_MECH
+    m = mm.argon(10, 1).to_c()
+    m.diff_kind[0], m.diff_p1[0] = abi.DIFF_TE_PRES, 0.0
+    assert lib.vd_mech_init(C.byref(m)) == abi.ERR_MECH
+    m = mm.argon(10, 1).to_c()
+    m.rxn[0].kind, m.rxn[0].fit = abi.RATE_TOWNSEND, 0
+    assert lib.vd_mech_init(C.byref(m)) == abi.ERR_MECH
 
 
 def test_calls_before_mech_init_fail_cleanly(lib):
@@ -79,13 +94,14 @@ def test_calls_before_mech_init_fail_cleanly(lib):
     assert rc in (abi.ERR_MECH, abi.ERR_CUDA, abi.ERR_ARG, abi.ERR_DIM)
 
 
-def _co2fits():
+def _fixture_mech(name):
     from tests._util import load_fixture
-    return load_fixture("co2fits_2d")[0].mech
+    return load_fixture(name)[0].mech
 
 
 @pytest.mark.parametrize("mech", [mm.argon(10, 20261204), mm.synthetic(8, 40, 20261224),
-                                  mm.synthetic(24, 150, 20261214), _co2fits()], ids=lambda m: m.name)
+                                  mm.synthetic(24, 150, 20261214), _fixture_mech("co2fits_2d"),
+                                  _fixture_mech("streamer_2d"), _fixture_mech("he_rf_1d")], ids=lambda m: m.name)
 def test_specialised_chemistry_compiles_for_sm100a(lib, mech):
     """vd_mech_init compiles the mechanism-specialised chemistry with NVRTC; the same
     source must compile here (no GPU needed) without local-memory spills of note."""

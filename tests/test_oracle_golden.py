@@ -7,7 +7,8 @@ restated per-box loops of Source/ScalarSolve.cpp and Source/ElecEnergySource.cpp
 -- compiled against the AMReX shim.  ar_dc_1d_2d and advect_2d use the
 reference's own case headers unchanged (test/models/Ar_DC_1d,
 test/verification/Advect); axisym_ar_2d and ionelec_{1,2}d use the
-Axisymmetric_streamer_Ar and ionelec_DC_1d headers unchanged."""
+Axisymmetric_streamer_Ar and ionelec_DC_1d headers unchanged; streamer_2d and
+he_rf_1d the test/verification/Streamer and He_RF_1d headers."""
 import numpy as np
 import pytest
 
@@ -58,6 +59,9 @@ def test_fixture_set_complete():
     assert "ar_dc_1d_2d" in FIXTURES and "advect_2d" in FIXTURES
     # every case header of test/models: Ar_DC_1d, Axisymmetric_streamer_Ar, ionelec_DC_1d
     assert {"axisym_ar_2d", "ionelec_1d", "ionelec_2d"} <= set(FIXTURES)
+    # the verification headers with field-dependent transport and rates, and the
+    # CO2 reactor header's fit rates
+    assert {"streamer_2d", "he_rf_1d", "co2fits_2d"} <= set(FIXTURES)
     dims = {load_fixture(n)[1]["dim"] for n in FIXTURES}
     assert dims == {1, 2, 3}
 
@@ -73,3 +77,34 @@ def test_ar_dc_1d_mechanism_parsed():
     # ionization AR + E => ARp + E + E: k = 42581353.6 Te^0.60983 exp(-1.8712e5/Te)
     r0 = m.reactions[0]
     assert (r0.A, r0.b, r0.C, r0.rxntype, r0.eexci) == (42581353.6, 0.60983, 1.8712e5, 2, 16.0)
+
+
+def test_streamer_mechanism_parsed():
+    """test/verification/Streamer/Chemistry.H:164-282: mu_e = -2.3987 |E|^-0.26,
+    D_e = 4.3628e-3 |E|^0.22, the energy's 5/3 of both, and the one field-driven
+    ionisation N2 + E => E + N2p + E, first order in the electrons"""
+    from vidyut_b200 import _abi as abi
+    m = load_fixture("streamer_2d")[0].mech
+    assert m.species == ["E", "N2", "N2p"]
+    assert (m.mob_kind[0], m.mob_p0[0], m.mob_p1[0]) == (abi.MOB_POW_EMAG, -2.3987, -0.26)
+    assert (m.diff_kind[0], m.diff_factor[0], m.diff_p1[0]) == (abi.DIFF_POW_EMAG, 4.3628e-3, 0.22)
+    assert (m.mob_kind[3], m.diff_kind[3]) == (abi.MOB_SCALED, abi.DIFF_SCALED)
+    (r,) = m.reactions
+    assert r.kind == abi.RATE_TOWNSEND and r.reactants == [0]
+    assert r.fit["jc"][:6] == [1.1944e6, 4.3666e26, 2.73e7, 340.75, 2.3987, -0.26]
+    assert [tuple(t) for t in r.terms] == [(0, 1.0), (1, -1.0), (2, 1.0)]
+
+
+def test_he_rf_mechanism_parsed():
+    """test/verification/He_RF_1d/Chemistry.H:217-299: He+ and He2+ share the
+    2.69 (1 + 1.2e-3 x^2 + 4.2e-8 x^4)^-0.125 mobility, the electrons' mean-energy
+    fit, pressure-scaled diffusion; nine reactions, elastic loss on 4 amu"""
+    from vidyut_b200 import _abi as abi
+    m = load_fixture("he_rf_1d")[0].mech
+    assert m.species == ["E", "HE", "HEp", "HEm", "HE2p", "HE2m"]
+    assert m.mob_kind[:6] == [abi.MOB_EXP_MEANE, 0, abi.MOB_EN_POLY, 0, abi.MOB_EN_POLY, 0]
+    assert m.mob_coef["0"] == [55.0, 0.3942, 2.134, -0.6433, 0.07112]
+    assert m.mob_coef["2"] == m.mob_coef["4"] == [1.2e-3, 4.2e-8]
+    assert m.diff_kind[:6] == [abi.DIFF_TE_PRES, 0] + [abi.DIFF_PRES] * 4
+    assert (m.diff_factor[0], m.diff_p1[0]) == (0.1737, 17406.0)
+    assert len(m.reactions) == 9 and m.elastic_loss == 1

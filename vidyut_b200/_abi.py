@@ -25,11 +25,13 @@ BC_PER, BC_DIRC, BC_HNEU, BC_IHNEU, BC_ROBIN = 0, 1, 2, 3, 4
 CLASS_ELECTRON, CLASS_ENERGY, CLASS_ION, CLASS_NEUTRAL = 0, 1, 2, 3
 
 RATE_ARRHENIUS_TE, RATE_CONST, RATE_ARRHENIUS_TG = 0, 1, 2
-RATE_JANEV, RATE_FFIT, RATE_JANEV_FFIT = 3, 4, 5
+RATE_JANEV, RATE_FFIT, RATE_JANEV_FFIT, RATE_TOWNSEND = 3, 4, 5, 6
 RXN_NONE, RXN_EXCITATION, RXN_IONIZATION, RXN_RECOMB, RXN_ELASTIC = 0, 1, 2, 3, 5
 RXN_ATTACH, RXN_DETACH = 4, 7
 MOB_ZERO, MOB_ELECTRON, MOB_ION_TG, MOB_SCALED, MOB_CONST_N, MOB_CONST = 0, 1, 2, 3, 4, 5
+MOB_POW_EMAG, MOB_EN_POLY, MOB_EXP_MEANE = 6, 7, 8
 DIFF_ZERO, DIFF_TE_ABSMOB, DIFF_TG_MOB, DIFF_CONST = 0, 1, 2, 3
+DIFF_POW_EMAG, DIFF_PRES, DIFF_TE_PRES, DIFF_SCALED = 4, 5, 6, 7
 PREC_FP64, PREC_MIXED = 0, 1
 NOALLOC_SCRATCH_BYTES = 64 << 20
 
@@ -77,7 +79,7 @@ class VdMech(C.Structure):
                 ("mob_kind", C.c_int32 * (MAX_SPECIES + 1)), ("mob_ref", C.c_int32 * (MAX_SPECIES + 1)),
                 ("mob_p0", C.c_double * (MAX_SPECIES + 1)), ("mob_p1", C.c_double * (MAX_SPECIES + 1)),
                 ("diff_kind", C.c_int32 * (MAX_SPECIES + 1)), ("diff_ref", C.c_int32 * (MAX_SPECIES + 1)),
-                ("diff_factor", C.c_double * (MAX_SPECIES + 1)),
+                ("diff_factor", C.c_double * (MAX_SPECIES + 1)), ("diff_p1", C.c_double * (MAX_SPECIES + 1)),
                 ("elastic_loss", C.c_int32), ("pad0", C.c_int32), ("elastic_mass", C.c_double),
                 ("rxn", VdReaction * MAX_REACTIONS), ("nfits", C.c_int32), ("pad1", C.c_int32),
                 ("fits", VdRateFit * MAX_FITS)]

@@ -264,9 +264,14 @@ static int build_mech_table(const vd_mech* m, VdMechDev** out)
     if (nr < 0 || nr > VD_MAX_REACTIONS)
         return fail(VD_ERR_MECH, "nreactions %d outside [0,%d]", nr, VD_MAX_REACTIONS);
     if (m->e_id < 0 || m->e_id >= ns) return fail(VD_ERR_MECH, "electron index %d invalid", m->e_id);
+    if (m->nfits < 0 || m->nfits > VD_MAX_FITS) return fail(VD_ERR_MECH, "nfits %d outside [0,%d]", m->nfits, VD_MAX_FITS);
     for (int s = 0; s <= ns; s++) {
         int k = m->mob_kind[s];
-        if (k < 0 || k > 5) return fail(VD_ERR_MECH, "species %d: unknown mobility kind %d", s, k);
+        if (k < 0 || k > 8) return fail(VD_ERR_MECH, "species %d: unknown mobility kind %d", s, k);
+        if ((k == VD_MOB_POW_EMAG || k == VD_MOB_EN_POLY) && !std::isfinite(m->mob_p1[s]))
+            return fail(VD_ERR_MECH, "species %d: mobility exponent must be finite", s);
+        if ((k == VD_MOB_EN_POLY || k == VD_MOB_EXP_MEANE) && (m->mob_ref[s] < 0 || m->mob_ref[s] >= m->nfits))
+            return fail(VD_ERR_MECH, "species %d: mobility fit index %d outside [0,%d)", s, m->mob_ref[s], m->nfits);
         if (k == VD_MOB_SCALED) {
             int r = m->mob_ref[s];
             if (r < 0 || r > ns || m->mob_kind[r] == VD_MOB_SCALED)
@@ -277,12 +282,18 @@ static int build_mech_table(const vd_mech* m, VdMechDev** out)
         if (k == VD_MOB_ION_TG && !(m->mob_p1[s] > 0.0))
             return fail(VD_ERR_MECH, "species %d: particle mass must be > 0", s);
         int dk = m->diff_kind[s];
-        if (dk < 0 || dk > 3) return fail(VD_ERR_MECH, "species %d: unknown diffusion kind %d", s, dk);
-        if ((dk == VD_DIFF_TE_ABSMOB || dk == VD_DIFF_TG_MOB) && (m->diff_ref[s] < 0 || m->diff_ref[s] > ns))
+        if (dk < 0 || dk > 7) return fail(VD_ERR_MECH, "species %d: unknown diffusion kind %d", s, dk);
+        if (dk == VD_DIFF_POW_EMAG && !std::isfinite(m->diff_p1[s]))
+            return fail(VD_ERR_MECH, "species %d: |E| exponent must be finite", s);
+        if (dk == VD_DIFF_TE_PRES && !(std::isfinite(m->diff_p1[s]) && m->diff_p1[s] != 0.0))
+            return fail(VD_ERR_MECH, "species %d: temperature scale must be finite and nonzero", s);
+        if ((dk == VD_DIFF_TE_ABSMOB || dk == VD_DIFF_TG_MOB || dk == VD_DIFF_SCALED) &&
+            (m->diff_ref[s] < 0 || m->diff_ref[s] > ns))
             return fail(VD_ERR_MECH, "species %d: diffusion reference invalid", s);
+        if (dk == VD_DIFF_SCALED && m->diff_kind[m->diff_ref[s]] == VD_DIFF_SCALED)
+            return fail(VD_ERR_MECH, "species %d: scaled diffusion must refer to an unscaled model", s);
     }
     if (m->elastic_loss && !(m->elastic_mass > 0.0)) return fail(VD_ERR_MECH, "elastic_mass must be > 0");
-    if (m->nfits < 0 || m->nfits > VD_MAX_FITS) return fail(VD_ERR_MECH, "nfits %d outside [0,%d]", m->nfits, VD_MAX_FITS);
     for (int f = 0; f < m->nfits; f++) {
         const vd_rate_fit& F = m->fits[f];
         bool ok = std::isfinite(F.jA) && std::isfinite(F.fA) && F.jA >= 0.0 && F.fA >= 0.0 && std::isfinite(F.switch_ev);
@@ -292,7 +303,7 @@ static int build_mech_table(const vd_mech* m, VdMechDev** out)
     }
     for (int r = 0; r < nr; r++) {
         const vd_reaction& R = m->rxn[r];
-        if (R.kind < 0 || R.kind > 5) return fail(VD_ERR_MECH, "reaction %d: unknown rate kind %d", r, R.kind);
+        if (R.kind < 0 || R.kind > 6) return fail(VD_ERR_MECH, "reaction %d: unknown rate kind %d", r, R.kind);
         if (R.kind >= VD_RATE_JANEV && (R.fit < 0 || R.fit >= m->nfits))
             return fail(VD_ERR_MECH, "reaction %d: fit index %d outside [0,%d)", r, R.fit, m->nfits);
         if (R.nreac < 1 || R.nreac > VD_MAX_REACTANTS)
@@ -326,6 +337,7 @@ static int build_mech_table(const vd_mech* m, VdMechDev** out)
         d->diff_kind[s] = (int8_t)m->diff_kind[s];
         d->diff_ref[s] = (int8_t)m->diff_ref[s];
         d->diff_factor[s] = m->diff_factor[s];
+        d->diff_p1[s] = m->diff_p1[s];
         if (m->mob_kind[s] == VD_MOB_ELECTRON) d->mob_c[s] = (-ECHARGE / ME) / std::sqrt(8.0 * K_B / PI / ME);
         else if (m->mob_kind[s] == VD_MOB_ION_TG)
             d->mob_c[s] = (ECHARGE / m->mob_p1[s]) / std::sqrt(8.0 * K_B / PI / m->mob_p1[s]);
@@ -341,6 +353,46 @@ static int build_mech_table(const vd_mech* m, VdMechDev** out)
         G.switch_ev = F.switch_ev;
         G.l2jA = F.jA > 0.0 ? std::log2(F.jA * NA_CE) : -INFINITY;
         G.l2fA = F.fA > 0.0 ? std::log2(F.fA * NA_CE) : -INFINITY;
+    }
+    // |E| reaches the electrons' transport when their mobility (or the one it
+    // scales, or their diffusion coefficient's) is a power of |E|
+    // (or a function of |E|/N)
+    auto mob_emag = [&](int s) {
+        int k = m->mob_kind[s];
+        if (k == VD_MOB_SCALED) k = m->mob_kind[m->mob_ref[s]];
+        return k == VD_MOB_POW_EMAG || k == VD_MOB_EN_POLY;
+    };
+    auto diff_emag = [&](int s) {
+        int dk = m->diff_kind[s];
+        if (dk == VD_DIFF_SCALED) {
+            s = m->diff_ref[s];
+            dk = m->diff_kind[s];
+        }
+        return dk == VD_DIFF_POW_EMAG || ((dk == VD_DIFF_TE_ABSMOB || dk == VD_DIFF_TG_MOB) && mob_emag(m->diff_ref[s]));
+    };
+    {
+        const int e = m->e_id;
+        d->emag_e = (int8_t)(mob_emag(e) || diff_emag(e));
+        bool en = m->elastic_loss && mob_emag(e);
+        for (int r = 0; r < nr; r++) en = en || m->rxn[r].kind == VD_RATE_TOWNSEND;
+        d->need_en = (int8_t)en;
+    }
+    {
+        // the transport tile stages at most kMaxBases velocity bases
+        VelBasis bs[VD_MAX_SPECIES + 1];
+        int nb = 0;
+        for (int s = 0; s <= ns; s++) {
+            VelBasis b;
+            double K;
+            if (!velocity_basis(*d, s, 300.0, &b, &K)) continue;
+            bool seen = false;
+            for (int q = 0; q < nb; q++) seen = seen || same_basis(*d, bs[q], b);
+            if (!seen) bs[nb++] = b;
+        }
+        if (nb > kMaxBases) {
+            delete d;
+            return fail(VD_ERR_MECH, "the mobility models need %d velocity bases (at most %d)", nb, kMaxBases);
+        }
     }
     for (int r = 0; r < nr; r++) {
         const vd_reaction& R = m->rxn[r];

@@ -35,50 +35,99 @@ __device__ __forceinline__ float rcp_approx(float x)
 // ---------------------------------------------------------------------------
 // Mobility (specMob, test/models/Ar_DC_1d/Chemistry.H:177-202) by model kind.
 // FP64: mob_c = -e/me / sqrt(8 kB/(pi me)) (electron) or e/M / sqrt(8 kB/(pi M))
-// (ion), so mu = mob_c / (sqrt(T) N sigma): one sqrt and one division.
-__device__ __forceinline__ double mob_base_fp64(int s, double Te, double N, double Tg)
+// (ion), so mu = mob_c / (sqrt(T) N sigma): one sqrt and one division.  emag is
+// the field magnitude |E| the caller's reference loop passes to specMob (power
+// laws in |E|, test/verification/Streamer/Chemistry.H:165-183).
+// The He_RF_1d header's models (test/verification/He_RF_1d/Chemistry.H:229-243),
+// in its order of operations: the ion form (1 + c0 x^2 + c1 x^4)^p of x = |E|/N,
+// and the electron form exp(c0 + c1 ln m + c2/m + c3/m^2 + c4/m^3) of the mean
+// energy m = 1.5 Te/eV (the constant factor and the 1/N are the caller's).
+__device__ __forceinline__ double mob_en_poly(const double* c, double p, double emag, double N)
+{
+    const double x = emag / N;
+    return pow(1.0 + c[0] * pow(x, 2.0) + c[1] * pow(x, 4.0), p);
+}
+__device__ __forceinline__ double mob_exp_meane(const double* c, double Te)
+{
+    const double m = 1.5 * Te / EV;
+    return exp(c[0] + c[1] * log(m) + c[2] / m + c[3] / pow(m, 2.0) + c[4] / pow(m, 3.0));
+}
+__device__ __forceinline__ double mob_base_fp64(int s, double Te, double N, double Tg, double emag)
 {
     switch (c_mech.mob_kind[s]) {
     case VD_MOB_ELECTRON: return c_mech.mob_c[s] / (sqrt(Te) * N * c_mech.mob_p0[s]);
     case VD_MOB_ION_TG: return c_mech.mob_c[s] / (sqrt(Tg) * N * c_mech.mob_p0[s]);
     case VD_MOB_CONST_N: return c_mech.mob_p0[s] / N;
     case VD_MOB_CONST: return c_mech.mob_p0[s];
+    case VD_MOB_POW_EMAG: return c_mech.mob_p0[s] * pow(emag, c_mech.mob_p1[s]);
+    case VD_MOB_EN_POLY: return c_mech.mob_p0[s] * mob_en_poly(c_mech.fits[c_mech.mob_ref[s]].jc, c_mech.mob_p1[s], emag, N);
+    case VD_MOB_EXP_MEANE: return c_mech.mob_p0[s] * mob_exp_meane(c_mech.fits[c_mech.mob_ref[s]].jc, Te) / N;
     default: return 0.0;
     }
 }
-__device__ __forceinline__ double mob_fp64(int s, double Te, double N, double Tg)
+__device__ __forceinline__ double mob_fp64(int s, double Te, double N, double Tg, double emag)
 {
     if (c_mech.mob_kind[s] == VD_MOB_SCALED)
-        return c_mech.mob_p0[s] * mob_base_fp64(c_mech.mob_ref[s], Te, N, Tg);
-    return mob_base_fp64(s, Te, N, Tg);
+        return c_mech.mob_p0[s] * mob_base_fp64(c_mech.mob_ref[s], Te, N, Tg, emag);
+    return mob_base_fp64(s, Te, N, Tg, emag);
 }
-__device__ __forceinline__ float mob_base_f32(int s, float Te, float N, float Tg)
+__device__ __forceinline__ float mob_base_f32(int s, float Te, float N, float Tg, float emag)
 {
     switch (c_mech.mob_kind[s]) {
     case VD_MOB_ELECTRON: return (float)c_mech.mob_c[s] * rsqrtf(Te) * rcp_approx(N * (float)c_mech.mob_p0[s]);
     case VD_MOB_ION_TG: return (float)c_mech.mob_c[s] * rsqrtf(Tg) * rcp_approx(N * (float)c_mech.mob_p0[s]);
     case VD_MOB_CONST_N: return (float)c_mech.mob_p0[s] * rcp_approx(N);
     case VD_MOB_CONST: return (float)c_mech.mob_p0[s];
+    case VD_MOB_POW_EMAG: return (float)c_mech.mob_p0[s] * exp2f((float)c_mech.mob_p1[s] * log2f(emag));
+    // the exponential's argument is too large for FP32 (e^55 in the He_RF_1d fit)
+    case VD_MOB_EN_POLY:
+    case VD_MOB_EXP_MEANE: return (float)mob_base_fp64(s, Te, N, Tg, emag);
     default: return 0.0f;
     }
 }
-__device__ __forceinline__ float mob_f32(int s, float Te, float N, float Tg)
+__device__ __forceinline__ float mob_f32(int s, float Te, float N, float Tg, float emag)
 {
     if (c_mech.mob_kind[s] == VD_MOB_SCALED)
-        return (float)c_mech.mob_p0[s] * mob_base_f32(c_mech.mob_ref[s], Te, N, Tg);
-    return mob_base_f32(s, Te, N, Tg);
+        return (float)c_mech.mob_p0[s] * mob_base_f32(c_mech.mob_ref[s], Te, N, Tg, emag);
+    return mob_base_f32(s, Te, N, Tg, emag);
 }
 // specDiff (test/models/Ar_DC_1d/Chemistry.H:204-239) by model kind.
-__device__ __forceinline__ double diff_fp64(int s, double Te, double N, double Tg)
+__device__ __forceinline__ double diff_base_fp64(int s, double Te, double N, double Tg, double emag)
 {
     switch (c_mech.diff_kind[s]) {
     case VD_DIFF_TE_ABSMOB:
-        return c_mech.diff_factor[s] * (Te / EV) * fabs(mob_fp64(c_mech.diff_ref[s], Te, N, Tg));
+        return c_mech.diff_factor[s] * (Te / EV) * fabs(mob_fp64(c_mech.diff_ref[s], Te, N, Tg, emag));
     case VD_DIFF_TG_MOB:
-        return c_mech.diff_factor[s] * (Tg / EV) * mob_fp64(c_mech.diff_ref[s], Te, N, Tg);
+        return c_mech.diff_factor[s] * (Tg / EV) * mob_fp64(c_mech.diff_ref[s], Te, N, Tg, emag);
     case VD_DIFF_CONST: return c_mech.diff_factor[s];
+    case VD_DIFF_POW_EMAG: return c_mech.diff_factor[s] * pow(emag, c_mech.diff_p1[s]);
+    // P_NTP / (N kB Tg) (test/verification/He_RF_1d/Chemistry.H:270-296)
+    case VD_DIFF_PRES: return c_mech.diff_factor[s] * (P_NTP / (N * K_B * Tg));
+    case VD_DIFF_TE_PRES: return c_mech.diff_factor[s] * (Te / c_mech.diff_p1[s]) * (P_NTP / (N * K_B * Tg));
     default: return 0.0;
     }
+}
+// specDiff with the scaled model (D = factor * D[ref], the energy's 5/3 of the
+// electrons' coefficient in the Streamer and He_RF_1d headers)
+__device__ __forceinline__ double diff_fp64(int s, double Te, double N, double Tg, double emag)
+{
+    if (c_mech.diff_kind[s] == VD_DIFF_SCALED)
+        return c_mech.diff_factor[s] * diff_base_fp64(c_mech.diff_ref[s], Te, N, Tg, emag);
+    return diff_base_fp64(s, Te, N, Tg, emag);
+}
+__device__ __forceinline__ float diff_f32(int s, float Te, float N, float Tg, float emag, float mu_e)
+{
+    // mu_e: the electron mobility when s's model refers to it (saves its re-evaluation)
+    const int dk = c_mech.diff_kind[s], dr = c_mech.diff_ref[s];
+    if (dk == VD_DIFF_TE_ABSMOB || dk == VD_DIFF_TG_MOB) {
+        const float mr = dr == c_mech.e_id ? mu_e : mob_f32(dr, Te, N, Tg, emag);
+        if (dk == VD_DIFF_TE_ABSMOB) return (float)c_mech.diff_factor[s] * (Te * (float)(1.0 / EV)) * fabsf(mr);
+        return (float)c_mech.diff_factor[s] * (Tg * (float)(1.0 / EV)) * mr;
+    }
+    if (dk == VD_DIFF_CONST) return (float)c_mech.diff_factor[s];
+    if (dk == VD_DIFF_POW_EMAG) return (float)c_mech.diff_factor[s] * exp2f((float)c_mech.diff_p1[s] * log2f(emag));
+    if (dk == VD_DIFF_ZERO) return 0.0f;
+    return (float)diff_fp64(s, Te, N, Tg, emag);
 }
 
 // ---------------------------------------------------------------------------
@@ -447,6 +496,16 @@ __device__ __forceinline__ double fit_rate(int kind, const VdFitDev& F, const do
     return (double)exp2_split(fma(sum, LOG2E, janev ? F.l2jA : F.l2fA));
 }
 
+// Field-driven ionisation rate (test/verification/Streamer/Chemistry.H:266-280):
+// alpha = (c0 + c1/E^3) exp(-c2/E), the attachment c3, mu_e = c4 E^c5,
+// k = (alpha - c3) mu_e E, in the header's order of operations (FP64 in both paths).
+__device__ __forceinline__ double townsend_rate(const double* c, double E)
+{
+    const double alpha = (c[0] + c[1] / pow(E, 3.0)) * exp(-c[2] / E);
+    const double mu_e = c[4] * pow(E, c[5]);
+    return (alpha - c[3]) * mu_e * E;
+}
+
 // ---------------------------------------------------------------------------
 // CKWC for one cell (Source/ScalarSolve.cpp:143-157 + the generated productionRate,
 // test/models/Ar_DC_1d/Chemistry.H:315-506).  The thread's species arrays live in
@@ -456,7 +515,7 @@ __device__ __forceinline__ double fit_rate(int kind, const VdFitDev& F, const do
 // On entry sc[s*st] holds the number density of species s [1/m^3]; on exit
 // wd[s*st] holds rxn_s [1/m^3/s]; returns the energy exchange [W/m^3].
 template <int PREC>
-__device__ __forceinline__ double chem_cell(double* sc, double* wd, const int st, double Te, double Tg)
+__device__ __forceinline__ double chem_cell(double* sc, double* wd, const int st, double Te, double Tg, double EN)
 {
     const int ns = c_mech.ns;
     const int eid = c_mech.e_id;
@@ -483,6 +542,14 @@ __device__ __forceinline__ double chem_cell(double* sc, double* wd, const int st
     // (test/Reactor/CO2_H2_Ar_mechanism_reduced/Chemistry.H:945-952)
     double tep[9], itp[4], teev = 0.0;
     if (c_mech.nfits > 0) fit_powers<PREC>(Te, tep, itp, teev);
+    // the field magnitude of the field-driven rates: E = EN N 1e-21
+    // (test/verification/Streamer/Chemistry.H:262-264)
+    double efm = 0.0;
+    if (c_mech.need_en) {
+        double mix = 0.0;
+        for (int s = 0; s < ns; s++) mix += sc[s * st];
+        efm = EN * (mix * N_A) * 1e-21;
+    }
     double ee = 0.0;
     const int nr = c_mech.nr;
     for (int r = 0; r < nr; r++) {
@@ -490,6 +557,8 @@ __device__ __forceinline__ double chem_cell(double* sc, double* wd, const int st
         double k;
         if (R.kind == VD_RATE_CONST) {
             k = R.A;
+        } else if (R.kind == VD_RATE_TOWNSEND) {
+            k = townsend_rate(c_mech.fits[R.fit].jc, efm);
         } else if (R.kind >= VD_RATE_JANEV) {
             k = fit_rate<PREC>(R.kind, c_mech.fits[R.fit], tep, itp, teev);
         } else {
@@ -522,7 +591,9 @@ __device__ __forceinline__ double chem_cell(double* sc, double* wd, const int st
     if (c_mech.elastic_loss) {
         double nd = 0.0;
         for (int s = 0; s < ns; s++) nd += sc[s * st] * N_A;
-        double mu = mob_fp64(eid, Te, nd, Tg);
+        // |E| = EN N 1e-21 (the He_RF_1d header's CKWC, Chemistry.H:618); the argon
+        // headers pass 0 there, with mobilities that do not read it
+        double mu = mob_fp64(eid, Te, nd, Tg, EN * nd * 1.0e-21);
         double nu = -ECHARGE / ME / mu;
         ee -= 1.5 * K_B * sce * N_A * dT * nu * c_mech.elastic_coef;
     }

@@ -335,7 +335,13 @@ __global__ void __launch_bounds__(128) k_dif_cell_d(DifArgs a, double* Dg, int g
     double nd = 0.0;
     for (int s = 0; s < ns; s++) nd += a.st.p[o + (int64_t)s * a.st.ns];
     const double te = a.st.p[o + (int64_t)VD_ETEMP(ns) * a.st.ns];
-    Dg[(int64_t)i + (int64_t)g0 * (j + (int64_t)g1 * k)] = diff_fp64(a.spec, te, nd, a.Tg);
+    // |E| over the active directions (Source/ScalarSolve.cpp:486-488)
+    double esum = 0.0;
+    for (int d = 0; d < DIM; d++) {
+        const double e = a.st.p[o + (int64_t)(VD_EFX(ns) + d) * a.st.ns];
+        esum += e * e;
+    }
+    Dg[(int64_t)i + (int64_t)g0 * (j + (int64_t)g1 * k)] = diff_fp64(a.spec, te, nd, a.Tg, sqrt(esum));
 }
 
 // level-0 face coefficients of direction D: harmonic mean of the two cells
@@ -375,7 +381,10 @@ __global__ void __launch_bounds__(128) k_dif_bcval(DifArgs a, DLevel L, double* 
     double nd = 0.0;
     for (int q = 0; q < ns; q++) nd += at(q, cint);
     const double te = at(VD_ETEMP(ns), cint);
-    const double Dc = diff_fp64(a.spec, te, nd, a.Tg);
+    // |E| of the three state components (Source/PlasmaChem.H:114-116)
+    const double ex = at(VD_EFX(ns), cint), ey = at(VD_EFY(ns), cint), ez = at(VD_EFZ(ns), cint);
+    const double emag = sqrt(ex * ex + ey * ey + ez * ez);
+    const double Dc = diff_fp64(a.spec, te, nd, a.Tg, emag);
     double g;
     if (a.spec == a.e_id) {
         const double cbar = sqrt(8.0 * K_B * te / PI / ME);
@@ -386,7 +395,7 @@ __global__ void __launch_bounds__(128) k_dif_bcval(DifArgs a, DLevel L, double* 
         const double flx = (2.0 * K_B * te) * at(a.e_id, cint) * cbar / 4.0 * (double)sgn;
         g = -flx / Dc;
     } else if (a.charge[a.spec] != 0) {
-        const double mu = mob_fp64(a.spec, te, nd, a.Tg);
+        const double mu = mob_fp64(a.spec, te, nd, a.Tg, emag);
         const double drift = mu * at(a.spec, cint) * at(VD_EFX(ns) + D, cint);
         g = (drift * (double)sgn >= 0.0) ? (-drift / Dc) : 0.0;
     } else {

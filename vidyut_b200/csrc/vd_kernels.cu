@@ -160,7 +160,8 @@ __global__ void __launch_bounds__(128) k_reaction_source(BoxIdx b, A4 sb, A4 rxn
         const int64_t o = sb.off(i, j, k);
         for (int s = 0; s < ns; s++) sc[s * st] = sb.p[o + s * sb.ns];
         double Te = sb.p[o + (int64_t)VD_ETEMP(ns) * sb.ns];
-        double ee = chem_cell<PREC>(sc, wd, st, Te, Tg);
+        const double EN = c_mech.need_en ? sb.p[o + (int64_t)VD_REF(ns) * sb.ns] : 0.0;
+        double ee = chem_cell<PREC>(sc, wd, st, Te, Tg, EN);
         const int64_t r = rxn.off(i, j, k);
         for (int s = 0; s < ns; s++) rxn.p[r + s * rxn.ns] = wd[s * st];
         rxn.p[r + (int64_t)ns * rxn.ns] = ee;
@@ -202,7 +203,13 @@ __device__ __forceinline__ double vel_cell(const A4& phi, int i, int j, int k, i
     double N = 0.0;
     for (int q = 0; q < ns; q++) N += phi.p[o + q * phi.ns];
     double Te = phi.p[o + (int64_t)VD_ETEMP(ns) * phi.ns];
-    double mu = mob_fp64(s, Te, N, Tg);
+    // |E| of the three state components, as compute_vel takes it
+    double esum = 0.0;
+    for (int q = 0; q < 3; q++) {
+        const double e = phi.p[o + (int64_t)(VD_EFX(ns) + q) * phi.ns];
+        esum += e * e;
+    }
+    double mu = mob_fp64(s, Te, N, Tg, sqrt(esum));
     return mu * phi.p[o + (int64_t)(VD_EFX(ns) + d) * phi.ns];
 }
 
@@ -358,7 +365,8 @@ __device__ __forceinline__ void prep_cell(const PrepArgs& a, int64_t idx, double
     const int64_t ro = a.rxn.off(i, j, k);
     if (a.do_reactions) {
         double Te = a.sb.p[o + (int64_t)VD_ETEMP(ns) * a.sb.ns];
-        double ee = chem_cell<PREC>(sc, wd, st, Te, a.Tg);
+        const double EN = c_mech.need_en ? a.sb.p[o + (int64_t)VD_REF(ns) * a.sb.ns] : 0.0;
+        double ee = chem_cell<PREC>(sc, wd, st, Te, a.Tg, EN);
         for (int s = 0; s < ns; s++) a.rxn.p[ro + s * a.rxn.ns] = wd[s * st];
         a.rxn.p[ro + (int64_t)ns * a.rxn.ns] = ee;
     } else {
@@ -550,9 +558,12 @@ cudaError_t launch_prep(const PrepArgs& a, int prec, int ns, cudaStream_t st)
 // species constant K times a per-cell basis: electron-type mu = c/(sqrt(Te) N s0)
 // gives K = c/s0 on E/(sqrt(Te) N); ion-type mu = c/(sqrt(Tg) N s0) gives
 // K = c/(sqrt(Tg) s0) on E/N; mu = p0/N gives K = p0 on E/N; a constant mu gives
-// K = p0 on E; a scaled model multiplies its reference's K.
-static bool velocity_basis(const VdMechDev& m, int s, double Tg, int* kind, double* K)
+// K = p0 on E; mu = p0 |E|^p1 gives K = p0 on E |E|^p1 (one basis per exponent);
+// a scaled model multiplies its reference's K.
+bool velocity_basis(const VdMechDev& m, int s, double Tg, VelBasis* b, double* K)
 {
+    b->pw = 0.0;
+    b->fit = 0;
     double scale = 1.0;
     int k = m.mob_kind[s];
     if (k == VD_MOB_SCALED) {
@@ -561,39 +572,61 @@ static bool velocity_basis(const VdMechDev& m, int s, double Tg, int* kind, doub
         k = m.mob_kind[s];
     }
     switch (k) {
-    case VD_MOB_ELECTRON: *kind = 0; *K = scale * (m.mob_c[s] / m.mob_p0[s]); return true;
-    case VD_MOB_ION_TG: *kind = 1; *K = scale * (m.mob_c[s] / (std::sqrt(Tg) * m.mob_p0[s])); return true;
-    case VD_MOB_CONST_N: *kind = 1; *K = scale * m.mob_p0[s]; return true;
-    case VD_MOB_CONST: *kind = 2; *K = scale * m.mob_p0[s]; return true;
+    case VD_MOB_ELECTRON: b->kind = 0; *K = scale * (m.mob_c[s] / m.mob_p0[s]); return true;
+    case VD_MOB_ION_TG: b->kind = 1; *K = scale * (m.mob_c[s] / (std::sqrt(Tg) * m.mob_p0[s])); return true;
+    case VD_MOB_CONST_N: b->kind = 1; *K = scale * m.mob_p0[s]; return true;
+    case VD_MOB_CONST: b->kind = 2; *K = scale * m.mob_p0[s]; return true;
+    case VD_MOB_POW_EMAG: b->kind = 3; *K = scale * m.mob_p0[s]; b->pw = m.mob_p1[s]; return true;
+    case VD_MOB_EN_POLY:
+        b->kind = 4;
+        *K = scale * m.mob_p0[s];
+        b->pw = m.mob_p1[s];
+        b->fit = m.mob_ref[s];
+        return true;
+    case VD_MOB_EXP_MEANE: b->kind = 5; *K = scale * m.mob_p0[s]; b->fit = m.mob_ref[s]; return true;
     default: return false;
     }
+}
+
+bool same_basis(const VdMechDev& m, const VelBasis& x, const VelBasis& y)
+{
+    if (x.kind != y.kind || x.pw != y.pw) return false;
+    if (x.kind < 4) return true;
+    const int nc = x.kind == 4 ? 2 : 5;  // coefficients the kind reads
+    for (int j = 0; j < nc; j++)
+        if (m.fits[x.fit].jc[j] != m.fits[y.fit].jc[j]) return false;
+    return true;
 }
 
 void finish_species_lists(TransportArgs& a, const VdMechDev& m)
 {
     a.nfl = a.nnf = a.nb = 0;
-    int slot_of_kind[3] = {-1, -1, -1};
+    VelBasis bs[4];
     for (int it = 0; it < a.ntr; it++) {
         const int s = a.tr_sp[it];
         if (!a.tr_flux[it]) {
             a.nf_sp[a.nnf++] = (int8_t)s;
             continue;
         }
-        int kind = 0;
         double K = 0.0;
         int slot = -1;
         if (a.udv) {
             K = 1.0;  // v = the user velocity of the sweep direction
         } else {
-            if (!velocity_basis(m, s, a.Tg, &kind, &K)) {
+            VelBasis b;
+            if (!velocity_basis(m, s, a.Tg, &b, &K)) {
                 a.nf_sp[a.nnf++] = (int8_t)s;
                 continue;
             }
-            if (slot_of_kind[kind] < 0) {
-                slot_of_kind[kind] = a.nb;
-                a.bkind[a.nb++] = (int8_t)kind;
+            for (int q = 0; q < a.nb; q++)
+                if (same_basis(m, bs[q], b)) slot = q;
+            if (slot < 0) {  // vd_mech_init admits at most kMaxBases distinct bases
+                slot = a.nb;
+                bs[a.nb] = b;
+                a.bkind[a.nb] = (int8_t)b.kind;
+                a.bfit[a.nb] = (int8_t)b.fit;
+                a.bpow[a.nb++] = b.pw;
             }
-            slot = slot_of_kind[kind];
         }
         a.fl_sp[a.nfl] = (int8_t)s;
         a.fl_cls[a.nfl] = a.tr_cls[it];
@@ -809,8 +842,8 @@ __global__ void __launch_bounds__(256) k_time_scales(BoxIdx b, int dim, A4 st, T
         const double emag = sqrt(esum);
         double nd = 0.0;
         for (int s = 0; s < ns; s++) nd += st.p[o + (int64_t)s * st.ns];
-        const double dc = a.const_ele_trans ? a.ele_diff / nd : diff_fp64(eidx, etemp, nd, a.Tg);
-        const double mu = a.const_ele_trans ? a.ele_mob / nd : mob_fp64(eidx, etemp, nd, a.Tg);
+        const double dc = a.const_ele_trans ? a.ele_diff / nd : diff_fp64(eidx, etemp, nd, a.Tg, emag);
+        const double mu = a.const_ele_trans ? a.ele_mob / nd : mob_fp64(eidx, etemp, nd, a.Tg, emag);
         m[0] = fmax(m[0], fabs(mu) * emag);
         m[1] = fmax(m[1], dc);
         m[2] = fmax(m[2], fabs(mu) * st.p[o + (int64_t)eidx * st.ns]);

@@ -35,11 +35,15 @@ struct TransportArgs {
     // with a drift flux, in update order, and those without.  A fluxed species'
     // face velocity is fl_K * (velocity basis fl_slot of the cell): the mobility
     // models of specMob factor into a species constant and a per-cell basis
-    // (bkind 0: E/(sqrt(Te) N), 1: E/N, 2: E); fl_slot < 0 means the user velocity.
+    // (bkind 0: E/(sqrt(Te) N), 1: E/N, 2: E, 3: E |E|^p, 4: E (1 + c0 x^2 + c1 x^4)^p
+    // with x = |E|/N, 5: E exp(c0 + c1 ln m + c2/m + c3/m^2 + c4/m^3) / N with
+    // m = 1.5 Te/eV); fl_slot < 0 means the user velocity.
     int nfl, nnf, nb;
     int8_t fl_sp[VD_MAX_SPECIES + 1], fl_cls[VD_MAX_SPECIES + 1], fl_slot[VD_MAX_SPECIES + 1];
     int8_t nf_sp[VD_MAX_SPECIES + 1];
     int8_t bkind[4];
+    int8_t bfit[4];   // bkind 4, 5: the mechanism fit holding c
+    double bpow[4];   // bkind 3, 4: the exponent p
     double fl_K[VD_MAX_SPECIES + 1];
     float fl_Kf[VD_MAX_SPECIES + 1];  // fl_K rounded to FP32 (the mixed path's constant)
     // zero-flux faces of a fluxed species: bit d set when its class has IHNEUBC at
@@ -62,6 +66,18 @@ __host__ __device__ inline bool joule_in_tile(const TransportArgs& a, int prec)
 // Fills the derived fluxed / unfluxed lists and velocity bases of a from its tr_*
 // lists and the mechanism table m (host).
 void finish_species_lists(TransportArgs& a, const VdMechDev& m);
+// A velocity basis: the per-cell factor of a mobility model times E (the kinds of
+// TransportArgs::bkind, with their exponent and coefficient fit).
+struct VelBasis {
+    int kind;
+    double pw;
+    int fit;
+};
+// species s's mobility as K times a velocity basis; false when it has no drift (host)
+bool velocity_basis(const VdMechDev& m, int s, double Tg, VelBasis* b, double* K);
+// the two bases evaluate to the same values (host)
+bool same_basis(const VdMechDev& m, const VelBasis& x, const VelBasis& y);
+constexpr int kMaxBases = 3;  // velocity bases a tile stages
 
 // Arguments of the per-cell prep kernel: N = sum_s n_s over the grown box, and
 // rxn (chemistry) over the valid box.

@@ -81,7 +81,7 @@ __device__ __forceinline__ float exp2_split(double x)
 
 // electron mobility of the table (mob_fp64 in vd_device.cuh) as an expression of
 // Te, nd (density sum) and Tg
-std::string mob_expr(const VdMechDev& m, int s, const char* Te, const char* nd, const char* Tg)
+std::string mob_expr(const VdMechDev& m, int s, const char* Te, const char* nd, const char* Tg, const char* emag)
 {
     int kind = m.mob_kind[s];
     double scale = 1.0;
@@ -97,6 +97,22 @@ std::string mob_expr(const VdMechDev& m, int s, const char* Te, const char* nd, 
     case VD_MOB_ION_TG: o << "(" << hexd(m.mob_c[s]) << " / (sqrt(" << Tg << ") * " << nd << " * " << hexd(m.mob_p0[s]) << "))"; break;
     case VD_MOB_CONST_N: o << "(" << hexd(m.mob_p0[s]) << " / " << nd << ")"; break;
     case VD_MOB_CONST: o << hexd(m.mob_p0[s]); break;
+    case VD_MOB_POW_EMAG: o << "(" << hexd(m.mob_p0[s]) << " * pow(" << emag << ", " << hexd(m.mob_p1[s]) << "))"; break;
+    case VD_MOB_EN_POLY: {  // mob_en_poly in vd_device.cuh
+        const double* c = m.fits[m.mob_ref[s]].jc;
+        const std::string x = std::string("(") + emag + " / " + nd + ")";
+        o << "(" << hexd(m.mob_p0[s]) << " * pow(1.0 + " << hexd(c[0]) << " * pow(" << x << ", 2.0) + " << hexd(c[1])
+          << " * pow(" << x << ", 4.0), " << hexd(m.mob_p1[s]) << "))";
+        break;
+    }
+    case VD_MOB_EXP_MEANE: {  // mob_exp_meane in vd_device.cuh
+        const double* c = m.fits[m.mob_ref[s]].jc;
+        const std::string me = std::string("(1.5 * ") + Te + " / " + hexd(EV) + ")";
+        o << "(" << hexd(m.mob_p0[s]) << " * exp(" << hexd(c[0]) << " + " << hexd(c[1]) << " * log(" << me << ") + "
+          << hexd(c[2]) << " / " << me << " + " << hexd(c[3]) << " / pow(" << me << ", 2.0) + " << hexd(c[4])
+          << " / pow(" << me << ", 3.0)) / " << nd << ")";
+        break;
+    }
     default: o << "0.0"; break;
     }
     o << ")";
@@ -181,6 +197,7 @@ std::string gen_prep_kernel(const VdMechDev& m, int prec)
     for (int s = 0; s <= ns; s++) o << "      rx[" << s << " * rs] = 0.0;\n";
     o << "      return;\n    }\n";
     o << "    const double Te = p[" << (ns + 1) << " * cs];\n    const double Tg = a.Tg;\n";
+    if (m.need_en) o << "    const double EN = p[" << (ns + 9) << " * cs];\n";  // REF
     for (int s = 0; s < ns; s++) o << "    const double sc" << s << " = n" << s << " * 1.0e-6 / N_A * 1.0e6;\n";
     for (int s = 0; s < ns; s++) o << "    double w" << s << " = 0.0;\n";
     o << "    const double ne = sc" << eid << " * NA_CE;\n"
@@ -191,6 +208,12 @@ std::string gen_prep_kernel(const VdMechDev& m, int prec)
     if (prec == PREC_FP64) o << "    const double lTe = log(Te), lTg = log(Tg);\n";
     else o << "    const double lTe = log2(Te), lTg = log2(Tg);\n";
     o << "    const double invTe = 1.0 / Te, invTg = 1.0 / Tg;\n    double ee = 0.0;\n";
+    if (m.need_en) {
+        // E = EN N 1e-21 of the field-driven rates (townsend_rate in vd_device.cuh)
+        o << "    double mix = 0.0;\n";
+        for (int s = 0; s < ns; s++) o << "    mix += sc" << s << ";\n";
+        o << "    const double efm = EN * (mix * N_A) * 1e-21;\n";
+    }
     if (m.nfits > 0) {
         // the powers the Janev / F-fit rates share (fit_powers in vd_device.cuh)
         o << "    const double teev = Te / " << hexd(TE_FIT_EV) << ", lte = log(teev);\n"
@@ -225,6 +248,12 @@ std::string gen_prep_kernel(const VdMechDev& m, int prec)
         o << "    { // reaction " << r << "\n      double k;\n";
         if (R.kind == VD_RATE_CONST) {
             o << "      k = " << hexd(R.A) << ";\n";
+        } else if (R.kind == VD_RATE_TOWNSEND) {
+            const double* c = m.fits[R.fit].jc;
+            o << "      {\n        const double alpha = (" << hexd(c[0]) << " + " << hexd(c[1]) << " / pow(efm, 3.0)) * exp(-"
+              << hexd(c[2]) << " / efm);\n"
+              << "        const double mu_e = " << hexd(c[4]) << " * pow(efm, " << hexd(c[5]) << ");\n"
+              << "        k = (alpha - " << hexd(c[3]) << ") * mu_e * efm;\n      }\n";
         } else if (R.kind >= VD_RATE_JANEV) {
             const VdFitDev& F = m.fits[R.fit];
             if (R.kind == VD_RATE_JANEV_FFIT) {
@@ -270,7 +299,8 @@ std::string gen_prep_kernel(const VdMechDev& m, int prec)
     if (m.elastic_loss) {
         o << "    {\n      double nd = 0.0;\n";
         for (int s = 0; s < ns; s++) o << "      nd += sc" << s << " * N_A;\n";
-        o << "      const double mu = " << mob_expr(m, eid, "Te", "nd", "Tg") << ";\n"
+        o << "      const double mu = "
+          << mob_expr(m, eid, "Te", "nd", "Tg", m.need_en ? "(EN * nd * 1.0e-21)" : "0.0") << ";\n"
           << "      const double nu = " << hexd(-ECHARGE / ME) << " / mu;\n"
           << "      ee -= 1.5 * K_B * sc" << eid << " * N_A * dT * nu * " << hexd(m.elastic_coef) << ";\n    }\n";
     }

@@ -50,6 +50,14 @@ __device__ __forceinline__ double joule_cell(const TransportArgs& a, int dim, in
             const int64_t cs = a.sb.ns;
             double etemp = 0.5 * (p[ol + VD_ETEMP(ns) * cs] + p[orr + VD_ETEMP(ns) * cs]);
             const double evf_d = 0.5 * (p[ol + (VD_EFX(ns) + idim) * cs] + p[orr + (VD_EFX(ns) + idim) * cs]);
+            // |E| of the face-averaged field over the active directions
+            // (Source/ElecEnergySource.cpp:103-119)
+            double esum = 0.0;
+            for (int d = 0; d < dim; d++) {
+                const double e = 0.5 * (p[ol + (VD_EFX(ns) + d) * cs] + p[orr + (VD_EFX(ns) + d) * cs]);
+                esum += e * e;
+            }
+            const double emag = sqrt(esum);
             double nel = p[ol + eidx * cs], ner = p[orr + eidx * cs];
             double ne = 0.5 * (nel + ner);
             double ef = a.cs_technique ? evf_d : a.ef[idim](face[0], face[1], face[2]);
@@ -61,8 +69,8 @@ __device__ __forceinline__ double joule_cell(const TransportArgs& a, int dim, in
                 ndens = 0.0;
                 for (int s = 0; s < ns; s++) ndens += 0.5 * (p[ol + s * cs] + p[orr + s * cs]);
             }
-            double mu = a.const_ele_trans ? a.ele_mob / ndens : mob_fp64(eidx, etemp, ndens, a.Tg);
-            double dc = a.const_ele_trans ? a.ele_diff / ndens : diff_fp64(eidx, etemp, ndens, a.Tg);
+            double mu = a.const_ele_trans ? a.ele_mob / ndens : mob_fp64(eidx, etemp, ndens, a.Tg, emag);
+            double dc = a.const_ele_trans ? a.ele_diff / ndens : diff_fp64(eidx, etemp, ndens, a.Tg, emag);
             double cur = a.charge_e * (mu * ne * ef - dc * gn);
             jheat += cur * ef;
         }
@@ -176,11 +184,25 @@ constexpr int group_fit()
     return 1;
 }
 
+// |E| of the field averaged over a face's two cells (state offsets ol, orr), over
+// the active directions (Source/ElecEnergySource.cpp:103-119)
+__device__ __forceinline__ double face_emag(const TransportArgs& a, int64_t ol, int64_t orr, int dim)
+{
+    const double* p = a.sb.p;
+    const int64_t cs = a.sb.ns;
+    double esum = 0.0;
+    for (int d = 0; d < dim; d++) {
+        const double e = 0.5 * (p[ol + (VD_EFX(a.ns) + d) * cs] + p[orr + (VD_EFX(a.ns) + d) * cs]);
+        esum += e * e;
+    }
+    return sqrt(esum);
+}
+
 // Joule heating carried by face g of direction D (the face between cells g - e_D
 // and g): q (mu ne E_f - D grad ne) E_f with face averages of Te, ne and the density
 // sum (Source/ElecEnergySource.cpp:86-160, one face of the per-cell loop).  Each
 // cell adds half of its faces' values, after the domain-face substitution.
-__device__ __forceinline__ double joule_face(const TransportArgs& a, int D, const int* g)
+__device__ __forceinline__ double joule_face(const TransportArgs& a, int D, const int* g, int dim)
 {
     const int ns = a.ns, eidx = a.e_id;
     int l[3] = {g[0], g[1], g[2]};
@@ -196,17 +218,19 @@ __device__ __forceinline__ double joule_face(const TransportArgs& a, int D, cons
     const double ef = a.cs_technique ? evf_d : a.ef[D](g[0], g[1], g[2]);
     const double gn = a.gradne_from_state ? (ner - nel) / a.dx[D] : a.gne[D](g[0], g[1], g[2]);
     const double ndens = 0.5 * (a.Nv.p[a.Nv.off(l[0], l[1], l[2])] + a.Nv.p[a.Nv.off(g[0], g[1], g[2])]);
+    double emag = 0.0;
+    if (c_mech.emag_e) emag = face_emag(a, ol, orr, dim);
     double mu, dc;
     if (a.const_ele_trans) {
         mu = a.ele_mob / ndens;
         dc = a.ele_diff / ndens;
     } else {
-        mu = mob_fp64(eidx, etemp, ndens, a.Tg);
+        mu = mob_fp64(eidx, etemp, ndens, a.Tg, emag);
         // the usual electron diffusion model refers to the electron mobility itself
         if (c_mech.diff_kind[eidx] == VD_DIFF_TE_ABSMOB && c_mech.diff_ref[eidx] == eidx)
             dc = c_mech.diff_factor[eidx] * (etemp / EV) * fabs(mu);
         else
-            dc = diff_fp64(eidx, etemp, ndens, a.Tg);
+            dc = diff_fp64(eidx, etemp, ndens, a.Tg, emag);
     }
     const double cur = a.charge_e * (mu * ne * ef - dc * gn);
     return cur * ef;
@@ -215,7 +239,7 @@ __device__ __forceinline__ double joule_face(const TransportArgs& a, int D, cons
 // the arithmetic of joule_face_mixed from the face's Te and density-sum averages,
 // the two cells' ne, the face field and the density gradient
 __device__ __forceinline__ double joule_mixed_core(const TransportArgs& a, float etemp, float ndens, double nel,
-                                                   double ner, double ef, double gn)
+                                                   double ner, double ef, double gn, float emag)
 {
     const int eidx = a.e_id;
     const float Tg = (float)a.Tg;
@@ -225,13 +249,8 @@ __device__ __forceinline__ double joule_mixed_core(const TransportArgs& a, float
         mu = (float)a.ele_mob * rn;
         dc = (float)a.ele_diff * rn;
     } else {
-        mu = mob_f32(eidx, etemp, ndens, Tg);
-        const int dk = c_mech.diff_kind[eidx], dr = c_mech.diff_ref[eidx];
-        const float mr = dr == eidx ? mu : mob_f32(dr, etemp, ndens, Tg);
-        if (dk == VD_DIFF_TE_ABSMOB) dc = (float)c_mech.diff_factor[eidx] * (etemp * (float)(1.0 / EV)) * fabsf(mr);
-        else if (dk == VD_DIFF_TG_MOB) dc = (float)c_mech.diff_factor[eidx] * (Tg * (float)(1.0 / EV)) * mr;
-        else if (dk == VD_DIFF_CONST) dc = (float)c_mech.diff_factor[eidx];
-        else dc = 0.0f;
+        mu = mob_f32(eidx, etemp, ndens, Tg, emag);
+        dc = diff_f32(eidx, etemp, ndens, Tg, emag, mu);
     }
     const double drift = (double)(mu * (float)(0.5 * (nel + ner)) * (float)ef);
     const double diffusion = (double)(dc * (float)gn);
@@ -242,7 +261,7 @@ __device__ __forceinline__ double joule_mixed_core(const TransportArgs& a, float
 // two current products (mu ne E_f and D grad ne) in FP32 on the special-function
 // unit's reciprocal and square root, as for the drift fluxes; their difference,
 // the charge and the product with E_f in FP64.
-__device__ __forceinline__ double joule_face_mixed(const TransportArgs& a, int D, const int* g)
+__device__ __forceinline__ double joule_face_mixed(const TransportArgs& a, int D, const int* g, int dim)
 {
     const int ns = a.ns, eidx = a.e_id;
     int l[3] = {g[0], g[1], g[2]};
@@ -257,7 +276,8 @@ __device__ __forceinline__ double joule_face_mixed(const TransportArgs& a, int D
                                      : a.ef[D](g[0], g[1], g[2]);
     const double gn = a.gradne_from_state ? (ner - nel) * a.idx[D] : a.gne[D](g[0], g[1], g[2]);
     const float ndens = 0.5f * ((float)a.Nv.p[a.Nv.off(l[0], l[1], l[2])] + (float)a.Nv.p[a.Nv.off(g[0], g[1], g[2])]);
-    return joule_mixed_core(a, etemp, ndens, nel, ner, ef, gn);
+    const float emag = c_mech.emag_e ? (float)face_emag(a, ol, orr, dim) : 0.0f;
+    return joule_mixed_core(a, etemp, ndens, nel, ner, ef, gn, emag);
 }
 
 // Joule term of every valid cell of tile `tile` (x fastest over the box's
@@ -301,7 +321,7 @@ __device__ __forceinline__ void joule_tile(const TransportArgs& a, int tile, dou
                 int l[3] = {c[0], c[1], c[2]};
                 l[d] += f;
                 double jf = 0.0;
-                if (!skip) jf = PREC == PREC_FP64 ? joule_face(a, d, gf) : joule_face_mixed(a, d, gf);
+                if (!skip) jf = PREC == PREC_FP64 ? joule_face(a, d, gf, DIM) : joule_face_mixed(a, d, gf, DIM);
                 sJ[d * FBOX + l[0] + FB0 * (l[1] + FB1 * l[2])] = jf;
             }
         }
@@ -375,17 +395,36 @@ __device__ __forceinline__ void stage_basis(const TransportArgs& a, int cc, cons
         Te = p[VD_ETEMP(ns) * cs];
         if (a.status && !(isfinite(E) && isfinite(Te) && isfinite(N))) atomicOr(a.status, 1u);
         if (joule_staged<DIM, PREC>() && jst) ne = p[a.e_id * cs];
+        // |E| of the three state components, as compute_vel takes it
+        // (Source/PlasmaChem.H:194-196), for the models in |E| and |E|/N
+        double emag = 0.0;
+        bool need_emag = c_mech.emag_e;
+        for (int k = 0; k < a.nb; k++) need_emag = need_emag || a.bkind[k] == 3 || a.bkind[k] == 4;
+        if (need_emag) {
+            const double ex = p[VD_EFX(ns) * cs], ey = p[VD_EFY(ns) * cs], ez = p[VD_EFZ(ns) * cs];
+            emag = sqrt(ex * ex + ey * ey + ez * ez);
+        }
         for (int k = 0; k < a.nb; k++) {
             const int kind = a.bkind[k];
+            if (kind == 4) {  // FP64 in both paths (the argument spans many decades)
+                b[k] = (VT)(E * mob_en_poly(c_mech.fits[a.bfit[k]].jc, a.bpow[k], emag, N));
+                continue;
+            }
+            if (kind == 5) {
+                b[k] = (VT)(E * mob_exp_meane(c_mech.fits[a.bfit[k]].jc, Te) / N);
+                continue;
+            }
             if constexpr (PREC == PREC_FP64) {
                 if (kind == 0) b[k] = E / (sqrt(Te) * N);
                 else if (kind == 1) b[k] = E / N;
-                else b[k] = E;
+                else if (kind == 2) b[k] = E;
+                else b[k] = E * pow(emag, a.bpow[k]);
             } else {
                 const float Ef = (float)E, rN = rcp_approx((float)N);
                 if (kind == 0) b[k] = Ef * rsqrtf((float)Te) * rN;
                 else if (kind == 1) b[k] = Ef * rN;
-                else b[k] = Ef;
+                else if (kind == 2) b[k] = Ef;
+                else b[k] = Ef * exp2f((float)a.bpow[k] * log2f((float)emag));
             }
         }
     }
@@ -730,7 +769,8 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
                 for (int e = 0; e < DIM; e++)
                     if (e != d) ok = ok && g[e] <= a.hi[e];
                 double jf = 0.0;
-                if constexpr (joule_staged<DIM, PREC>()) {
+                // a field-dependent electron mobility needs the face's |E|: global reads
+                if (joule_staged<DIM, PREC>() && !c_mech.emag_e) {
                     if (ok) {
                         // staged index of the face's rel cell (f_d - 3 + q) is f_d + q
                         // along d: the cells below and above are q = 2 and 3
@@ -751,10 +791,10 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
                         }
                         const double gn = a.gradne_from_state ? (ner - nel) * a.idx[d] : a.gne[d](g[0], g[1], g[2]);
                         jf = joule_mixed_core(a, 0.5f * (js.te[pl] + js.te[pr]), 0.5f * (js.nd[pl] + js.nd[pr]), nel,
-                                              ner, ef, gn);
+                                              ner, ef, gn, 0.0f);
                     }
                 } else {
-                    if (ok) jf = joule_face_mixed(a, d, g);
+                    if (ok) jf = joule_face_mixed(a, d, g, DIM);
                 }
                 sJ[f] = jf;
             }

@@ -15,6 +15,7 @@ constexpr double PI = 3.14159265358979323846264338327950288;
 constexpr double ECHARGE = 1.60217662e-19;
 constexpr double ME = 9.10938188e-31;
 constexpr double EV = ECHARGE / K_B;          // kelvin per eV
+constexpr double P_NTP = 101325.0;             // pressure at normal conditions [Pa]
 constexpr double NA_CE = 6.02214085774e23;    // Avogadro as written in comp_ener_exch
 constexpr double KB_CE = 1.380649e-23;
 constexpr double EV2J = 1.602176620800000e-19;
@@ -49,12 +50,15 @@ struct VdMechDev {
     double mob_p1[VD_MAX_SPECIES + 1];
     double mob_c[VD_MAX_SPECIES + 1];          // folded constant of the mobility model
     double diff_factor[VD_MAX_SPECIES + 1];
+    double diff_p1[VD_MAX_SPECIES + 1];
     int8_t charge[VD_MAX_SPECIES];
     int8_t mob_kind[VD_MAX_SPECIES + 1];
     int8_t mob_ref[VD_MAX_SPECIES + 1];
     int8_t diff_kind[VD_MAX_SPECIES + 1];
     int8_t diff_ref[VD_MAX_SPECIES + 1];
-    int8_t pad[3];
+    int8_t emag_e;        // the electron mobility or diffusion depends on |E|
+    int8_t need_en;       // the chemistry reads the reduced field (REF)
+    int8_t pad;
     int32_t nfits;
     VdRxnDev rxn[VD_MAX_REACTIONS];
     VdFitDev fits[VD_MAX_FITS];

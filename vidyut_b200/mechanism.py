@@ -89,6 +89,10 @@ class Mechanism:
     elastic_loss: int = 0
     elastic_mass: float = 0.0  # kg
     bg_species: list = field(default_factory=list)
+    diff_p1: list | None = None   # DIFF_POW_EMAG exponent / DIFF_TE_PRES scale (default 0)
+    # MOB_EN_POLY / MOB_EXP_MEANE coefficients c per species ({str(s): [c0, ...]});
+    # to_c stores them as fits and points mob_ref at them
+    mob_coef: dict = field(default_factory=dict)
 
     @property
     def ns(self) -> int:
@@ -116,6 +120,7 @@ class Mechanism:
             m.diff_kind[s] = int(self.diff_kind[s])
             m.diff_ref[s] = int(self.diff_ref[s])
             m.diff_factor[s] = float(self.diff_factor[s])
+            m.diff_p1[s] = float(self.diff_p1[s]) if self.diff_p1 is not None else 0.0
         m.elastic_loss = int(self.elastic_loss)
         m.elastic_mass = float(self.elastic_mass)
         nfits = 0
@@ -135,7 +140,7 @@ class Mechanism:
                 c.term_sp[t] = s
                 c.term_coef[t] = coef
             c.A, c.b, c.C, c.eexci = float(r.A), float(r.b), float(r.C), float(r.eexci)
-            if r.kind >= abi.RATE_JANEV:
+            if r.kind >= abi.RATE_JANEV:  # the Townsend kind keeps its c in jc
                 if nfits >= abi.MAX_FITS:
                     raise ValueError("too many fit rates")
                 f = m.fits[nfits]
@@ -146,6 +151,15 @@ class Mechanism:
                     f.fc[j] = float(v)
                 f.switch_ev = float(r.fit.get("switch_ev", 0.0))
                 c.fit = nfits
+                nfits += 1
+        for s in range(self.ns + 1):
+            if self.mob_kind[s] in (abi.MOB_EN_POLY, abi.MOB_EXP_MEANE):
+                if nfits >= abi.MAX_FITS:
+                    raise ValueError("too many fits")
+                coef = self.mob_coef[str(s)]
+                for j, v in enumerate(coef):
+                    m.fits[nfits].jc[j] = float(v)
+                m.mob_ref[s] = nfits
                 nfits += 1
         m.nfits = nfits
         return m
