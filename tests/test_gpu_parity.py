@@ -296,11 +296,19 @@ def test_specialised_and_table_chemistry_agree(name):
 def test_fit_rates_table_and_specialised_kernels_agree():
     """The Janev / F-fit rates of the CO2 reactor header (golden fixture co2fits_2d)
     through the mechanism-specialised kernels and the table-driven ones agree, and
-    the mixed-precision rates stay within the mixed tolerance of FP64."""
+    the mixed-precision rates and updates stay within the mixed tolerance of FP64.
+    The mixed path's rate coefficients are FP32 values: a fit that falls below
+    FP32's range (k < 2^-126 at a low Te, where the polynomial in ln Te runs to
+    large negative exponents) is zero there, so the rates are compared on the
+    gross scale floored at 1e-20 of each component's largest over the box."""
     case, meta, outs = load_fixture("co2fits_2d")
     port = oracle.Port(case.mech)
     rs = port.rxn_scale(case)
-    got = {}
+    rs_floor = np.maximum(rs, 1e-20 * rs.reshape(rs.shape[0], -1).max(axis=1).reshape((-1,) + (1,) * (rs.ndim - 1)))
+    prm = case.vd_params()
+    _, _, nsc = update_scales(port, case, prm)
+    ns = case.mech.ns
+    got, pn = {}, {}
     for spec in (1, 0):
         abi.lib().vd_set_specialize(spec)
         try:
@@ -312,10 +320,14 @@ def test_fit_rates_table_and_specialised_kernels_agree():
                 api.explicit_update_all(dc, case.vd_params(precision=prec), phi_new, dsdt, rxn)
                 torch.cuda.synchronize()
                 got[(spec, prec)] = rxn.cpu().numpy()
+                pn[(spec, prec)] = phi_new.cpu().numpy()
         finally:
             abi.lib().vd_set_specialize(1)
     api.mech_init(case.mech)
     assert scaled_err(got[(1, abi.PREC_FP64)], got[(0, abi.PREC_FP64)], rs) <= 1e-12
     assert scaled_err(got[(1, abi.PREC_FP64)], outs["upd_rxn"], rs) <= meta["rate_tol"]
     for spec in (1, 0):
-        assert scaled_err(got[(spec, abi.PREC_MIXED)], got[(1, abi.PREC_FP64)], rs) <= TOL_MIXED
+        er = scaled_err(got[(spec, abi.PREC_MIXED)], got[(1, abi.PREC_FP64)], rs_floor)
+        en = max(scaled_err(pn[(spec, abi.PREC_MIXED)][s], pn[(1, abi.PREC_FP64)][s], nsc[s]) for s in range(ns + 1))
+        print(f"co2fits mixed vs FP64 (specialised {spec}): rates {er:.3e}, updates {en:.3e}")
+        assert er <= TOL_MIXED and en <= TOL_MIXED

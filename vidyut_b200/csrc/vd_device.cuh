@@ -32,6 +32,20 @@ __device__ __forceinline__ float rcp_approx(float x)
     return r;
 }
 
+// 2^x for an FP64 exponent x as an FP32 value: x = i + f with i = rint(x) (exact in
+// FP64), 2^f for f in [-1/2, 1/2] on the FP32 special-function unit (exp2f, ~2 ulp)
+// and 2^i through the exponent bits.  Relative error ~2.4e-7 whatever |x|;
+// results below 2^-126 flush to zero, above 2^127 saturate to infinity.
+__device__ __forceinline__ float exp2_split(double x)
+{
+    const double xi = rint(x);
+    const float f = exp2f((float)(x - xi));
+    int i = (int)fmax(fmin(xi, 128.0), -127.0);
+    if (i <= -127) return 0.0f;
+    if (i >= 128) return __int_as_float(0x7f800000);
+    return f * __int_as_float((i + 127) << 23);
+}
+
 // ---------------------------------------------------------------------------
 // Mobility (specMob, test/models/Ar_DC_1d/Chemistry.H:177-202) by model kind.
 // FP64: mob_c = -e/me / sqrt(8 kB/(pi me)) (electron) or e/M / sqrt(8 kB/(pi M))
@@ -52,6 +66,27 @@ __device__ __forceinline__ double mob_exp_meane(const double* c, double Te)
     const double m = 1.5 * Te / EV;
     return exp(c[0] + c[1] * log(m) + c[2] / m + c[3] / pow(m, 2.0) + c[4] / pow(m, 3.0));
 }
+// The field-dependent models in FP64, out of line: their pow / exp / log code,
+// inlined into the transport tile, would cost every mechanism registers that only
+// these models use.
+static __device__ __noinline__ double mob_field_fp64(int s, double Te, double N, double emag)
+{
+    switch (c_mech.mob_kind[s]) {
+    case VD_MOB_POW_EMAG: return c_mech.mob_p0[s] * pow(emag, c_mech.mob_p1[s]);
+    case VD_MOB_EN_POLY: return c_mech.mob_p0[s] * mob_en_poly(c_mech.fits[c_mech.mob_ref[s]].jc, c_mech.mob_p1[s], emag, N);
+    case VD_MOB_EXP_MEANE: return c_mech.mob_p0[s] * mob_exp_meane(c_mech.fits[c_mech.mob_ref[s]].jc, Te) / N;
+    default: return 0.0;
+    }
+}
+// velocity basis kinds 3, 4 and 5 of the FP64 transport tile (E times the per-cell
+// factor of VD_MOB_POW_EMAG / VD_MOB_EN_POLY / VD_MOB_EXP_MEANE), out of line
+static __device__ __noinline__ double basis_field_fp64(int kind, int fit, double pw, double E, double emag, double N,
+                                                       double Te)
+{
+    if (kind == 3) return E * pow(emag, pw);
+    if (kind == 4) return E * mob_en_poly(c_mech.fits[fit].jc, pw, emag, N);
+    return E * mob_exp_meane(c_mech.fits[fit].jc, Te) / N;
+}
 __device__ __forceinline__ double mob_base_fp64(int s, double Te, double N, double Tg, double emag)
 {
     switch (c_mech.mob_kind[s]) {
@@ -59,9 +94,9 @@ __device__ __forceinline__ double mob_base_fp64(int s, double Te, double N, doub
     case VD_MOB_ION_TG: return c_mech.mob_c[s] / (sqrt(Tg) * N * c_mech.mob_p0[s]);
     case VD_MOB_CONST_N: return c_mech.mob_p0[s] / N;
     case VD_MOB_CONST: return c_mech.mob_p0[s];
-    case VD_MOB_POW_EMAG: return c_mech.mob_p0[s] * pow(emag, c_mech.mob_p1[s]);
-    case VD_MOB_EN_POLY: return c_mech.mob_p0[s] * mob_en_poly(c_mech.fits[c_mech.mob_ref[s]].jc, c_mech.mob_p1[s], emag, N);
-    case VD_MOB_EXP_MEANE: return c_mech.mob_p0[s] * mob_exp_meane(c_mech.fits[c_mech.mob_ref[s]].jc, Te) / N;
+    case VD_MOB_POW_EMAG:
+    case VD_MOB_EN_POLY:
+    case VD_MOB_EXP_MEANE: return mob_field_fp64(s, Te, N, emag);
     default: return 0.0;
     }
 }
@@ -70,6 +105,24 @@ __device__ __forceinline__ double mob_fp64(int s, double Te, double N, double Tg
     if (c_mech.mob_kind[s] == VD_MOB_SCALED)
         return c_mech.mob_p0[s] * mob_base_fp64(c_mech.mob_ref[s], Te, N, Tg, emag);
     return mob_base_fp64(s, Te, N, Tg, emag);
+}
+// The He_RF_1d models for the mixed path: the polynomial in FP32; the
+// mean-energy exponent (about 55, whose FP32 rounding alone would be 4e-6 of the
+// mobility) summed in FP64 from an FP32 logarithm and raised by exp2_split.
+__device__ __forceinline__ float mob_en_poly_f32(const double* c, float p, float emag, float N)
+{
+    const float x = emag * rcp_approx(N);
+    const float x2 = x * x;
+    const float q = fmaf((float)c[1], x2 * x2, fmaf((float)c[0], x2, 1.0f));
+    return exp2f(p * log2f(q));
+}
+__device__ __forceinline__ float mob_exp_meane_f32(const double* c, float Te)
+{
+    constexpr double LN2 = 0.69314718055994530942, LOG2E = 1.4426950408889634074;
+    const double m = 1.5 * (double)Te / EV;
+    const double im = 1.0 / m;
+    const double sum = fma((double)log2f((float)m), c[1] * LN2, c[0]) + im * fma(im, fma(im, c[4], c[3]), c[2]);
+    return exp2_split(sum * LOG2E);
 }
 __device__ __forceinline__ float mob_base_f32(int s, float Te, float N, float Tg, float emag)
 {
@@ -81,7 +134,10 @@ __device__ __forceinline__ float mob_base_f32(int s, float Te, float N, float Tg
     case VD_MOB_POW_EMAG: return (float)c_mech.mob_p0[s] * exp2f((float)c_mech.mob_p1[s] * log2f(emag));
     // the exponential's argument is too large for FP32 (e^55 in the He_RF_1d fit)
     case VD_MOB_EN_POLY:
-    case VD_MOB_EXP_MEANE: return (float)mob_base_fp64(s, Te, N, Tg, emag);
+        return (float)c_mech.mob_p0[s] *
+               mob_en_poly_f32(c_mech.fits[c_mech.mob_ref[s]].jc, (float)c_mech.mob_p1[s], emag, N);
+    case VD_MOB_EXP_MEANE:
+        return (float)c_mech.mob_p0[s] * mob_exp_meane_f32(c_mech.fits[c_mech.mob_ref[s]].jc, Te) * rcp_approx(N);
     default: return 0.0f;
     }
 }
@@ -91,7 +147,18 @@ __device__ __forceinline__ float mob_f32(int s, float Te, float N, float Tg, flo
         return (float)c_mech.mob_p0[s] * mob_base_f32(c_mech.mob_ref[s], Te, N, Tg, emag);
     return mob_base_f32(s, Te, N, Tg, emag);
 }
-// specDiff (test/models/Ar_DC_1d/Chemistry.H:204-239) by model kind.
+// specDiff (test/models/Ar_DC_1d/Chemistry.H:204-239) by model kind; the
+// field- and pressure-dependent ones out of line, as mob_field_fp64.
+static __device__ __noinline__ double diff_field_fp64(int s, double Te, double N, double Tg, double emag)
+{
+    switch (c_mech.diff_kind[s]) {
+    case VD_DIFF_POW_EMAG: return c_mech.diff_factor[s] * pow(emag, c_mech.diff_p1[s]);
+    // P_NTP / (N kB Tg) (test/verification/He_RF_1d/Chemistry.H:270-296)
+    case VD_DIFF_PRES: return c_mech.diff_factor[s] * (P_NTP / (N * K_B * Tg));
+    case VD_DIFF_TE_PRES: return c_mech.diff_factor[s] * (Te / c_mech.diff_p1[s]) * (P_NTP / (N * K_B * Tg));
+    default: return 0.0;
+    }
+}
 __device__ __forceinline__ double diff_base_fp64(int s, double Te, double N, double Tg, double emag)
 {
     switch (c_mech.diff_kind[s]) {
@@ -100,10 +167,9 @@ __device__ __forceinline__ double diff_base_fp64(int s, double Te, double N, dou
     case VD_DIFF_TG_MOB:
         return c_mech.diff_factor[s] * (Tg / EV) * mob_fp64(c_mech.diff_ref[s], Te, N, Tg, emag);
     case VD_DIFF_CONST: return c_mech.diff_factor[s];
-    case VD_DIFF_POW_EMAG: return c_mech.diff_factor[s] * pow(emag, c_mech.diff_p1[s]);
-    // P_NTP / (N kB Tg) (test/verification/He_RF_1d/Chemistry.H:270-296)
-    case VD_DIFF_PRES: return c_mech.diff_factor[s] * (P_NTP / (N * K_B * Tg));
-    case VD_DIFF_TE_PRES: return c_mech.diff_factor[s] * (Te / c_mech.diff_p1[s]) * (P_NTP / (N * K_B * Tg));
+    case VD_DIFF_POW_EMAG:
+    case VD_DIFF_PRES:
+    case VD_DIFF_TE_PRES: return diff_field_fp64(s, Te, N, Tg, emag);
     default: return 0.0;
     }
 }
@@ -115,19 +181,31 @@ __device__ __forceinline__ double diff_fp64(int s, double Te, double N, double T
         return c_mech.diff_factor[s] * diff_base_fp64(c_mech.diff_ref[s], Te, N, Tg, emag);
     return diff_base_fp64(s, Te, N, Tg, emag);
 }
-__device__ __forceinline__ float diff_f32(int s, float Te, float N, float Tg, float emag, float mu_e)
+__device__ __forceinline__ float diff_base_f32(int s, float Te, float N, float Tg, float emag, float mu_e)
 {
     // mu_e: the electron mobility when s's model refers to it (saves its re-evaluation)
     const int dk = c_mech.diff_kind[s], dr = c_mech.diff_ref[s];
-    if (dk == VD_DIFF_TE_ABSMOB || dk == VD_DIFF_TG_MOB) {
+    const float f = (float)c_mech.diff_factor[s];
+    switch (dk) {
+    case VD_DIFF_TE_ABSMOB:
+    case VD_DIFF_TG_MOB: {
         const float mr = dr == c_mech.e_id ? mu_e : mob_f32(dr, Te, N, Tg, emag);
-        if (dk == VD_DIFF_TE_ABSMOB) return (float)c_mech.diff_factor[s] * (Te * (float)(1.0 / EV)) * fabsf(mr);
-        return (float)c_mech.diff_factor[s] * (Tg * (float)(1.0 / EV)) * mr;
+        if (dk == VD_DIFF_TE_ABSMOB) return f * (Te * (float)(1.0 / EV)) * fabsf(mr);
+        return f * (Tg * (float)(1.0 / EV)) * mr;
     }
-    if (dk == VD_DIFF_CONST) return (float)c_mech.diff_factor[s];
-    if (dk == VD_DIFF_POW_EMAG) return (float)c_mech.diff_factor[s] * exp2f((float)c_mech.diff_p1[s] * log2f(emag));
-    if (dk == VD_DIFF_ZERO) return 0.0f;
-    return (float)diff_fp64(s, Te, N, Tg, emag);
+    case VD_DIFF_CONST: return f;
+    case VD_DIFF_POW_EMAG: return f * exp2f((float)c_mech.diff_p1[s] * log2f(emag));
+    case VD_DIFF_PRES: return f * ((float)P_NTP * rcp_approx(N * (float)K_B * Tg));
+    case VD_DIFF_TE_PRES:
+        return f * (Te * (float)(1.0 / c_mech.diff_p1[s])) * ((float)P_NTP * rcp_approx(N * (float)K_B * Tg));
+    default: return 0.0f;
+    }
+}
+__device__ __forceinline__ float diff_f32(int s, float Te, float N, float Tg, float emag, float mu_e)
+{
+    if (c_mech.diff_kind[s] == VD_DIFF_SCALED)
+        return (float)c_mech.diff_factor[s] * diff_base_f32(c_mech.diff_ref[s], Te, N, Tg, emag, mu_e);
+    return diff_base_f32(s, Te, N, Tg, emag, mu_e);
 }
 
 // ---------------------------------------------------------------------------
@@ -435,19 +513,6 @@ __device__ __forceinline__ float weno_combine_f32(float y1, float y2, float y3, 
     return fmaf(a1, p1, fmaf(a2, p2, a3 * p3)) * rcp_approx(a1 + a2 + a3);
 }
 
-// 2^x for an FP64 exponent x as an FP32 value: x = i + f with i = rint(x) (exact in
-// FP64), 2^f for f in [-1/2, 1/2] on the FP32 special-function unit (exp2f, ~2 ulp)
-// and 2^i through the exponent bits.  Relative error ~2.4e-7 whatever |x|;
-// results below 2^-126 flush to zero, above 2^127 saturate to infinity.
-__device__ __forceinline__ float exp2_split(double x)
-{
-    const double xi = rint(x);
-    const float f = exp2f((float)(x - xi));
-    int i = (int)fmax(fmin(xi, 128.0), -127.0);
-    if (i <= -127) return 0.0f;
-    if (i >= 128) return __int_as_float(0x7f800000);
-    return f * __int_as_float((i + 127) << 23);
-}
 
 // ---------------------------------------------------------------------------
 // Janev / F-fit electron-impact rates (test/Reactor/CO2_H2_Ar_mechanism_reduced/

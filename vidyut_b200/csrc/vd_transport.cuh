@@ -406,25 +406,20 @@ __device__ __forceinline__ void stage_basis(const TransportArgs& a, int cc, cons
         }
         for (int k = 0; k < a.nb; k++) {
             const int kind = a.bkind[k];
-            if (kind == 4) {  // FP64 in both paths (the argument spans many decades)
-                b[k] = (VT)(E * mob_en_poly(c_mech.fits[a.bfit[k]].jc, a.bpow[k], emag, N));
-                continue;
-            }
-            if (kind == 5) {
-                b[k] = (VT)(E * mob_exp_meane(c_mech.fits[a.bfit[k]].jc, Te) / N);
-                continue;
-            }
             if constexpr (PREC == PREC_FP64) {
                 if (kind == 0) b[k] = E / (sqrt(Te) * N);
                 else if (kind == 1) b[k] = E / N;
                 else if (kind == 2) b[k] = E;
-                else b[k] = E * pow(emag, a.bpow[k]);
+                else b[k] = basis_field_fp64(kind, a.bfit[k], a.bpow[k], E, emag, N, Te);
             } else {
                 const float Ef = (float)E, rN = rcp_approx((float)N);
                 if (kind == 0) b[k] = Ef * rsqrtf((float)Te) * rN;
                 else if (kind == 1) b[k] = Ef * rN;
                 else if (kind == 2) b[k] = Ef;
-                else b[k] = Ef * exp2f((float)a.bpow[k] * log2f((float)emag));
+                else if (kind == 3) b[k] = Ef * exp2f((float)a.bpow[k] * log2f((float)emag));
+                else if (kind == 4)
+                    b[k] = Ef * mob_en_poly_f32(c_mech.fits[a.bfit[k]].jc, (float)a.bpow[k], (float)emag, (float)N);
+                else b[k] = Ef * mob_exp_meane_f32(c_mech.fits[a.bfit[k]].jc, (float)Te) * rN;
             }
         }
     }
