@@ -904,7 +904,16 @@ def measure_serving(n_requests: int = 48, budget_gb: float = 8.0, quantum: int =
         t_start = time.perf_counter()
         th.start()
         th.join()
-        lat = [s.wait(i)[1] for i in ids]
+        # a request whose state met a NaN or infinity comes back failed (the
+        # reference aborts such a run); it is counted, and left out of the latencies
+        lat, failed = [], 0
+        for i in ids:
+            try:
+                lat.append(s.wait(i)[1])
+            except abi.VidyutError as e:
+                if e.status != abi.ERR_NONFINITE:
+                    raise
+                failed += 1
         wall = time.perf_counter() - t_start
         st = s.stats()
     clocks = clock.stop()
@@ -917,7 +926,7 @@ def measure_serving(n_requests: int = 48, budget_gb: float = 8.0, quantum: int =
            "wall_s": wall, "peak_bytes_used": st["peak_bytes_used"], "budget_bytes": budget, "quanta": st["quanta"],
            "graph_builds": st["graph_builds"], "quantum_steps": quantum, "gpu_launches": int(launches),
            "h2d_bytes": int(nbytes), "d2h_bytes": int(nbytes), "clocks": clocks,
-           "lat_mean_ms": float(sum(lat) / len(lat))}
+           "lat_mean_ms": float(sum(lat) / len(lat)) if lat else None, "failed_nonfinite": failed}
     if plain_fp64:
         import numpy as np
         service = []

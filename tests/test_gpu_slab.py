@@ -5,8 +5,10 @@ The halo exchange itself runs between processes (tests/test_slab_gloo.py); here
 the slabs are cut from the single box with their ghost planes already holding the
 neighbours' cells (what the exchange delivers), so the GPU side of the slab path
 is checked on one GPU with no kernels waiting on each other: every slab's update
-must equal the single box's update of the same cells (FP64 bit for bit; the
-mixed path within 1e-12 of the gross scale).
+must equal the single box's update of the same cells: FP64 bit for bit; the
+mixed path to FP32 rounding (1e-6 elementwise), because its face flux scales each
+run of faces by a power of two chosen from the run's cells and the slabs' tiles
+group the faces into runs differently.
 """
 import dataclasses
 
@@ -14,8 +16,7 @@ import numpy as np
 import pytest
 import torch
 
-import oracle
-from tests._util import scaled_err, update_scales
+from tests._util import max_elem_rel
 from vidyut_b200 import _abi as abi
 from vidyut_b200 import api, inputs
 from vidyut_b200 import mechanism as mm
@@ -54,7 +55,6 @@ def test_slab_updates_equal_single_box(dim, periodic, world, prec):
     api.mech_init(case.mech)
     whole = _update(case, _params(case, periodic, prec))
     ns = case.mech.ns
-    _, _, nsc = update_scales(oracle.Port(case.mech), case, case.vd_params())
     g = case.ghost
     for rank in range(world):
         sl = Slab(case.n, dim, g, rank, world, periodic=periodic)
@@ -90,5 +90,6 @@ def test_slab_updates_equal_single_box(dim, periodic, world, prec):
         if prec == abi.PREC_FP64:
             assert np.array_equal(got, want), (rank, np.max(np.abs(got - want)))
         else:
-            s = nsc[tuple(w)]
-            assert max(scaled_err(got[c], want[c], s[c]) for c in range(ns + 1)) <= 1e-12, rank
+            err = max_elem_rel(got[:ns + 1], want[:ns + 1])
+            print(f"slab {rank} of {world}, {dim}-D, mixed: {err:.3e}")
+            assert err <= 1e-6, rank

@@ -408,27 +408,45 @@ struct WenoY64 {
 };
 __device__ __forceinline__ WenoY64 weno_center_fp64(double a, double b, double c, double d, double e, int scheme)
 {
+    // every product-sum written as an explicit fma or as separate roundings, so the
+    // compiler contracts nothing: a centre gives the same bits wherever in a run of
+    // faces it is evaluated (the tile decomposition then cannot change a result)
+    constexpr double C1312 = 13.0 / 12.0;
     const double eps = 1e-20;
-    const double t1 = a - 2.0 * b + c, t2 = a - 4.0 * b + 3.0 * c;
-    const double b1 = (13.0 / 12.0) * (t1 * t1) + 0.25 * (t2 * t2);
-    const double t3 = b - 2.0 * c + d, t4 = b - d;
-    const double b2 = (13.0 / 12.0) * (t3 * t3) + 0.25 * (t4 * t4);
-    const double t5 = c - 2.0 * d + e, t6 = 3.0 * c - 4.0 * d + e;
-    const double b3 = (13.0 / 12.0) * (t5 * t5) + 0.25 * (t6 * t6);
+    const double t1 = fma(-2.0, b, a) + c, t2 = fma(3.0, c, fma(-4.0, b, a));
+    const double b1 = fma(C1312 * t1, t1, 0.25 * (t2 * t2));
+    const double t3 = fma(-2.0, c, b) + d, t4 = b - d;
+    const double b2 = fma(C1312 * t3, t3, 0.25 * (t4 * t4));
+    const double t5 = fma(-2.0, d, c) + e, t6 = fma(3.0, c, fma(-4.0, d, e));
+    const double b3 = fma(C1312 * t5, t5, 0.25 * (t6 * t6));
     const double r1 = 1.0 / (b1 + eps), r2 = 1.0 / (b2 + eps), r3 = 1.0 / (b3 + eps);
     WenoY64 y;
     if (scheme == 3) {
         const double tau = fabs(b1 - b3);
         const double s1 = tau * r1, s2 = tau * r2, s3 = tau * r3;
-        y.y1 = 1.0 + s1 * s1;
-        y.y2 = 1.0 + s2 * s2;
-        y.y3 = 1.0 + s3 * s3;
+        y.y1 = fma(s1, s1, 1.0);
+        y.y2 = fma(s2, s2, 1.0);
+        y.y3 = fma(s3, s3, 1.0);
     } else {
         y.y1 = r1 * r1;
         y.y2 = r2 * r2;
         y.y3 = r3 * r3;
     }
     return y;
+}
+// fused multiply-add in the precision of R (fmaf for float, fma for double)
+template <class R> __device__ __forceinline__ R fmx(R a, R b, R c)
+{
+    if constexpr (sizeof(R) == sizeof(float)) return fmaf(a, b, c);
+    else return fma(a, b, c);
+}
+// the mapping of WENO-M (Henrick et al.) with its products and sums pinned as in
+// weno_center_fp64
+template <class R> __device__ __forceinline__ R gk_map_pinned(R wk, R g)
+{
+    const R num = fmx(wk, wk, fmx(R(-3) * g, wk, g + g * g));
+    const R den = fmx(wk, R(1) - R(2) * g, g * g);
+    return wk * num / den;
 }
 // sum_k alpha_k p_k / sum_k alpha_k with alpha = gamma (0.1, 0.6, 0.3) times (y1, y2, y3)
 __device__ __forceinline__ double weno_combine_fp64(double y1, double y2, double y3, double p1, double p2, double p3,
@@ -437,26 +455,27 @@ __device__ __forceinline__ double weno_combine_fp64(double y1, double y2, double
     double a1 = 0.1 * y1, a2 = 0.6 * y2, a3 = 0.3 * y3;
     if (scheme == 2) {
         const double is = 1.0 / (a1 + a2 + a3);
-        a1 = gk_map(a1 * is, 0.1);
-        a2 = gk_map(a2 * is, 0.6);
-        a3 = gk_map(a3 * is, 0.3);
+        a1 = gk_map_pinned(a1 * is, 0.1);
+        a2 = gk_map_pinned(a2 * is, 0.6);
+        a3 = gk_map_pinned(a3 * is, 0.3);
     }
     const double is = 1.0 / (a1 + a2 + a3);
-    return (a1 * is) * p1 + (a2 * is) * p2 + (a3 * is) * p3;
+    return fma(a1 * is, p1, fma(a2 * is, p2, (a3 * is) * p3));
 }
 // the candidate polynomials: the value at x2 + 1/2 of the parabola through a window
-// (x0, x1, x2) (p1 of the reference), at x1 + 1/2 (p2) and at x0 + 1/2 (p3)
+// (x0, x1, x2) (p1 of the reference), at x1 + 1/2 (p2) and at x0 + 1/2 (p3), each
+// as two explicit fmas (no contraction left to the compiler)
 template <class R> __device__ __forceinline__ R wpoly_end(R x0, R x1, R x2)
 {
-    return (R(1) / R(3)) * x0 - (R(7) / R(6)) * x1 + (R(11) / R(6)) * x2;
+    return fmx(R(11) / R(6), x2, fmx(-(R(7) / R(6)), x1, (R(1) / R(3)) * x0));
 }
 template <class R> __device__ __forceinline__ R wpoly_mid(R x0, R x1, R x2)
 {
-    return -(R(1) / R(6)) * x0 + (R(5) / R(6)) * x1 + (R(1) / R(3)) * x2;
+    return fmx(R(1) / R(3), x2, fmx(R(5) / R(6), x1, -(R(1) / R(6)) * x0));
 }
 template <class R> __device__ __forceinline__ R wpoly_near(R x0, R x1, R x2)
 {
-    return (R(1) / R(3)) * x0 + (R(5) / R(6)) * x1 - (R(1) / R(6)) * x2;
+    return fmx(-(R(1) / R(6)), x2, fmx(R(5) / R(6), x1, (R(1) / R(3)) * x0));
 }
 
 // FP32 form from values scaled by an exact power of two s (max |value| of the run
@@ -471,7 +490,7 @@ struct WenoY32 {
 };
 __device__ __forceinline__ WenoY32 weno_center_f32(float a, float b, float c, float d, float e, int scheme, float eps4)
 {
-    const float t1 = fmaf(-2.0f, b, a) + c, t2 = fmaf(-4.0f, b, a) + 3.0f * c;
+    const float t1 = fmaf(-2.0f, b, a) + c, t2 = fmaf(3.0f, c, fmaf(-4.0f, b, a));
     const float b1 = fmaf(13.0f / 3.0f, t1 * t1, t2 * t2);
     const float t3 = fmaf(-2.0f, c, b) + d, t4 = b - d;
     const float b2 = fmaf(13.0f / 3.0f, t3 * t3, t4 * t4);
@@ -506,9 +525,9 @@ __device__ __forceinline__ float weno_combine_f32(float y1, float y2, float y3, 
     float a1 = 0.1f * y1, a2 = 0.6f * y2, a3 = 0.3f * y3;
     if (scheme == 2) {
         const float is = rcp_approx(a1 + a2 + a3);
-        a1 = gk_map(a1 * is, 0.1f);
-        a2 = gk_map(a2 * is, 0.6f);
-        a3 = gk_map(a3 * is, 0.3f);
+        a1 = gk_map_pinned(a1 * is, 0.1f);
+        a2 = gk_map_pinned(a2 * is, 0.6f);
+        a3 = gk_map_pinned(a3 * is, 0.3f);
     }
     return fmaf(a1, p1, fmaf(a2, p2, a3 * p3)) * rcp_approx(a1 + a2 + a3);
 }

@@ -579,7 +579,7 @@ __device__ __forceinline__ void run_faces(const TransportArgs& a, int2 ri, int z
             const double fp = weno_combine_fp64(yf.y1, yf.y2, yf.y3, wpoly_end(f[i], f[i + 1], f[i + 2]), pf2, pf3, scheme);
             const double fm = weno_combine_fp64(zf.y3, zf.y2, zf.y1, wpoly_end(f[i + 5], f[i + 4], f[i + 3]), pf3, pf2, scheme);
             const double l = fabs(lam[i]);
-            store(i, 0.5 * (fp + l * up) + 0.5 * (fm - l * um));
+            store(i, fma(0.5, fma(l, up, fp), 0.5 * fma(-l, um, fm)));
             yu = zu;
             yf = zf;
         }
