@@ -132,8 +132,15 @@ struct JStage {
 
 __host__ __device__ constexpr size_t smem_align(size_t x) { return (x + 15) & ~(size_t)15; }
 
-// Faces per run of the face phase (run_faces) for a tile shape.
-template <int DIM, class TS> constexpr int run_len() { return 3; }
+// The face phase of the FP64 path takes the faces in runs along the lines
+// (run_faces: the WENO smoothness indicators and weights of a cell centre are
+// shared by the faces and reconstructions that use them); the mixed path computes
+// each face on its own (face_tab: fewer live registers, an even split of the faces
+// over the threads), which measured faster for its FP32 arithmetic on B200.
+template <int DIM, int PREC> constexpr bool by_runs() { return PREC == PREC_FP64; }
+// Faces per run: 2 in 3-D, where the T + 1 = 9 faces of a line then make 5 runs
+// (960 per species for an 8^3 tile, an even load for its 512 threads), else 3.
+template <int DIM, class TS> constexpr int run_len() { return DIM == 3 ? 2 : 3; }
 
 // Dynamic shared memory of one tile with nb velocity bases and species groups of
 // GRP, in this order: the Joule term of every face (FP64, mixed path); the run
@@ -148,7 +155,8 @@ struct TileSmem {
     static constexpr size_t joule() { return PREC == PREC_MIXED ? smem_align((size_t)G::FTOT * sizeof(double)) : 0; }
     static constexpr size_t finfo()
     {
-        return smem_align((size_t)RunGeom<DIM, TS, run_len<DIM, TS>()>::NRUN * sizeof(int2));
+        return by_runs<DIM, PREC>() ? smem_align((size_t)RunGeom<DIM, TS, run_len<DIM, TS>()>::NRUN * sizeof(int2))
+                                    : smem_align((size_t)G::FTOT * sizeof(int));
     }
     static constexpr size_t soffs() { return smem_align((size_t)G::STOT * sizeof(int)); }
     static constexpr size_t flux(int grp) { return smem_align((size_t)grp * G::FTOT * sizeof(VT)); }
@@ -443,6 +451,69 @@ __device__ __forceinline__ typename VelT<PREC>::T stage_density(const TransportA
 }
 
 // ---------------------------------------------------------------------------
+// Single faces (the mixed path).  Face info word of face f of the tile (faces of
+// all directions in one index range, direction D from FOFF_D, x fastest), built
+// once per tile: bits 0-15 the staged index of the face's first stencil cell (rel
+// cell f_d - 3 + q has staged index f_d + q along d), bits 16-17 the direction,
+// then whether the box updates the face and whether it is the low or high domain
+// face of its direction.
+constexpr int kFaceOk = 1 << 18, kFaceDomLo = 1 << 19, kFaceDomHi = 1 << 20;
+template <int DIM, class TS>
+__device__ __forceinline__ int face_info(const TransportArgs& a, int f, const int* org)
+{
+    using G = TileGeom<DIM, TS>;
+    static_assert(G::STOT < (1 << 16), "staged index fits 16 bits");
+    int D = 0, ff = f;
+    if (DIM > 2 && f >= G::FOFF2) {
+        D = 2;
+        ff = f - G::FOFF2;
+    } else if (DIM > 1 && f >= G::FOFF1) {
+        D = 1;
+        ff = f - G::FOFF1;
+    }
+    const int F0 = TS::X + (D == 0), F1 = TS::Y + (D == 1);
+    const int l[3] = {ff % F0, (ff / F0) % F1, ff / (F0 * F1)};
+    const int S0 = TS::X + (D == 0 ? 6 : 0), S1 = TS::Y + (D == 1 ? 6 : 0);
+    const int soff = D == 0 ? 0 : (D == 1 ? G::SOFF1 : G::SOFF2);
+    const int g[3] = {org[0] + l[0], org[1] + l[1], org[2] + l[2]};
+    bool ok = g[D] <= a.hi[D] + 1;
+#pragma unroll
+    for (int e = 0; e < DIM; e++)
+        if (e != D) ok = ok && (g[e] <= a.hi[e]);
+    return (soff + l[0] + S0 * (l[1] + S1 * l[2])) | (D << 16) | (ok ? kFaceOk : 0) |
+           (g[D] == a.domlo[D] ? kFaceDomLo : 0) | (g[D] == a.domhi[D] + 1 ? kFaceDomHi : 0);
+}
+
+// Flux of one species through the face with info word `info`: sU / sB the
+// species' staged densities and velocity basis over all line sets (sB null: the
+// user velocity of the face's direction), k its velocity constant, zm its
+// zero-flux mask (TransportArgs::fl_zm); zero for a face the box does not update
+// or where IHNEUBC holds (Source/compute_explicit_flux.H:200-326).
+template <int DIM, int PREC, class TS>
+__device__ __forceinline__ typename VelT<PREC>::T face_tab(const TransportArgs& a, int info, int zm,
+                                                           const typename VelT<PREC>::T* sU,
+                                                           const typename VelT<PREC>::T* sB,
+                                                           typename VelT<PREC>::T k)
+{
+    using VT = typename VelT<PREC>::T;
+    if (!(info & kFaceOk)) return VT(0);
+    const int D = (info >> 16) & 3, base = info & 0xffff;
+    const int STR = D == 0 ? 1 : (D == 1 ? TS::X : TS::X * TS::Y);
+    if (!sB) k = (VT)a.uvel[D];
+    VT u[6], v[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        u[q] = sU[base + q * STR];
+        v[q] = sB ? k * sB[base + q * STR] : k;
+    }
+    VT F;
+    if constexpr (PREC == PREC_FP64) F = face_flux_fp64(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
+    else F = face_flux_mixed32(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
+    if (((info & kFaceDomLo) && ((zm >> D) & 1)) || ((info & kFaceDomHi) && ((zm >> (3 + D)) & 1))) F = VT(0);
+    return F;
+}
+
+// ---------------------------------------------------------------------------
 // Runs of faces.  The faces of the tile along a line of direction D (T_D + 1 of
 // them) are taken in runs of up to RUN consecutive faces; one thread computes a
 // run: it loads the run's RUN + 5 stencil cells once, evaluates the WENO
@@ -645,7 +716,8 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     constexpr int RUN = run_len<DIM, TS>();
     using RG = RunGeom<DIM, TS, RUN>;
     double* sJ = reinterpret_cast<double*>(smem);  // mixed path only
-    int2* sRI = reinterpret_cast<int2*>(smem + SM::joule());
+    int2* sRI = reinterpret_cast<int2*>(smem + SM::joule());  // by_runs
+    int* sFI = reinterpret_cast<int*>(smem + SM::joule());    // single faces
     int* sSO = reinterpret_cast<int*>(smem + SM::joule() + SM::finfo());
     const size_t o_f = SM::joule() + SM::finfo() + SM::soffs();
     VT* sF = reinterpret_cast<VT*>(smem + o_f);
@@ -729,8 +801,12 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     };
 
     if (nfl > 0) {
-        // (0) run info words and the velocity bases of every staged position
-        for (int r = tid; r < RG::NRUN; r += NTH) sRI[r] = run_info<DIM, TS, RUN>(a, r, org);
+        // (0) run or face info words and the velocity bases of every staged position
+        if constexpr (by_runs<DIM, PREC>()) {
+            for (int r = tid; r < RG::NRUN; r += NTH) sRI[r] = run_info<DIM, TS, RUN>(a, r, org);
+        } else {
+            for (int f = tid; f < G::FTOT; f += NTH) sFI[f] = face_info<DIM, TS>(a, f, org);
+        }
         for (int c = tid; c < G::STOT; c += NTH) {
             if (c < G::SOFF1) {
                 stage_basis<DIM, PREC, 0, TS>(a, c, org, sB, js, jin, sSO);
@@ -817,15 +893,23 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
             sU[q] = u;
         }
         __syncthreads();
-        // (2) every face flux of the group, by runs of faces along the lines
-        for (int q = tid; q < gn * RG::NRUN; q += NTH) {
-            const int j = q / RG::NRUN, r = q - j * RG::NRUN;
-            const int sl = a.fl_slot[g0 + j];
-            VT k;
-            if constexpr (PREC == PREC_FP64) k = a.fl_K[g0 + j];
-            else k = a.fl_Kf[g0 + j];
-            run_faces<DIM, PREC, TS, RUN>(a, sRI[r], a.fl_zm[g0 + j], sU + j * G::STOT,
-                                          sl >= 0 ? sB + sl * G::STOT : nullptr, k, sF + j * G::FTOT);
+        // (2) every face flux of the group: by runs of faces along the lines, or
+        // face by face
+        if constexpr (by_runs<DIM, PREC>()) {
+            for (int q = tid; q < gn * RG::NRUN; q += NTH) {
+                const int j = q / RG::NRUN, r = q - j * RG::NRUN;
+                const int sl = a.fl_slot[g0 + j];
+                run_faces<DIM, PREC, TS, RUN>(a, sRI[r], a.fl_zm[g0 + j], sU + j * G::STOT,
+                                              sl >= 0 ? sB + sl * G::STOT : nullptr, (VT)a.fl_K[g0 + j],
+                                              sF + j * G::FTOT);
+            }
+        } else {
+            for (int q = tid; q < gn * G::FTOT; q += NTH) {
+                const int j = q / G::FTOT, f = q - j * G::FTOT;
+                const int sl = a.fl_slot[g0 + j];
+                sF[q] = face_tab<DIM, PREC, TS>(a, sFI[f], a.fl_zm[g0 + j], sU + j * G::STOT,
+                                                sl >= 0 ? sB + sl * G::STOT : nullptr, (VT)a.fl_Kf[g0 + j]);
+            }
         }
         __syncthreads();
         // (3) divergence + sources of the own cell: dsdt = (Fx_lo - Fx_hi)/dx + rxn,
