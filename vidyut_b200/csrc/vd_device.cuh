@@ -349,6 +349,14 @@ __device__ __forceinline__ double face_flux_fp64(const double* u, const double* 
 // as in FP64).  The flux is unscaled by the exact power of two; the result is
 // returned in FP32, which holds it exactly while it is a normal FP32 value (the
 // FP64 route serves the one scale, 2^-127, that FP32 cannot hold).
+// The first- and second-order schemes (FP64 arithmetic in both paths), out of
+// line: inlined beside the WENO arithmetic they would cost the tile registers and
+// instruction-cache space on every face.
+static __device__ __noinline__ double face_flux_low(const double* u, const double* v, int hyp_order, int scheme,
+                                                    double dxmin, double dt)
+{
+    return face_flux_fp64(u, v, hyp_order, scheme, dxmin, dt);
+}
 __device__ __forceinline__ float face_flux_mixed32(const float* u, const float* v, int hyp_order, int scheme,
                                                    double dxmin, double dt)
 {
@@ -359,7 +367,7 @@ __device__ __forceinline__ float face_flux_mixed32(const float* u, const float* 
             ud[q] = (double)u[q];
             vd[q] = (double)v[q];
         }
-        return (float)face_flux_fp64(ud, vd, hyp_order, scheme, dxmin, dt);
+        return (float)face_flux_low(ud, vd, hyp_order, scheme, dxmin, dt);
     }
     const float m = fmaxf(fmaxf(fmaxf(fabsf(u[0]), fabsf(u[1])), fmaxf(fabsf(u[2]), fabsf(u[3]))),
                           fmaxf(fabsf(u[4]), fabsf(u[5])));
@@ -478,59 +486,6 @@ template <class R> __device__ __forceinline__ R wpoly_near(R x0, R x1, R x2)
     return fmx(-(R(1) / R(6)), x2, fmx(R(5) / R(6), x1, (R(1) / R(3)) * x0));
 }
 
-// FP32 form from values scaled by an exact power of two s (max |value| of the run
-// of cells in [1/2, 1)); eps4 = 4 eps s^2 (the indicators are kept as 4 beta_k:
-// 13/3 and 1 for 13/12 and 1/4, an exact power-of-two scaling), which may be zero
-// when it underflows: q_k = beta_k + eps is held at the smallest normal FP32 value
-// so that a stencil of equal values (beta = 0) gets the reference's limit.  The Y_k
-// are rescaled by a common factor so that nothing overflows whatever the spread of
-// the indicators (a positive multiple of the reference's; weno_f32 explains it).
-struct WenoY32 {
-    float y1, y2, y3;
-};
-__device__ __forceinline__ WenoY32 weno_center_f32(float a, float b, float c, float d, float e, int scheme, float eps4)
-{
-    const float t1 = fmaf(-2.0f, b, a) + c, t2 = fmaf(3.0f, c, fmaf(-4.0f, b, a));
-    const float b1 = fmaf(13.0f / 3.0f, t1 * t1, t2 * t2);
-    const float t3 = fmaf(-2.0f, c, b) + d, t4 = b - d;
-    const float b2 = fmaf(13.0f / 3.0f, t3 * t3, t4 * t4);
-    const float t5 = fmaf(-2.0f, d, c) + e, t6 = fmaf(3.0f, c, fmaf(-4.0f, d, e));
-    const float b3 = fmaf(13.0f / 3.0f, t5 * t5, t6 * t6);
-    const float tiny = 1.17549435e-38f;
-    const float q1 = fmaxf(b1 + eps4, tiny), q2 = fmaxf(b2 + eps4, tiny), q3 = fmaxf(b3 + eps4, tiny);
-    const float m = fminf(q1, fminf(q2, q3));
-    const float r1 = rcp_approx(q1), r2 = rcp_approx(q2), r3 = rcp_approx(q3);
-    WenoY32 y;
-    if (scheme == 3) {
-        const float tau = fabsf(b1 - b3);
-        const bool big = tau > m;
-        const float cr = big ? m * rcp_approx(tau) : 1.0f;
-        const float t = big ? m : tau;
-        const float B1 = t * r1, B2 = t * r2, B3 = t * r3;
-        const float c2 = cr * cr;
-        y.y1 = fmaf(B1, B1, c2);
-        y.y2 = fmaf(B2, B2, c2);
-        y.y3 = fmaf(B3, B3, c2);
-    } else {
-        const float B1 = m * r1, B2 = m * r2, B3 = m * r3;
-        y.y1 = B1 * B1;
-        y.y2 = B2 * B2;
-        y.y3 = B3 * B3;
-    }
-    return y;
-}
-__device__ __forceinline__ float weno_combine_f32(float y1, float y2, float y3, float p1, float p2, float p3,
-                                                  int scheme)
-{
-    float a1 = 0.1f * y1, a2 = 0.6f * y2, a3 = 0.3f * y3;
-    if (scheme == 2) {
-        const float is = rcp_approx(a1 + a2 + a3);
-        a1 = gk_map_pinned(a1 * is, 0.1f);
-        a2 = gk_map_pinned(a2 * is, 0.6f);
-        a3 = gk_map_pinned(a3 * is, 0.3f);
-    }
-    return fmaf(a1, p1, fmaf(a2, p2, a3 * p3)) * rcp_approx(a1 + a2 + a3);
-}
 
 
 // ---------------------------------------------------------------------------

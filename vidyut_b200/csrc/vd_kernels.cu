@@ -601,6 +601,7 @@ bool same_basis(const VdMechDev& m, const VelBasis& x, const VelBasis& y)
 void finish_species_lists(TransportArgs& a, const VdMechDev& m)
 {
     a.nfl = a.nnf = a.nb = 0;
+    a.stage_emag = m.emag_e;
     VelBasis bs[4];
     for (int it = 0; it < a.ntr; it++) {
         const int s = a.tr_sp[it];
@@ -625,6 +626,7 @@ void finish_species_lists(TransportArgs& a, const VdMechDev& m)
                 bs[a.nb] = b;
                 a.bkind[a.nb] = (int8_t)b.kind;
                 a.bfit[a.nb] = (int8_t)b.fit;
+                if (b.kind == 3 || b.kind == 4) a.stage_emag = 1;
                 a.bpow[a.nb++] = b.pw;
             }
         }

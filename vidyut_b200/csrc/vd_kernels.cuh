@@ -43,6 +43,7 @@ struct TransportArgs {
     int8_t nf_sp[VD_MAX_SPECIES + 1];
     int8_t bkind[4];
     int8_t bfit[4];   // bkind 4, 5: the mechanism fit holding c
+    int8_t stage_emag;  // the staged cells need |E| (a basis of kind 3 or 4, or the electrons' models)
     double bpow[4];   // bkind 3, 4: the exponent p
     double fl_K[VD_MAX_SPECIES + 1];
     float fl_Kf[VD_MAX_SPECIES + 1];  // fl_K rounded to FP32 (the mixed path's constant)

@@ -384,9 +384,10 @@ __device__ __forceinline__ bool staged_cell(const TransportArgs& a, int cc, cons
 // so[cc]: the position's cell offset in the state (-1: stages as zero), read by
 // every species group's staging
 template <int DIM, int PREC, int D, class TS>
-__device__ __forceinline__ void stage_basis(const TransportArgs& a, int cc, const int* org,
+__device__ __forceinline__ bool stage_basis(const TransportArgs& a, int cc, const int* org,
                                             typename VelT<PREC>::T* sB, JStage js, bool jst, int* so)
 {
+    bool bad = false;  // a NaN or infinity in the position's E, Te or density sum
     using G = TileGeom<DIM, TS>;
     using VT = typename VelT<PREC>::T;
     int g[3];
@@ -401,14 +402,12 @@ __device__ __forceinline__ void stage_basis(const TransportArgs& a, int cc, cons
         const double E = p[(VD_EFX(ns) + D) * cs];
         N = a.Nv(g[0], g[1], g[2]);
         Te = p[VD_ETEMP(ns) * cs];
-        if (a.status && !(isfinite(E) && isfinite(Te) && isfinite(N))) atomicOr(a.status, 1u);
+        bad = !(isfinite(E) && isfinite(Te) && isfinite(N));
         if (joule_staged<DIM, PREC>() && jst) ne = p[a.e_id * cs];
         // |E| of the three state components, as compute_vel takes it
         // (Source/PlasmaChem.H:194-196), for the models in |E| and |E|/N
         double emag = 0.0;
-        bool need_emag = c_mech.emag_e;
-        for (int k = 0; k < a.nb; k++) need_emag = need_emag || a.bkind[k] == 3 || a.bkind[k] == 4;
-        if (need_emag) {
+        if (a.stage_emag) {
             const double ex = p[VD_EFX(ns) * cs], ey = p[VD_EFY(ns) * cs], ez = p[VD_EFZ(ns) * cs];
             emag = sqrt(ex * ex + ey * ey + ez * ez);
         }
@@ -437,6 +436,7 @@ __device__ __forceinline__ void stage_basis(const TransportArgs& a, int cc, cons
         js.te[cc] = (float)Te;
         js.nd[cc] = (float)N;
     }
+    return bad;
 }
 
 // density of species s at staged position cc of direction D
@@ -614,84 +614,48 @@ __device__ __forceinline__ void run_faces(const TransportArgs& a, int2 ri, int z
                 ud[q] = (double)sU[base + (i + q) * STR];
                 vd[q] = (double)(sB ? k * sB[base + (i + q) * STR] : k);
             }
-            store(i, (VT)face_flux_fp64(ud, vd, a.hyp_order, a.weno, a.dxmin, a.dt));
+            store(i, (VT)face_flux_low(ud, vd, a.hyp_order, a.weno, a.dxmin, a.dt));
         }
         return;
     }
-    // the run's cells: densities u and drift fluxes f = u v; lam[i] = |v| at face i
-    VT u[NC], f[NC], lam[RUN];
+    // one field at a time (the densities u, then the drift fluxes f = u v), so that
+    // only one field's run of cells is live; face i lies between centres i+2 (left)
+    // and i+3 (right)
+    static_assert(PREC == PREC_FP64, "runs of faces serve the FP64 path");
+    const int scheme = a.weno;
+    double w[NC];
+#pragma unroll
+    for (int i = 0; i < NC; i++) w[i] = i < nf + 5 ? (double)sU[base + i * STR] : 0.0;
+    auto recon = [&](double* plus, double* minus) {
+        WenoY64 yl = weno_center_fp64(w[0], w[1], w[2], w[3], w[4], scheme);
+#pragma unroll
+        for (int i = 0; i < RUN; i++) {
+            if (i >= nf) break;
+            const WenoY64 yr = weno_center_fp64(w[i + 1], w[i + 2], w[i + 3], w[i + 4], w[i + 5], scheme);
+            const double p2 = wpoly_mid(w[i + 1], w[i + 2], w[i + 3]), p3 = wpoly_near(w[i + 2], w[i + 3], w[i + 4]);
+            plus[i] = weno_combine_fp64(yl.y1, yl.y2, yl.y3, wpoly_end(w[i], w[i + 1], w[i + 2]), p2, p3, scheme);
+            minus[i] = weno_combine_fp64(yr.y3, yr.y2, yr.y1, wpoly_end(w[i + 5], w[i + 4], w[i + 3]), p3, p2, scheme);
+            yl = yr;
+        }
+    };
+    double up[RUN], um[RUN], fp[RUN], fm[RUN], lam[RUN];
+    recon(up, um);
     {
-        VT vp = VT(0);
+        double vp = 0.0;
 #pragma unroll
         for (int i = 0; i < NC; i++) {
-            const bool in = i < nf + 5;
-            const VT ui = in ? sU[base + i * STR] : VT(0);
-            const VT vi = in ? (sB ? k * sB[base + i * STR] : k) : VT(0);
-            u[i] = ui;
-            f[i] = ui * vi;
-            if (i >= 3 && i - 3 < RUN) lam[i - 3] = VT(0.5) * (vp + vi);
+            const double vi = i < nf + 5 ? (double)(sB ? k * sB[base + i * STR] : k) : 0.0;
+            w[i] *= vi;
+            if (i >= 3 && i - 3 < RUN) lam[i - 3] = 0.5 * (vp + vi);
             vp = vi;
         }
     }
-    const int scheme = a.weno;
-    if constexpr (PREC == PREC_FP64) {
-        // face i lies between centres i+2 (left) and i+3 (right)
-        WenoY64 yu = weno_center_fp64(u[0], u[1], u[2], u[3], u[4], scheme);
-        WenoY64 yf = weno_center_fp64(f[0], f[1], f[2], f[3], f[4], scheme);
+    recon(fp, fm);
 #pragma unroll
-        for (int i = 0; i < RUN; i++) {
-            if (i >= nf) break;
-            const WenoY64 zu = weno_center_fp64(u[i + 1], u[i + 2], u[i + 3], u[i + 4], u[i + 5], scheme);
-            const double pu2 = wpoly_mid(u[i + 1], u[i + 2], u[i + 3]), pu3 = wpoly_near(u[i + 2], u[i + 3], u[i + 4]);
-            const double up = weno_combine_fp64(yu.y1, yu.y2, yu.y3, wpoly_end(u[i], u[i + 1], u[i + 2]), pu2, pu3, scheme);
-            const double um = weno_combine_fp64(zu.y3, zu.y2, zu.y1, wpoly_end(u[i + 5], u[i + 4], u[i + 3]), pu3, pu2, scheme);
-            const WenoY64 zf = weno_center_fp64(f[i + 1], f[i + 2], f[i + 3], f[i + 4], f[i + 5], scheme);
-            const double pf2 = wpoly_mid(f[i + 1], f[i + 2], f[i + 3]), pf3 = wpoly_near(f[i + 2], f[i + 3], f[i + 4]);
-            const double fp = weno_combine_fp64(yf.y1, yf.y2, yf.y3, wpoly_end(f[i], f[i + 1], f[i + 2]), pf2, pf3, scheme);
-            const double fm = weno_combine_fp64(zf.y3, zf.y2, zf.y1, wpoly_end(f[i + 5], f[i + 4], f[i + 3]), pf3, pf2, scheme);
-            const double l = fabs(lam[i]);
-            store(i, fma(0.5, fma(l, up, fp), 0.5 * fma(-l, um, fm)));
-            yu = zu;
-            yf = zf;
-        }
-    } else {
-        // one exact power-of-two scale for the run: s = 2^-e with max |u| in
-        // [2^(e-1), 2^e) (1 for zero, denormal or non-finite maxima); the
-        // reconstructions work on u s and f s and each face flux is unscaled by
-        // 1/s, which is exact
-        float mx = 0.0f;
-#pragma unroll
-        for (int i = 0; i < NC; i++) mx = fmaxf(mx, fabsf(u[i]));
-        const int eb = (__float_as_int(mx) >> 23) & 0xff;
-        int e = (eb > 0 && eb < 255) ? eb - 126 : 0;
-        e = max(-125, min(e, 126));
-        const float s = __int_as_float((127 - e) << 23), inv_s = __int_as_float((127 + e) << 23);
-        const int b2 = 127 - 2 * e;
-        const float s2 = b2 > 0 ? __int_as_float(min(b2, 254) << 23) : 0.0f;  // s^2, 0 when it underflows
-        const float eps4 = 4e-20f * s2;
-#pragma unroll
-        for (int i = 0; i < NC; i++) {
-            u[i] *= s;
-            f[i] *= s;
-        }
-        WenoY32 yu = weno_center_f32(u[0], u[1], u[2], u[3], u[4], scheme, eps4);
-        WenoY32 yf = weno_center_f32(f[0], f[1], f[2], f[3], f[4], scheme, eps4);
-#pragma unroll
-        for (int i = 0; i < RUN; i++) {
-            if (i >= nf) break;
-            const WenoY32 zu = weno_center_f32(u[i + 1], u[i + 2], u[i + 3], u[i + 4], u[i + 5], scheme, eps4);
-            const float pu2 = wpoly_mid(u[i + 1], u[i + 2], u[i + 3]), pu3 = wpoly_near(u[i + 2], u[i + 3], u[i + 4]);
-            const float up = weno_combine_f32(yu.y1, yu.y2, yu.y3, wpoly_end(u[i], u[i + 1], u[i + 2]), pu2, pu3, scheme);
-            const float um = weno_combine_f32(zu.y3, zu.y2, zu.y1, wpoly_end(u[i + 5], u[i + 4], u[i + 3]), pu3, pu2, scheme);
-            const WenoY32 zf = weno_center_f32(f[i + 1], f[i + 2], f[i + 3], f[i + 4], f[i + 5], scheme, eps4);
-            const float pf2 = wpoly_mid(f[i + 1], f[i + 2], f[i + 3]), pf3 = wpoly_near(f[i + 2], f[i + 3], f[i + 4]);
-            const float fp = weno_combine_f32(yf.y1, yf.y2, yf.y3, wpoly_end(f[i], f[i + 1], f[i + 2]), pf2, pf3, scheme);
-            const float fm = weno_combine_f32(zf.y3, zf.y2, zf.y1, wpoly_end(f[i + 5], f[i + 4], f[i + 3]), pf3, pf2, scheme);
-            const float l = fabsf(lam[i]);
-            store(i, 0.5f * (fmaf(l, up, fp) + fmaf(-l, um, fm)) * inv_s);
-            yu = zu;
-            yf = zf;
-        }
+    for (int i = 0; i < RUN; i++) {
+        if (i >= nf) break;
+        const double l = fabs(lam[i]);
+        store(i, (VT)fma(0.5, fma(l, up[i], fp[i]), 0.5 * fma(-l, um[i], fm[i])));
     }
 }
 
@@ -745,6 +709,7 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     auto state = [&](int s) -> double { return __ldg(a.sb.p + own_o + s * cs); };
     auto rate = [&](int s) -> double { return __ldg(a.rxn.p + own_r + s * a.rxn.ns); };
     double ne_new = 0.0, een_new = 0.0;
+    bool bad = false;  // this thread met a NaN or infinity (reported once per warp at the end)
     const int nfl = a.nfl;
     // the mixed path's Joule faces, evaluated here (a barrier follows them)
     const bool jin = joule_in_tile(a, PREC);
@@ -793,7 +758,7 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
             const double lo = (s == a.e_id) ? a.min_elec : a.min_spec;
             if (nn < lo) nn = lo;
         }
-        if (a.status && !isfinite(nn)) atomicOr(a.status, 1u);
+        bad |= !isfinite(nn);
         a.pn(gi, gj, gk, s) = nn;
         if (a.dsdt.p) a.dsdt(gi, gj, gk, s) = acc;
         if (s == a.e_id) ne_new = nn;
@@ -809,14 +774,14 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
         }
         for (int c = tid; c < G::STOT; c += NTH) {
             if (c < G::SOFF1) {
-                stage_basis<DIM, PREC, 0, TS>(a, c, org, sB, js, jin, sSO);
+                bad |= stage_basis<DIM, PREC, 0, TS>(a, c, org, sB, js, jin, sSO);
             } else if (DIM > 1 && c < G::SOFF2) {
                 const JStage j1{js.ne + G::SOFF1, js.te + G::SOFF1, js.nd + G::SOFF1};
-                stage_basis<DIM, PREC, (DIM > 1 ? 1 : 0), TS>(a, c - G::SOFF1, org, sB + G::SOFF1, j1, jin,
+                bad |= stage_basis<DIM, PREC, (DIM > 1 ? 1 : 0), TS>(a, c - G::SOFF1, org, sB + G::SOFF1, j1, jin,
                                                               sSO + G::SOFF1);
             } else if (DIM > 2) {
                 const JStage j2{js.ne + G::SOFF2, js.te + G::SOFF2, js.nd + G::SOFF2};
-                stage_basis<DIM, PREC, (DIM > 2 ? 2 : 0), TS>(a, c - G::SOFF2, org, sB + G::SOFF2, j2, jin,
+                bad |= stage_basis<DIM, PREC, (DIM > 2 ? 2 : 0), TS>(a, c - G::SOFF2, org, sB + G::SOFF2, j2, jin,
                                                               sSO + G::SOFF2);
             }
         }
@@ -954,7 +919,7 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
                 v += r * a.dt;
                 if (v < a.min_spec && a.bound_specden) v = a.min_spec;
             }
-            if (a.status && !isfinite(v)) atomicOr(a.status, 1u);
+            bad |= !isfinite(v);
             a.pn(gi, gj, gk, s) = v;
             if (a.dsdt.p) a.dsdt(gi, gj, gk, s) = r;
         }
@@ -967,6 +932,10 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
             }
             a.pn(gi, gj, gk, VD_ETEMP(ns)) = te;
         }
+    }
+    if (a.status) {  // uniform over the CTA; every lane of every warp reaches it
+        const unsigned any = __ballot_sync(0xffffffffu, bad);
+        if (any && (threadIdx.x & 31) == 0) atomicOr(a.status, 1u);
     }
 }
 

@@ -355,6 +355,31 @@ def config_batched(seed: int = BASE_SEED, n_cases: int = 64, side=(64, 512), n_s
     return mech, cases
 
 
+SERVING_ADVECTIVE_CFL = 0.2
+
+
+def electron_time_scales(case: BoxCase) -> tuple:
+    """(dt_edrift, dt_diel_relax) of the case's initial state as
+    Vidyut::find_time_scales computes them (Source/TimeStep.cpp:32-118):
+    min over directions of dx / max |mu_e| |E|, and eps0 / (e max |mu_e| ne), for
+    the collisional electron mobility (VD_MOB_ELECTRON) of the synthetic
+    mechanisms."""
+    m = case.mech
+    if m.mob_kind[m.e_id] != abi.MOB_ELECTRON:
+        raise NotImplementedError("time scales of this electron mobility model")
+    ns, g = m.ns, case.gvec
+    v = (slice(g[2], g[2] + case.n[2]), slice(g[1], g[1] + case.n[1]), slice(g[0], g[0] + case.n[0]))
+    st = case.state
+    N = st[:ns][(slice(None),) + v].sum(axis=0)
+    te = st[abi.ETEMP(ns)][v]
+    emag = np.sqrt(sum(st[abi.EFX(ns) + d][v] ** 2 for d in range(3)))
+    echarge, me, eps0 = 1.60217662e-19, 9.10938188e-31, 8.854187817e-12
+    mu = (echarge / me) / (np.sqrt(8.0 * K_B * te / np.pi / me) * N * m.mob_p0[m.e_id])
+    dt_edrift = min(case.dx[:case.dim]) / float((mu * emag).max())
+    dt_diel = eps0 / echarge / float((mu * st[m.e_id][v]).max())
+    return dt_edrift, dt_diel
+
+
 def config_serving(seed: int = BASE_SEED, n_requests: int = 48, rate_per_s: float = 500.0,
                    side=(256, 1024), steps=(50, 2000), voltage_kv=(0.5, 5.0), pressure_bar=(0.1, 10.0),
                    frac_2d: float = 0.5):
@@ -363,8 +388,14 @@ def config_serving(seed: int = BASE_SEED, n_requests: int = 48, rate_per_s: floa
     in `side` cells, applied voltage uniform in voltage_kv (the potential ramp's
     amplitude), pressure log-uniform in pressure_bar scaling the background gas
     (2.4e25 m^-3 at 1 bar), step count log-uniform in `steps`, the batched
-    workload's 8-species / 40-reaction mechanism.  Returns (mechanism, [(arrival
-    time [s], BoxCase, nsteps)])."""
+    workload's 8-species / 40-reaction mechanism.  Each case's time step is the
+    reference's adaptive one for its initial state (Source/TimeStep.cpp:14-31:
+    the electron drift and dielectric relaxation limits times their CFL numbers,
+    capped at dt_max = 1e-12 s), with an advective CFL of SERVING_ADVECTIVE_CFL:
+    the explicit forward-Euler update with WENO fluxes needs a smaller one than
+    the reference's semi-implicit default of 0.7, and at dt = 1e-12 s the
+    strong-field, low-pressure cases of this distribution run past it and blow
+    up.  Returns (mechanism, [(arrival time [s], BoxCase, nsteps)])."""
     mech = synthetic(8, 40, seed + 21)
     rng = np.random.default_rng(seed + 31)
     t = 0.0
@@ -379,6 +410,8 @@ def config_serving(seed: int = BASE_SEED, n_requests: int = 48, rate_per_s: floa
         case = build_case(mech, dim, n, (1e-5,) * dim, seed + 5000 + i, density="loguniform_smooth",
                           dens_range=(1e10, 1e18), te_range_ev=(0.3, 10.0), voltage=v, bg_density=2.4e25 * p,
                           params=dict(MULTISTEP_PARAMS), n_modes=4)
+        dt_edrift, dt_diel = electron_time_scales(case)
+        case.params["dt"] = min(MULTISTEP_PARAMS["dt"], SERVING_ADVECTIVE_CFL * dt_edrift, dt_diel)
         out.append((t, case, ns))
     return mech, out
 
