@@ -3,13 +3,15 @@
 // One CTA updates a TX x TY x TZ tile of one box.
 // (0) Once per tile, for every cell of the stencil lines of each sweep direction d
 //     (cells rel -3 .. T_d+2 along d of each tile row), the velocity bases of the
-//     mobility models -- E_d/(sqrt(Te) N), E_d/N, E_d, as the mechanism needs --
-//     are computed from Te, E and the density sum and kept in shared memory.  A
-//     species' face velocity is then its constant times one basis (specMob).
+//     mobility models -- E_d/(sqrt(Te) N), E_d/N, E_d, E_d |E|^p, E_d f(|E|/N),
+//     E_d g(Te)/N, as the mechanism needs -- are computed from Te, E and the
+//     density sum and kept in shared memory.  A species' face velocity is then its
+//     constant times one basis (specMob).
 // (1) The transported species with a drift flux go in groups of up to GRP: the
 //     densities of the whole group on all staged lines are loaded at once (many
 //     independent loads in flight), then every face flux of every species of the
-//     group is computed once (all directions, faces spread over the threads), then
+//     group is computed once (all directions; faces spread over the threads one by
+//     one in the mixed path, in runs along the lines in the FP64 path), then
 //     each thread takes the divergence of its own cell, adds rxn (and the Joule
 //     term for the electron energy) and writes n + dt*dsdt in FP64.  Two barriers
 //     per group.  The Joule term: the mixed path evaluates every face of the
@@ -23,6 +25,7 @@
 // tile) and the batched persistent kernel (CTAs loop over a work list of
 // (box, tile) items of many boxes) share it.
 #pragma once
+#include <type_traits>
 #include "vd_device.cuh"
 #include "vd_kernels.cuh"
 
@@ -488,8 +491,9 @@ __device__ __forceinline__ int face_info(const TransportArgs& a, int f, const in
 // species' staged densities and velocity basis over all line sets (sB null: the
 // user velocity of the face's direction), k its velocity constant, zm its
 // zero-flux mask (TransportArgs::fl_zm); zero for a face the box does not update
-// or where IHNEUBC holds (Source/compute_explicit_flux.H:200-326).
-template <int DIM, int PREC, class TS>
+// or where IHNEUBC holds (Source/compute_explicit_flux.H:200-326).  W5: the
+// caller has checked hyp_order == 5 (the WENO loop then holds no low-order code).
+template <int DIM, int PREC, class TS, bool W5>
 __device__ __forceinline__ typename VelT<PREC>::T face_tab(const TransportArgs& a, int info, int zm,
                                                            const typename VelT<PREC>::T* sU,
                                                            const typename VelT<PREC>::T* sB,
@@ -507,8 +511,8 @@ __device__ __forceinline__ typename VelT<PREC>::T face_tab(const TransportArgs& 
         v[q] = sB ? k * sB[base + q * STR] : k;
     }
     VT F;
-    if constexpr (PREC == PREC_FP64) F = face_flux_fp64(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
-    else F = face_flux_mixed32(u, v, a.hyp_order, a.weno, a.dxmin, a.dt);
+    if constexpr (PREC == PREC_FP64) F = face_flux_fp64(u, v, W5 ? 5 : a.hyp_order, a.weno, a.dxmin, a.dt);
+    else F = face_flux_mixed32(u, v, W5 ? 5 : a.hyp_order, a.weno, a.dxmin, a.dt);
     if (((info & kFaceDomLo) && ((zm >> D) & 1)) || ((info & kFaceDomHi) && ((zm >> (3 + D)) & 1))) F = VT(0);
     return F;
 }
@@ -587,7 +591,7 @@ __device__ __forceinline__ int2 run_info(const TransportArgs& a, int r, const in
 // (TransportArgs::fl_zm); writes the nf face fluxes to sF (tile face numbering),
 // zero where the box updates no face or IHNEUBC holds
 // (Source/compute_explicit_flux.H:200-326).
-template <int DIM, int PREC, class TS, int RUN>
+template <int DIM, int PREC, class TS, int RUN, bool W5>
 __device__ __forceinline__ void run_faces(const TransportArgs& a, int2 ri, int zm,
                                           const typename VelT<PREC>::T* __restrict__ sU,
                                           const typename VelT<PREC>::T* __restrict__ sB,
@@ -605,8 +609,8 @@ __device__ __forceinline__ void run_faces(const TransportArgs& a, int2 ri, int z
         if (i >= nok || (i == ilo && zlo) || (i == ihi && zhi)) F = VT(0);
         sF[fbase + i * STR] = F;
     };
-    if (a.hyp_order != 5) {
-        // upwind / WAF: FP64 arithmetic on the face's own stencil (both paths)
+    if constexpr (!W5) {
+        // upwind / WAF: FP64 arithmetic on the face's own stencil
         for (int i = 0; i < nf; i++) {
             double ud[6], vd[6];
 #pragma unroll
@@ -860,21 +864,32 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
         __syncthreads();
         // (2) every face flux of the group: by runs of faces along the lines, or
         // face by face
-        if constexpr (by_runs<DIM, PREC>()) {
+        // face by face; one loop per scheme family, so that the WENO loop carries
+        // no low-order code
+        auto runs = [&](auto w5) {
             for (int q = tid; q < gn * RG::NRUN; q += NTH) {
                 const int j = q / RG::NRUN, r = q - j * RG::NRUN;
                 const int sl = a.fl_slot[g0 + j];
-                run_faces<DIM, PREC, TS, RUN>(a, sRI[r], a.fl_zm[g0 + j], sU + j * G::STOT,
-                                              sl >= 0 ? sB + sl * G::STOT : nullptr, (VT)a.fl_K[g0 + j],
-                                              sF + j * G::FTOT);
+                run_faces<DIM, PREC, TS, RUN, decltype(w5)::value>(a, sRI[r], a.fl_zm[g0 + j], sU + j * G::STOT,
+                                                                   sl >= 0 ? sB + sl * G::STOT : nullptr,
+                                                                   (VT)a.fl_K[g0 + j], sF + j * G::FTOT);
             }
-        } else {
+        };
+        auto faces = [&](auto w5) {
             for (int q = tid; q < gn * G::FTOT; q += NTH) {
                 const int j = q / G::FTOT, f = q - j * G::FTOT;
                 const int sl = a.fl_slot[g0 + j];
-                sF[q] = face_tab<DIM, PREC, TS>(a, sFI[f], a.fl_zm[g0 + j], sU + j * G::STOT,
-                                                sl >= 0 ? sB + sl * G::STOT : nullptr, (VT)a.fl_Kf[g0 + j]);
+                sF[q] = face_tab<DIM, PREC, TS, decltype(w5)::value>(a, sFI[f], a.fl_zm[g0 + j], sU + j * G::STOT,
+                                                                     sl >= 0 ? sB + sl * G::STOT : nullptr,
+                                                                     (VT)a.fl_Kf[g0 + j]);
             }
+        };
+        if constexpr (by_runs<DIM, PREC>()) {
+            if (a.hyp_order == 5) runs(std::true_type{});
+            else runs(std::false_type{});
+        } else {
+            if (a.hyp_order == 5) faces(std::true_type{});
+            else faces(std::false_type{});
         }
         __syncthreads();
         // (3) divergence + sources of the own cell: dsdt = (Fx_lo - Fx_hi)/dx + rxn,
