@@ -141,9 +141,11 @@ __host__ __device__ constexpr size_t smem_align(size_t x) { return (x + 15) & ~(
 // each face on its own (face_tab: fewer live registers, an even split of the faces
 // over the threads), which measured faster for its FP32 arithmetic on B200.
 template <int DIM, int PREC> constexpr bool by_runs() { return PREC == PREC_FP64; }
-// Faces per run: 2 in 3-D, where the T + 1 = 9 faces of a line then make 5 runs
-// (960 per species for an 8^3 tile, an even load for its 512 threads), else 3.
-template <int DIM, class TS> constexpr int run_len() { return DIM == 3 ? 2 : 3; }
+// Faces per run: 5 in 3-D, where the T + 1 = 9 faces of a line then make two runs
+// (384 per species for an 8^3 tile: one pass of its 512 threads), else 3.  Timed
+// on B200 for the 3-D workload: runs of 2, 3, 4, 5 faces 3.20, 3.19, 4.05,
+// 3.09 ms (4 leaves a third pass with one face); for 2-D tiles 3 beats 2 and 4.
+template <int DIM, class TS> constexpr int run_len() { return DIM == 3 ? 5 : 3; }
 
 // Dynamic shared memory of one tile with nb velocity bases and species groups of
 // GRP, in this order: the Joule term of every face (FP64, mixed path); the run
