@@ -119,7 +119,7 @@ def test_batch_fp64_matches_multistep_oracle(mech):
 
 
 def test_batch_mixed_within_1e5_of_oracle(mech):
-    """<= 1e-5 max relative error in every species density
+    """the mixed-precision bound: <= 1e-5 max relative error in every species density
     (and the energy, Te) after 20 mixed-precision steps"""
     cases = make_cases(mech, [(48, 40), (33, 57), (128,)], seed=99)
     got, _ = run_batch(cases, abi.PREC_MIXED, 20)
