@@ -746,7 +746,9 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     };
 
     // one species' own-cell result
-    auto finish = [&](int s, double acc) {
+    // (st: the species' old value, state(s), loaded by the caller so that several
+    // species' loads can be in flight together)
+    auto finish = [&](int s, double acc, double st) {
         if (s == ns) {
             if (jin) {
                 const double jh = joule_own();
@@ -758,7 +760,7 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
             }
             if (a.write_diag) a.pn(gi, gj, gk, VD_EIH(ns)) = rate(ns);
         }
-        double nn = state(s) + a.dt * acc;
+        double nn = st + a.dt * acc;
         if (a.bound_specden && s != ns) {
             // solution clipping of the species solve (Source/ScalarSolve.cpp:597-622)
             const double lo = (s == a.e_id) ? a.min_elec : a.min_spec;
@@ -847,14 +849,31 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
     for (int g0 = 0; g0 < nfl; g0 += GRP) {
         const int gn = nfl - g0 < GRP ? nfl - g0 : GRP;
         // (1) densities of the group on the staged lines
-        for (int q = tid; q < gn * G::STOT; q += NTH) {
+        if (stab) {
+            // four positions per thread at a time: their loads in flight together
+            constexpr int CH = 4;
+            const int tot = gn * G::STOT;
+            for (int q0 = tid; q0 < tot; q0 += CH * NTH) {
+                VT u[CH];
+#pragma unroll
+                for (int k = 0; k < CH; k++) {
+                    const int q = q0 + k * NTH;
+                    u[k] = VT(0);
+                    if (q < tot) {
+                        const int j = q / G::STOT, c = q - j * G::STOT;
+                        const int o = sSO[c];
+                        if (o >= 0) u[k] = (VT)__ldg(a.sb.p + o + (int64_t)a.fl_sp[g0 + j] * cs);
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < CH; k++)
+                    if (q0 + k * NTH < tot) sU[q0 + k * NTH] = u[k];
+            }
+        } else for (int q = tid; q < gn * G::STOT; q += NTH) {
             const int j = q / G::STOT, c = q - j * G::STOT;
             const int s = a.fl_sp[g0 + j];
             VT u;
-            if (stab) {
-                const int o = sSO[c];
-                u = o >= 0 ? (VT)__ldg(a.sb.p + o + (int64_t)s * cs) : VT(0);
-            } else if (c < G::SOFF1) {
+            if (c < G::SOFF1) {
                 u = stage_density<DIM, PREC, 0, TS>(a, c, s, org);
             } else if (DIM > 1 && c < G::SOFF2) {
                 u = stage_density<DIM, PREC, (DIM > 1 ? 1 : 0), TS>(a, c - G::SOFF1, s, org);
@@ -897,14 +916,16 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
         // (3) divergence + sources of the own cell: dsdt = (Fx_lo - Fx_hi)/dx + rxn,
         // then += y and z terms (Source/ScalarSolve.cpp:45-51)
         if (own) {
-#pragma unroll 1
-            for (int j = 0; j < gn; j++) {
+            // the own cell's dsdt of species j of the group, with its rate r, in the
+            // reference's order: x faces + rate, then y, then z
+            // (Source/ScalarSolve.cpp:45-51)
+            auto divergence = [&](int j, double r) -> double {
                 const VT* Fj = sF + j * G::FTOT;
                 double acc;
                 {
                     constexpr int F0 = G::template FE<0>(0), F1 = G::template FE<0>(1);
                     const int lo_f = cx + F0 * (cy + F1 * cz);
-                    acc = ((double)Fj[lo_f] - (double)Fj[lo_f + 1]) * a.idx[0] + rate(a.fl_sp[g0 + j]);
+                    acc = ((double)Fj[lo_f] - (double)Fj[lo_f + 1]) * a.idx[0] + r;
                 }
                 if constexpr (DIM > 1) {
                     constexpr int F0 = G::template FE<1>(0), F1 = G::template FE<1>(1);
@@ -916,7 +937,16 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
                     const int lo_f = G::FOFF2 + cx + F0 * (cy + F1 * cz);
                     acc += ((double)Fj[lo_f] - (double)Fj[lo_f + F0 * F1]) * a.idx[2];
                 }
-                finish(a.fl_sp[g0 + j], acc);
+                return acc;
+            };
+            // two species at a time: their four loads in flight together
+#pragma unroll 1
+            for (int j = 0; j < gn; j += 2) {
+                const bool two = j + 1 < gn;
+                const int s0 = a.fl_sp[g0 + j], s1 = two ? a.fl_sp[g0 + j + 1] : s0;
+                const double r0 = rate(s0), r1 = rate(s1), st0 = state(s0), st1 = state(s1);
+                finish(s0, divergence(j, r0), st0);
+                if (two) finish(s1, divergence(j + 1, r1), st1);
             }
         }
         // the next group's staging overwrites sU only after every thread has passed
@@ -924,21 +954,42 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
         // by which time every divergence read of this group is done
     }
     if (own) {
-        for (int j = 0; j < a.nnf; j++) {
-            const int s = a.nf_sp[j];
-            finish(s, rate(s));
-        }
-        for (int ib = 0; ib < a.nbg; ib++) {
-            const int s = a.bg_sp[ib];
-            double v = state(s);
-            double r = rate(s);
-            if (a.do_bg) {
-                v += r * a.dt;
-                if (v < a.min_spec && a.bound_specden) v = a.min_spec;
+        // four species at a time: their loads in flight together
+        constexpr int CH = 4;
+#pragma unroll 1
+        for (int j0 = 0; j0 < a.nnf; j0 += CH) {
+            double r[CH], st[CH];
+#pragma unroll
+            for (int k = 0; k < CH; k++) {
+                const int s = a.nf_sp[j0 + k < a.nnf ? j0 + k : a.nnf - 1];
+                r[k] = rate(s);
+                st[k] = state(s);
             }
-            bad |= !isfinite(v);
-            a.pn(gi, gj, gk, s) = v;
-            if (a.dsdt.p) a.dsdt(gi, gj, gk, s) = r;
+#pragma unroll
+            for (int k = 0; k < CH; k++)
+                if (j0 + k < a.nnf) finish(a.nf_sp[j0 + k], r[k], st[k]);
+        }
+#pragma unroll 1
+        for (int j0 = 0; j0 < a.nbg; j0 += CH) {
+            double r[CH], v[CH];
+#pragma unroll
+            for (int k = 0; k < CH; k++) {
+                const int s = a.bg_sp[j0 + k < a.nbg ? j0 + k : a.nbg - 1];
+                r[k] = rate(s);
+                v[k] = state(s);
+            }
+#pragma unroll
+            for (int k = 0; k < CH; k++) {
+                if (j0 + k >= a.nbg) continue;
+                const int s = a.bg_sp[j0 + k];
+                if (a.do_bg) {
+                    v[k] += r[k] * a.dt;
+                    if (v[k] < a.min_spec && a.bound_specden) v[k] = a.min_spec;
+                }
+                bad |= !isfinite(v[k]);
+                a.pn(gi, gj, gk, s) = v[k];
+                if (a.dsdt.p) a.dsdt(gi, gj, gk, s) = r[k];
+            }
         }
         if (a.update_te && a.elecenergy) {
             // Source/ScalarSolve.cpp:659-666
