@@ -124,6 +124,15 @@ __device__ __forceinline__ float mob_exp_meane_f32(const double* c, float Te)
     const double sum = fma((double)log2f((float)m), c[1] * LN2, c[0]) + im * fma(im, fma(im, c[4], c[3]), c[2]);
     return exp2_split(sum * LOG2E);
 }
+// velocity basis kinds 3, 4 and 5 of the mixed transport tile, out of line (as
+// basis_field_fp64)
+static __device__ __noinline__ float basis_field_f32(int kind, int fit, float pw, float E, float emag, float N,
+                                                     float Te)
+{
+    if (kind == 3) return E * exp2f(pw * log2f(emag));
+    if (kind == 4) return E * mob_en_poly_f32(c_mech.fits[fit].jc, pw, emag, N);
+    return E * mob_exp_meane_f32(c_mech.fits[fit].jc, Te) * rcp_approx(N);
+}
 __device__ __forceinline__ float mob_base_f32(int s, float Te, float N, float Tg, float emag)
 {
     switch (c_mech.mob_kind[s]) {

@@ -428,10 +428,7 @@ __device__ __forceinline__ bool stage_basis(const TransportArgs& a, int cc, cons
                 if (kind == 0) b[k] = Ef * rsqrtf((float)Te) * rN;
                 else if (kind == 1) b[k] = Ef * rN;
                 else if (kind == 2) b[k] = Ef;
-                else if (kind == 3) b[k] = Ef * exp2f((float)a.bpow[k] * log2f((float)emag));
-                else if (kind == 4)
-                    b[k] = Ef * mob_en_poly_f32(c_mech.fits[a.bfit[k]].jc, (float)a.bpow[k], (float)emag, (float)N);
-                else b[k] = Ef * mob_exp_meane_f32(c_mech.fits[a.bfit[k]].jc, (float)Te) * rN;
+                else b[k] = basis_field_f32(kind, a.bfit[k], (float)a.bpow[k], Ef, (float)emag, (float)N, (float)Te);
             }
         }
     }
@@ -780,17 +777,35 @@ __device__ __forceinline__ void transport_tile_update(const TransportArgs& a, in
         } else {
             for (int f = tid; f < G::FTOT; f += NTH) sFI[f] = face_info<DIM, TS>(a, f, org);
         }
-        for (int c = tid; c < G::STOT; c += NTH) {
-            if (c < G::SOFF1) {
-                bad |= stage_basis<DIM, PREC, 0, TS>(a, c, org, sB, js, jin, sSO);
-            } else if (DIM > 1 && c < G::SOFF2) {
-                const JStage j1{js.ne + G::SOFF1, js.te + G::SOFF1, js.nd + G::SOFF1};
-                bad |= stage_basis<DIM, PREC, (DIM > 1 ? 1 : 0), TS>(a, c - G::SOFF1, org, sB + G::SOFF1, j1, jin,
-                                                              sSO + G::SOFF1);
-            } else if (DIM > 2) {
-                const JStage j2{js.ne + G::SOFF2, js.te + G::SOFF2, js.nd + G::SOFF2};
-                bad |= stage_basis<DIM, PREC, (DIM > 2 ? 2 : 0), TS>(a, c - G::SOFF2, org, sB + G::SOFF2, j2, jin,
-                                                              sSO + G::SOFF2);
+        if constexpr (PREC == PREC_MIXED) {
+            // one loop per direction's line set, two positions per iteration, so
+            // that the loads of both positions are in flight together (measured
+            // faster for the mixed tile, slower for the FP64 one, whose positions
+            // then split less evenly over the threads)
+            auto bases = [&](auto dtag) {
+                constexpr int D = decltype(dtag)::value;
+                constexpr int off = D == 0 ? 0 : (D == 1 ? G::SOFF1 : G::SOFF2);
+                const JStage jd{js.ne + off, js.te + off, js.nd + off};
+#pragma unroll 2
+                for (int cc = tid; cc < G::template NS<D>(); cc += NTH)
+                    bad |= stage_basis<DIM, PREC, D, TS>(a, cc, org, sB + off, jd, jin, sSO + off);
+            };
+            bases(std::integral_constant<int, 0>{});
+            if constexpr (DIM > 1) bases(std::integral_constant<int, 1>{});
+            if constexpr (DIM > 2) bases(std::integral_constant<int, 2>{});
+        } else {
+            for (int c = tid; c < G::STOT; c += NTH) {
+                if (c < G::SOFF1) {
+                    bad |= stage_basis<DIM, PREC, 0, TS>(a, c, org, sB, js, jin, sSO);
+                } else if (DIM > 1 && c < G::SOFF2) {
+                    const JStage j1{js.ne + G::SOFF1, js.te + G::SOFF1, js.nd + G::SOFF1};
+                    bad |= stage_basis<DIM, PREC, (DIM > 1 ? 1 : 0), TS>(a, c - G::SOFF1, org, sB + G::SOFF1, j1,
+                                                                         jin, sSO + G::SOFF1);
+                } else if (DIM > 2) {
+                    const JStage j2{js.ne + G::SOFF2, js.te + G::SOFF2, js.nd + G::SOFF2};
+                    bad |= stage_basis<DIM, PREC, (DIM > 2 ? 2 : 0), TS>(a, c - G::SOFF2, org, sB + G::SOFF2, j2,
+                                                                         jin, sSO + G::SOFF2);
+                }
             }
         }
         // the offset table and the staged Joule inputs are read by other threads
