@@ -629,37 +629,34 @@ __device__ __forceinline__ void run_faces(const TransportArgs& a, int2 ri, int z
     double w[NC];
 #pragma unroll
     for (int i = 0; i < NC; i++) w[i] = i < nf + 5 ? (double)sU[base + i * STR] : 0.0;
-    auto recon = [&](double* plus, double* minus) {
+    // the reconstructions of the field in w at each face of the run, handed to
+    // emit(i, left-biased value, right-biased value) as they are made
+    auto recon = [&](auto&& emit) {
         WenoY64 yl = weno_center_fp64(w[0], w[1], w[2], w[3], w[4], scheme);
 #pragma unroll
         for (int i = 0; i < RUN; i++) {
             if (i >= nf) break;
             const WenoY64 yr = weno_center_fp64(w[i + 1], w[i + 2], w[i + 3], w[i + 4], w[i + 5], scheme);
             const double p2 = wpoly_mid(w[i + 1], w[i + 2], w[i + 3]), p3 = wpoly_near(w[i + 2], w[i + 3], w[i + 4]);
-            plus[i] = weno_combine_fp64(yl.y1, yl.y2, yl.y3, wpoly_end(w[i], w[i + 1], w[i + 2]), p2, p3, scheme);
-            minus[i] = weno_combine_fp64(yr.y3, yr.y2, yr.y1, wpoly_end(w[i + 5], w[i + 4], w[i + 3]), p3, p2, scheme);
+            emit(i, weno_combine_fp64(yl.y1, yl.y2, yl.y3, wpoly_end(w[i], w[i + 1], w[i + 2]), p2, p3, scheme),
+                 weno_combine_fp64(yr.y3, yr.y2, yr.y1, wpoly_end(w[i + 5], w[i + 4], w[i + 3]), p3, p2, scheme));
             yl = yr;
         }
     };
-    double up[RUN], um[RUN], fp[RUN], fm[RUN], lam[RUN];
-    recon(up, um);
-    {
-        double vp = 0.0;
+    auto vel = [&](int i) -> double { return (double)(sB ? k * sB[base + i * STR] : k); };
+    double up[RUN], um[RUN];
+    recon([&](int i, double pl, double mi) {
+        up[i] = pl;
+        um[i] = mi;
+    });
 #pragma unroll
-        for (int i = 0; i < NC; i++) {
-            const double vi = i < nf + 5 ? (double)(sB ? k * sB[base + i * STR] : k) : 0.0;
-            w[i] *= vi;
-            if (i >= 3 && i - 3 < RUN) lam[i - 3] = 0.5 * (vp + vi);
-            vp = vi;
-        }
-    }
-    recon(fp, fm);
-#pragma unroll
-    for (int i = 0; i < RUN; i++) {
-        if (i >= nf) break;
-        const double l = fabs(lam[i]);
-        store(i, (VT)fma(0.5, fma(l, up[i], fp[i]), 0.5 * fma(-l, um[i], fm[i])));
-    }
+    for (int i = 0; i < NC; i++) w[i] *= i < nf + 5 ? vel(i) : 0.0;
+    // the drift fluxes' reconstructions go straight into the face flux (the face's
+    // |v| from the two cells' velocities, reloaded from shared memory)
+    recon([&](int i, double fp, double fm) {
+        const double l = fabs(0.5 * (vel(i + 2) + vel(i + 3)));
+        store(i, (VT)fma(0.5, fma(l, up[i], fp), 0.5 * fma(-l, um[i], fm)));
+    });
 }
 
 // Update tile `tile` (index over a.ntile) of the box described by a.  Every thread
