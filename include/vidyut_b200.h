@@ -409,7 +409,9 @@ int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_array4 efield_e
  * (Source/PlasmaChem.H:75-184): VD_BC_DIRC holds that value at the face,
  * VD_BC_IHNEU takes it as the derivative along the direction, VD_BC_HNEU and
  * VD_BC_ROBIN (species_bc's default robin coefficients) zero gradient; a periodic
- * direction is refused (VD_ERR_ARG).  n_old from state_old, the explicit source
+ * direction (VD_BC_PER on both sides, an even number of cells, the state's ghost
+ * cells filled periodically) couples its first and last cells (odd counts and
+ * one-sided VD_BC_PER are refused, VD_ERR_ARG).  n_old from state_old, the explicit source
  * from component dp->dsdt_comp of dsdt.  The initial guess is the current state;
  * FP64 V(2,2) cycles until max|residual| <= tol_rel * max|rhs| (tol_rel > 0, one
  * host synchronisation per cycle) or max_vcycles (tol_rel == 0: exactly that many,

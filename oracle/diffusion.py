@@ -123,8 +123,9 @@ def solve(case, spec, state_old, dsdt, prm, port, robin=None):
     cls = species_class(mech, spec)
     bclo = [prm.bc_lo[cls][d] for d in range(3)]
     bchi = [prm.bc_hi[cls][d] for d in range(3)]
-    if any(bclo[d] == BC_PER or bchi[d] == BC_PER for d in range(dim)):
-        raise ValueError("periodic directions are not covered")
+    per = [d < dim and bclo[d] == BC_PER for d in range(3)]
+    if any((bclo[d] == BC_PER) != (bchi[d] == BC_PER) for d in range(dim)):
+        raise ValueError("a periodic direction needs VD_BC_PER on both sides")
     mw = mech.mw[spec] if spec < ns else 0.0
     Dg = cell_diffusivity(case, spec, Tg, port)
     N = n[0] * n[1] * n[2]
@@ -151,6 +152,11 @@ def solve(case, spec, state_old, dsdt, prm, port, robin=None):
                 Dc, Dn = Dg[gc[2], gc[1], gc[0]], Dg[gnb[2], gnb[1], gnb[0]]
                 b = 2.0 * Dc * Dn / (Dc + Dn) if (Dc + Dn) != 0.0 else 0.0
                 r = idx[k, j, i]
+                if per[d] and not 0 <= nb[d] < n[d]:
+                    # across the periodic direction: the cell on the other side,
+                    # through the face whose D comes from the ghost cell (a periodic
+                    # image of that cell)
+                    nb[d] %= n[d]
                 if 0 <= nb[d] < n[d]:
                     rows.append(r)
                     cols.append(idx[nb[2], nb[1], nb[0]])
@@ -200,6 +206,10 @@ def solve(case, spec, state_old, dsdt, prm, port, robin=None):
                         m = list(f)
                         m[d] -= 1
                         G[c] = (sol[k, j, i] - sol[m[2], m[1], m[0]]) / dx[d]
+                    elif per[d]:
+                        first, last = list(f), list(f)
+                        first[d], last[d] = 0, n[d] - 1
+                        G[c] = (sol[first[2], first[1], first[0]] - sol[last[2], last[1], last[0]]) / dx[d]
                     else:
                         sgn = -1 if f[d] == 0 else 1
                         bc, val, b = bfaces[(d, sgn, tuple(f))]

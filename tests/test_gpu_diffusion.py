@@ -24,9 +24,9 @@ def mech():
     return m
 
 
-def make(mech, dim, n, seed, dt, bc_lo=None, bc_hi=None, bound=1):
+def make(mech, dim, n, seed, dt, bc_lo=None, bc_hi=None, bound=1, periodic=(0, 0, 0)):
     case = inputs.build_case(mech, dim, n, (1e-5,) * dim, seed, density="loguniform_smooth",
-                             dens_range=(1e14, 1e18), te_range_ev=(0.5, 5.0))
+                             dens_range=(1e14, 1e18), te_range_ev=(0.5, 5.0), periodic=periodic)
     prm = case.vd_params(dt=dt, bc_lo=bc_lo, bc_hi=bc_hi, bound_specden=bound)
     rng = np.random.default_rng(seed + 1)
     ns = mech.ns
@@ -120,12 +120,36 @@ def test_diffusion_dominated_step(mech, dim, n):
                 assert rel(grads[d], ref_grads[d]) <= 1e-9
 
 
+@pytest.mark.parametrize("dim,n,per", [(1, (64,), (1, 0, 0)), (2, (32, 16), (1, 0, 0)), (2, (16, 16), (1, 1, 0)),
+                                       (3, (8, 8, 6), (0, 1, 1))])
+def test_periodic_directions(mech, dim, n, per):
+    """Periodic directions (the state's ghosts filled periodically, as FillPatch
+    does) against the direct solve, with zero-gradient walls elsewhere; a long
+    step so that the wrap carries diffusion across the coarse levels."""
+    b = [[abi.BC_PER if per[d] else abi.BC_HNEU for d in range(3)] for _ in range(4)]
+    for spec in (mech.e_id, mech.ns, 3):
+        case, prm, old, dsdt = make(mech, dim, n, 1010 + dim + spec, dt=1e-9, bc_lo=b, bc_hi=b, periodic=per)
+        got, grads, nv, rr = run(mech, case, prm, old, dsdt, spec)
+        assert nv >= 1 and rr <= 1e-13
+        sol, ref_grads, _ = odf.solve(case, spec, old, dsdt[spec], prm, oracle.Port(mech))
+        assert rel(got[spec], sol) <= 1e-10
+        if grads is not None:
+            for d in range(dim):
+                assert rel(grads[d], ref_grads[d]) <= 1e-9
+
+
 def test_fixed_cycles_and_refusals(mech):
     case, prm, old, dsdt = make(mech, 2, (16, 8), 970, dt=1e-12)
     _, _, nv, rr = run(mech, case, prm, old, dsdt, 3, tol=0.0, cycles=3)
     assert nv == 3 and rr == -1.0
+    # periodic on one side only; an odd number of cells in a periodic direction
     lo = [[abi.BC_PER] * 3 for _ in range(4)]
-    case, prm, old, dsdt = make(mech, 2, (16, 8), 971, dt=1e-12, bc_lo=lo, bc_hi=lo)
+    hi = [[abi.BC_HNEU] * 3 for _ in range(4)]
+    case, prm, old, dsdt = make(mech, 2, (16, 8), 971, dt=1e-12, bc_lo=lo, bc_hi=hi)
+    with pytest.raises(abi.VidyutError) as e:
+        run(mech, case, prm, old, dsdt, 3)
+    assert e.value.status == abi.ERR_ARG
+    case, prm, old, dsdt = make(mech, 2, (15, 8), 972, dt=1e-12, bc_lo=lo, bc_hi=lo, periodic=(1, 1, 0))
     with pytest.raises(abi.VidyutError) as e:
         run(mech, case, prm, old, dsdt, 3)
     assert e.value.status == abi.ERR_ARG

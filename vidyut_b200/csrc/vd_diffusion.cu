@@ -13,8 +13,11 @@
 //  - domain faces from species_bc (Source/PlasmaChem.H:75-184): one value per face,
 //    the value at the face for VD_BC_DIRC, the derivative along the coordinate
 //    direction for VD_BC_IHNEU; VD_BC_HNEU and VD_BC_ROBIN (species_bc's default
-//    robin a = 0, b = 1, f = 0) give zero gradient; periodic directions are
-//    refused;
+//    robin a = 0, b = 1, f = 0) give zero gradient; a periodic direction (both
+//    sides VD_BC_PER, an even number of cells) couples its first and last cells
+//    through the face between them, whose coefficient comes from the state's
+//    ghost cells as any face's (the caller fills them periodically, as FillPatch
+//    does);
 //  - V(2,2) cycles of red-black Gauss-Seidel, averaging restriction, linear
 //    prolongation, a one-CTA bottom solve on the coarsest grid;
 //  - afterwards the density floor (:590-617), the electrons' face gradients
@@ -63,6 +66,7 @@ struct DBc {
     // faces of type kBcUserRobin: a n + b dn/dnu = f (nu the outward normal), per
     // [side][direction]; f is zero on the correction levels
     double ra[2][3], rb[2][3], rf[2][3];
+    int per[3];  // 1: periodic direction
 };
 // the caller's Robin coefficients (vd_diffusion_params.user_robin) on a face
 constexpr int kBcUserRobin = 100;
@@ -110,7 +114,8 @@ __device__ __forceinline__ void dstencil(const DLevel& L, const DBc& bc, int dim
         p[d] += 1;
         const double blo = L.b[d][flin(L, d, i, j, k)];
         const double bhi = L.b[d][flin(L, d, p[0], p[1], p[2])];
-        if (c[d] > 0) {
+        if (c[d] > 0 || bc.per[d]) {
+            if (c[d] == 0) m[d] = L.n[d] - 1;  // periodic: the last cell, through face 0
             off -= blo * w * phi[dlin(L, m[0], m[1], m[2])];
             diag += blo * w;
         } else if (bc.type_lo[d] == VD_BC_DIRC) {
@@ -124,7 +129,8 @@ __device__ __forceinline__ void dstencil(const DLevel& L, const DBc& bc, int dim
             diag += blo * w * bc.ra[0][d] / den;
             off -= blo * w * bc.rf[0][d] / den;
         }
-        if (c[d] < L.n[d] - 1) {
+        if (c[d] < L.n[d] - 1 || bc.per[d]) {
+            if (c[d] == L.n[d] - 1) p[d] = 0;  // periodic: the first cell, through face n
             off -= bhi * w * phi[dlin(L, p[0], p[1], p[2])];
             diag += bhi * w;
         } else if (bc.type_hi[d] == VD_BC_DIRC) {
@@ -233,7 +239,8 @@ __global__ void __launch_bounds__(128) k_dif_coarsen_b(DLevel F, DLevel C)
 
 // fine phi += linear interpolation of the coarse correction; outside a domain face
 // the correction's mirror value: -c for a Dirichlet face, the homogeneous ghost
-// relation for a Robin face, c otherwise
+// relation for a Robin face, c otherwise; across a periodic direction the cell on
+// the other side
 template <int DIM>
 __global__ void __launch_bounds__(128) k_dif_prolong(DLevel F, DLevel C, DBc bc)
 {
@@ -262,7 +269,11 @@ __global__ void __launch_bounds__(128) k_dif_prolong(DLevel F, DLevel C, DBc bc)
                     w *= m[d] ? 0.25 : 0.75;
                     if (m[d]) {
                         q[d] += nb[d];
-                        if (q[d] < 0) {
+                        if (q[d] < 0 && bc.per[d]) {
+                            q[d] = C.n[d] - 1;
+                        } else if (q[d] >= C.n[d] && bc.per[d]) {
+                            q[d] = 0;
+                        } else if (q[d] < 0) {
                             q[d] = 0;
                             if (bc.type_lo[d] == VD_BC_DIRC) sign = -sign;
                             if (bc.type_lo[d] == kBcUserRobin)
@@ -460,6 +471,10 @@ __global__ void __launch_bounds__(128) k_dif_grad(DLevel L, DBc bc, A4 out, int 
     double g = 0.0;
     if (f[D] > 0 && f[D] < L.n[D]) {
         g = (L.phi[c] - L.phi[c - s1]) / h;
+    } else if (bc.per[D]) {
+        // the face between the last cell and the first
+        const int64_t first = f[D] == 0 ? c : c - (int64_t)L.n[D] * s1;
+        g = (L.phi[first] - L.phi[first + (int64_t)(L.n[D] - 1) * s1]) / h;
     } else if (f[D] == 0) {
         if (bc.type_lo[D] == VD_BC_DIRC) g = (L.phi[c] - bc.val_lo[D][plin(L, D, f)]) / (0.5 * h);
         else if (bc.type_lo[D] == VD_BC_IHNEU) g = bc.val_lo[D][plin(L, D, f)];
@@ -619,11 +634,18 @@ extern "C" int vd_implicit_species_solve(const vd_box* bx, vd_array4 state, vd_a
     for (int d = 0; d < dim; d++) {
         bc.type_lo[d] = prm->bc_lo[cls][d];
         bc.type_hi[d] = prm->bc_hi[cls][d];
-        if (bc.type_lo[d] == VD_BC_PER || bc.type_hi[d] == VD_BC_PER)
-            return derr(VD_ERR_ARG, "periodic direction %d: not covered by this solve", d);
+        if ((bc.type_lo[d] == VD_BC_PER) != (bc.type_hi[d] == VD_BC_PER))
+            return derr(VD_ERR_ARG, "direction %d periodic on one side only", d);
         if (bc.type_lo[d] < VD_BC_PER || bc.type_lo[d] > VD_BC_ROBIN || bc.type_hi[d] < VD_BC_PER ||
             bc.type_hi[d] > VD_BC_ROBIN)
             return derr(VD_ERR_ARG, "unknown boundary code in direction %d", d);
+        if (bc.type_lo[d] == VD_BC_PER) {
+            // red-black sweeps couple the first and last cells through the wrap:
+            // they must differ in colour on every level
+            if (n[d] % 2) return derr(VD_ERR_ARG, "periodic direction %d needs an even number of cells", d);
+            bc.per[d] = 1;
+            continue;
+        }
         if (dp->user_robin) {
             // the caller's species_bc coefficients replace the default face values
             for (int side = 0; side < 2; side++) {
@@ -724,6 +746,10 @@ extern "C" int vd_implicit_species_solve(const vd_box* bx, vd_array4 state, vd_a
     double* bv_lo[3] = {nullptr, nullptr, nullptr};
     double* bv_hi[3] = {nullptr, nullptr, nullptr};
     for (int d = 0; d < dim; d++) {
+        if (bc.per[d]) {  // no domain faces
+            p += 2 * plane[d];
+            continue;
+        }
         bv_lo[d] = p;
         p += plane[d];
         bv_hi[d] = p;
