@@ -262,7 +262,9 @@ __device__ __forceinline__ double weno_fp64(double a, double b, double c, double
     return (a1 / s) * p1 + (a2 / s) * p2 + (a3 / s) * p3;
 }
 
-// FP32 reconstruction of values already scaled to O(1).  The nonlinear weights are
+
+// One FP32 reconstruction of values already scaled to O(1), from its three 4 beta_k
+// and candidate polynomials.  The nonlinear weights are
 // rescaled so that no term can overflow and the smoothest stencil always keeps a
 // weight of order gamma (the sum never underflows to zero, whatever the spread of
 // the smoothness indicators): with q_k = beta_k + eps and m = min_k q_k,
@@ -274,18 +276,9 @@ __device__ __forceinline__ double weno_fp64(double a, double b, double c, double
 // 13/12 and 1/4) and eps4 is 4 eps: every weight is a ratio of these, and scaling
 // by a power of two changes no rounding, so the result is the same and each
 // indicator costs one multiply less.
-__device__ __forceinline__ float weno_f32(float a, float b, float c, float d, float e, int scheme,
-                                          float eps4)
+__device__ __forceinline__ float weno_weights_f32(float b1, float b2, float b3, float p1, float p2, float p3, int scheme,
+                                                  float eps4)
 {
-    float p1 = fmaf(1.0f / 3.0f, a, fmaf(-7.0f / 6.0f, b, (11.0f / 6.0f) * c));
-    float p2 = fmaf(-1.0f / 6.0f, b, fmaf(5.0f / 6.0f, c, (1.0f / 3.0f) * d));
-    float p3 = fmaf(1.0f / 3.0f, c, fmaf(5.0f / 6.0f, d, (-1.0f / 6.0f) * e));
-    float t1 = fmaf(-2.0f, b, a) + c, t2 = fmaf(-4.0f, b, a) + 3.0f * c;
-    float b1 = fmaf(13.0f / 3.0f, t1 * t1, t2 * t2);
-    float t3 = fmaf(-2.0f, c, b) + d, t4 = b - d;
-    float b2 = fmaf(13.0f / 3.0f, t3 * t3, t4 * t4);
-    float t5 = fmaf(-2.0f, d, c) + e, t6 = fmaf(3.0f, c, fmaf(-4.0f, d, e));
-    float b3 = fmaf(13.0f / 3.0f, t5 * t5, t6 * t6);
     const float q1 = b1 + eps4, q2 = b2 + eps4, q3 = b3 + eps4;
     const float m = fminf(q1, fminf(q2, q3));
     const float r1 = rcp_approx(q1), r2 = rcp_approx(q2), r3 = rcp_approx(q3);
@@ -312,8 +305,38 @@ __device__ __forceinline__ float weno_f32(float a, float b, float c, float d, fl
             a3 = gk_map(a3 * is, 0.3f);
         }
     }
-    float is = rcp_approx(a1 + a2 + a3);
-    return fmaf(a1, p1, fmaf(a2, p2, a3 * p3)) * is;
+    return fmaf(a1, p1, fmaf(a2, p2, a3 * p3)) * rcp_approx(a1 + a2 + a3);
+}
+
+// Both reconstructions of one field at a face from its six stencil values x0..x5:
+// plus, the left-biased WENO-5 value from x0..x4, and minus, the right-biased one
+// from x5..x1 (weno(e,d,c,b,a) of the reference).
+// They share two of their three second differences (x1-2x2+x3, x2-2x3+x4) with
+// their squared terms, and two of their candidate polynomials (the parabola
+// through x1..x3 at x2+1/2 and through x2..x4 at x3+1/2), which are computed once.
+__device__ __forceinline__ void weno_pair_f32(const float* x, int scheme, float eps4, float& plus, float& minus)
+{
+    // second differences and the 13/3 d^2 terms of the windows centred at x1..x4
+    const float d1 = fmaf(-2.0f, x[1], x[0]) + x[2], d2 = fmaf(-2.0f, x[2], x[1]) + x[3];
+    const float d3 = fmaf(-2.0f, x[3], x[2]) + x[4], d4 = fmaf(-2.0f, x[4], x[3]) + x[5];
+    const float c2 = (13.0f / 3.0f) * (d2 * d2), c3 = (13.0f / 3.0f) * (d3 * d3);
+    // the polynomials the two share
+    const float pm = fmaf(-1.0f / 6.0f, x[1], fmaf(5.0f / 6.0f, x[2], (1.0f / 3.0f) * x[3]));
+    const float pn = fmaf(1.0f / 3.0f, x[2], fmaf(5.0f / 6.0f, x[3], (-1.0f / 6.0f) * x[4]));
+    {
+        const float p1 = fmaf(1.0f / 3.0f, x[0], fmaf(-7.0f / 6.0f, x[1], (11.0f / 6.0f) * x[2]));
+        const float t2 = fmaf(3.0f, x[2], fmaf(-4.0f, x[1], x[0])), t4 = x[1] - x[3];
+        const float t6 = fmaf(3.0f, x[2], fmaf(-4.0f, x[3], x[4]));
+        const float b1 = fmaf(13.0f / 3.0f, d1 * d1, t2 * t2), b2 = fmaf(t4, t4, c2), b3 = fmaf(t6, t6, c3);
+        plus = weno_weights_f32(b1, b2, b3, p1, pm, pn, scheme, eps4);
+    }
+    {
+        const float p1 = fmaf(1.0f / 3.0f, x[5], fmaf(-7.0f / 6.0f, x[4], (11.0f / 6.0f) * x[3]));
+        const float t2 = fmaf(3.0f, x[3], fmaf(-4.0f, x[4], x[5])), t4 = x[4] - x[2];
+        const float t6 = fmaf(3.0f, x[3], fmaf(-4.0f, x[2], x[1]));
+        const float b1 = fmaf(13.0f / 3.0f, d4 * d4, t2 * t2), b2 = fmaf(t4, t4, c3), b3 = fmaf(t6, t6, c2);
+        minus = weno_weights_f32(b1, b2, b3, p1, pn, pm, scheme, eps4);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -389,7 +412,7 @@ __device__ __forceinline__ float face_flux_mixed32(const float* u, const float* 
     int b2 = 127 - 2 * e;
     b2 = b2 < 0 ? 0 : (b2 > 255 ? 255 : b2);
     const float s2 = __int_as_float(b2 << 23);        // 2^-2e, 0 or inf at the ends
-    const float eps = 4.0f * fminf(fmaxf(1e-20f * s2, 1e-30f), 1e30f);  // weno_f32 takes 4 eps
+    const float eps = 4.0f * fminf(fmaxf(1e-20f * s2, 1e-30f), 1e30f);  // the weights take 4 eps
     float us[6], fs[6];
 #pragma unroll
     for (int q = 0; q < 6; q++) {
@@ -397,10 +420,9 @@ __device__ __forceinline__ float face_flux_mixed32(const float* u, const float* 
         fs[q] = us[q] * v[q];
     }
     const float lam = fabsf(0.5f * (v[2] + v[3]));
-    const float fp = weno_f32(fs[0], fs[1], fs[2], fs[3], fs[4], scheme, eps);
-    const float fm = weno_f32(fs[5], fs[4], fs[3], fs[2], fs[1], scheme, eps);
-    const float up = weno_f32(us[0], us[1], us[2], us[3], us[4], scheme, eps);
-    const float um = weno_f32(us[5], us[4], us[3], us[2], us[1], scheme, eps);
+    float fp, fm, up, um;
+    weno_pair_f32(fs, scheme, eps, fp, fm);
+    weno_pair_f32(us, scheme, eps, up, um);
     const float F = 0.5f * (fmaf(lam, up, fp) + fmaf(-lam, um, fm));
     if (bs < 254) return F * __int_as_float((254 - bs) << 23);  // 2^(127-bs)
     return (float)((double)F * __longlong_as_double((long long)(1150 - bs) << 52));
