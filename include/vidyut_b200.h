@@ -375,8 +375,9 @@ int vd_fill_ghosts(const vd_box* bx, vd_array4 state, int ghost, const int32_t* 
  * same discrete problem, and Vidyut::update_cc_efields,
  * Source/PotentialSolve.cpp:391-430): del^2 phi = -(e/eps0) sum_k z_k n_k on the
  * cell-centred grid, faces with bc_* == VD_BC_DIRC hold phi = value_* at the face,
- * the others zero normal gradient.  Geometric multigrid in FP64 from the state's
- * POT component as initial guess, V(2,2) cycles until max|residual| <=
+ * the others zero normal gradient.  Geometric multigrid from the state's POT
+ * component as initial guess: FP64 defect correction of the potential with FP32
+ * V(2,2) cycles of the correction equation, until the FP64 max|residual| <=
  * tol_rel * max|rhs| (tol_rel > 0; one host synchronisation per cycle) or
  * max_vcycles (tol_rel == 0: exactly max_vcycles, no synchronisation).  Writes POT,
  * EFX..EFZ (centred differences, one-sided at domain faces), REF (|E|/N in Td) in
@@ -385,8 +386,9 @@ int vd_fill_ghosts(const vd_box* bx, vd_array4 state, int ghost, const int32_t* 
  * prm->cs_technique).  user_rhs (p == NULL: none) is added to the right-hand side
  * cell by cell (one component covering the box, in the units of del^2 phi): the
  * reference's user_sources::add_user_potential_sources
- * (Source/PotentialSolve.cpp:220-222).  Scratch (3 doubles per cell over the
- * hierarchy) comes from the library's stream-ordered pool. */
+ * (Source/PotentialSolve.cpp:220-222).  Scratch (2 doubles per cell, and 3
+ * floats per cell over the hierarchy) comes from the library's stream-ordered
+ * pool. */
 typedef struct {
     int32_t bc_lo[3], bc_hi[3];
     double  value_lo[3], value_hi[3];

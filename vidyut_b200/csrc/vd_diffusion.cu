@@ -158,8 +158,11 @@ __global__ void __launch_bounds__(128) k_dif_rbgs(DLevel L, DBc bc, int color)
     L.phi[c] = (L.rhs[c] - off) / diag;
 }
 
+// blkmax (null: not wanted): max |residual| of each block, one value per block in
+// block order, reduced by k_dif_maxabs afterwards (one atomic per warp on a single
+// address would serialise in L2 on large grids)
 template <int DIM>
-__global__ void __launch_bounds__(128) k_dif_residual(DLevel L, DBc bc, unsigned long long* maxabs)
+__global__ void __launch_bounds__(128) k_dif_residual(DLevel L, DBc bc, double* blkmax)
 {
     const int j = blockIdx.y, k = blockIdx.z;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -172,9 +175,14 @@ __global__ void __launch_bounds__(128) k_dif_residual(DLevel L, DBc bc, unsigned
         L.res[c] = r;
         m = r == r ? fabs(r) : INFINITY;  // a NaN residual counts as the largest
     }
-    if (maxabs) {
+    if (blkmax) {
+        __shared__ double wmax[4];  // one per warp of the 128-thread block
         for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if ((threadIdx.x & 31) == 0) atomicMax(maxabs, (unsigned long long)__double_as_longlong(m));
+        if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+        __syncthreads();
+        if (threadIdx.x == 0)
+            blkmax[blockIdx.x + (int64_t)gridDim.x * (blockIdx.y + (int64_t)gridDim.y * blockIdx.z)] =
+                fmax(fmax(wmax[0], wmax[1]), fmax(wmax[2], wmax[3]));
     }
 }
 
@@ -521,7 +529,7 @@ struct DifOps {
         ProfScope ps("k_dif_rbgs", st);
         k_dif_rbgs<DIM><<<dgrid(L, 0, 2), 128, 0, st>>>(L, b, color);
     }
-    static void residual(const DLevel& L, const DBc& b, unsigned long long* mx, cudaStream_t st)
+    static void residual(const DLevel& L, const DBc& b, double* mx, cudaStream_t st)
     {
         ProfScope ps("k_dif_residual", st);
         k_dif_residual<DIM><<<dgrid(L), 128, 0, st>>>(L, b, mx);
@@ -581,7 +589,7 @@ struct DifOps {
 
 struct DifTable {
     void (*rbgs)(const DLevel&, const DBc&, int, cudaStream_t);
-    void (*residual)(const DLevel&, const DBc&, unsigned long long*, cudaStream_t);
+    void (*residual)(const DLevel&, const DBc&, double*, cudaStream_t);
     void (*restrict_)(const DLevel&, const DLevel&, cudaStream_t);
     void (*prolong)(const DLevel&, const DLevel&, const DBc&, cudaStream_t);
     void (*bottom)(const DLevel&, const DBc&, int, cudaStream_t);
@@ -725,6 +733,9 @@ extern "C" int vd_implicit_species_solve(const vd_box* bx, vd_array4 state, vd_a
         plane[d] = (int64_t)n[e0] * n[e1];
         total += 2 * (size_t)plane[d];
     }
+    const dim3 g0 = dgrid(lv[0]);
+    const int64_t nblk0 = (int64_t)g0.x * g0.y * g0.z;  // residual blocks of the finest level
+    total += (size_t)nblk0;
     double* buf = nullptr;
     cudaError_t e = vd_host::scratch_alloc(reinterpret_cast<void**>(&buf), (total + 1) * sizeof(double) + 64, st);
     if (e != cudaSuccess) return derr(VD_ERR_NOMEM, "solver scratch of %zu bytes: %s", total * 8, cudaGetErrorString(e));
@@ -757,6 +768,8 @@ extern "C" int vd_implicit_species_solve(const vd_box* bx, vd_array4 state, vd_a
         bc.val_lo[d] = bv_lo[d];
         bc.val_hi[d] = bv_hi[d];
     }
+    double* blkmax = p;
+    p += nblk0;
     unsigned long long* d_max = reinterpret_cast<unsigned long long*>(p);
     DBc bc0 = bc;  // homogeneous faces for the correction levels
     for (int d = 0; d < 3; d++) {
@@ -836,7 +849,10 @@ extern "C" int vd_implicit_species_solve(const vd_box* bx, vd_array4 state, vd_a
     auto maxabs = [&](bool resid, double* out) -> int {
         cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), st);
         if (resid) {
-            ops.residual(lv[0], bc, d_max, st);
+            ops.residual(lv[0], bc, blkmax, st);
+            ProfScope ps("k_dif_maxabs", st);
+            const unsigned g = (unsigned)std::min<int64_t>((nblk0 + 255) / 256, 148 * 32);
+            k_dif_maxabs<<<g < 1 ? 1 : g, 256, 0, st>>>(blkmax, nblk0, d_max);
         } else {
             ProfScope ps("k_dif_maxabs", st);
             const int64_t nc = lv[0].cells();

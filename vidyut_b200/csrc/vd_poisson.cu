@@ -10,7 +10,10 @@
 // one box that is the whole domain: cell-centred 2D+1-point Laplacian, Dirichlet
 // faces (the applied potential at the face) or zero-gradient faces, V(2,2) cycles
 // of red-black Gauss-Seidel, full-weighting restriction, linear prolongation, a
-// 64-sweep bottom solve on the coarsest grid.  All in FP64.
+// 64-sweep bottom solve on the coarsest grid.  The potential, its defect and the
+// fields are FP64; the cycles solve for the correction in FP32 (half the bytes
+// per sweep), and the defect of the corrected FP64 potential decides convergence,
+// so the solution meets the same FP64 tolerance.
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
@@ -24,21 +27,30 @@ namespace {
 
 constexpr double EPS0 = 8.854187817e-12;  // Source/UnivConstants.H:12
 
-struct Level {
+// One grid of the hierarchy.  The potential itself is FP64 (Level: phi, rhs); the
+// V-cycles solve for its correction in FP32 (CLevel: phi the correction, rhs the
+// defect, res the residual), with 1/dx^2 scaled so the correction equation has
+// O(1) coefficients (defect correction: the defect of every cycle is formed from
+// the FP64 potential, so the FP32 cycles only set how fast it converges).
+template <class T>
+struct LevelT {
     int n[3];          // cells per direction (1 beyond dim)
-    double idx2[3];    // 1/dx^2 (0 beyond dim)
-    double* phi;
-    double* rhs;
-    double* res;
+    double idx2[3];    // 1/dx^2 (0 beyond dim), times the scale on correction levels
+    T* phi;
+    T* rhs;
+    T* res;
     __host__ __device__ int64_t cells() const { return (int64_t)n[0] * n[1] * n[2]; }
 };
+using Level = LevelT<double>;
+using CLevel = LevelT<float>;
 
 struct BcInfo {
     int dir_lo[3], dir_hi[3];    // 1: Dirichlet face
     double val_lo[3], val_hi[3]; // its value (0 on the correction levels)
 };
 
-__device__ __forceinline__ int64_t lin(const Level& L, int i, int j, int k)
+template <class T>
+__device__ __forceinline__ int64_t lin(const LevelT<T>& L, int i, int j, int k)
 {
     return (int64_t)i + (int64_t)L.n[0] * (j + (int64_t)L.n[1] * k);
 }
@@ -48,45 +60,46 @@ __device__ __forceinline__ int64_t lin(const Level& L, int i, int j, int k)
 // inside neighbour adds phi_nb and -phi_c; a Dirichlet face holds phi = V at the
 // face, so phi_out = 2V - phi_c (constant 2V/dx^2, diagonal -2/dx^2); a
 // zero-gradient face has phi_out = phi_c and adds nothing.
-__device__ __forceinline__ void stencil(const Level& L, const BcInfo& bc, int dim, int i, int j, int k,
-                                        const double* phi, double& off, double& diag)
+template <class T>
+__device__ __forceinline__ void stencil(const LevelT<T>& L, const BcInfo& bc, int dim, int i, int j, int k,
+                                        const T* phi, T& off, T& diag)
 {
     const int c[3] = {i, j, k};
-    off = 0.0;
-    diag = 0.0;
+    const int64_t str[3] = {1, L.n[0], (int64_t)L.n[0] * L.n[1]};
+    const int64_t cc = lin(L, i, j, k);
+    off = T(0);
+    diag = T(0);
     for (int d = 0; d < dim; d++) {
-        const double w = L.idx2[d];
-        int m[3] = {i, j, k}, p[3] = {i, j, k};
-        m[d] -= 1;
-        p[d] += 1;
+        const T w = (T)L.idx2[d];
         if (c[d] > 0) {
-            off += w * phi[lin(L, m[0], m[1], m[2])];
+            off += w * phi[cc - str[d]];
             diag -= w;
         } else if (bc.dir_lo[d]) {
-            off += 2.0 * w * bc.val_lo[d];
-            diag -= 2.0 * w;
+            off += T(2) * w * (T)bc.val_lo[d];
+            diag -= T(2) * w;
         }
         if (c[d] < L.n[d] - 1) {
-            off += w * phi[lin(L, p[0], p[1], p[2])];
+            off += w * phi[cc + str[d]];
             diag -= w;
         } else if (bc.dir_hi[d]) {
-            off += 2.0 * w * bc.val_hi[d];
-            diag -= 2.0 * w;
+            off += T(2) * w * (T)bc.val_hi[d];
+            diag -= T(2) * w;
         }
     }
 }
 
 // Multigrid kernels: one thread per cell (or per cell of one colour) with i over
 // the x threads and j, k from the y and z block indices, so no index division.
+// The V-cycle kernels run on the FP32 correction levels.
 
 // one red-black Gauss-Seidel half sweep: cells with (i + j + k) % 2 == color
 template <int DIM>
-__global__ void __launch_bounds__(128) k_mg_rbgs(Level L, BcInfo bc, int color)
+__global__ void __launch_bounds__(128) k_mg_rbgs(CLevel L, BcInfo bc, int color)
 {
     const int j = blockIdx.y, k = blockIdx.z;
     const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((j + k + color) & 1);
     if (i >= L.n[0]) return;
-    double off, diag;
+    float off, diag;
     stencil(L, bc, DIM, i, j, k, L.phi, off, diag);
     // L phi = off + diag phi = rhs  ->  phi = (rhs - off) / diag
     const int64_t c = lin(L, i, j, k);
@@ -94,34 +107,67 @@ __global__ void __launch_bounds__(128) k_mg_rbgs(Level L, BcInfo bc, int color)
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(128) k_mg_residual(Level L, BcInfo bc, unsigned long long* maxabs)
+__global__ void __launch_bounds__(128) k_mg_residual(CLevel L, BcInfo bc)
+{
+    const int j = blockIdx.y, k = blockIdx.z;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L.n[0]) return;
+    float off, diag;
+    stencil(L, bc, DIM, i, j, k, L.phi, off, diag);
+    const int64_t c = lin(L, i, j, k);
+    L.res[c] = L.rhs[c] - (off + diag * L.phi[c]);
+}
+
+// The defect of the FP64 potential P, r = rhs - L phi (FP64, inhomogeneous faces),
+// becomes the right-hand side of the finest correction level (times the scale of
+// its coefficients, rounded to FP32), whose correction starts at zero.
+// blkmax (null: not wanted): max |r| of each block, one value per block in block
+// order, reduced by k_maxabs afterwards (one atomic per warp on a single address
+// would serialise in L2: 1.8 M of them on a 384^3 grid).
+template <int DIM>
+__global__ void __launch_bounds__(128) k_mg_defect(Level P, BcInfo bc, CLevel E, double scale, double* blkmax)
 {
     const int j = blockIdx.y, k = blockIdx.z;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double m = 0.0;
-    if (i < L.n[0]) {
+    if (i < P.n[0]) {
         double off, diag;
-        stencil(L, bc, DIM, i, j, k, L.phi, off, diag);
-        const int64_t c = lin(L, i, j, k);
-        const double r = L.rhs[c] - (off + diag * L.phi[c]);
-        L.res[c] = r;
+        stencil(P, bc, DIM, i, j, k, P.phi, off, diag);
+        const int64_t c = lin(P, i, j, k);
+        const double r = P.rhs[c] - (off + diag * P.phi[c]);
+        E.rhs[c] = (float)(r * scale);
+        E.phi[c] = 0.0f;
         m = fabs(r);
     }
-    if (maxabs) {
-        // non-negative doubles order like their bit patterns
+    if (blkmax) {
+        __shared__ double wmax[4];  // one per warp of the 128-thread block
         for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if ((threadIdx.x & 31) == 0) atomicMax(maxabs, (unsigned long long)__double_as_longlong(m));
+        if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+        __syncthreads();
+        if (threadIdx.x == 0)
+            blkmax[blockIdx.x + (int64_t)gridDim.x * (blockIdx.y + (int64_t)gridDim.y * blockIdx.z)] =
+                fmax(fmax(wmax[0], wmax[1]), fmax(wmax[2], wmax[3]));
     }
+}
+
+// P phi += the correction of the finest correction level
+__global__ void __launch_bounds__(128) k_mg_correct(Level P, CLevel E)
+{
+    const int j = blockIdx.y, k = blockIdx.z;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n[0]) return;
+    const int64_t c = lin(P, i, j, k);
+    P.phi[c] += (double)E.phi[c];
 }
 
 // coarse rhs = average of the 2^dim fine residuals (full weighting for cell centres)
 template <int DIM>
-__global__ void __launch_bounds__(128) k_mg_restrict(Level F, Level C)
+__global__ void __launch_bounds__(128) k_mg_restrict(CLevel F, CLevel C)
 {
     const int j = blockIdx.y, k = blockIdx.z;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= C.n[0]) return;
-    double s = 0.0;
+    float s = 0.0f;
 #pragma unroll
     for (int dz = 0; dz < (DIM > 2 ? 2 : 1); dz++)
 #pragma unroll
@@ -130,53 +176,57 @@ __global__ void __launch_bounds__(128) k_mg_restrict(Level F, Level C)
             for (int dx = 0; dx < 2; dx++)
                 s += F.res[lin(F, 2 * i + dx, DIM > 1 ? 2 * j + dy : j, DIM > 2 ? 2 * k + dz : k)];
     const int64_t c = lin(C, i, j, k);
-    C.rhs[c] = s * (1.0 / (double)(1 << DIM));
-    C.phi[c] = 0.0;
+    C.rhs[c] = s * (1.0f / (float)(1 << DIM));
+    C.phi[c] = 0.0f;
 }
 
 // fine phi += linear interpolation of the coarse correction (weights 3/4, 1/4 per
 // direction; at a domain face the outside coarse value is the correction's
 // boundary value: -c for a Dirichlet face (zero at the face), c for zero gradient)
 template <int DIM>
-__global__ void __launch_bounds__(128) k_mg_prolong(Level F, Level C, BcInfo bc)
+__global__ void __launch_bounds__(128) k_mg_prolong(CLevel F, CLevel C, BcInfo bc)
 {
     const int j = blockIdx.y, k = blockIdx.z;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= F.n[0]) return;
     const int f[3] = {i, j, k};
-    int ci[3] = {i, j, k}, nb[3] = {0, 0, 0};
+    // per direction the two coarse cells (as offsets) and their weights; beyond a
+    // domain face the second is the parent itself, weighted -1/4 or 1/4; beyond dim
+    // the coarse index is the fine one
+    const int64_t str[3] = {1, C.n[0], (int64_t)C.n[0] * C.n[1]};
+    int64_t off[3][2];
+    float w[3][2];
 #pragma unroll
-    for (int d = 0; d < DIM; d++) {
-        ci[d] = f[d] >> 1;
-        nb[d] = (f[d] & 1) ? 1 : -1;  // the other coarse cell this fine cell leans towards
+    for (int d = 0; d < 3; d++) {
+        if (d >= DIM) {
+            off[d][0] = off[d][1] = (int64_t)f[d] * str[d];
+            w[d][0] = 1.0f;
+            w[d][1] = 0.0f;
+            continue;
+        }
+        const int ci = f[d] >> 1, q = ci + ((f[d] & 1) ? 1 : -1);
+        off[d][0] = (int64_t)ci * str[d];
+        w[d][0] = 0.75f;
+        if (q < 0) {
+            off[d][1] = off[d][0];
+            w[d][1] = bc.dir_lo[d] ? -0.25f : 0.25f;
+        } else if (q >= C.n[d]) {
+            off[d][1] = off[d][0];
+            w[d][1] = bc.dir_hi[d] ? -0.25f : 0.25f;
+        } else {
+            off[d][1] = (int64_t)q * str[d];
+            w[d][1] = 0.25f;
+        }
     }
-    double acc = 0.0;
+    float acc = 0.0f;
 #pragma unroll
     for (int mz = 0; mz < (DIM > 2 ? 2 : 1); mz++)
 #pragma unroll
-        for (int my = 0; my < (DIM > 1 ? 2 : 1); my++)
-#pragma unroll
-            for (int mx = 0; mx < 2; mx++) {
-                const int m[3] = {mx, my, mz};
-                double w = 1.0;
-                int q[3] = {ci[0], ci[1], ci[2]};
-                double sign = 1.0;
-#pragma unroll
-                for (int d = 0; d < DIM; d++) {
-                    w *= m[d] ? 0.25 : 0.75;
-                    if (m[d]) {
-                        q[d] += nb[d];
-                        if (q[d] < 0) {
-                            q[d] = 0;
-                            if (bc.dir_lo[d]) sign = -sign;
-                        } else if (q[d] >= C.n[d]) {
-                            q[d] = C.n[d] - 1;
-                            if (bc.dir_hi[d]) sign = -sign;
-                        }
-                    }
-                }
-                acc += w * sign * C.phi[lin(C, q[0], q[1], q[2])];
-            }
+        for (int my = 0; my < (DIM > 1 ? 2 : 1); my++) {
+            const int64_t row = off[1][my] + off[2][mz];
+            const float v = w[0][0] * C.phi[row + off[0][0]] + w[0][1] * C.phi[row + off[0][1]];
+            acc += (w[1][my] * w[2][mz]) * v;
+        }
     F.phi[lin(F, i, j, k)] += acc;
 }
 
@@ -185,7 +235,7 @@ __global__ void __launch_bounds__(128) k_mg_prolong(Level F, Level C, BcInfo bc)
 constexpr int kBottomCells = 4096;
 
 template <int DIM>
-__global__ void __launch_bounds__(256) k_mg_bottom(Level L, BcInfo bc, int sweeps)
+__global__ void __launch_bounds__(256) k_mg_bottom(CLevel L, BcInfo bc, int sweeps)
 {
     const int n0 = L.n[0], n1 = L.n[1];
     const int nc = (int)L.cells();
@@ -194,7 +244,7 @@ __global__ void __launch_bounds__(256) k_mg_bottom(Level L, BcInfo bc, int sweep
             for (int c = threadIdx.x; c < nc; c += blockDim.x) {
                 const int k = c / (n0 * n1), r = c - k * n0 * n1, j = r / n0, i = r - j * n0;
                 if (((i + j + k) & 1) != color) continue;
-                double off, diag;
+                float off, diag;
                 stencil(L, bc, DIM, i, j, k, L.phi, off, diag);
                 L.phi[c] = (L.rhs[c] - off) / diag;
             }
@@ -202,7 +252,8 @@ __global__ void __launch_bounds__(256) k_mg_bottom(Level L, BcInfo bc, int sweep
         }
 }
 
-dim3 grid_cells(const Level& L, int per_thread = 1)
+template <class T>
+dim3 grid_cells(const LevelT<T>& L, int per_thread = 1)
 {
     const int nx = (L.n[0] + per_thread - 1) / per_thread;
     return dim3((unsigned)((nx + 127) / 128), (unsigned)L.n[1], (unsigned)L.n[2]);
@@ -210,46 +261,53 @@ dim3 grid_cells(const Level& L, int per_thread = 1)
 
 template <int DIM>
 struct Mg {
-    static void rbgs(const Level& L, const BcInfo& b, int color, cudaStream_t st)
+    static void rbgs(const CLevel& L, const BcInfo& b, int color, cudaStream_t st)
     {
         ProfScope ps("k_mg_rbgs", st);
         k_mg_rbgs<DIM><<<grid_cells(L, 2), 128, 0, st>>>(L, b, color);
     }
-    static void residual(const Level& L, const BcInfo& b, unsigned long long* mx, cudaStream_t st)
+    static void residual(const CLevel& L, const BcInfo& b, cudaStream_t st)
     {
         ProfScope ps("k_mg_residual", st);
-        k_mg_residual<DIM><<<grid_cells(L), 128, 0, st>>>(L, b, mx);
+        k_mg_residual<DIM><<<grid_cells(L), 128, 0, st>>>(L, b);
     }
-    static void restrict_(const Level& F, const Level& C, cudaStream_t st)
+    static void restrict_(const CLevel& F, const CLevel& C, cudaStream_t st)
     {
         ProfScope ps("k_mg_restrict", st);
         k_mg_restrict<DIM><<<grid_cells(C), 128, 0, st>>>(F, C);
     }
-    static void bottom(const Level& L, const BcInfo& b, int sweeps, cudaStream_t st)
+    static void bottom(const CLevel& L, const BcInfo& b, int sweeps, cudaStream_t st)
     {
         ProfScope ps("k_mg_bottom", st);
         k_mg_bottom<DIM><<<1, 256, 0, st>>>(L, b, sweeps);
     }
-    static void prolong(const Level& F, const Level& C, const BcInfo& b, cudaStream_t st)
+    static void prolong(const CLevel& F, const CLevel& C, const BcInfo& b, cudaStream_t st)
     {
         ProfScope ps("k_mg_prolong", st);
         k_mg_prolong<DIM><<<grid_cells(F), 128, 0, st>>>(F, C, b);
     }
+    static void defect(const Level& P, const BcInfo& b, const CLevel& E, double scale, double* blkmax,
+                       cudaStream_t st)
+    {
+        ProfScope ps("k_mg_defect", st);
+        k_mg_defect<DIM><<<grid_cells(P), 128, 0, st>>>(P, b, E, scale, blkmax);
+    }
 };
 
 struct MgOps {
-    void (*rbgs)(const Level&, const BcInfo&, int, cudaStream_t);
-    void (*residual)(const Level&, const BcInfo&, unsigned long long*, cudaStream_t);
-    void (*restrict_)(const Level&, const Level&, cudaStream_t);
-    void (*prolong)(const Level&, const Level&, const BcInfo&, cudaStream_t);
-    void (*bottom)(const Level&, const BcInfo&, int, cudaStream_t);
+    void (*rbgs)(const CLevel&, const BcInfo&, int, cudaStream_t);
+    void (*residual)(const CLevel&, const BcInfo&, cudaStream_t);
+    void (*restrict_)(const CLevel&, const CLevel&, cudaStream_t);
+    void (*prolong)(const CLevel&, const CLevel&, const BcInfo&, cudaStream_t);
+    void (*bottom)(const CLevel&, const BcInfo&, int, cudaStream_t);
+    void (*defect)(const Level&, const BcInfo&, const CLevel&, double, double*, cudaStream_t);
 };
 
 MgOps mg_ops(int dim)
 {
-    if (dim == 1) return {Mg<1>::rbgs, Mg<1>::residual, Mg<1>::restrict_, Mg<1>::prolong, Mg<1>::bottom};
-    if (dim == 2) return {Mg<2>::rbgs, Mg<2>::residual, Mg<2>::restrict_, Mg<2>::prolong, Mg<2>::bottom};
-    return {Mg<3>::rbgs, Mg<3>::residual, Mg<3>::restrict_, Mg<3>::prolong, Mg<3>::bottom};
+    if (dim == 1) return {Mg<1>::rbgs, Mg<1>::residual, Mg<1>::restrict_, Mg<1>::prolong, Mg<1>::bottom, Mg<1>::defect};
+    if (dim == 2) return {Mg<2>::rbgs, Mg<2>::residual, Mg<2>::restrict_, Mg<2>::prolong, Mg<2>::bottom, Mg<2>::defect};
+    return {Mg<3>::rbgs, Mg<3>::residual, Mg<3>::restrict_, Mg<3>::prolong, Mg<3>::bottom, Mg<3>::defect};
 }
 
 __global__ void k_maxabs(const double* x, int64_t n, unsigned long long* out)
@@ -447,21 +505,32 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
     for (int d = 0; d < dim; d++) any_dir = any_dir || bc.dir_lo[d] || bc.dir_hi[d];
     if (!any_dir) return err(VD_ERR_ARG, "the potential needs at least one Dirichlet face");
 
-    // hierarchy: halve every active direction while all stay even and above 2
-    std::vector<Level> lv;
+    // the potential (FP64) and the hierarchy of its correction (FP32), whose
+    // coefficients are 1/dx^2 times scale = min dx^2, so they are at most 1: the
+    // correction of a potential in volts then stays far inside FP32's range.
+    // Hierarchy: halve every active direction while all stay even and above 2.
+    Level P;
+    double scale = 0.0;
+    for (int d = 0; d < 3; d++) {
+        P.n[d] = n[d];
+        P.idx2[d] = d < dim ? 1.0 / (prm->dx[d] * prm->dx[d]) : 0.0;
+        scale = std::max(scale, P.idx2[d]);
+    }
+    scale = 1.0 / scale;
+    std::vector<CLevel> lv;
     {
-        Level L0;
+        CLevel L0;
         for (int d = 0; d < 3; d++) {
             L0.n[d] = n[d];
-            L0.idx2[d] = d < dim ? 1.0 / (prm->dx[d] * prm->dx[d]) : 0.0;
+            L0.idx2[d] = P.idx2[d] * scale;
         }
         lv.push_back(L0);
         for (;;) {
-            const Level& f = lv.back();
+            const CLevel& f = lv.back();
             bool ok = true;
             for (int d = 0; d < dim; d++) ok = ok && (f.n[d] % 2 == 0) && f.n[d] > 2;
             if (!ok || lv.size() >= 24) break;
-            Level c;
+            CLevel c;
             for (int d = 0; d < 3; d++) {
                 c.n[d] = d < dim ? f.n[d] / 2 : f.n[d];
                 c.idx2[d] = f.idx2[d] * 0.25;
@@ -469,13 +538,24 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
             lv.push_back(c);
         }
     }
-    size_t total = 0;
-    for (auto& L : lv) total += 3 * (size_t)L.cells();
+    // scratch: P's phi and rhs, the block maxima of the defect, the max (FP64);
+    // phi, rhs and res of every correction level (FP32)
+    const dim3 g0 = grid_cells(P);
+    const int64_t nblk0 = (int64_t)g0.x * g0.y * g0.z;  // defect blocks
+    size_t nf = 0;
+    for (auto& L : lv) nf += 3 * (size_t)L.cells();
+    const size_t nd = 2 * (size_t)P.cells() + (size_t)nblk0 + 1;
     double* buf = nullptr;
-    cudaError_t e = vd_host::scratch_alloc(reinterpret_cast<void**>(&buf), (total + 1) * sizeof(double) + 64, st);
-    if (e != cudaSuccess) return err(VD_ERR_NOMEM, "multigrid scratch of %zu bytes: %s", total * 8, cudaGetErrorString(e));
+    const size_t bytes = nd * sizeof(double) + nf * sizeof(float) + 64;
+    cudaError_t e = vd_host::scratch_alloc(reinterpret_cast<void**>(&buf), bytes, st);
+    if (e != cudaSuccess) return err(VD_ERR_NOMEM, "multigrid scratch of %zu bytes: %s", bytes, cudaGetErrorString(e));
+    P.phi = buf;
+    P.rhs = buf + P.cells();
+    P.res = nullptr;
+    double* blkmax = buf + 2 * P.cells();
+    unsigned long long* d_max = reinterpret_cast<unsigned long long*>(blkmax + nblk0);
     {
-        double* p = buf;
+        float* p = reinterpret_cast<float*>(buf + nd);
         for (auto& L : lv) {
             L.phi = p;
             p += L.cells();
@@ -485,7 +565,6 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
             p += L.cells();
         }
     }
-    unsigned long long* d_max = reinterpret_cast<unsigned long long*>(buf + total);
     BcInfo bc0;  // homogeneous version for the correction levels
     bc0 = bc;
     for (int d = 0; d < 3; d++) bc0.val_lo[d] = bc0.val_hi[d] = 0.0;
@@ -513,102 +592,100 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
 
     {
         ProfScope ps("k_pois_rhs", st);
-        k_pois_rhs<<<grid_cells(lv[0]), 128, 0, st>>>(pa, lv[0]);
+        k_pois_rhs<<<grid_cells(P), 128, 0, st>>>(pa, P);
     }
     if ((rc = launch_check("k_pois_rhs"))) return rc;
-    // |rhs| scale for the relative residual: residual of phi = 0 would be rhs; use
-    // the residual of the initial guess when nothing better is known
     double rhs_scale = 0.0;
     const bool check = pp->tol_rel > 0.0;
     const MgOps ops = mg_ops(dim);
+    // one V(2,2) cycle of the correction equation, from a zero correction
     auto vcycle = [&]() {
         const int nl = (int)lv.size();
         for (int l = 0; l < nl; l++) {
-            const BcInfo& b = l == 0 ? bc : bc0;
             if (l == nl - 1 && lv[l].cells() <= kBottomCells) {
-                ops.bottom(lv[l], b, 64, st);  // one CTA, all sweeps in one launch
+                ops.bottom(lv[l], bc0, 64, st);  // one CTA, all sweeps in one launch
             } else {
                 const int sweeps = (l == nl - 1) ? 64 : 2;
                 for (int s = 0; s < sweeps; s++) {
-                    ops.rbgs(lv[l], b, 0, st);
-                    ops.rbgs(lv[l], b, 1, st);
+                    ops.rbgs(lv[l], bc0, 0, st);
+                    ops.rbgs(lv[l], bc0, 1, st);
                 }
             }
             if (l < nl - 1) {
-                ops.residual(lv[l], b, nullptr, st);
+                ops.residual(lv[l], bc0, st);
                 ops.restrict_(lv[l], lv[l + 1], st);
             }
         }
         for (int l = nl - 2; l >= 0; l--) {
-            const BcInfo& b = l == 0 ? bc : bc0;
             ops.prolong(lv[l], lv[l + 1], bc0, st);
             for (int s = 0; s < 2; s++) {
-                ops.rbgs(lv[l], b, 0, st);
-                ops.rbgs(lv[l], b, 1, st);
+                ops.rbgs(lv[l], bc0, 0, st);
+                ops.rbgs(lv[l], bc0, 1, st);
             }
         }
+        ProfScope ps("k_mg_correct", st);
+        k_mg_correct<<<grid_cells(P), 128, 0, st>>>(P, lv[0]);
     };
-    auto resid_max = [&](double* out) -> int {
+    // the max of the n doubles (non-negative doubles order like their bit patterns)
+    auto read_max = [&](const double* x, int64_t nx, double* out) -> int {
         cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), st);
-        ops.residual(lv[0], bc, d_max, st);
+        {
+            ProfScope ps("k_maxabs", st);
+            k_maxabs<<<grid_of(nx), 256, 0, st>>>(x, nx, d_max);
+        }
         unsigned long long h = 0;
         cudaError_t ce = cudaMemcpyAsync(&h, d_max, sizeof(h), cudaMemcpyDeviceToHost, st);
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
         if (ce != cudaSuccess) return err(VD_ERR_CUDA, "residual norm: %s", cudaGetErrorString(ce));
-        double v;
-        memcpy(&v, &h, sizeof(v));
-        *out = v;
+        memcpy(out, &h, sizeof(*out));
         return VD_OK;
     };
     int done = 0;
     double rel = -1.0;
     if (check) {
         // scale of the relative residual: max |rhs|
-        cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), st);
-        {
-            ProfScope ps("k_maxabs", st);
-            k_maxabs<<<grid_of(lv[0].cells()), 256, 0, st>>>(lv[0].rhs, lv[0].cells(), d_max);
-        }
-        unsigned long long h = 0;
-        cudaError_t ce = cudaMemcpyAsync(&h, d_max, sizeof(h), cudaMemcpyDeviceToHost, st);
-        if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
-        if (ce != cudaSuccess) {
+        if ((rc = read_max(P.rhs, P.cells(), &rhs_scale))) {
             cudaFreeAsync(buf, st);
-            return err(VD_ERR_CUDA, "rhs norm: %s", cudaGetErrorString(ce));
+            return rc;
         }
-        memcpy(&rhs_scale, &h, sizeof(rhs_scale));
         if (rhs_scale == 0.0) rhs_scale = 1.0;
     }
+    ops.defect(P, bc, lv[0], scale, nullptr, st);
     for (done = 0; done < pp->max_vcycles;) {
         vcycle();
         done++;
         if (check) {
+            // the defect of the corrected potential: the convergence test and the
+            // right-hand side of the next cycle
+            ops.defect(P, bc, lv[0], scale, blkmax, st);
             double r = 0.0;
-            if ((rc = resid_max(&r))) {
+            if ((rc = read_max(blkmax, nblk0, &r))) {
                 cudaFreeAsync(buf, st);
                 return rc;
             }
             rel = r / rhs_scale;
             if (rel <= pp->tol_rel) break;
+        } else if (done < pp->max_vcycles) {
+            ops.defect(P, bc, lv[0], scale, nullptr, st);
         }
     }
     if ((rc = launch_check("multigrid"))) return rc;
     D3 dxs{{prm->dx[0], prm->dx[1], prm->dx[2]}};
     {
         ProfScope ps("k_pois_cell_fields", st);
-        k_pois_cell_fields<<<grid_cells(lv[0]), 128, 0, st>>>(pa, lv[0], dxs);
+        k_pois_cell_fields<<<grid_cells(P), 128, 0, st>>>(pa, P, dxs);
     }
     if (!prm->cs_technique)
         for (int d = 0; d < dim; d++) {
-            Level L = lv[0];
+            const Level& L = P;
             int nf[3] = {L.n[0], L.n[1], L.n[2]};
             nf[d] += 1;
             ProfScope ps("k_pois_face_field", st);
             const dim3 g((unsigned)((nf[0] + 127) / 128), (unsigned)nf[1], (unsigned)nf[2]);
             const A4 efd(efield_ec[d]);
-            if (d == 0) k_pois_face_field<0><<<g, 128, 0, st>>>(lv[0], bc, efd, prm->dx[0]);
-            else if (d == 1) k_pois_face_field<1><<<g, 128, 0, st>>>(lv[0], bc, efd, prm->dx[1]);
-            else k_pois_face_field<2><<<g, 128, 0, st>>>(lv[0], bc, efd, prm->dx[2]);
+            if (d == 0) k_pois_face_field<0><<<g, 128, 0, st>>>(P, bc, efd, prm->dx[0]);
+            else if (d == 1) k_pois_face_field<1><<<g, 128, 0, st>>>(P, bc, efd, prm->dx[1]);
+            else k_pois_face_field<2><<<g, 128, 0, st>>>(P, bc, efd, prm->dx[2]);
         }
     if ((rc = launch_check("potential fields"))) return rc;
     // ghosts of the potential, the cell field and the reduced field
