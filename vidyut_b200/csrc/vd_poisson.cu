@@ -60,26 +60,46 @@ __device__ __forceinline__ int64_t lin(const LevelT<T>& L, int i, int j, int k)
 // inside neighbour adds phi_nb and -phi_c; a Dirichlet face holds phi = V at the
 // face, so phi_out = 2V - phi_c (constant 2V/dx^2, diagonal -2/dx^2); a
 // zero-gradient face has phi_out = phi_c and adds nothing.
-template <class T>
-__device__ __forceinline__ void stencil(const LevelT<T>& L, const BcInfo& bc, int dim, int i, int j, int k,
-                                        const T* phi, T& off, T& diag)
+template <int DIM, class T>
+struct Nbr {
+    T lo[DIM], hi[DIM];
+};
+// every neighbour load first, unconditionally (the cell itself stands in beyond a
+// domain face, where its value is not used): the loads of a thread are then all
+// in flight together, which these latency-bound sweeps need
+template <int DIM, class T>
+__device__ __forceinline__ Nbr<DIM, T> stencil_load(const LevelT<T>& L, int i, int j, int k, const T* phi)
 {
     const int c[3] = {i, j, k};
     const int64_t str[3] = {1, L.n[0], (int64_t)L.n[0] * L.n[1]};
     const int64_t cc = lin(L, i, j, k);
+    Nbr<DIM, T> v;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        v.lo[d] = phi[c[d] > 0 ? cc - str[d] : cc];
+        v.hi[d] = phi[c[d] < L.n[d] - 1 ? cc + str[d] : cc];
+    }
+    return v;
+}
+template <int DIM, class T>
+__device__ __forceinline__ void stencil_apply(const LevelT<T>& L, const BcInfo& bc, int i, int j, int k,
+                                              const Nbr<DIM, T>& v, T& off, T& diag)
+{
+    const int c[3] = {i, j, k};
     off = T(0);
     diag = T(0);
-    for (int d = 0; d < dim; d++) {
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
         const T w = (T)L.idx2[d];
         if (c[d] > 0) {
-            off += w * phi[cc - str[d]];
+            off += w * v.lo[d];
             diag -= w;
         } else if (bc.dir_lo[d]) {
             off += T(2) * w * (T)bc.val_lo[d];
             diag -= T(2) * w;
         }
         if (c[d] < L.n[d] - 1) {
-            off += w * phi[cc + str[d]];
+            off += w * v.hi[d];
             diag -= w;
         } else if (bc.dir_hi[d]) {
             off += T(2) * w * (T)bc.val_hi[d];
@@ -87,23 +107,49 @@ __device__ __forceinline__ void stencil(const LevelT<T>& L, const BcInfo& bc, in
         }
     }
 }
+template <int DIM, class T>
+__device__ __forceinline__ void stencil(const LevelT<T>& L, const BcInfo& bc, int i, int j, int k, const T* phi,
+                                        T& off, T& diag)
+{
+    stencil_apply<DIM>(L, bc, i, j, k, stencil_load<DIM>(L, i, j, k, phi), off, diag);
+}
 
 // Multigrid kernels: one thread per cell (or per cell of one colour) with i over
 // the x threads and j, k from the y and z block indices, so no index division.
 // The V-cycle kernels run on the FP32 correction levels.
 
-// one red-black Gauss-Seidel half sweep: cells with (i + j + k) % 2 == color
+// one red-black Gauss-Seidel half sweep: cells with (i + j + k) % 2 == color.  A
+// thread takes two cells, `half` apart along the slowest active direction (k in
+// 3-D, j in 2-D; half = 0 in 1-D: one cell), with all their loads issued first.
 template <int DIM>
-__global__ void __launch_bounds__(128) k_mg_rbgs(CLevel L, BcInfo bc, int color)
+__global__ void __launch_bounds__(128) k_mg_rbgs(CLevel L, BcInfo bc, int color, int half)
 {
-    const int j = blockIdx.y, k = blockIdx.z;
-    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((j + k + color) & 1);
-    if (i >= L.n[0]) return;
-    float off, diag;
-    stencil(L, bc, DIM, i, j, k, L.phi, off, diag);
-    // L phi = off + diag phi = rhs  ->  phi = (rhs - off) / diag
-    const int64_t c = lin(L, i, j, k);
-    L.phi[c] = (L.rhs[c] - off) / diag;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int ii[2], jj[2], kk[2];
+    bool ok[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        jj[h] = blockIdx.y + (DIM == 2 ? h * half : 0);
+        kk[h] = blockIdx.z + (DIM == 3 ? h * half : 0);
+        ii[h] = 2 * t + ((jj[h] + kk[h] + color) & 1);
+        ok[h] = ii[h] < L.n[0] && jj[h] < L.n[1] && kk[h] < L.n[2] && (h == 0 || half > 0);
+    }
+    Nbr<DIM, float> v[2];
+    float r[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+        if (ok[h]) {
+            v[h] = stencil_load<DIM>(L, ii[h], jj[h], kk[h], L.phi);
+            r[h] = L.rhs[lin(L, ii[h], jj[h], kk[h])];
+        }
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+        if (ok[h]) {
+            float off, diag;
+            stencil_apply<DIM>(L, bc, ii[h], jj[h], kk[h], v[h], off, diag);
+            // L phi = off + diag phi = rhs  ->  phi = (rhs - off) / diag
+            L.phi[lin(L, ii[h], jj[h], kk[h])] = (r[h] - off) / diag;
+        }
 }
 
 template <int DIM>
@@ -113,7 +159,7 @@ __global__ void __launch_bounds__(128) k_mg_residual(CLevel L, BcInfo bc)
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= L.n[0]) return;
     float off, diag;
-    stencil(L, bc, DIM, i, j, k, L.phi, off, diag);
+    stencil<DIM>(L, bc, i, j, k, L.phi, off, diag);
     const int64_t c = lin(L, i, j, k);
     L.res[c] = L.rhs[c] - (off + diag * L.phi[c]);
 }
@@ -132,7 +178,7 @@ __global__ void __launch_bounds__(128) k_mg_defect(Level P, BcInfo bc, CLevel E,
     double m = 0.0;
     if (i < P.n[0]) {
         double off, diag;
-        stencil(P, bc, DIM, i, j, k, P.phi, off, diag);
+        stencil<DIM>(P, bc, i, j, k, P.phi, off, diag);
         const int64_t c = lin(P, i, j, k);
         const double r = P.rhs[c] - (off + diag * P.phi[c]);
         E.rhs[c] = (float)(r * scale);
@@ -245,7 +291,7 @@ __global__ void __launch_bounds__(256) k_mg_bottom(CLevel L, BcInfo bc, int swee
                 const int k = c / (n0 * n1), r = c - k * n0 * n1, j = r / n0, i = r - j * n0;
                 if (((i + j + k) & 1) != color) continue;
                 float off, diag;
-                stencil(L, bc, DIM, i, j, k, L.phi, off, diag);
+                stencil<DIM>(L, bc, i, j, k, L.phi, off, diag);
                 L.phi[c] = (L.rhs[c] - off) / diag;
             }
             __syncthreads();
@@ -264,7 +310,13 @@ struct Mg {
     static void rbgs(const CLevel& L, const BcInfo& b, int color, cudaStream_t st)
     {
         ProfScope ps("k_mg_rbgs", st);
-        k_mg_rbgs<DIM><<<grid_cells(L, 2), 128, 0, st>>>(L, b, color);
+        // pairs along the slowest active direction
+        const int ns = DIM == 3 ? L.n[2] : (DIM == 2 ? L.n[1] : 1);
+        const int half = DIM == 1 ? 0 : (ns + 1) / 2;
+        dim3 g = grid_cells(L, 2);
+        if (DIM == 3) g.z = (unsigned)half;
+        else if (DIM == 2) g.y = (unsigned)half;
+        k_mg_rbgs<DIM><<<g, 128, 0, st>>>(L, b, color, half);
     }
     static void residual(const CLevel& L, const BcInfo& b, cudaStream_t st)
     {
