@@ -67,6 +67,12 @@ extern "C" __global__ void vd_spec_sizeof(unsigned long long* out)
     out[0] = sizeof(PrepArgs);
     out[1] = sizeof(BatchCtl);
 }
+// The FP64 rate exponential, called out of line: inlined, its instructions
+// repeated for every reaction made the straight-line chemistry overflow the
+// instruction cache (stall "no instruction"); out of line the FP64 prep kernel of
+// 150 reactions ran 10 % faster on B200, with bit-identical results.  The mixed
+// path's exp2 stays inline (out of line it was slower).
+__device__ __noinline__ double vd_exp64(double x) { return exp(x); }
 // 2^x as FP32 from an FP64 exponent (same as exp2_split in vd_device.cuh)
 __device__ __forceinline__ float exp2_split(double x)
 {
@@ -238,7 +244,7 @@ std::string gen_prep_kernel(const VdMechDev& m, int prec)
             for (int j = 0; j < 4; j++)
                 o << "        sum = __dadd_rn(sum, __dmul_rn(" << hexd(F.fc[j]) << ", itp" << j << "));\n";
         if (prec == PREC_FP64)
-            o << "        k = " << hexd(janev ? F.jA : F.fA) << " * exp(sum) * NA_CE;\n";
+            o << "        k = " << hexd(janev ? F.jA : F.fA) << " * vd_exp64(sum) * NA_CE;\n";
         else
             o << "        k = (double)exp2_split(fma(sum, " << hexd(1.4426950408889634074) << ", "
               << hexd(janev ? F.l2jA : F.l2fA) << "));\n";
@@ -274,7 +280,7 @@ std::string gen_prep_kernel(const VdMechDev& m, int prec)
             const char* lT = te ? "lTe" : "lTg";
             const char* iT = te ? "invTe" : "invTg";
             if (prec == PREC_FP64) {
-                o << "      k = exp(fma(" << hexd(R.b) << ", " << lT << ", " << hexd(R.lnA) << ") - " << hexd(R.C)
+                o << "      k = vd_exp64(fma(" << hexd(R.b) << ", " << lT << ", " << hexd(R.lnA) << ") - " << hexd(R.C)
                   << " * " << iT << ");\n";
             } else {
                 o << "      k = (double)exp2_split(fma(" << hexd(R.b) << ", " << lT << ", " << hexd(R.l2A) << ") - "
