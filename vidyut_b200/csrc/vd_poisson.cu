@@ -121,18 +121,22 @@ __device__ __forceinline__ void stencil(const LevelT<T>& L, const BcInfo& bc, in
 // one red-black Gauss-Seidel half sweep: cells with (i + j + k) % 2 == color.  A
 // thread takes two cells, `half` apart along the slowest active direction (k in
 // 3-D, j in 2-D; half = 0 in 1-D: one cell), with all their loads issued first.
+// corr (null: none): the last half sweep of a cycle on the finest correction
+// level also adds the finished correction to the FP64 potential corr, for its
+// two cells and their x neighbours of the other colour (so every cell once).
 template <int DIM>
-__global__ void __launch_bounds__(128) k_mg_rbgs(CLevel L, BcInfo bc, int color, int half)
+__global__ void __launch_bounds__(128) k_mg_rbgs(CLevel L, BcInfo bc, int color, int half, double* corr)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     int ii[2], jj[2], kk[2];
-    bool ok[2];
+    bool row[2], ok[2];
 #pragma unroll
     for (int h = 0; h < 2; h++) {
         jj[h] = blockIdx.y + (DIM == 2 ? h * half : 0);
         kk[h] = blockIdx.z + (DIM == 3 ? h * half : 0);
         ii[h] = 2 * t + ((jj[h] + kk[h] + color) & 1);
-        ok[h] = ii[h] < L.n[0] && jj[h] < L.n[1] && kk[h] < L.n[2] && (h == 0 || half > 0);
+        row[h] = jj[h] < L.n[1] && kk[h] < L.n[2] && (h == 0 || half > 0);
+        ok[h] = row[h] && ii[h] < L.n[0];
     }
     Nbr<DIM, float> v[2];
     float r[2];
@@ -143,13 +147,22 @@ __global__ void __launch_bounds__(128) k_mg_rbgs(CLevel L, BcInfo bc, int color,
             r[h] = L.rhs[lin(L, ii[h], jj[h], kk[h])];
         }
 #pragma unroll
-    for (int h = 0; h < 2; h++)
+    for (int h = 0; h < 2; h++) {
         if (ok[h]) {
             float off, diag;
             stencil_apply<DIM>(L, bc, ii[h], jj[h], kk[h], v[h], off, diag);
             // L phi = off + diag phi = rhs  ->  phi = (rhs - off) / diag
-            L.phi[lin(L, ii[h], jj[h], kk[h])] = (r[h] - off) / diag;
+            const int64_t c = lin(L, ii[h], jj[h], kk[h]);
+            const float e = (r[h] - off) / diag;
+            L.phi[c] = e;
+            if (corr) corr[c] += (double)e;
         }
+        const int io = ii[h] ^ 1;  // the other cell of the pair (2t, 2t + 1)
+        if (corr && row[h] && io < L.n[0]) {
+            const int64_t c = lin(L, io, jj[h], kk[h]);
+            corr[c] += (double)L.phi[c];
+        }
+    }
 }
 
 template <int DIM>
@@ -307,7 +320,7 @@ dim3 grid_cells(const LevelT<T>& L, int per_thread = 1)
 
 template <int DIM>
 struct Mg {
-    static void rbgs(const CLevel& L, const BcInfo& b, int color, cudaStream_t st)
+    static void rbgs(const CLevel& L, const BcInfo& b, int color, double* corr, cudaStream_t st)
     {
         ProfScope ps("k_mg_rbgs", st);
         // pairs along the slowest active direction
@@ -316,7 +329,7 @@ struct Mg {
         dim3 g = grid_cells(L, 2);
         if (DIM == 3) g.z = (unsigned)half;
         else if (DIM == 2) g.y = (unsigned)half;
-        k_mg_rbgs<DIM><<<g, 128, 0, st>>>(L, b, color, half);
+        k_mg_rbgs<DIM><<<g, 128, 0, st>>>(L, b, color, half, corr);
     }
     static void residual(const CLevel& L, const BcInfo& b, cudaStream_t st)
     {
@@ -347,7 +360,7 @@ struct Mg {
 };
 
 struct MgOps {
-    void (*rbgs)(const CLevel&, const BcInfo&, int, cudaStream_t);
+    void (*rbgs)(const CLevel&, const BcInfo&, int, double*, cudaStream_t);
     void (*residual)(const CLevel&, const BcInfo&, cudaStream_t);
     void (*restrict_)(const CLevel&, const CLevel&, cudaStream_t);
     void (*prolong)(const CLevel&, const CLevel&, const BcInfo&, cudaStream_t);
@@ -650,7 +663,8 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
     double rhs_scale = 0.0;
     const bool check = pp->tol_rel > 0.0;
     const MgOps ops = mg_ops(dim);
-    // one V(2,2) cycle of the correction equation, from a zero correction
+    // one V(2,2) cycle of the correction equation, from a zero correction, then the
+    // correction added to the potential (inside the last half sweep)
     auto vcycle = [&]() {
         const int nl = (int)lv.size();
         for (int l = 0; l < nl; l++) {
@@ -659,8 +673,8 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
             } else {
                 const int sweeps = (l == nl - 1) ? 64 : 2;
                 for (int s = 0; s < sweeps; s++) {
-                    ops.rbgs(lv[l], bc0, 0, st);
-                    ops.rbgs(lv[l], bc0, 1, st);
+                    ops.rbgs(lv[l], bc0, 0, nullptr, st);
+                    ops.rbgs(lv[l], bc0, 1, nullptr, st);
                 }
             }
             if (l < nl - 1) {
@@ -671,12 +685,14 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
         for (int l = nl - 2; l >= 0; l--) {
             ops.prolong(lv[l], lv[l + 1], bc0, st);
             for (int s = 0; s < 2; s++) {
-                ops.rbgs(lv[l], bc0, 0, st);
-                ops.rbgs(lv[l], bc0, 1, st);
+                ops.rbgs(lv[l], bc0, 0, nullptr, st);
+                ops.rbgs(lv[l], bc0, 1, (l == 0 && s == 1) ? P.phi : nullptr, st);
             }
         }
-        ProfScope ps("k_mg_correct", st);
-        k_mg_correct<<<grid_cells(P), 128, 0, st>>>(P, lv[0]);
+        if (nl == 1) {  // no coarser level: the cycle was the bottom solve
+            ProfScope ps("k_mg_correct", st);
+            k_mg_correct<<<grid_cells(P), 128, 0, st>>>(P, lv[0]);
+        }
     };
     // the max of the n doubles (non-negative doubles order like their bit patterns)
     auto read_max = [&](const double* x, int64_t nx, double* out) -> int {
