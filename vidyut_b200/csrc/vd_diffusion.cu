@@ -95,28 +95,52 @@ __device__ __forceinline__ int64_t plin(const DLevel& L, int d, const int* c)
     return (int64_t)c[e0] + (int64_t)L.n[e0] * c[e1];
 }
 
+// The cell's face coefficients and neighbour values, loaded before any is used
+// (the neighbour through a periodic direction wraps; beyond a domain face the
+// cell itself stands in, unused): a thread's loads are then in flight together.
+template <int DIM>
+struct DNbr {
+    double blo[DIM], bhi[DIM], vlo[DIM], vhi[DIM];
+};
+template <int DIM>
+__device__ __forceinline__ DNbr<DIM> dstencil_load(const DLevel& L, const DBc& bc, int i, int j, int k,
+                                                   const double* phi)
+{
+    const int c[3] = {i, j, k};
+    const int64_t str[3] = {1, L.n[0], (int64_t)L.n[0] * L.n[1]};
+    const int64_t cc = dlin(L, i, j, k);
+    DNbr<DIM> v;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        int p[3] = {i, j, k};
+        p[d] += 1;
+        v.blo[d] = L.b[d][flin(L, d, i, j, k)];
+        v.bhi[d] = L.b[d][flin(L, d, p[0], p[1], p[2])];
+        const int64_t wrap = (int64_t)(L.n[d] - 1) * str[d];
+        v.vlo[d] = phi[c[d] > 0 ? cc - str[d] : (bc.per[d] ? cc + wrap : cc)];
+        v.vhi[d] = phi[c[d] < L.n[d] - 1 ? cc + str[d] : (bc.per[d] ? cc - wrap : cc)];
+    }
+    return v;
+}
 // The operator row of cell (i,j,k): diag * n_c + off = a n_c - div(b grad n) with
 // the domain faces folded in.  An inside neighbour adds b/dx^2 to diag and
 // -b n_nb/dx^2 to off; a Dirichlet face holds n = v at the face (half a cell
 // away: 2b/dx^2 to diag, -2b v/dx^2 to off); a face with a given derivative g
 // along its direction carries the flux b g (sgn b g/dx moved to off with the
 // opposite sign); a zero-gradient face adds nothing.
-__device__ __forceinline__ void dstencil(const DLevel& L, const DBc& bc, int dim, int i, int j, int k,
-                                         const double* phi, double& off, double& diag)
+template <int DIM>
+__device__ __forceinline__ void dstencil_apply(const DLevel& L, const DBc& bc, int i, int j, int k,
+                                               const DNbr<DIM>& v, double& off, double& diag)
 {
     const int c[3] = {i, j, k};
     off = 0.0;
     diag = L.a;
-    for (int d = 0; d < dim; d++) {
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
         const double w = L.idx2[d];
-        int m[3] = {i, j, k}, p[3] = {i, j, k};
-        m[d] -= 1;
-        p[d] += 1;
-        const double blo = L.b[d][flin(L, d, i, j, k)];
-        const double bhi = L.b[d][flin(L, d, p[0], p[1], p[2])];
+        const double blo = v.blo[d], bhi = v.bhi[d];
         if (c[d] > 0 || bc.per[d]) {
-            if (c[d] == 0) m[d] = L.n[d] - 1;  // periodic: the last cell, through face 0
-            off -= blo * w * phi[dlin(L, m[0], m[1], m[2])];
+            off -= blo * w * v.vlo[d];
             diag += blo * w;
         } else if (bc.type_lo[d] == VD_BC_DIRC) {
             diag += 2.0 * blo * w;
@@ -130,8 +154,7 @@ __device__ __forceinline__ void dstencil(const DLevel& L, const DBc& bc, int dim
             off -= blo * w * bc.rf[0][d] / den;
         }
         if (c[d] < L.n[d] - 1 || bc.per[d]) {
-            if (c[d] == L.n[d] - 1) p[d] = 0;  // periodic: the first cell, through face n
-            off -= bhi * w * phi[dlin(L, p[0], p[1], p[2])];
+            off -= bhi * w * v.vhi[d];
             diag += bhi * w;
         } else if (bc.type_hi[d] == VD_BC_DIRC) {
             diag += 2.0 * bhi * w;
@@ -145,17 +168,44 @@ __device__ __forceinline__ void dstencil(const DLevel& L, const DBc& bc, int dim
         }
     }
 }
-
 template <int DIM>
-__global__ void __launch_bounds__(128) k_dif_rbgs(DLevel L, DBc bc, int color)
+__device__ __forceinline__ void dstencil(const DLevel& L, const DBc& bc, int i, int j, int k, const double* phi,
+                                         double& off, double& diag)
 {
-    const int j = blockIdx.y, k = blockIdx.z;
-    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((j + k + color) & 1);
-    if (i >= L.n[0]) return;
-    double off, diag;
-    dstencil(L, bc, DIM, i, j, k, L.phi, off, diag);
-    const int64_t c = dlin(L, i, j, k);
-    L.phi[c] = (L.rhs[c] - off) / diag;
+    dstencil_apply<DIM>(L, bc, i, j, k, dstencil_load<DIM>(L, bc, i, j, k, phi), off, diag);
+}
+
+// one red-black Gauss-Seidel half sweep: cells with (i + j + k) % 2 == color.  A
+// thread takes two cells, `half` apart along the slowest active direction (k in
+// 3-D, j in 2-D; half = 0 in 1-D: one cell), with all their loads issued first.
+template <int DIM>
+__global__ void __launch_bounds__(128) k_dif_rbgs(DLevel L, DBc bc, int color, int half)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int ii[2], jj[2], kk[2];
+    bool ok[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        jj[h] = blockIdx.y + (DIM == 2 ? h * half : 0);
+        kk[h] = blockIdx.z + (DIM == 3 ? h * half : 0);
+        ii[h] = 2 * t + ((jj[h] + kk[h] + color) & 1);
+        ok[h] = ii[h] < L.n[0] && jj[h] < L.n[1] && kk[h] < L.n[2] && (h == 0 || half > 0);
+    }
+    DNbr<DIM> v[2];
+    double r[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+        if (ok[h]) {
+            v[h] = dstencil_load<DIM>(L, bc, ii[h], jj[h], kk[h], L.phi);
+            r[h] = L.rhs[dlin(L, ii[h], jj[h], kk[h])];
+        }
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+        if (ok[h]) {
+            double off, diag;
+            dstencil_apply<DIM>(L, bc, ii[h], jj[h], kk[h], v[h], off, diag);
+            L.phi[dlin(L, ii[h], jj[h], kk[h])] = (r[h] - off) / diag;
+        }
 }
 
 // blkmax (null: not wanted): max |residual| of each block, one value per block in
@@ -169,7 +219,7 @@ __global__ void __launch_bounds__(128) k_dif_residual(DLevel L, DBc bc, double* 
     double m = 0.0;
     if (i < L.n[0]) {
         double off, diag;
-        dstencil(L, bc, DIM, i, j, k, L.phi, off, diag);
+        dstencil<DIM>(L, bc, i, j, k, L.phi, off, diag);
         const int64_t c = dlin(L, i, j, k);
         const double r = L.rhs[c] - (off + diag * L.phi[c]);
         L.res[c] = r;
@@ -312,7 +362,7 @@ __global__ void __launch_bounds__(256) k_dif_bottom(DLevel L, DBc bc, int sweeps
                 const int k = c / (n0 * n1), r = c - k * n0 * n1, j = r / n0, i = r - j * n0;
                 if (((i + j + k) & 1) != color) continue;
                 double off, diag;
-                dstencil(L, bc, DIM, i, j, k, L.phi, off, diag);
+                dstencil<DIM>(L, bc, i, j, k, L.phi, off, diag);
                 L.phi[c] = (L.rhs[c] - off) / diag;
             }
             __syncthreads();
@@ -527,7 +577,13 @@ struct DifOps {
     static void rbgs(const DLevel& L, const DBc& b, int color, cudaStream_t st)
     {
         ProfScope ps("k_dif_rbgs", st);
-        k_dif_rbgs<DIM><<<dgrid(L, 0, 2), 128, 0, st>>>(L, b, color);
+        // pairs along the slowest active direction
+        const int ns = DIM == 3 ? L.n[2] : (DIM == 2 ? L.n[1] : 1);
+        const int half = DIM == 1 ? 0 : (ns + 1) / 2;
+        dim3 g = dgrid(L, 0, 2);
+        if (DIM == 3) g.z = (unsigned)half;
+        else if (DIM == 2) g.y = (unsigned)half;
+        k_dif_rbgs<DIM><<<g, 128, 0, st>>>(L, b, color, half);
     }
     static void residual(const DLevel& L, const DBc& b, double* mx, cudaStream_t st)
     {

@@ -153,7 +153,9 @@ __global__ void __launch_bounds__(128) k_mg_rbgs(CLevel L, BcInfo bc, int color,
             stencil_apply<DIM>(L, bc, ii[h], jj[h], kk[h], v[h], off, diag);
             // L phi = off + diag phi = rhs  ->  phi = (rhs - off) / diag
             const int64_t c = lin(L, ii[h], jj[h], kk[h]);
-            const float e = (r[h] - off) / diag;
+            // fast division (2 ulp): a smoother needs no correctly rounded quotient,
+            // and the sweep is issue bound
+            const float e = __fdividef(r[h] - off, diag);
             L.phi[c] = e;
             if (corr) corr[c] += (double)e;
         }
@@ -305,7 +307,7 @@ __global__ void __launch_bounds__(256) k_mg_bottom(CLevel L, BcInfo bc, int swee
                 if (((i + j + k) & 1) != color) continue;
                 float off, diag;
                 stencil<DIM>(L, bc, i, j, k, L.phi, off, diag);
-                L.phi[c] = (L.rhs[c] - off) / diag;
+                L.phi[c] = __fdividef(L.rhs[c] - off, diag);
             }
             __syncthreads();
         }
