@@ -449,8 +449,8 @@ cudaError_t launch_prep_batch(const PrepArgs* boxes, const int2* items, int nite
     return cudaGetLastError();
 }
 
-// ghost cell idx (0 <= idx < a.count) of a box, ordered by direction d, side,
-// layer, then the other coordinates: copy the components in comps[] from the
+// ghost cell idx (0 <= idx < a.count) of a box, ordered by direction d, side, then
+// layer and the other coordinates: copy the components in comps[] from the
 // nearest valid cell (first-order extrapolation) or the periodic image
 __device__ __forceinline__ void ghost_cell(const GhostArgs& a, int64_t idx)
 {
@@ -468,9 +468,11 @@ __device__ __forceinline__ void ghost_cell(const GhostArgs& a, int64_t idx)
         idx -= cnt;
     }
     if (d >= a.dim) return;
+    // x faces take their G layers fastest (a row's ghost cells of one side share a
+    // sector), the other directions their transverse position (coalesced along x)
     const int side = (int)(idx / ((int64_t)G * P));
-    const int g = (int)((idx / P) % G) + 1;
-    int64_t rest = idx % P;
+    const int g = d == 0 ? (int)(idx % G) + 1 : (int)((idx / P) % G) + 1;
+    int64_t rest = d == 0 ? (idx / G) % P : idx % P;
     int c[3] = {a.lo[0], a.lo[1], a.lo[2]};
     for (int e = 0; e < a.dim; e++) {
         if (e == d) continue;

@@ -70,14 +70,16 @@ struct Nbr {
 template <int DIM, class T>
 __device__ __forceinline__ Nbr<DIM, T> stencil_load(const LevelT<T>& L, int i, int j, int k, const T* phi)
 {
+    // offsets from the cell in 32 bits (a plane of the grid holds < 2^31 cells):
+    // one 64-bit address, then one wide multiply-add per load
     const int c[3] = {i, j, k};
-    const int64_t str[3] = {1, L.n[0], (int64_t)L.n[0] * L.n[1]};
-    const int64_t cc = lin(L, i, j, k);
+    const int str[3] = {1, L.n[0], L.n[0] * L.n[1]};
+    const T* pc = phi + lin(L, i, j, k);
     Nbr<DIM, T> v;
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
-        v.lo[d] = phi[c[d] > 0 ? cc - str[d] : cc];
-        v.hi[d] = phi[c[d] < L.n[d] - 1 ? cc + str[d] : cc];
+        v.lo[d] = pc[c[d] > 0 ? -str[d] : 0];
+        v.hi[d] = pc[c[d] < L.n[d] - 1 ? str[d] : 0];
     }
     return v;
 }
