@@ -188,20 +188,42 @@ __global__ void __launch_bounds__(128) k_mg_residual(CLevel L, BcInfo bc)
 // order, reduced by k_maxabs afterwards (one atomic per warp on a single address
 // would serialise in L2: 1.8 M of them on a 384^3 grid).
 template <int DIM>
-__global__ void __launch_bounds__(128) k_mg_defect(Level P, BcInfo bc, CLevel E, double scale, double* blkmax)
+__global__ void __launch_bounds__(128) k_mg_defect(Level P, BcInfo bc, CLevel E, double scale, int half,
+                                                   double* blkmax)
 {
-    const int j = blockIdx.y, k = blockIdx.z;
+    // two cells per thread, `half` apart along the slowest active direction (as in
+    // k_mg_rbgs), with all their loads issued first
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double m = 0.0;
-    if (i < P.n[0]) {
-        double off, diag;
-        stencil<DIM>(P, bc, i, j, k, P.phi, off, diag);
-        const int64_t c = lin(P, i, j, k);
-        const double r = P.rhs[c] - (off + diag * P.phi[c]);
-        E.rhs[c] = (float)(r * scale);
-        E.phi[c] = 0.0f;
-        m = fabs(r);
+    int jj[2], kk[2];
+    bool ok[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        jj[h] = blockIdx.y + (DIM == 2 ? h * half : 0);
+        kk[h] = blockIdx.z + (DIM == 3 ? h * half : 0);
+        ok[h] = i < P.n[0] && jj[h] < P.n[1] && kk[h] < P.n[2] && (h == 0 || half > 0);
     }
+    Nbr<DIM, double> v[2];
+    double rh[2], pc[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+        if (ok[h]) {
+            v[h] = stencil_load<DIM>(P, i, jj[h], kk[h], P.phi);
+            const int64_t c = lin(P, i, jj[h], kk[h]);
+            rh[h] = P.rhs[c];
+            pc[h] = P.phi[c];
+        }
+    double m = 0.0;
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+        if (ok[h]) {
+            double off, diag;
+            stencil_apply<DIM>(P, bc, i, jj[h], kk[h], v[h], off, diag);
+            const int64_t c = lin(P, i, jj[h], kk[h]);
+            const double r = rh[h] - (off + diag * pc[h]);
+            E.rhs[c] = (float)(r * scale);
+            E.phi[c] = 0.0f;
+            m = fmax(m, fabs(r));
+        }
     if (blkmax) {
         __shared__ double wmax[4];  // one per warp of the 128-thread block
         for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -322,17 +344,26 @@ dim3 grid_cells(const LevelT<T>& L, int per_thread = 1)
     return dim3((unsigned)((nx + 127) / 128), (unsigned)L.n[1], (unsigned)L.n[2]);
 }
 
+// grid of the two-cells-per-thread kernels: the slowest active direction halved
+// (half, returned, is the distance between a thread's two cells; 0 in 1-D)
+template <class T>
+dim3 grid_pairs(const LevelT<T>& L, int dim, int per_thread, int* half)
+{
+    dim3 g = grid_cells(L, per_thread);
+    const int ns = dim == 3 ? L.n[2] : (dim == 2 ? L.n[1] : 1);
+    *half = dim == 1 ? 0 : (ns + 1) / 2;
+    if (dim == 3) g.z = (unsigned)*half;
+    else if (dim == 2) g.y = (unsigned)*half;
+    return g;
+}
+
 template <int DIM>
 struct Mg {
     static void rbgs(const CLevel& L, const BcInfo& b, int color, double* corr, cudaStream_t st)
     {
         ProfScope ps("k_mg_rbgs", st);
-        // pairs along the slowest active direction
-        const int ns = DIM == 3 ? L.n[2] : (DIM == 2 ? L.n[1] : 1);
-        const int half = DIM == 1 ? 0 : (ns + 1) / 2;
-        dim3 g = grid_cells(L, 2);
-        if (DIM == 3) g.z = (unsigned)half;
-        else if (DIM == 2) g.y = (unsigned)half;
+        int half = 0;
+        const dim3 g = grid_pairs(L, DIM, 2, &half);
         k_mg_rbgs<DIM><<<g, 128, 0, st>>>(L, b, color, half, corr);
     }
     static void residual(const CLevel& L, const BcInfo& b, cudaStream_t st)
@@ -359,7 +390,9 @@ struct Mg {
                        cudaStream_t st)
     {
         ProfScope ps("k_mg_defect", st);
-        k_mg_defect<DIM><<<grid_cells(P), 128, 0, st>>>(P, b, E, scale, blkmax);
+        int half = 0;
+        const dim3 g = grid_pairs(P, DIM, 1, &half);
+        k_mg_defect<DIM><<<g, 128, 0, st>>>(P, b, E, scale, half, blkmax);
     }
 };
 
@@ -609,7 +642,8 @@ extern "C" int vd_poisson_solve(const vd_box* bx, vd_array4 state, const vd_arra
     }
     // scratch: P's phi and rhs, the block maxima of the defect, the max (FP64);
     // phi, rhs and res of every correction level (FP32)
-    const dim3 g0 = grid_cells(P);
+    int half0 = 0;
+    const dim3 g0 = grid_pairs(P, dim, 1, &half0);
     const int64_t nblk0 = (int64_t)g0.x * g0.y * g0.z;  // defect blocks
     size_t nf = 0;
     for (auto& L : lv) nf += 3 * (size_t)L.cells();
